@@ -1,0 +1,242 @@
+/*
+ * prt_cuda.h - C ABI of the B200 render device for ProtoRay's path-tracing hot path.
+ *
+ * The library (libprt_cuda.so) is a new render Device that sits beside the reference's
+ * DeviceCpu (render/device_cpu.h:16). Every entry point takes plain pointers and sizes;
+ * no C++ or torch types cross this boundary. Host pointers are borrowed for the duration
+ * of a call only. All entry points return PRT_OK (0) or a negative status; the text of the
+ * last error on a context is returned by prt_cuda_last_error().
+ *
+ * Threading: one context per host thread; calls on one context are not re-entrant. Work is
+ * issued on the context's CUDA stream, and every call that returns host-visible results is
+ * synchronous (the reference's Device::render is synchronous, render/device.h:70).
+ */
+#ifndef PRT_CUDA_H
+#define PRT_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------------------------
+ * The reference throws std::invalid_argument / std::logic_error / std::runtime_error
+ * (render/path_renderer_stream.h:109-112,154; render/renderer_factory_stream.cpp:75).
+ * The C ABI maps them to distinct codes; the C++ wrapper rethrows the same types. */
+#define PRT_OK                 0
+#define PRT_ERR_INVALID_ARG   -1  /* std::invalid_argument */
+#define PRT_ERR_LOGIC         -2  /* std::logic_error (e.g. image size not divisible by the tile) */
+#define PRT_ERR_OUT_OF_MEMORY -3
+#define PRT_ERR_CUDA          -4  /* a CUDA runtime call failed */
+#define PRT_ERR_DEVICE_ABORT  -5  /* a device loop hit its iteration cap or a bounds check */
+#define PRT_ERR_STATE         -6  /* call order violated (e.g. render before scene upload) */
+
+typedef struct prt_context prt_context;
+
+/* ---- scene description ----------------------------------------------------------------
+ * A scene is a list of triangle meshes, each bound to one Standard material, plus the
+ * environment lights. This is the flattened form of what Scene::loadScene builds from an
+ * rkscene file (render/scene.cpp:174-330): one TriangleMesh per geometry, material IDs
+ * remapped so that emissive materials come first (render/scene.cpp:254-268), and the
+ * triangle area lights derived from emissive meshes (render/scene.cpp:79-116). */
+typedef struct prt_mesh
+{
+  const float*   positions;   /* vertex_count * 3 */
+  const float*   normals;     /* vertex_count * 3, or NULL (geometric normal is used) */
+  const float*   texcoords;   /* vertex_count * 2 (UV set 0), or NULL (hit barycentrics are used) */
+  const int32_t* indices;     /* tri_count * 3 */
+  int32_t        vertex_count;
+  int32_t        tri_count;
+  int32_t        material;    /* index into prt_scene_desc.materials */
+  int32_t        reserved;
+} prt_mesh;
+
+/* Parameters of the reference's "Standard" (OpenPBR-like) material, default mode
+ * (material/standard.cpp:21-76). Field defaults are those of rkscene::Material
+ * (rkscene/rkscene.h:161-207); prt_cuda_material_defaults() fills them. A *_texture field
+ * is an index into prt_scene_desc.textures, or -1; a textured parameter is the texture
+ * value times the factor (material/material_param.h:36-47). */
+typedef struct prt_material
+{
+  float base_weight;
+  float base_color[3];
+  float metalness;
+  float diffuse_roughness;
+  float specular_weight;
+  float specular_color[3];
+  float specular_roughness;
+  float specular_ior;
+  float transmission_weight;
+  float transmission_color[3];
+  float transmission_depth;
+  float subsurface_weight;
+  float subsurface_color[3];
+  float subsurface_anisotropy;
+  float coat_weight;
+  float coat_color[3];
+  float coat_roughness;
+  float coat_ior;
+  float sheen_weight;
+  float sheen_color[3];
+  float sheen_roughness;
+  float emission_luminance;
+  float emission_color[3];
+  float opacity;
+  int32_t thin_walled;
+  int32_t base_color_texture;
+  int32_t reserved[2];
+} prt_material;
+
+/* An RGB FP32 image (row 0 at the top, as stored by the reference's ImageIo). */
+typedef struct prt_texture
+{
+  const float* rgb;   /* width * height * 3 */
+  int32_t width;
+  int32_t height;
+} prt_texture;
+
+/* Environment lights, in the order Scene::initLights adds them (render/scene.cpp:365-450):
+ * distant, ambient, image. A sun-sky light (light/sun_sky_light.cpp:17-193) is passed as
+ * its two products: the sun as the distant light and the sky as the image light. */
+typedef struct prt_env_desc
+{
+  float   distant_color[3];     /* "distantLight"; all zero = none */
+  float   distant_dir[3];       /* "distantLightDir" (toward the light) */
+  float   distant_angle;        /* "distantLightAngle": angular diameter in radians */
+  float   ambient_color[3];     /* "ambientLight"; all zero = none */
+  const float* image_rgb;       /* "imageLight": equirectangular RGB FP32, or NULL */
+  int32_t image_width;
+  int32_t image_height;
+  int32_t image_lut_size;       /* "imageLightLutSize"; 0 = the reference default */
+  int32_t reserved;
+} prt_env_desc;
+
+typedef struct prt_scene_desc
+{
+  const prt_mesh*     meshes;
+  int32_t             mesh_count;
+  int32_t             material_count;
+  const prt_material* materials;
+  const prt_texture*  textures;
+  int32_t             texture_count;
+  int32_t             reserved;
+  prt_env_desc        env;
+} prt_scene_desc;
+
+/* Pinhole camera (camera/pinhole_camera.h:20-59). The basis is (U right, V up, N back):
+ * the view direction is -N. fov is the vertical field of view in radians. */
+typedef struct prt_camera_desc
+{
+  float position[3];
+  float basis_u[3];
+  float basis_v[3];
+  float basis_n[3];
+  float fov;
+  float near_clip;
+} prt_camera_desc;
+
+/* Renderer settings: the Props keys of PathRendererStream and IntegratorBase
+ * (render/path_renderer_stream.h:114-116, render/integrator.h:60-62). */
+typedef struct prt_renderer_desc
+{
+  int32_t max_depth;      /* "maxDepth", reference default 100 */
+  int32_t rr_depth;       /* "rrDepth", reference default 8 */
+  float   min_weight;     /* "minWeight", reference default 1e-4 */
+  float   max_radiance;   /* "maxRadiance", reference default FLT_MAX (no clamping) */
+} prt_renderer_desc;
+
+/* AOV selection bits for prt_cuda_frame (render/device_cpu.cpp:178-232). */
+#define PRT_AOV_ALBEDO1  (1 << 0)   /* "aovAlbedo1": first-hit albedo */
+#define PRT_AOV_NORMAL1  (1 << 1)   /* "aovNormal1": first-hit normal */
+
+/* AOV identifiers for prt_cuda_blit. */
+#define PRT_BLIT_HDR      0
+#define PRT_BLIT_ALBEDO1  1
+#define PRT_BLIT_NORMAL1  2
+
+/* Per-call statistics, the reference's Props stats of one render() (render/path_renderer_stream.h:175-178). */
+typedef struct prt_render_stats
+{
+  double  mray;         /* (closest + shadow rays) / 1e6 / seconds */
+  int64_t rays;         /* closest + shadow rays traced */
+  int64_t spp;          /* samples per pixel rendered by this call */
+  double  render_ms;    /* device time of the call */
+} prt_render_stats;
+
+/* ---- context ----------------------------------------------------------------------------- */
+
+/* Creates a device context on the given CUDA device (Device ctor, render/device_cpu.cpp:20-23,
+ * which also precomputes the BSDF albedo tables). */
+int prt_cuda_create(int device_ordinal, prt_context** out_ctx);
+int prt_cuda_destroy(prt_context* ctx);
+const char* prt_cuda_last_error(const prt_context* ctx);
+
+/* Fills a material with the reference's Standard defaults. */
+void prt_cuda_material_defaults(prt_material* m);
+
+/* ---- scene, renderer, camera, frame ----------------------------------------------------- */
+
+/* Device::initScene + initLights (render/device_cpu.cpp:96-107): copies the scene to HBM,
+ * builds the BVH8 on the host and derives area lights and the light-pick distribution. */
+int prt_cuda_scene_upload(prt_context* ctx, const prt_scene_desc* scene);
+
+/* Device::initRenderer (render/device_cpu.cpp:32-46) for type "pathStream", sampler "sobolBurley". */
+int prt_cuda_renderer(prt_context* ctx, const prt_renderer_desc* renderer);
+
+/* Device::initSampler (render/device_cpu.cpp:48-51): seed, and resets the sample index to 0. */
+int prt_cuda_init_sampler(prt_context* ctx, uint32_t seed);
+
+/* Device::initCamera (render/device_cpu.cpp:110-125). */
+int prt_cuda_camera(prt_context* ctx, const prt_camera_desc* camera);
+
+/* Device::initFrame (render/device_cpu.cpp:178-232); width must be a multiple of 32 and
+ * height a multiple of 8 (render/path_renderer_stream.h:109-112). */
+int prt_cuda_frame(prt_context* ctx, int32_t width, int32_t height, int32_t aov_mask);
+
+/* Device::clearFrame (render/device_cpu.cpp:304-307). */
+int prt_cuda_clear(prt_context* ctx);
+
+/* Renders spp samples per pixel: equivalent to spp calls of Device::render
+ * (render/device_cpu.cpp:53-59), each advancing the sample index by one. */
+int prt_cuda_render(prt_context* ctx, int32_t spp, prt_render_stats* stats);
+
+/* Device::blitFrame (render/device_cpu.cpp:316-366): sum * rcpSafe(weight) per pixel, as
+ * width*height*3 floats. dst may be host or device memory. */
+int prt_cuda_blit(prt_context* ctx, int32_t aov, float* dst);
+
+/* ---- parity and query entry points ----------------------------------------------------- */
+
+/* Sobol-Burley samples as the stream renderer draws them (sampling/sobol_burley_sampler_simd.h:36-84):
+ * for each i, setSample(sample_index[i], pixel_id[i]) with the context seed, then a
+ * `dims`-dimensional draw (1, 2 or 3) from dimension set dim_set[i]. out has n*dims floats. */
+int prt_cuda_sobol(prt_context* ctx, int64_t n, const uint32_t* sample_index, const uint32_t* pixel_id,
+                   const uint32_t* dim_set, int32_t dims, float* out);
+
+/* Closest-hit query for n rays (org xyz, near, dir xyz, far per ray: 8 floats). Writes
+ * geom_id, prim_id (-1 on miss), t (far on miss) and barycentrics u, v. */
+int prt_cuda_trace(prt_context* ctx, int64_t n, const float* rays, int32_t* geom_id, int32_t* prim_id,
+                   float* t, float* u, float* v);
+
+/* Any-hit query: occluded[i] = 1 if a triangle lies within [near, far] of ray i. */
+int prt_cuda_occluded(prt_context* ctx, int64_t n, const float* rays, int32_t* occluded);
+
+/* Primary rays of sample `sample_index` for every pixel (render/path_renderer_stream.h:209-262)
+ * and their closest hits: rays_out has width*height*8 floats, geom_id/prim_id width*height. */
+int prt_cuda_query_primary(prt_context* ctx, uint32_t sample_index, float* rays_out,
+                           int32_t* geom_id, int32_t* prim_id, float* t);
+
+/* Host-only (no GPU needed): builds the BVH8 over tri_count triangles given as 9 floats each
+ * (v0, v1, v2) and walks it with the counting traversal, the scalar twin of the closest-hit
+ * kernel. For each of the n rays (8 floats) writes the global triangle index (-1 on a miss)
+ * and t; adds the node visits and triangle tests to *node_visits / *tri_tests and stores the
+ * node count. Used to state the algorithmic bytes per ray; the reference's counterpart is its
+ * nodes/prims per-ray statistic (render/path_renderer_stream.h:180-184). */
+int prt_bvh8_count(const float* tri_verts, int64_t tri_count, int64_t n, const float* rays, int32_t* tri_out,
+                   float* t_out, int64_t* node_visits, int64_t* tri_tests, int64_t* node_count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PRT_CUDA_H */

@@ -1,0 +1,528 @@
+// Host BVH8 builder: binned-SAH binary BVH, greedy collapse to 8-wide nodes, octant slot
+// assignment and 8-bit child-box quantisation. See bvh8.h for the node format.
+#include "bvh8.h"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <future>
+#include <stdexcept>
+#include <thread>
+
+namespace prt {
+namespace {
+
+struct Box
+{
+  float lo[3], hi[3];
+  void reset()
+  {
+    for (int k = 0; k < 3; ++k) { lo[k] = FLT_MAX; hi[k] = -FLT_MAX; }
+  }
+  void grow(const Box& b)
+  {
+    for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], b.lo[k]); hi[k] = std::max(hi[k], b.hi[k]); }
+  }
+  float area() const
+  {
+    const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+    if (dx < 0.f) return 0.f;
+    return 2.f * (dx * dy + dy * dz + dz * dx);
+  }
+};
+
+struct BinNode
+{
+  Box box;
+  int left;   // -1 for leaves
+  int right;
+  int first;  // leaves: first index into the primitive order
+  int count;  // leaves: number of primitives (1..3)
+};
+
+constexpr int kMaxLeaf = 3;
+constexpr int kBins = 32;
+
+struct BinaryBuilder
+{
+  const std::vector<Box>& primBox;
+  std::vector<float> cx, cy, cz;
+  std::vector<int> order;
+  std::vector<BinNode> nodes;
+  std::atomic<int> nextNode{0};
+  std::atomic<int> activeTasks{0};
+  int maxTasks;
+
+  BinaryBuilder(const std::vector<Box>& boxes, int threads) : primBox(boxes)
+  {
+    const size_t n = boxes.size();
+    cx.resize(n); cy.resize(n); cz.resize(n);
+    order.resize(n);
+    for (size_t i = 0; i < n; ++i)
+    {
+      cx[i] = 0.5f * (boxes[i].lo[0] + boxes[i].hi[0]);
+      cy[i] = 0.5f * (boxes[i].lo[1] + boxes[i].hi[1]);
+      cz[i] = 0.5f * (boxes[i].lo[2] + boxes[i].hi[2]);
+      order[i] = (int)i;
+    }
+    nodes.resize(std::max<size_t>(2 * n, 1));
+    maxTasks = std::max(threads, 1);
+  }
+
+  float centroid(int p, int axis) const { return axis == 0 ? cx[p] : (axis == 1 ? cy[p] : cz[p]); }
+
+  int alloc2() { return nextNode.fetch_add(2); }
+
+  void build(int nodeIndex, int begin, int end)
+  {
+    BinNode& node = nodes[nodeIndex];
+    Box bb, cb;
+    bb.reset();
+    cb.reset();
+    for (int i = begin; i < end; ++i)
+    {
+      const int p = order[i];
+      bb.grow(primBox[p]);
+      const float c[3] = {cx[p], cy[p], cz[p]};
+      for (int k = 0; k < 3; ++k) { cb.lo[k] = std::min(cb.lo[k], c[k]); cb.hi[k] = std::max(cb.hi[k], c[k]); }
+    }
+    node.box = bb;
+    const int count = end - begin;
+    if (count == 1)
+    {
+      makeLeaf(node, begin, count);
+      return;
+    }
+    // Binned SAH over all three axes.
+    float bestCost = FLT_MAX;
+    int bestAxis = -1, bestSplit = -1;
+    for (int axis = 0; axis < 3; ++axis)
+    {
+      const float ext = cb.hi[axis] - cb.lo[axis];
+      if (!(ext > 0.f)) continue;
+      const float scale = kBins / ext;
+      Box binBox[kBins];
+      int binCount[kBins];
+      for (int b = 0; b < kBins; ++b) { binBox[b].reset(); binCount[b] = 0; }
+      for (int i = begin; i < end; ++i)
+      {
+        const int p = order[i];
+        int b = (int)((centroid(p, axis) - cb.lo[axis]) * scale);
+        b = std::min(std::max(b, 0), kBins - 1);
+        binCount[b]++;
+        binBox[b].grow(primBox[p]);
+      }
+      float rightArea[kBins];
+      int rightCount[kBins];
+      Box acc;
+      acc.reset();
+      int cnt = 0;
+      for (int b = kBins - 1; b > 0; --b)
+      {
+        acc.grow(binBox[b]);
+        cnt += binCount[b];
+        rightArea[b] = acc.area();
+        rightCount[b] = cnt;
+      }
+      acc.reset();
+      cnt = 0;
+      for (int b = 1; b < kBins; ++b)
+      {
+        acc.grow(binBox[b - 1]);
+        cnt += binCount[b - 1];
+        if (cnt == 0 || rightCount[b] == 0) continue;
+        const float cost = acc.area() * cnt + rightArea[b] * rightCount[b];
+        if (cost < bestCost) { bestCost = cost; bestAxis = axis; bestSplit = b; }
+      }
+    }
+    // Leaf if small enough and splitting does not pay (traversal cost 1, triangle cost 1).
+    const float leafCost = bb.area() * count;
+    if (count <= kMaxLeaf && (bestAxis < 0 || leafCost <= bb.area() + bestCost))
+    {
+      makeLeaf(node, begin, count);
+      return;
+    }
+    int mid;
+    if (bestAxis >= 0)
+    {
+      const float ext = cb.hi[bestAxis] - cb.lo[bestAxis];
+      const float scale = kBins / ext;
+      const float lo = cb.lo[bestAxis];
+      const int axis = bestAxis;
+      int* p = std::partition(order.data() + begin, order.data() + end, [&](int prim) {
+        int b = (int)((centroid(prim, axis) - lo) * scale);
+        b = std::min(std::max(b, 0), kBins - 1);
+        return b < bestSplit;
+      });
+      mid = (int)(p - order.data());
+      if (mid == begin || mid == end) mid = begin + count / 2;
+    }
+    else
+    {
+      // All centroids coincide: split the range in the middle.
+      mid = begin + count / 2;
+    }
+    const int left = alloc2();
+    node.left = left;
+    node.right = left + 1;
+    node.first = 0;
+    node.count = 0;
+    const bool spawn = (end - begin) > 65536 && activeTasks.load() < maxTasks;
+    if (spawn)
+    {
+      activeTasks++;
+      auto fut = std::async(std::launch::async, [this, left, begin, mid]() { build(left, begin, mid); });
+      build(left + 1, mid, end);
+      fut.get();
+      activeTasks--;
+    }
+    else
+    {
+      build(left, begin, mid);
+      build(left + 1, mid, end);
+    }
+  }
+
+  void makeLeaf(BinNode& node, int begin, int count)
+  {
+    node.left = node.right = -1;
+    node.first = begin;
+    node.count = count;
+  }
+};
+
+struct WideBuilder
+{
+  const BinaryBuilder& bin;
+  const float* verts;
+  Bvh8& out;
+  int maxDepth = 0;
+
+  WideBuilder(const BinaryBuilder& b, const float* v, Bvh8& o) : bin(b), verts(v), out(o) {}
+
+  static void quantAxis(float lo, float hi, float& p, uint8_t& e)
+  {
+    p = lo;
+    const double ext = (double)hi - (double)lo;
+    // Smallest power of two with ext / scale <= 253, leaving room to round outward.
+    int ex = -126;
+    if (ext > 0.0)
+    {
+      ex = (int)std::ceil(std::log2(ext / 253.0));
+      while (std::ldexp(253.0, ex) < ext) ++ex;
+      ex = std::max(ex, -126);
+    }
+    if (ex > 127) throw std::runtime_error("BVH8: scene extent too large for 8-bit quantisation");
+    e = (uint8_t)(ex + 127);
+  }
+
+  static void quantChild(float p, uint8_t e, float clo, float chi, uint8_t& qlo, uint8_t& qhi)
+  {
+    const double scale = std::ldexp(1.0, (int)e - 127);
+    const float fs = (float)scale;
+    double a = std::floor(((double)clo - (double)p) / scale);
+    double b = std::ceil(((double)chi - (double)p) / scale);
+    // One extra quantum where the bound lands exactly on the grid, so that rounding in the
+    // kernel's plane distances never shrinks a box; then verify in single precision.
+    if (a > 0.0 && (double)p + a * scale == (double)clo) a -= 1.0;
+    if ((double)p + b * scale == (double)chi) b += 1.0;
+    a = std::max(a, 0.0);
+    b = std::min(b, 255.0);
+    while (a > 0.0 && p + (float)a * fs > clo) a -= 1.0;
+    while (b < 255.0 && p + (float)b * fs < chi) b += 1.0;
+    qlo = (uint8_t)a;
+    qhi = (uint8_t)b;
+  }
+
+  // Emits the wide node `wideIndex` for binary node `binIndex`.
+  void emit(int wideIndex, int binIndex, int depth)
+  {
+    maxDepth = std::max(maxDepth, depth + 1);
+    int children[8];
+    int n = 0;
+    const BinNode& root = bin.nodes[binIndex];
+    if (root.left < 0)
+    {
+      children[n++] = binIndex;
+    }
+    else
+    {
+      children[n++] = root.left;
+      children[n++] = root.right;
+      while (n < 8)
+      {
+        int best = -1;
+        float bestArea = -1.f;
+        for (int i = 0; i < n; ++i)
+        {
+          const BinNode& c = bin.nodes[children[i]];
+          if (c.left >= 0 && c.box.area() > bestArea) { bestArea = c.box.area(); best = i; }
+        }
+        if (best < 0) break;
+        const BinNode& c = bin.nodes[children[best]];
+        children[best] = c.left;
+        children[n++] = c.right;
+      }
+    }
+    // Node box.
+    Box nb;
+    nb.reset();
+    for (int i = 0; i < n; ++i) nb.grow(bin.nodes[children[i]].box);
+    // Slot assignment: slot s stands for the direction whose axis k is negative iff bit k of
+    // s is set; a child goes to the free slot that maximises dot(child centre - node centre,
+    // slot direction). A ray whose negative-axis bits are r then visits hit children by
+    // descending (slot ^ r), which is approximately front to back.
+    float cost[8][8];
+    for (int i = 0; i < n; ++i)
+    {
+      const Box& b = bin.nodes[children[i]].box;
+      float d[3];
+      for (int k = 0; k < 3; ++k) d[k] = 0.5f * (b.lo[k] + b.hi[k]) - 0.5f * (nb.lo[k] + nb.hi[k]);
+      for (int s = 0; s < 8; ++s)
+      {
+        float c = 0.f;
+        for (int k = 0; k < 3; ++k) c += ((s >> k) & 1) ? -d[k] : d[k];
+        cost[i][s] = c;
+      }
+    }
+    int slotOf[8];
+    int childOfSlot[8];
+    bool usedChild[8] = {false, false, false, false, false, false, false, false};
+    for (int s = 0; s < 8; ++s) childOfSlot[s] = -1;
+    for (int round = 0; round < n; ++round)
+    {
+      float best = -FLT_MAX;
+      int bi = -1, bs = -1;
+      for (int i = 0; i < n; ++i)
+      {
+        if (usedChild[i]) continue;
+        for (int s = 0; s < 8; ++s)
+        {
+          if (childOfSlot[s] >= 0) continue;
+          if (cost[i][s] > best) { best = cost[i][s]; bi = i; bs = s; }
+        }
+      }
+      usedChild[bi] = true;
+      childOfSlot[bs] = bi;
+      slotOf[bi] = bs;
+    }
+    (void)slotOf;
+
+    Bvh8Node node;
+    std::memset(&node, 0, sizeof(node));
+    quantAxis(nb.lo[0], nb.hi[0], node.px, node.ex);
+    quantAxis(nb.lo[1], nb.hi[1], node.py, node.ey);
+    quantAxis(nb.lo[2], nb.hi[2], node.pz, node.ez);
+
+    // Leaf triangles first (contiguous per node), then inner children as one block.
+    int innerCount = 0;
+    for (int s = 0; s < 8; ++s)
+    {
+      if (childOfSlot[s] < 0) continue;
+      if (bin.nodes[children[childOfSlot[s]]].left >= 0) innerCount++;
+    }
+    node.triBase = (uint32_t)out.tris.size();
+    int triOffset = 0;
+    int innerSlots[8];
+    int innerN = 0;
+    for (int s = 0; s < 8; ++s)
+    {
+      const int ci = childOfSlot[s];
+      if (ci < 0) continue;
+      const BinNode& c = bin.nodes[children[ci]];
+      quantChild(node.px, node.ex, c.box.lo[0], c.box.hi[0], node.qlox[s], node.qhix[s]);
+      quantChild(node.py, node.ey, c.box.lo[1], c.box.hi[1], node.qloy[s], node.qhiy[s]);
+      quantChild(node.pz, node.ez, c.box.lo[2], c.box.hi[2], node.qloz[s], node.qhiz[s]);
+      if (c.left >= 0)
+      {
+        node.imask |= (uint8_t)(1u << s);
+        innerSlots[innerN++] = children[ci];
+      }
+      else
+      {
+        node.meta[s] = (uint8_t)((c.count << 5) | triOffset);
+        for (int j = 0; j < c.count; ++j)
+        {
+          const int prim = bin.order[c.first + j];
+          const float* v = verts + 9 * (size_t)prim;
+          Bvh8Tri t;
+          t.v0x = v[0]; t.v0y = v[1]; t.v0z = v[2];
+          t.triId = prim;
+          t.e1x = v[3] - v[0]; t.e1y = v[4] - v[1]; t.e1z = v[5] - v[2];
+          t.e2x = v[6] - v[0]; t.e2y = v[7] - v[1]; t.e2z = v[8] - v[2];
+          t.pad1 = t.pad2 = 0.f;
+          out.tris.push_back(t);
+        }
+        triOffset += c.count;
+      }
+    }
+    node.childBase = (uint32_t)out.nodes.size();
+    out.nodes.resize(out.nodes.size() + innerN);
+    out.nodes[wideIndex] = node;
+    const uint32_t base = node.childBase;
+    for (int i = 0; i < innerN; ++i)
+      emit((int)base + i, innerSlots[i], depth + 1);
+  }
+};
+
+} // namespace
+
+void buildBvh8(const float* triVerts, int64_t triCount, Bvh8& out, int threads)
+{
+  auto t0 = std::chrono::steady_clock::now();
+  if (triCount < 0 || triCount > (int64_t)0x3fffffff)
+    throw std::invalid_argument("BVH8: triangle count out of range");
+  out.nodes.clear();
+  out.tris.clear();
+  out.maxDepth = 0;
+  if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int n = (int)triCount;
+  if (n == 0)
+  {
+    Bvh8Node empty;
+    std::memset(&empty, 0, sizeof(empty));
+    out.nodes.push_back(empty);
+    out.maxDepth = 1;
+    for (int k = 0; k < 3; ++k) { out.lo[k] = 0.f; out.hi[k] = 0.f; }
+    return;
+  }
+  std::vector<Box> boxes(n);
+  for (int i = 0; i < n; ++i)
+  {
+    const float* v = triVerts + 9 * (size_t)i;
+    for (int k = 0; k < 3; ++k)
+    {
+      // Boxes of the triangle as the kernel sees it (v0 + e1, v0 + e2 reconstructed in float).
+      const float a = v[k];
+      const float b = v[k] + (v[3 + k] - v[k]);
+      const float c = v[k] + (v[6 + k] - v[k]);
+      boxes[i].lo[k] = std::min(std::min(a, b), std::min(c, std::min(v[3 + k], v[6 + k])));
+      boxes[i].hi[k] = std::max(std::max(a, b), std::max(c, std::max(v[3 + k], v[6 + k])));
+    }
+  }
+  BinaryBuilder bb(boxes, threads);
+  bb.nextNode = 1;
+  bb.build(0, 0, n);
+  out.tris.reserve(n);
+  out.nodes.reserve(n / 2 + 1);
+  out.nodes.resize(1);
+  WideBuilder wb(bb, triVerts, out);
+  wb.emit(0, 0, 0);
+  out.maxDepth = wb.maxDepth;
+  for (int k = 0; k < 3; ++k) { out.lo[k] = bb.nodes[0].box.lo[k]; out.hi[k] = bb.nodes[0].box.hi[k]; }
+  out.buildMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// ---- host reference traversal (counting) ------------------------------------------------
+namespace {
+
+inline float fmaF(float a, float b, float c) { return std::fmaf(a, b, c); }
+
+inline bool triTest(const Bvh8Tri& t, const float o[3], const float d[3], float tnear, float tfar,
+                    float& tt, float& uu, float& vv)
+{
+  const float e1[3] = {t.e1x, t.e1y, t.e1z}, e2[3] = {t.e2x, t.e2y, t.e2z};
+  const float p[3] = {fmaF(d[1], e2[2], -(d[2] * e2[1])), fmaF(d[2], e2[0], -(d[0] * e2[2])),
+                      fmaF(d[0], e2[1], -(d[1] * e2[0]))};
+  const float det = fmaF(e1[0], p[0], fmaF(e1[1], p[1], e1[2] * p[2]));
+  if (!(det != 0.f)) return false;
+  const float s[3] = {o[0] - t.v0x, o[1] - t.v0y, o[2] - t.v0z};
+  const float q[3] = {fmaF(s[1], e1[2], -(s[2] * e1[1])), fmaF(s[2], e1[0], -(s[0] * e1[2])),
+                      fmaF(s[0], e1[1], -(s[1] * e1[0]))};
+  const float inv = 1.0f / det;
+  const float u = fmaF(s[0], p[0], fmaF(s[1], p[1], s[2] * p[2])) * inv;
+  const float v = fmaF(d[0], q[0], fmaF(d[1], q[1], d[2] * q[2])) * inv;
+  const float tv = fmaF(e2[0], q[0], fmaF(e2[1], q[1], e2[2] * q[2])) * inv;
+  if (!(u >= 0.f) || !(v >= 0.f) || !(u + v <= 1.f)) return false;
+  if (!(tv >= tnear) || !(tv <= tfar)) return false;
+  tt = tv; uu = u; vv = v;
+  return true;
+}
+
+inline float expScale(uint8_t e)
+{
+  uint32_t bits = (uint32_t)e << 23;
+  float f;
+  std::memcpy(&f, &bits, 4);
+  return f;
+}
+
+} // namespace
+
+int bvh8TraceCount(const Bvh8& bvh, const float org[3], const float dir[3], float tnear, float& tfar,
+                   int64_t& nodeVisits, int64_t& triTests)
+{
+  float inv[3];
+  for (int k = 0; k < 3; ++k)
+  {
+    float d = dir[k];
+    if (std::fabs(d) < 8.271806e-25f) d = std::copysign(8.271806e-25f, d); // 2^-80
+    inv[k] = 1.0f / d;
+  }
+  const int oct = (dir[0] < 0.f ? 1 : 0) | (dir[1] < 0.f ? 2 : 0) | (dir[2] < 0.f ? 4 : 0);
+  struct Entry { uint32_t node; };
+  std::vector<uint32_t> stack;
+  stack.push_back(0);
+  int best = -1;
+  float bestT = tfar;
+  while (!stack.empty())
+  {
+    const Bvh8Node& n = bvh.nodes[stack.back()];
+    stack.pop_back();
+    nodeVisits++;
+    const float sx = expScale(n.ex), sy = expScale(n.ey), sz = expScale(n.ez);
+    const float ax = (n.px - org[0]) * inv[0], ay = (n.py - org[1]) * inv[1], az = (n.pz - org[2]) * inv[2];
+    const float bx = sx * inv[0], by = sy * inv[1], bz = sz * inv[2];
+    // Hit children in traversal order (descending slot ^ oct); push inner ones far-first.
+    uint32_t order[8];
+    int nh = 0;
+    for (int b = 7; b >= 0; --b)
+    {
+      const int s = b ^ oct;
+      if (!(n.imask & (1 << s)) && n.meta[s] == 0) continue;
+      const float x0 = fmaF((float)n.qlox[s], bx, ax), x1 = fmaF((float)n.qhix[s], bx, ax);
+      const float y0 = fmaF((float)n.qloy[s], by, ay), y1 = fmaF((float)n.qhiy[s], by, ay);
+      const float z0 = fmaF((float)n.qloz[s], bz, az), z1 = fmaF((float)n.qhiz[s], bz, az);
+      const float tmin = std::max(std::max(std::min(x0, x1), std::min(y0, y1)), std::max(std::min(z0, z1), tnear));
+      const float tmax = std::min(std::min(std::max(x0, x1), std::max(y0, y1)), std::min(std::max(z0, z1), bestT));
+      if (!(tmin <= tmax * 1.000002f)) continue;
+      order[nh++] = (uint32_t)s;
+    }
+    for (int i = nh - 1; i >= 0; --i)
+    {
+      const int s = (int)order[i];
+      if (n.imask & (1 << s))
+      {
+        const uint32_t rel = (uint32_t)__builtin_popcount(n.imask & ((1u << s) - 1u));
+        stack.push_back(n.childBase + rel);
+      }
+    }
+    for (int i = 0; i < nh; ++i)
+    {
+      const int s = (int)order[i];
+      if (n.imask & (1 << s)) continue;
+      const int cnt = n.meta[s] >> 5, off = n.meta[s] & 31;
+      for (int j = 0; j < cnt; ++j)
+      {
+        const Bvh8Tri& t = bvh.tris[n.triBase + off + j];
+        triTests++;
+        float tt, uu, vv;
+        if (triTest(t, org, dir, tnear, bestT, tt, uu, vv))
+        {
+          if (tt < bestT || best < 0 || t.triId < best)
+          {
+            bestT = tt;
+            best = t.triId;
+          }
+        }
+      }
+    }
+  }
+  if (best >= 0) tfar = bestT;
+  return best;
+}
+
+} // namespace prt

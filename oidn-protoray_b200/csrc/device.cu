@@ -1,0 +1,881 @@
+// C ABI of the B200 render device (include/prt_cuda.h) and its host runtime: context,
+// scene upload (BVH8 build, materials, lights, media), camera, frame and render calls.
+// This is the CUDA sibling of the reference's DeviceCpu (render/device_cpu.cpp).
+#include "../../include/prt_cuda.h"
+#include "runtime.h"
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+using namespace prt;
+
+struct prt_context
+{
+  Context c;
+};
+
+namespace {
+
+struct ApiError
+{
+  int code;
+  std::string msg;
+};
+
+void cuCheck(cudaError_t e, const char* what)
+{
+  if (e == cudaErrorMemoryAllocation)
+    throw ApiError{PRT_ERR_OUT_OF_MEMORY, std::string(what) + ": " + cudaGetErrorString(e)};
+  if (e != cudaSuccess) throw ApiError{PRT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
+}
+
+template <class F>
+int guarded(prt_context* ctx, F&& f)
+{
+  if (!ctx) return PRT_ERR_INVALID_ARG;
+  try
+  {
+    f(ctx->c);
+    return PRT_OK;
+  }
+  catch (const ApiError& e)
+  {
+    ctx->c.lastError = e.msg;
+    return e.code;
+  }
+  catch (const std::bad_alloc&)
+  {
+    ctx->c.lastError = "host out of memory";
+    return PRT_ERR_OUT_OF_MEMORY;
+  }
+  catch (const std::invalid_argument& e)
+  {
+    ctx->c.lastError = e.what();
+    return PRT_ERR_INVALID_ARG;
+  }
+  catch (const std::logic_error& e)
+  {
+    ctx->c.lastError = e.what();
+    return PRT_ERR_LOGIC;
+  }
+  catch (const std::exception& e)
+  {
+    ctx->c.lastError = e.what();
+    return PRT_ERR_CUDA;
+  }
+}
+
+void* devAlloc(Context& c, size_t bytes, std::vector<DevBuf>* owner)
+{
+  void* p = nullptr;
+  if (bytes == 0) bytes = 16;
+  cuCheck(cudaMalloc(&p, bytes), "cudaMalloc");
+  if (owner) owner->push_back(DevBuf{p, bytes});
+  return p;
+}
+
+template <class T>
+T* upload(Context& c, const std::vector<T>& v)
+{
+  T* p = (T*)devAlloc(c, v.size() * sizeof(T), &c.sceneBufs);
+  if (!v.empty()) cuCheck(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c.stream), "upload");
+  return p;
+}
+
+void freeScene(Context& c)
+{
+  cudaStreamSynchronize(c.stream);
+  for (auto& b : c.sceneBufs) cudaFree(b.ptr);
+  c.sceneBufs.clear();
+  c.hasScene = false;
+}
+
+void freeFrame(Context& c)
+{
+  cudaStreamSynchronize(c.stream);
+  auto f = [](auto*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+  };
+  f(c.accum);
+  f(c.accumA);
+  f(c.accumN);
+  PathState& s = c.ps;
+  f(s.rayO); f(s.rayD); f(s.hit); f(s.thr); f(s.rad); f(s.info);
+  f(s.shO); f(s.shD); f(s.shL); f(s.out); f(s.aovA); f(s.aovN);
+  f(s.queue[0]); f(s.queue[1]);
+  s.capacity = 0;
+}
+
+// Bit-level host mirror of float operations used to build light tables.
+float luminanceHost(const float c[3]) { return 0.212671f * c[0] + 0.715160f * c[1] + 0.072169f * c[2]; }
+
+// Distribution1D::init (sampling/distribution1d.cpp:14-28).
+void cdfInit(float* cdf, const float* f, int size)
+{
+  cdf[0] = 0.f;
+  for (int i = 1; i < size + 1; ++i) cdf[i] = cdf[i - 1] + f[i - 1];
+  const float norm = (cdf[size] == 0.f) ? 0.f : 1.f / cdf[size];
+  for (int i = 1; i < size + 1; ++i) cdf[i] *= norm;
+  cdf[size] = 1.f;
+}
+
+void makeFrameHost(const float N[3], float U[3], float V[3])
+{
+  const float U0[3] = {0.f, N[2], -N[1]};
+  const float U1[3] = {-N[2], 0.f, N[0]};
+  const float l0 = U0[0] * U0[0] + U0[1] * U0[1] + U0[2] * U0[2];
+  const float l1 = U1[0] * U1[0] + U1[1] * U1[1] + U1[2] * U1[2];
+  const float* u = l0 > l1 ? U0 : U1;
+  const float il = 1.f / std::sqrt(l0 > l1 ? l0 : l1);
+  for (int k = 0; k < 3; ++k) U[k] = u[k] * il;
+  V[0] = N[1] * U[2] - N[2] * U[1];
+  V[1] = N[2] * U[0] - N[0] * U[2];
+  V[2] = N[0] * U[1] - N[1] * U[0];
+  const float iv = 1.f / std::sqrt(V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
+  for (int k = 0; k < 3; ++k) V[k] *= iv;
+}
+
+// Reads a Standard material as StandardMaterial's constructor does (material/standard.cpp:21-150).
+DevMaterial resolveMaterial(const prt_material& m, std::vector<float>& media, int textureCount)
+{
+  DevMaterial d;
+  std::memset(&d, 0, sizeof(d));
+  auto ior = [](float x) {
+    x = std::max(x, 0.f);
+    return x < 1.f ? 1.f / x : x;
+  };
+  d.ambientIor = 1.f;
+  d.baseWeight = m.base_weight;
+  for (int k = 0; k < 3; ++k) d.baseColor[k] = m.base_color[k];
+  d.baseColorTex = m.base_color_texture;
+  if (d.baseColorTex >= textureCount) throw std::invalid_argument("material references a missing texture");
+  d.metalness = m.metalness;
+  d.diffuseRoughness = m.diffuse_roughness;
+  d.hasDiffuseRoughness = m.diffuse_roughness != 0.f;
+  d.specularWeight = m.specular_weight;
+  for (int k = 0; k < 3; ++k) d.specularColor[k] = m.specular_color[k];
+  d.specularRoughness = m.specular_roughness;
+  d.hasSpecularRoughness = m.specular_roughness != 0.f;
+  d.specularIor = ior(m.specular_ior);
+  d.transmissionWeight = m.transmission_weight;
+  for (int k = 0; k < 3; ++k) d.transmissionColor[k] = std::min(std::max(m.transmission_color[k], 0.f), 1.f);
+  d.transmissionDepth = std::max(m.transmission_depth, 0.f);
+  d.subsurfaceWeight = m.subsurface_weight;
+  for (int k = 0; k < 3; ++k) d.subsurfaceColor[k] = m.subsurface_color[k];
+  d.subsurfaceAnisotropy = m.subsurface_anisotropy;
+  d.coatWeight = m.coat_weight;
+  for (int k = 0; k < 3; ++k) d.coatColor[k] = m.coat_color[k];
+  d.coatRoughness = m.coat_roughness;
+  d.hasCoatRoughness = m.coat_roughness != 0.f;
+  d.coatIor = ior(m.coat_ior);
+  d.sheenWeight = m.sheen_weight;
+  for (int k = 0; k < 3; ++k) d.sheenColor[k] = m.sheen_color[k];
+  d.sheenRoughness = m.sheen_roughness;
+  for (int k = 0; k < 3; ++k) d.emission[k] = m.emission_color[k] * m.emission_luminance;
+  d.thinWalled = m.thin_walled;
+  d.opacity = m.opacity;
+  d.type = 0;
+  if (m.emission_luminance > 0.f) d.type |= kMatEmissive;
+  d.mediumInt = d.mediumExt = 0;
+  if (m.opacity != 1.f) d.type |= kMatTransparent;
+  if (m.transmission_weight != 0.f)
+  {
+    d.type |= kMatTransmissive;
+    if (m.thin_walled)
+      d.type |= kMatTransparent;
+    else
+    {
+      d.type |= kMatMediaInterface;
+      // MaterialFactory::makeMedium (material/material_factory.cpp:159-175): media are
+      // deduplicated by (colour, ior); medium 0 is the default (1, 1).
+      auto medium = [&](const float c[3], float n) {
+        const int count = (int)media.size() / 4;
+        for (int i = 0; i < count; ++i)
+          if (media[4 * i] == c[0] && media[4 * i + 1] == c[1] && media[4 * i + 2] == c[2] && media[4 * i + 3] == n)
+            return i;
+        media.insert(media.end(), {c[0], c[1], c[2], n});
+        return count;
+      };
+      float col[3];
+      for (int k = 0; k < 3; ++k) col[k] = std::pow(d.transmissionColor[k], d.transmissionDepth);
+      d.mediumInt = medium(col, d.specularIor);
+      const float one[3] = {1.f, 1.f, 1.f};
+      d.mediumExt = medium(one, d.ambientIor);
+    }
+  }
+  // Lobes the device implements: see resolveStandard (bsdf.cuh).
+  const bool unsupported = (d.metalness != 0.f) || (d.specularWeight != 0.f && std::fabs(d.specularIor - 1.f) > 1e-4f) ||
+                           d.transmissionWeight != 0.f || d.subsurfaceWeight != 0.f || d.coatWeight != 0.f ||
+                           d.sheenWeight != 0.f || d.opacity != 1.f || d.hasDiffuseRoughness;
+  if (unsupported && !(d.type & kMatEmissive))
+    throw std::invalid_argument("material uses lobes not yet supported by the CUDA device");
+  return d;
+}
+
+void uploadScene(Context& c, const prt_scene_desc* s)
+{
+  if (!s || s->mesh_count < 0 || s->material_count <= 0 || !s->materials)
+    throw std::invalid_argument("invalid scene description");
+  freeScene(c);
+  DevScene sc;
+  std::memset(&sc, 0, sizeof(sc));
+  // Materials and media.
+  std::vector<float> media = {1.f, 1.f, 1.f, 1.f};
+  std::vector<DevMaterial> mats;
+  for (int i = 0; i < s->material_count; ++i) mats.push_back(resolveMaterial(s->materials[i], media, s->texture_count));
+  // Textures, stored in texture-row order (bottom row first).
+  std::vector<DevTexture> texs;
+  for (int i = 0; i < s->texture_count; ++i)
+  {
+    const prt_texture& t = s->textures[i];
+    if (!t.rgb || t.width <= 0 || t.height <= 0) throw std::invalid_argument("invalid texture");
+    std::vector<float> flipped((size_t)t.width * t.height * 3);
+    for (int y = 0; y < t.height; ++y)
+      std::memcpy(&flipped[(size_t)y * t.width * 3], t.rgb + (size_t)(t.height - 1 - y) * t.width * 3,
+                  sizeof(float) * 3 * t.width);
+    DevTexture dt;
+    dt.rgb = upload(c, flipped);
+    dt.width = t.width;
+    dt.height = t.height;
+    texs.push_back(dt);
+  }
+  // Geometry: concatenated vertices and triangles.
+  int64_t totalTris = 0, totalVerts = 0;
+  for (int g = 0; g < s->mesh_count; ++g)
+  {
+    const prt_mesh& m = s->meshes[g];
+    if (m.tri_count < 0 || m.vertex_count < 0 || (m.tri_count > 0 && (!m.positions || !m.indices)))
+      throw std::invalid_argument("invalid mesh");
+    if (m.material < 0 || m.material >= s->material_count) throw std::invalid_argument("mesh material out of range");
+    totalTris += m.tri_count;
+    totalVerts += m.vertex_count;
+  }
+  if (totalTris > (int64_t)0x3fffffff || totalVerts > (int64_t)0x7fffffff)
+    throw std::invalid_argument("scene too large");
+  std::vector<float4> pos(totalVerts), nrm;
+  std::vector<float2> uv;
+  bool anyN = false, anyUV = false;
+  for (int g = 0; g < s->mesh_count; ++g)
+  {
+    anyN |= s->meshes[g].normals != nullptr;
+    anyUV |= s->meshes[g].texcoords != nullptr;
+  }
+  if (anyN) nrm.assign(totalVerts, make_float4(0.f, 0.f, 1.f, 0.f));
+  if (anyUV) uv.assign(totalVerts, make_float2(0.f, 0.f));
+  std::vector<int4> triVerts(totalTris);
+  std::vector<float> triPos((size_t)totalTris * 9);
+  std::vector<int> meshFlags(s->mesh_count), meshMat(s->mesh_count), meshOff(s->mesh_count), meshLight(s->mesh_count, -1);
+  float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  int64_t vbase = 0, tbase = 0;
+  for (int g = 0; g < s->mesh_count; ++g)
+  {
+    const prt_mesh& m = s->meshes[g];
+    meshFlags[g] = (m.normals ? 1 : 0) | (m.texcoords ? 2 : 0);
+    meshMat[g] = m.material;
+    meshOff[g] = (int)tbase;
+    for (int v = 0; v < m.vertex_count; ++v)
+    {
+      pos[vbase + v] = make_float4(m.positions[3 * v], m.positions[3 * v + 1], m.positions[3 * v + 2], 0.f);
+      if (m.normals) nrm[vbase + v] = make_float4(m.normals[3 * v], m.normals[3 * v + 1], m.normals[3 * v + 2], 0.f);
+      if (m.texcoords) uv[vbase + v] = make_float2(m.texcoords[2 * v], m.texcoords[2 * v + 1]);
+    }
+    for (int t = 0; t < m.tri_count; ++t)
+    {
+      int idx[3];
+      for (int k = 0; k < 3; ++k)
+      {
+        idx[k] = m.indices[3 * t + k];
+        if (idx[k] < 0 || idx[k] >= m.vertex_count) throw std::invalid_argument("triangle index out of range");
+      }
+      triVerts[tbase + t] = make_int4((int)(vbase + idx[0]), (int)(vbase + idx[1]), (int)(vbase + idx[2]), g);
+      float* tp = &triPos[(size_t)(tbase + t) * 9];
+      for (int k = 0; k < 3; ++k)
+        for (int a = 0; a < 3; ++a)
+        {
+          tp[3 * k + a] = m.positions[3 * idx[k] + a];
+          lo[a] = std::min(lo[a], tp[3 * k + a]);
+          hi[a] = std::max(hi[a], tp[3 * k + a]);
+        }
+    }
+    vbase += m.vertex_count;
+    tbase += m.tri_count;
+  }
+  if (totalTris == 0)
+    for (int a = 0; a < 3; ++a) lo[a] = hi[a] = 0.f;
+  // BVH8
+  buildBvh8(triPos.data(), totalTris, c.bvh);
+  sc.nodes = reinterpret_cast<const uint4*>(upload(c, c.bvh.nodes));
+  sc.tris = reinterpret_cast<const float4*>(upload(c, c.bvh.tris));
+  sc.triCount = totalTris;
+  sc.triVerts = upload(c, triVerts);
+  sc.pos = upload(c, pos);
+  sc.nrm = anyN ? upload(c, nrm) : nullptr;
+  sc.uv = anyUV ? upload(c, uv) : nullptr;
+  sc.meshFlags = upload(c, meshFlags);
+  sc.meshMaterial = upload(c, meshMat);
+  sc.meshTriOffset = upload(c, meshOff);
+  sc.meshCount = s->mesh_count;
+  sc.materials = upload(c, mats);
+  sc.materialCount = (int)mats.size();
+  sc.textures = upload(c, texs);
+  c.meshTriOffsetHost = meshOff;
+  // Scene radius (render/scene.cpp:367): half the diagonal of the bounds.
+  const float ext[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
+  const float sceneRadius = std::sqrt(ext[0] * ext[0] + ext[1] * ext[1] + ext[2] * ext[2]) * 0.5f;
+  sc.sceneRadius = sceneRadius;
+  // Area lights: one TriangleLight per emissive mesh (render/scene.cpp:79-116, light/triangle_light.h:29-60).
+  std::vector<float> etris, areaCdf, lightPower;
+  std::vector<int> areaOff, areaCnt, areaCdfOff;
+  for (int g = 0; g < s->mesh_count; ++g)
+  {
+    const prt_mesh& m = s->meshes[g];
+    const DevMaterial& mat = mats[m.material];
+    if (!(mat.type & kMatEmissive) || m.tri_count == 0) continue;
+    meshLight[g] = (int)areaOff.size();
+    areaOff.push_back((int)(etris.size() / 16));
+    areaCnt.push_back(m.tri_count);
+    std::vector<float> w(m.tri_count);
+    float sumL = 0.f;
+    for (int t = 0; t < m.tri_count; ++t)
+    {
+      const float* tp = &triPos[(size_t)(meshOff[g] + t) * 9];
+      const float e1[3] = {tp[3] - tp[0], tp[4] - tp[1], tp[5] - tp[2]};
+      const float e2[3] = {tp[6] - tp[0], tp[7] - tp[1], tp[8] - tp[2]};
+      const float n[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+      const float len = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+      w[t] = len * luminanceHost(mat.emission);
+      sumL += len * luminanceHost(mat.emission);
+      etris.insert(etris.end(), {tp[0], tp[1], tp[2], tp[3], tp[4], tp[5], tp[6], tp[7], tp[8], n[0], n[1], n[2],
+                                 mat.emission[0], mat.emission[1], mat.emission[2], 0.f});
+    }
+    areaCdfOff.push_back((int)areaCdf.size());
+    const size_t o = areaCdf.size();
+    areaCdf.resize(o + m.tri_count + 1);
+    cdfInit(&areaCdf[o], w.data(), m.tri_count);
+    lightPower.push_back(3.14159265358979323846f * sumL);
+  }
+  sc.areaLightCount = (int)areaOff.size();
+  sc.meshLight = upload(c, meshLight);
+  sc.areaTriOffset = upload(c, areaOff);
+  sc.areaTriCount = upload(c, areaCnt);
+  sc.areaCdfOffset = upload(c, areaCdfOff);
+  sc.areaCdf = upload(c, areaCdf);
+  sc.etris = upload(c, etris);
+  // Environment lights in Scene::initLights order (render/scene.cpp:372-440).
+  const prt_env_desc& e = s->env;
+  const float pi = 3.14159265358979323846f;
+  auto pos3 = [](const float* v) { return v[0] > 0.f || v[1] > 0.f || v[2] > 0.f; };
+  int ne = 0;
+  if (pos3(e.distant_color))
+  {
+    DevEnvLight& L = sc.env[ne++];
+    L.kind = kEnvDistant;
+    for (int k = 0; k < 3; ++k) L.color[k] = e.distant_color[k];
+    float d[3] = {e.distant_dir[0], e.distant_dir[1], e.distant_dir[2]};
+    const float il = 1.f / std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    for (int k = 0; k < 3; ++k) L.dir[k] = d[k] * il;
+    makeFrameHost(L.dir, L.frameU, L.frameV);
+    L.halfAngle = e.distant_angle * 0.5f;
+    L.cosAngle = std::cos(L.halfAngle);
+    const float sh = std::sin(0.5f * L.halfAngle);
+    L.conePdf = 1.f / (4.f * pi * sh * sh);
+    lightPower.push_back(4.f * pi * pi * sh * sh * sceneRadius * sceneRadius * luminanceHost(L.color));
+  }
+  if (pos3(e.ambient_color))
+  {
+    DevEnvLight& L = sc.env[ne++];
+    L.kind = kEnvAmbient;
+    for (int k = 0; k < 3; ++k) L.color[k] = e.ambient_color[k];
+    lightPower.push_back(4.f * pi * pi * sceneRadius * sceneRadius * luminanceHost(L.color));
+  }
+  if (e.image_rgb)
+  {
+    if (e.image_width <= 0 || e.image_height <= 0) throw std::invalid_argument("invalid image light");
+    DevEnvLight& L = sc.env[ne++];
+    L.kind = kEnvImage;
+    const int W = e.image_width, H = e.image_height;
+    // Texture-row order (bottom row first), as ImageTextureBuffer stores it.
+    std::vector<float> tex((size_t)W * H * 3);
+    for (int y = 0; y < H; ++y)
+      std::memcpy(&tex[(size_t)y * W * 3], e.image_rgb + (size_t)(H - 1 - y) * W * 3, sizeof(float) * 3 * W);
+    // ImageLight LUT (light/image_light.h:19-62).
+    int lw = W, lh = H, bucket = 1;
+    if (e.image_lut_size > 0)
+      while (std::max(lw, lh) > e.image_lut_size && lw % 2 == 0 && lh % 2 == 0)
+      {
+        lw /= 2;
+        lh /= 2;
+        bucket *= 2;
+      }
+    std::vector<float> weights((size_t)lw * lh);
+    for (int y = 0; y < lh; ++y)
+      for (int x = 0; x < lw; ++x)
+      {
+        float sum = 0.f;
+        for (int y2 = 0; y2 < bucket; ++y2)
+          for (int x2 = 0; x2 < bucket; ++x2)
+            sum += luminanceHost(&tex[3 * ((size_t)(y * bucket + y2) * W + (x * bucket + x2))]);
+        weights[(size_t)y * lw + x] = sum * std::sin((y + 0.5f) / lh * pi);
+      }
+    // Distribution2D::init (sampling/distribution2d.cpp:13-30).
+    std::vector<float> xCdfs((size_t)lh * (lw + 1)), fy(lh), yCdf(lh + 1);
+    for (int y = 0; y < lh; ++y)
+    {
+      fy[y] = 0.f;
+      for (int x = 0; x < lw; ++x) fy[y] += weights[(size_t)y * lw + x];
+      cdfInit(&xCdfs[(size_t)y * (lw + 1)], &weights[(size_t)y * lw], lw);
+    }
+    cdfInit(yCdf.data(), fy.data(), lh);
+    sc.image.rgb = upload(c, tex);
+    sc.image.width = W;
+    sc.image.height = H;
+    sc.image.lutW = lw;
+    sc.image.lutH = lh;
+    sc.image.yCdf = upload(c, yCdf);
+    sc.image.xCdfs = upload(c, xCdfs);
+    float sumL = 0.f;
+    for (int i = 0; i < W * H; ++i) sumL += luminanceHost(&tex[3 * (size_t)i]);
+    lightPower.push_back(4.f * pi * pi * sceneRadius * sceneRadius * (sumL / float(W * H)));
+  }
+  if (sc.areaLightCount == 0 && ne == 0)
+  {
+    // Default ambient light (render/scene.cpp:435-440).
+    DevEnvLight& L = sc.env[ne++];
+    L.kind = kEnvAmbient;
+    L.color[0] = L.color[1] = L.color[2] = 1.f;
+    lightPower.push_back(4.f * pi * pi * sceneRadius * sceneRadius * luminanceHost(L.color));
+  }
+  sc.envCount = ne;
+  sc.lightCount = sc.areaLightCount + ne;
+  std::vector<float> lightCdf(sc.lightCount + 1);
+  cdfInit(lightCdf.data(), lightPower.data(), sc.lightCount);
+  sc.lightCdf = upload(c, lightCdf);
+  std::vector<float> mediaColor;
+  for (size_t i = 0; i < media.size() / 4; ++i) mediaColor.insert(mediaColor.end(), {media[4 * i], media[4 * i + 1], media[4 * i + 2]});
+  sc.mediaColor = upload(c, mediaColor);
+  sc.mediaCount = (int)(media.size() / 4);
+  cuCheck(cudaStreamSynchronize(c.stream), "scene upload");
+  c.scene = sc;
+  c.hasScene = true;
+}
+
+void allocFrame(Context& c, int width, int height, int aovMask)
+{
+  if (width <= 0 || height <= 0) throw std::invalid_argument("invalid frame size");
+  if (width % 32 != 0 || height % 8 != 0)
+    throw std::logic_error("image size is not divisible by the tile size");
+  if (width > 4096 || height > 4096) throw std::logic_error("image size is too large");
+  freeFrame(c);
+  c.width = width;
+  c.height = height;
+  c.aovMask = aovMask;
+  const size_t px = (size_t)width * height;
+  c.accum = (float*)devAlloc(c, px * sizeof(float4), nullptr);
+  if (aovMask)
+  {
+    c.accumA = (float*)devAlloc(c, px * sizeof(float4), nullptr);
+    c.accumN = (float*)devAlloc(c, px * sizeof(float4), nullptr);
+  }
+  // Wave capacity: whole samples of the frame, up to ~16M paths (about 3 GB of path state).
+  const int64_t target = 16ll << 20;
+  c.waveSamples = (int)std::max<int64_t>(1, target / (int64_t)px);
+  const int64_t cap = (int64_t)c.waveSamples * px;
+  PathState& s = c.ps;
+  s.capacity = cap;
+  auto a4 = [&](size_t n) { return (float4*)devAlloc(c, n * sizeof(float4), nullptr); };
+  s.rayO = a4(cap); s.rayD = a4(cap); s.hit = a4(cap); s.thr = a4(cap); s.rad = a4(cap);
+  s.info = (uint4*)devAlloc(c, cap * sizeof(uint4), nullptr);
+  s.shO = a4(cap); s.shD = a4(cap); s.shL = a4(cap); s.out = a4(cap);
+  if (aovMask)
+  {
+    s.aovA = a4(cap);
+    s.aovN = a4(cap);
+  }
+  s.queue[0] = (int*)devAlloc(c, cap * sizeof(int), nullptr);
+  s.queue[1] = (int*)devAlloc(c, cap * sizeof(int), nullptr);
+  cuCheck(launchClear(c), "clear");
+  cuCheck(cudaStreamSynchronize(c.stream), "frame");
+}
+
+// Per-bounce queue counters: 2 * (maxDepth + 2) counts followed by as many work counters.
+void ensureCounters(Context& c)
+{
+  const size_t need = sizeof(int) * 4 * (size_t)(c.renderer.maxDepth + 2);
+  cudaStreamSynchronize(c.stream);
+  if (c.ps.counters) cudaFree(c.ps.counters);
+  c.ps.counters = (int*)devAlloc(c, need, nullptr);
+}
+
+// Borrowed buffer: device memory is used in place, host memory is staged through a
+// temporary device allocation.
+struct Staged
+{
+  void* dev = nullptr;
+  void* host = nullptr;
+  size_t bytes = 0;
+  bool owned = false;
+  Context* c = nullptr;
+
+  Staged(Context& ctx, const void* p, size_t n, bool copyIn) : bytes(n), c(&ctx)
+  {
+    cudaPointerAttributes attr;
+    if (p && cudaPointerGetAttributes(&attr, p) == cudaSuccess &&
+        (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged))
+    {
+      dev = const_cast<void*>(p);
+      return;
+    }
+    cudaGetLastError();
+    host = const_cast<void*>(p);
+    owned = true;
+    cuCheck(cudaMalloc(&dev, std::max<size_t>(n, 16)), "cudaMalloc");
+    if (copyIn && n) cuCheck(cudaMemcpyAsync(dev, p, n, cudaMemcpyHostToDevice, ctx.stream), "copy in");
+  }
+  void copyOut()
+  {
+    if (owned && host && bytes) cuCheck(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, c->stream), "copy out");
+  }
+  ~Staged()
+  {
+    if (owned && dev)
+    {
+      cudaStreamSynchronize(c->stream);
+      cudaFree(dev);
+    }
+  }
+};
+
+void checkDeviceErrors(Context& c)
+{
+  uint32_t err = 0;
+  cuCheck(cudaMemcpyAsync(&err, c.ps.err, sizeof(err), cudaMemcpyDeviceToHost, c.stream), "error flag");
+  cuCheck(cudaStreamSynchronize(c.stream), "sync");
+  if (err)
+  {
+    cudaMemsetAsync(c.ps.err, 0, sizeof(uint32_t), c.stream);
+    throw ApiError{PRT_ERR_DEVICE_ABORT, "device traversal aborted (flags " + std::to_string(err) +
+                                             "): stack overflow or iteration cap"};
+  }
+}
+
+void requireScene(Context& c)
+{
+  if (!c.hasScene) throw ApiError{PRT_ERR_STATE, "no scene uploaded"};
+}
+
+} // namespace
+
+extern "C" {
+
+int prt_cuda_create(int device_ordinal, prt_context** out_ctx)
+{
+  if (!out_ctx) return PRT_ERR_INVALID_ARG;
+  *out_ctx = nullptr;
+  auto* ctx = new (std::nothrow) prt_context();
+  if (!ctx) return PRT_ERR_OUT_OF_MEMORY;
+  Context& c = ctx->c;
+  c.device = device_ordinal;
+  cudaError_t e = cudaSetDevice(device_ordinal);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c.smCount, cudaDevAttrMultiProcessorCount, device_ordinal);
+  if (e == cudaSuccess) e = cudaMalloc(&c.ps.err, sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemset(c.ps.err, 0, sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaEventCreate(&c.ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&c.ev1);
+  if (e != cudaSuccess)
+  {
+    delete ctx;
+    return e == cudaErrorMemoryAllocation ? PRT_ERR_OUT_OF_MEMORY : PRT_ERR_CUDA;
+  }
+  *out_ctx = ctx;
+  return PRT_OK;
+}
+
+int prt_cuda_destroy(prt_context* ctx)
+{
+  if (!ctx) return PRT_ERR_INVALID_ARG;
+  Context& c = ctx->c;
+  cudaSetDevice(c.device);
+  freeScene(c);
+  freeFrame(c);
+  if (c.ps.counters) cudaFree(c.ps.counters);
+  if (c.ps.err) cudaFree(c.ps.err);
+  if (c.ev0) cudaEventDestroy(c.ev0);
+  if (c.ev1) cudaEventDestroy(c.ev1);
+  if (c.stream) cudaStreamDestroy(c.stream);
+  delete ctx;
+  return PRT_OK;
+}
+
+const char* prt_cuda_last_error(const prt_context* ctx)
+{
+  return ctx ? ctx->c.lastError.c_str() : "null context";
+}
+
+void prt_cuda_material_defaults(prt_material* m)
+{
+  if (!m) return;
+  std::memset(m, 0, sizeof(*m));
+  m->base_weight = 1.f;
+  m->base_color[0] = m->base_color[1] = m->base_color[2] = 0.8f;
+  m->specular_weight = 1.f;
+  m->specular_color[0] = m->specular_color[1] = m->specular_color[2] = 1.f;
+  m->specular_roughness = 0.3f;
+  m->specular_ior = 1.5f;
+  m->transmission_color[0] = m->transmission_color[1] = m->transmission_color[2] = 1.f;
+  m->transmission_depth = 1.f;
+  m->subsurface_color[0] = m->subsurface_color[1] = m->subsurface_color[2] = 0.8f;
+  m->coat_color[0] = m->coat_color[1] = m->coat_color[2] = 1.f;
+  m->coat_ior = 1.6f;
+  m->sheen_color[0] = m->sheen_color[1] = m->sheen_color[2] = 1.f;
+  m->sheen_roughness = 0.3f;
+  m->emission_color[0] = m->emission_color[1] = m->emission_color[2] = 1.f;
+  m->opacity = 1.f;
+  m->base_color_texture = -1;
+}
+
+int prt_cuda_scene_upload(prt_context* ctx, const prt_scene_desc* scene)
+{
+  return guarded(ctx, [&](Context& c) {
+    cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+    uploadScene(c, scene);
+  });
+}
+
+int prt_cuda_renderer(prt_context* ctx, const prt_renderer_desc* r)
+{
+  return guarded(ctx, [&](Context& c) {
+    if (!r || r->max_depth < 0 || r->max_depth > 1000) throw std::invalid_argument("invalid renderer settings");
+    c.renderer.maxDepth = r->max_depth;
+    c.renderer.rrDepth = r->rr_depth;
+    c.renderer.minWeight = r->min_weight;
+    c.renderer.maxRadiance = r->max_radiance;
+    c.hasRenderer = true;
+    c.sampleIndex = 0;
+    ensureCounters(c);
+  });
+}
+
+int prt_cuda_init_sampler(prt_context* ctx, uint32_t seed)
+{
+  return guarded(ctx, [&](Context& c) {
+    c.renderer.seed = seed;
+    c.sampleIndex = 0;
+  });
+}
+
+int prt_cuda_camera(prt_context* ctx, const prt_camera_desc* cam)
+{
+  return guarded(ctx, [&](Context& c) {
+    if (!cam) throw std::invalid_argument("null camera");
+    if (c.width <= 0) throw ApiError{PRT_ERR_STATE, "initialise the frame before the camera"};
+    // PinholeCamera constructor (camera/pinhole_camera.h:20-36).
+    const float aspect = float(c.width) / float(c.height);
+    const float hh = std::tan(0.5f * cam->fov);
+    const float hw = hh * aspect;
+    auto basis = [&](float x, float y, float z, float* out) {
+      for (int k = 0; k < 3; ++k) out[k] = x * cam->basis_u[k] + y * cam->basis_v[k] + z * cam->basis_n[k];
+    };
+    for (int k = 0; k < 3; ++k) c.camera.org[k] = cam->position[k];
+    basis(-hw, hh, -1.f, c.camera.imageO);
+    basis(2.f * hw, 0.f, 0.f, c.camera.imageDx);
+    basis(0.f, -2.f * hh, 0.f, c.camera.imageDy);
+    c.camera.nearClip = cam->near_clip;
+    c.hasCamera = true;
+  });
+}
+
+int prt_cuda_frame(prt_context* ctx, int32_t width, int32_t height, int32_t aov_mask)
+{
+  return guarded(ctx, [&](Context& c) {
+    cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+    allocFrame(c, width, height, aov_mask);
+  });
+}
+
+int prt_cuda_clear(prt_context* ctx)
+{
+  return guarded(ctx, [&](Context& c) {
+    if (!c.accum) throw ApiError{PRT_ERR_STATE, "no frame"};
+    cuCheck(launchClear(c), "clear");
+  });
+}
+
+int prt_cuda_render(prt_context* ctx, int32_t spp, prt_render_stats* stats)
+{
+  return guarded(ctx, [&](Context& c) {
+    requireScene(c);
+    if (!c.hasRenderer || !c.hasCamera || !c.accum) throw ApiError{PRT_ERR_STATE, "renderer, camera and frame are required"};
+    if (spp < 0) throw std::invalid_argument("spp must be >= 0");
+    cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+    cuCheck(cudaEventRecord(c.ev0, c.stream), "event");
+    int64_t rays = 0;
+    cuCheck(renderSamples(c, spp, rays), "render");
+    cuCheck(cudaEventRecord(c.ev1, c.stream), "event");
+    cuCheck(cudaEventSynchronize(c.ev1), "render sync");
+    checkDeviceErrors(c);
+    float ms = 0.f;
+    cuCheck(cudaEventElapsedTime(&ms, c.ev0, c.ev1), "event time");
+    if (stats)
+    {
+      stats->rays = rays;
+      stats->spp = spp;
+      stats->render_ms = ms;
+      stats->mray = ms > 0.f ? (double)rays / 1e6 / (ms * 1e-3) : 0.0;
+    }
+  });
+}
+
+int prt_cuda_blit(prt_context* ctx, int32_t aov, float* dst)
+{
+  return guarded(ctx, [&](Context& c) {
+    if (!c.accum || !dst) throw std::invalid_argument("no frame or null destination");
+    if (aov < 0 || aov > 2 || (aov > 0 && !c.accumA)) throw std::invalid_argument("AOV not enabled");
+    Staged out(c, dst, (size_t)c.width * c.height * 3 * sizeof(float), false);
+    cuCheck(launchBlit(c, aov, (float*)out.dev), "blit");
+    out.copyOut();
+    cuCheck(cudaStreamSynchronize(c.stream), "blit sync");
+  });
+}
+
+int prt_cuda_sobol(prt_context* ctx, int64_t n, const uint32_t* sample_index, const uint32_t* pixel_id,
+                   const uint32_t* dim_set, int32_t dims, float* out)
+{
+  return guarded(ctx, [&](Context& c) {
+    if (n < 0 || dims < 1 || dims > 3 || (n > 0 && (!sample_index || !pixel_id || !dim_set || !out)))
+      throw std::invalid_argument("invalid sobol query");
+    if (n == 0) return;
+    Staged si(c, sample_index, n * 4, true), pid(c, pixel_id, n * 4, true), ds(c, dim_set, n * 4, true);
+    Staged o(c, out, (size_t)n * dims * 4, false);
+    cuCheck(launchSobol(c, n, (const uint32_t*)si.dev, (const uint32_t*)pid.dev, (const uint32_t*)ds.dev, dims,
+                        (float*)o.dev), "sobol");
+    o.copyOut();
+    cuCheck(cudaStreamSynchronize(c.stream), "sobol sync");
+  });
+}
+
+int prt_cuda_trace(prt_context* ctx, int64_t n, const float* rays, int32_t* geom_id, int32_t* prim_id, float* t,
+                   float* u, float* v)
+{
+  return guarded(ctx, [&](Context& c) {
+    requireScene(c);
+    if (n < 0 || (n > 0 && (!rays || !geom_id || !prim_id || !t))) throw std::invalid_argument("invalid trace query");
+    if (n == 0) return;
+    Staged r(c, rays, (size_t)n * 32, true);
+    Staged tri(c, nullptr, (size_t)n * 4, false);
+    Staged to(c, t, (size_t)n * 4, false);
+    Staged uo(c, u, u ? (size_t)n * 4 : 0, false), vo(c, v, v ? (size_t)n * 4 : 0, false);
+    cuCheck(launchTrace(c, n, (const float*)r.dev, (int32_t*)tri.dev, (float*)to.dev, u ? (float*)uo.dev : nullptr,
+                        v ? (float*)vo.dev : nullptr), "trace");
+    std::vector<int32_t> triHost(n);
+    cuCheck(cudaMemcpyAsync(triHost.data(), tri.dev, n * 4, cudaMemcpyDeviceToHost, c.stream), "copy");
+    to.copyOut();
+    if (u) uo.copyOut();
+    if (v) vo.copyOut();
+    checkDeviceErrors(c);
+    // Global triangle index -> (mesh, triangle within mesh).
+    const std::vector<int>& off = c.meshTriOffsetHost;
+    for (int64_t i = 0; i < n; ++i)
+    {
+      const int id = triHost[i];
+      if (id < 0)
+      {
+        geom_id[i] = prim_id[i] = -1;
+        continue;
+      }
+      const int g = (int)(std::upper_bound(off.begin(), off.end(), id) - off.begin()) - 1;
+      geom_id[i] = g;
+      prim_id[i] = id - off[g];
+    }
+  });
+}
+
+int prt_cuda_occluded(prt_context* ctx, int64_t n, const float* rays, int32_t* occluded)
+{
+  return guarded(ctx, [&](Context& c) {
+    requireScene(c);
+    if (n < 0 || (n > 0 && (!rays || !occluded))) throw std::invalid_argument("invalid occlusion query");
+    if (n == 0) return;
+    Staged r(c, rays, (size_t)n * 32, true);
+    Staged o(c, occluded, (size_t)n * 4, false);
+    cuCheck(launchOccluded(c, n, (const float*)r.dev, (int32_t*)o.dev), "occluded");
+    o.copyOut();
+    checkDeviceErrors(c);
+  });
+}
+
+int prt_cuda_query_primary(prt_context* ctx, uint32_t sample_index, float* rays_out, int32_t* geom_id,
+                           int32_t* prim_id, float* t)
+{
+  return guarded(ctx, [&](Context& c) {
+    requireScene(c);
+    if (!c.hasCamera || c.width <= 0) throw ApiError{PRT_ERR_STATE, "camera and frame are required"};
+    if (!rays_out || !geom_id || !prim_id || !t) throw std::invalid_argument("null output");
+    const int64_t n = (int64_t)c.width * c.height;
+    Staged r(c, rays_out, (size_t)n * 32, false);
+    Staged tri(c, nullptr, (size_t)n * 4, false);
+    Staged to(c, t, (size_t)n * 4, false);
+    cuCheck(launchPrimary(c, sample_index, (float*)r.dev, (int32_t*)tri.dev, (float*)to.dev), "primary");
+    r.copyOut();
+    to.copyOut();
+    std::vector<int32_t> triHost(n);
+    cuCheck(cudaMemcpyAsync(triHost.data(), tri.dev, n * 4, cudaMemcpyDeviceToHost, c.stream), "copy");
+    checkDeviceErrors(c);
+    const std::vector<int>& off = c.meshTriOffsetHost;
+    for (int64_t i = 0; i < n; ++i)
+    {
+      const int id = triHost[i];
+      if (id < 0)
+      {
+        geom_id[i] = prim_id[i] = -1;
+        continue;
+      }
+      const int g = (int)(std::upper_bound(off.begin(), off.end(), id) - off.begin()) - 1;
+      geom_id[i] = g;
+      prim_id[i] = id - off[g];
+    }
+  });
+}
+
+int prt_bvh8_count(const float* tri_verts, int64_t tri_count, int64_t n, const float* rays, int32_t* tri_out,
+                   float* t_out, int64_t* node_visits, int64_t* tri_tests, int64_t* node_count)
+{
+  if (tri_count < 0 || n < 0 || (tri_count > 0 && !tri_verts) || (n > 0 && (!rays || !tri_out || !t_out)) ||
+      !node_visits || !tri_tests || !node_count)
+    return PRT_ERR_INVALID_ARG;
+  try
+  {
+    Bvh8 bvh;
+    buildBvh8(tri_verts, tri_count, bvh);
+    *node_count = (int64_t)bvh.nodes.size();
+    int64_t nv = 0, tt = 0;
+    for (int64_t i = 0; i < n; ++i)
+    {
+      const float* r = rays + 8 * i;
+      float tfar = r[7];
+      tri_out[i] = bvh8TraceCount(bvh, r, r + 4, r[3], tfar, nv, tt);
+      t_out[i] = tfar;
+    }
+    *node_visits += nv;
+    *tri_tests += tt;
+    return PRT_OK;
+  }
+  catch (const std::invalid_argument&)
+  {
+    return PRT_ERR_INVALID_ARG;
+  }
+  catch (...)
+  {
+    return PRT_ERR_LOGIC;
+  }
+}
+
+} // extern "C"

@@ -1,0 +1,144 @@
+// Device-resident scene, renderer and frame state shared by the host runtime and the kernels.
+// Plain structs of device pointers and scalars, passed to kernels by value.
+#pragma once
+
+#include <cstdint>
+
+namespace prt {
+
+// Material type bits (material/material.h MaterialType).
+enum : int
+{
+  kMatEmissive = 1 << 0,
+  kMatTransmissive = 1 << 1,
+  kMatMediaInterface = 1 << 2,
+  kMatTransparent = 1 << 3,
+};
+
+// A Standard material with its parameters read and clamped as StandardMaterial::getBsdfLobes
+// reads them (material/standard.cpp:410-620). "has*" flags mirror the MaterialParam truth
+// tests that pick rough versus smooth lobes (material/material_param.h:49,181).
+struct DevMaterial
+{
+  int type;
+  int baseColorTex;      // texture index or -1
+  int mediumInt, mediumExt;
+  float baseWeight;
+  float baseColor[3];    // factor (multiplies the texture when textured)
+  float metalness;
+  float diffuseRoughness;
+  int hasDiffuseRoughness;
+  float specularWeight;
+  float specularColor[3];
+  float specularRoughness;
+  int hasSpecularRoughness;
+  float specularIor;
+  float ambientIor;
+  float transmissionWeight;
+  float transmissionColor[3];
+  float transmissionDepth;
+  float subsurfaceWeight;
+  float subsurfaceColor[3];
+  float subsurfaceAnisotropy;
+  float coatWeight;
+  float coatColor[3];
+  float coatRoughness;
+  int hasCoatRoughness;
+  float coatIor;
+  float sheenWeight;
+  float sheenColor[3];
+  float sheenRoughness;
+  float emission[3];     // emissionColor * emissionLuminance
+  int thinWalled;
+  float opacity;
+};
+
+struct DevTexture
+{
+  const float* rgb;  // texture-row order: row 0 is the bottom image row
+  int width, height;
+};
+
+// Environment light kinds, in Scene::initLights order (render/scene.cpp:365-450).
+enum : int
+{
+  kEnvDistant = 1,
+  kEnvAmbient = 2,
+  kEnvImage = 3,
+};
+
+struct DevEnvLight
+{
+  int kind;
+  float color[3];     // distant/ambient radiance
+  float dir[3];       // distant: unit direction toward the light
+  float frameU[3], frameV[3];
+  float cosAngle;     // distant: cos of the cone half angle
+  float conePdf;      // distant: 1 / (4 pi sin^2(angle/2))
+  float halfAngle;
+};
+
+struct DevImageLight
+{
+  const float* rgb;       // width*height*3, texture-row order (row 0 = bottom)
+  int width, height;
+  int lutW, lutH;         // LUT (Distribution2D) size
+  const float* yCdf;      // lutH + 1
+  const float* xCdfs;     // lutH * (lutW + 1)
+};
+
+struct DevScene
+{
+  // BVH8 (bvh8.h)
+  const uint4* nodes;
+  const float4* tris;
+  int64_t triCount;
+  // Shading data per global triangle: vertex indices (global) and mesh index.
+  const int4* triVerts;      // x, y, z: global vertex indices; w: mesh index
+  const float4* pos;         // per vertex
+  const float4* nrm;         // per vertex, or null where a mesh has no normals
+  const float2* uv;          // per vertex, or null where a mesh has no texcoords
+  const int* meshFlags;      // bit 0: has normals, bit 1: has texcoords
+  const int* meshMaterial;   // material index per mesh
+  const int* meshTriOffset;  // first global triangle of each mesh
+  const int* meshLight;      // area light index per mesh, -1 if not emissive
+  int meshCount;
+  const DevMaterial* materials;
+  int materialCount;
+  const DevTexture* textures;
+  // Lights (render/scene.h:16-30): area lights first, then environment lights.
+  int lightCount;
+  int areaLightCount;
+  const float* lightCdf;         // lightCount + 1
+  const int* areaTriOffset;      // per area light: first emissive triangle
+  const int* areaTriCount;
+  const int* areaCdfOffset;      // per area light: offset of its (count + 1)-entry CDF
+  const float* areaCdf;
+  const float* etris;            // 16 floats per emissive triangle: v0 v1 v2 normal color pad
+  int envCount;
+  DevEnvLight env[4];
+  DevImageLight image;
+  // Media (material/medium.h): transmittance colour and IOR per medium id.
+  const float* mediaColor;       // 3 per medium
+  int mediaCount;
+  float sceneRadius;
+};
+
+struct DevCamera
+{
+  float org[3];
+  float imageO[3], imageDx[3], imageDy[3];
+  float nearClip;
+};
+
+// Renderer settings (render/path_renderer_stream.h:114-116, render/integrator.h:60-62).
+struct DevRenderer
+{
+  int maxDepth;
+  int rrDepth;
+  float minWeight;
+  float maxRadiance;
+  uint32_t seed;
+};
+
+} // namespace prt

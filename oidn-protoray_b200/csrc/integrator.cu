@@ -1,0 +1,614 @@
+// Wavefront path tracer kernels for sm_100a and their launchers.
+//
+// One wave = every pixel x a run of consecutive sample indices. Each kernel walks a queue of
+// path slots; slot = (sample - firstSample) * pixelCount + tileMortonIndex(pixel), so the
+// paths of one sample are contiguous and neighbouring slots are neighbouring pixels (8x8
+// Morton blocks, like the reference's tile order, image/morton.h:33). Per bounce:
+//   trace   : closest hit of every queued ray (persistent warps pull 32 rays at a time)
+//   shade   : miss / area-light / surface shading, NEE shadow ray, BSDF sampling, Russian
+//             roulette; extended paths and shadow rays are appended with warp-aggregated
+//             atomics (the GPU form of RayStreamChannel::packSet, core/ray_stream.h:54)
+//   shadow  : any-hit test; adds the NEE contribution and finishes paths that ended
+// After the last bounce, accumulate() adds each pixel's samples in sample order into the FP32
+// accumulation planes, reproducing AccumBuffer3f::addSerial (image/accum_buffer.h:439-486)
+// without atomics, so the image does not depend on scheduling.
+#include "runtime.h"
+#include "sobol_burley.cuh"
+#include "traverse.cuh"
+#include "bsdf.cuh"
+
+#include <algorithm>
+
+namespace prt {
+
+// Path flags kept in the high bits of pixelId (render/path_renderer_stream.h:69-79).
+constexpr uint32_t kPixelIdMask = 0x0fff0fffu;
+constexpr uint32_t kPathAov1Flag = 0x20000000u;
+constexpr uint32_t kPathAov2Flag = 0x10000000u;
+constexpr uint32_t kShadowFinish = 0x80000000u;
+
+// Sample dimensions (render/integrator.h:52-56, render/path_renderer_stream.h:24-33).
+constexpr uint32_t kDimPixel = 0, kDimLens = 2, kDimBase = 4;
+constexpr uint32_t kDimBsdf = 0, kDimLight = 3, kDimTerminate = 6, kDimBounce = 7;
+
+struct Launch
+{
+  DevScene sc;
+  DevCamera cam;
+  DevRenderer rd;
+  PathState ps;
+  int width, height, pixelCount;
+  uint32_t firstSample;
+  int samples;       // samples in this wave
+  int aovMask;
+};
+
+PRT_D int laneId() { return threadIdx.x & 31; }
+
+// Appends `pred` lanes of the calling (converged) warp to a queue; returns the slot or -1.
+PRT_D int warpAppend(int* counter, bool pred)
+{
+  const unsigned active = __activemask();
+  const unsigned ballot = __ballot_sync(active, pred);
+  if (ballot == 0u) return -1;
+  const int leader = __ffs(ballot) - 1;
+  int base = 0;
+  if (laneId() == leader) base = atomicAdd(counter, __popc(ballot));
+  base = __shfl_sync(active, base, leader);
+  return pred ? base + __popc(ballot & ((1u << laneId()) - 1u)) : -1;
+}
+
+// Pixel of a slot within one sample: 8x8 Morton blocks, blocks in row-major order.
+PRT_D void pixelOf(int idx, int width, int& x, int& y)
+{
+  const int block = idx >> 6, local = idx & 63;
+  const int bw = width >> 3;
+  const int bx = block % bw, by = block / bw;
+  const int lx = (local & 1) | ((local >> 1) & 2) | ((local >> 2) & 4);
+  const int ly = ((local >> 1) & 1) | ((local >> 2) & 2) | ((local >> 3) & 4);
+  x = bx * 8 + lx;
+  y = by * 8 + ly;
+}
+
+PRT_D int slotOfPixel(int x, int y, int width)
+{
+  const int block = (y >> 3) * (width >> 3) + (x >> 3);
+  const int lx = x & 7, ly = y & 7;
+  const int local = (lx & 1) | ((ly & 1) << 1) | ((lx & 2) << 1) | ((ly & 2) << 2) | ((lx & 4) << 2) | ((ly & 4) << 3);
+  return block * 64 + local;
+}
+
+// IntegratorBase::clampL (render/integrator.h:28-46).
+PRT_D f3 clampL(f3 L, float maxRadiance)
+{
+  f3 c = mk(0.f < L.x ? L.x : 0.f, 0.f < L.y ? L.y : 0.f, 0.f < L.z ? L.z : 0.f);
+  const float y = luminance(c);
+  if (y > maxRadiance) c *= maxRadiance * (1.f / y);
+  return c;
+}
+
+// MIS power heuristic (render/path_renderer_stream.h:1077-1080).
+PRT_D float misWeight(float a, float b) { return sqr(a) * rcpSafe(sqr(a) + sqr(b)); }
+
+// PinholeCamera::getRay (camera/pinhole_camera.h:78-83).
+PRT_D void cameraRay(const DevCamera& cam, float ix, float iy, f3& org, f3& dir, float& tnear)
+{
+  const f3 d = mk(cam.imageO[0], cam.imageO[1], cam.imageO[2]) + ix * mk(cam.imageDx[0], cam.imageDx[1], cam.imageDx[2]) +
+               iy * mk(cam.imageDy[0], cam.imageDy[1], cam.imageDy[2]);
+  const float len = sqrtf(lengthSqr(d));
+  dir = d * (1.f / len);
+  org = mk(cam.org[0], cam.org[1], cam.org[2]);
+  tnear = cam.nearClip * len;
+}
+
+// ---- query kernels --------------------------------------------------------------------------
+
+__global__ void kSobol(int64_t n, const uint32_t* __restrict__ si, const uint32_t* __restrict__ pid,
+                       const uint32_t* __restrict__ dims, int ndim, uint32_t seed, float* __restrict__ out)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+  {
+    const SobolState st = sobolSetSample(seed, si[i], pid[i]);
+    if (ndim == 1)
+      out[i] = sobolGet1D(st, dims[i]);
+    else if (ndim == 2)
+      sobolGet2D(st, dims[i], out[2 * i], out[2 * i + 1]);
+    else
+      sobolGet3D(st, dims[i], out[3 * i], out[3 * i + 1], out[3 * i + 2]);
+  }
+}
+
+__global__ void kTraceRays(DevScene sc, int64_t n, const float4* __restrict__ rays, int32_t* __restrict__ triOut,
+                           float* __restrict__ tOut, float* __restrict__ uOut, float* __restrict__ vOut,
+                           uint32_t* err)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+  {
+    const float4 a = rays[2 * i], b = rays[2 * i + 1];
+    const TraceHit h = traverse<false>(sc.nodes, sc.tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w, err);
+    triOut[i] = h.triId;
+    tOut[i] = h.t;
+    if (uOut) uOut[i] = h.u;
+    if (vOut) vOut[i] = h.v;
+  }
+}
+
+__global__ void kOccludedRays(DevScene sc, int64_t n, const float4* __restrict__ rays, int32_t* __restrict__ occ,
+                              uint32_t* err)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+  {
+    const float4 a = rays[2 * i], b = rays[2 * i + 1];
+    const TraceHit h = traverse<true>(sc.nodes, sc.tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w, err);
+    occ[i] = h.triId >= 0 ? 1 : 0;
+  }
+}
+
+// Primary rays of one sample for every pixel in row-major order, plus their closest hits.
+__global__ void kPrimary(DevScene sc, DevCamera cam, int width, int height, uint32_t seed, uint32_t sampleIndex,
+                         float4* __restrict__ raysOut, int32_t* __restrict__ triOut, float* __restrict__ tOut,
+                         uint32_t* err)
+{
+  const int n = width * height;
+  const float invW = 1.f / (float)width, invH = 1.f / (float)height;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+  {
+    const int x = i % width, y = i / width;
+    const uint32_t pixelId = (uint32_t)x | ((uint32_t)y << 16);
+    const SobolState st = sobolSetSample(seed, sampleIndex, pixelId);
+    float sx, sy;
+    sobolGet2D(st, kDimPixel, sx, sy);
+    f3 org, dir;
+    float tnear;
+    cameraRay(cam, ((float)x + sx) * invW, ((float)y + sy) * invH, org, dir, tnear);
+    raysOut[2 * i] = make_float4(org.x, org.y, org.z, tnear);
+    raysOut[2 * i + 1] = make_float4(dir.x, dir.y, dir.z, kPosMax);
+    const TraceHit h = traverse<false>(sc.nodes, sc.tris, org, dir, tnear, kPosMax, err);
+    triOut[i] = h.triId;
+    tOut[i] = h.t;
+  }
+}
+
+// ---- wavefront kernels -----------------------------------------------------------------------
+
+// Path initialisation (render/path_renderer_stream.h:209-262).
+__global__ void kRaygen(Launch L)
+{
+  const int64_t P = (int64_t)L.pixelCount * L.samples;
+  const float invW = 1.f / (float)L.width, invH = 1.f / (float)L.height;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P; p += (int64_t)gridDim.x * blockDim.x)
+  {
+    const int s = (int)(p / L.pixelCount);
+    const int idx = (int)(p - (int64_t)s * L.pixelCount);
+    int x, y;
+    pixelOf(idx, L.width, x, y);
+    const uint32_t pixelId = (uint32_t)x | ((uint32_t)y << 16);
+    const uint32_t sampleIndex = L.firstSample + (uint32_t)s;
+    const SobolState st = sobolSetSample(L.rd.seed, sampleIndex, pixelId);
+    float sx, sy;
+    sobolGet2D(st, kDimPixel, sx, sy);
+    f3 org, dir;
+    float tnear;
+    cameraRay(L.cam, ((float)x + sx) * invW, ((float)y + sy) * invH, org, dir, tnear);
+    L.ps.rayO[p] = make_float4(org.x, org.y, org.z, tnear);
+    L.ps.rayD[p] = make_float4(dir.x, dir.y, dir.z, kPosMax);
+    L.ps.thr[p] = make_float4(1.f, 1.f, 1.f, 1.f);
+    L.ps.rad[p] = make_float4(0.f, 0.f, 0.f, __int_as_float(kSpecularReflection));
+    L.ps.info[p] = make_uint4(pixelId, sampleIndex, 0u, 0u);
+    if (L.aovMask)
+    {
+      L.ps.aovA[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+      L.ps.aovN[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+}
+
+// Closest-hit traversal of the queued rays; persistent warps take 32 rays at a time.
+__global__ void __launch_bounds__(256) kTrace(Launch L, const int* __restrict__ queue, const int* __restrict__ count,
+                                              int* __restrict__ work)
+{
+  const int n = *count;
+  for (;;)
+  {
+    int base = 0;
+    if (laneId() == 0) base = atomicAdd(work, 32);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) return;
+    const int i = base + laneId();
+    if (i < n)
+    {
+      const int p = queue ? __ldg(queue + i) : i;
+      const float4 a = L.ps.rayO[p], b = L.ps.rayD[p];
+      const TraceHit h = traverse<false>(L.sc.nodes, L.sc.tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w, L.ps.err);
+      L.ps.hit[p] = make_float4(h.t, h.u, h.v, __int_as_float(h.triId));
+    }
+  }
+}
+
+// Any-hit test of the queued shadow rays; adds the unoccluded NEE contribution and
+// finishes paths that ended at this bounce (render/path_renderer_stream.h:953-1010).
+__global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__ count, int* __restrict__ work)
+{
+  const int n = *count;
+  for (;;)
+  {
+    int base = 0;
+    if (laneId() == 0) base = atomicAdd(work, 32);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) return;
+    const int i = base + laneId();
+    if (i < n)
+    {
+      const float4 a = L.ps.shO[i], b = L.ps.shD[i], c = L.ps.shL[i];
+      const uint32_t tag = __float_as_uint(c.w);
+      const int p = (int)(tag & 0x7fffffffu);
+      bool unoccluded = b.w > 0.f;
+      if (unoccluded)
+      {
+        const TraceHit h = traverse<true>(L.sc.nodes, L.sc.tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w, L.ps.err);
+        unoccluded = h.triId < 0;
+      }
+      float4 r = L.ps.rad[p];
+      if (unoccluded)
+      {
+        r.x += c.x;
+        r.y += c.y;
+        r.z += c.z;
+        L.ps.rad[p] = r;
+      }
+      if (tag & kShadowFinish)
+      {
+        const f3 cl = clampL(mk(r.x, r.y, r.z), L.rd.maxRadiance);
+        L.ps.out[p] = make_float4(cl.x, cl.y, cl.z, 1.f);
+      }
+    }
+  }
+}
+
+PRT_D void finishPath(const Launch& L, int p, f3 rad)
+{
+  const f3 c = clampL(rad, L.rd.maxRadiance);
+  L.ps.out[p] = make_float4(c.x, c.y, c.z, 1.f);
+}
+
+// Shading of one bounce (render/path_renderer_stream.h:276-949).
+__global__ void __launch_bounds__(256) kShade(Launch L, const int* __restrict__ queue, const int* __restrict__ count,
+                                              int depth, int* __restrict__ queueOut, int* __restrict__ extCount,
+                                              int* __restrict__ shadowCount)
+{
+  const int n = *count;
+  const uint32_t sampleDim = kDimBase + kDimBounce * (uint32_t)depth;
+  for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x)
+  {
+    const int i = base + threadIdx.x;
+    const bool active = i < n;
+    const int p = active ? (queue ? __ldg(queue + i) : i) : 0;
+    bool extend = false;
+    bool shadow = false;
+    float4 shO = make_float4(0.f, 0.f, 0.f, 0.f), shD = shO, shL = shO;
+    if (active)
+    {
+      const float4 ro = L.ps.rayO[p], rd = L.ps.rayD[p], hh = L.ps.hit[p];
+      float4 tp = L.ps.thr[p];
+      float4 ra = L.ps.rad[p];
+      uint4 info = L.ps.info[p];
+      const f3 org = mk(ro.x, ro.y, ro.z), dir = mk(rd.x, rd.y, rd.z);
+      const int triId = __float_as_int(hh.w);
+      f3 T = mk(tp.x, tp.y, tp.z);
+      f3 Lr = mk(ra.x, ra.y, ra.z);
+      const float lastPdf = tp.w;
+      const int lastType = __float_as_int(ra.w);
+      uint32_t pixelId = info.x;
+      const bool aov1 = (pixelId & kPathAov1Flag) == 0u;
+      if (triId < 0)
+      {
+        // Miss: environment lights (render/path_renderer_stream.h:287-415).
+        float lightPdf;
+        const f3 Le = evalEnvLights(L.sc, dir, lightPdf);
+        const float w = (lastType & kBsdfSmooth) == 0 ? 1.f : misWeight(lastPdf, lightPdf);
+        Lr += T * w * Le;
+        finishPath(L, p, Lr);
+        if (aov1 && L.aovMask)
+        {
+          L.ps.aovA[p] = make_float4(0.f, 0.f, 0.f, 1.f);
+          L.ps.aovN[p] = make_float4(0.f, 0.f, 0.f, 1.f);
+        }
+      }
+      else
+      {
+        const int4 tv = __ldg(L.sc.triVerts + triId);
+        const int mesh = tv.w;
+        const int matId = __ldg(L.sc.meshMaterial + mesh);
+        const DevMaterial& mat = L.sc.materials[matId];
+        if (mat.type & kMatEmissive)
+        {
+          // Area light hit (render/path_renderer_stream.h:421-582).
+          float lightPdf;
+          const int prim = triId - __ldg(L.sc.meshTriOffset + mesh);
+          const f3 Le = evalAreaLight(L.sc, mesh, prim, dir, hh.x, lightPdf);
+          const float w = (lastType & kBsdfSmooth) == 0 ? 1.f : misWeight(lastPdf, lightPdf);
+          Lr += T * w * Le;
+          finishPath(L, p, Lr);
+          if (aov1 && L.aovMask)
+          {
+            const f3 N = normalize(-dir);
+            L.ps.aovA[p] = make_float4(1.f, 1.f, 1.f, 1.f);
+            L.ps.aovN[p] = make_float4(N.x, N.y, N.z, 1.f);
+          }
+        }
+        else if (depth >= L.rd.maxDepth)
+        {
+          finishPath(L, p, Lr);
+        }
+        else
+        {
+          // Surface hit (render/path_renderer_stream.h:592-949).
+          ShadeCtx ctx;
+          postIntersect(L.sc, org, dir, hh.x, triId, hh.y, hh.z, ctx);
+          const f3 wo = -dir;
+          StdBsdf bsdf;
+          resolveStandard(L.sc, mat, ctx, wo, bsdf);
+          const SobolState st = sobolSetSample(L.rd.seed, info.y, pixelId & kPixelIdMask);
+          const bool aov2 = (pixelId & kPathAov2Flag) == 0u;
+          const bool rr = !(aov1 || aov2);
+          // Direct light (NEE)
+          if (bsdf.flags & kBsdfSmooth)
+          {
+            float lx, ly, lz;
+            sobolGet3D(st, sampleDim + kDimLight, lx, ly, lz);
+            f3 wi;
+            float lightPdf, dist;
+            const f3 Lw = sampleLight(L.sc, ctx.p, lx, ly, lz, wi, lightPdf, dist);
+            if (reduceMax(Lw) > 0.f && lightPdf > 0.f)
+            {
+              float bsdfPdf;
+              const f3 bv = bsdf.eval(wo, wi, bsdfPdf);
+              if (reduceMax(bv) > 0.f)
+              {
+                const f3 dirT = T * bv;
+                if (depth >= L.rd.rrDepth)
+                {
+                  const float contProb = rr ? fminf(luminance(dirT * (1.f / bsdfPdf)), 0.95f) : 1.f;
+                  bsdfPdf *= contProb;
+                }
+                const f3 dirL = dirT * misWeight(lightPdf, bsdfPdf) * Lw;
+                shadow = true;
+                shO = make_float4(ctx.p.x, ctx.p.y, ctx.p.z, ctx.eps);
+                shD = make_float4(wi.x, wi.y, wi.z, dist - ctx.eps);
+                shL = make_float4(dirL.x, dirL.y, dirL.z, 0.f);
+              }
+            }
+          }
+          // BSDF sampling
+          float bx, by, bz;
+          sobolGet3D(st, sampleDim + kDimBsdf, bx, by, bz);
+          f3 wi;
+          float bsdfPdf;
+          int bsdfType;
+          const f3 bw = bsdf.sample(wo, bx, by, bz, wi, bsdfPdf, bsdfType);
+          extend = reduceMax(bw) > 0.f && bsdfPdf > 0.f;
+          const int extType = extend ? bsdfType : 0;
+          if (aov1)
+          {
+            if (L.aovMask)
+            {
+              L.ps.aovA[p] = make_float4(bsdf.albedo.x, bsdf.albedo.y, bsdf.albedo.z, 1.f);
+              L.ps.aovN[p] = make_float4(bsdf.fr.N.x, bsdf.fr.N.y, bsdf.fr.N.z, 1.f);
+            }
+            pixelId |= kPathAov1Flag;
+          }
+          if (aov2 && (extType & kBsdfDelta) == 0) pixelId |= kPathAov2Flag;
+          T *= bw;
+          extend = extend && reduceMax(T) >= L.rd.minWeight;
+          if (depth >= L.rd.rrDepth)
+          {
+            const float contProb = rr ? fminf(luminance(T), 0.95f) : 1.f;
+            extend = extend && sobolGet1D(st, sampleDim + kDimTerminate) <= contProb;
+            T *= 1.f / contProb;
+            bsdfPdf *= contProb;
+          }
+          if (extend)
+          {
+            L.ps.rayO[p] = make_float4(ctx.p.x, ctx.p.y, ctx.p.z, ctx.eps);
+            L.ps.rayD[p] = make_float4(wi.x, wi.y, wi.z, kPosMax);
+            const bool update = (bsdfType & kBsdfContinuation) == 0;
+            L.ps.thr[p] = make_float4(T.x, T.y, T.z, update ? bsdfPdf : lastPdf);
+            ra.w = __int_as_float(update ? bsdfType : lastType);
+          }
+          info.x = pixelId;
+          L.ps.info[p] = info;
+          if (!extend && !shadow) finishPath(L, p, Lr);
+          if (shadow) shL.w = __uint_as_float((uint32_t)p | (extend ? 0u : kShadowFinish));
+          ra.x = Lr.x;
+          ra.y = Lr.y;
+          ra.z = Lr.z;
+          L.ps.rad[p] = ra;
+        }
+      }
+    }
+    const int e = warpAppend(extCount, extend);
+    if (extend) queueOut[e] = p;
+    const int s = warpAppend(shadowCount, shadow);
+    if (shadow)
+    {
+      L.ps.shO[s] = shO;
+      L.ps.shD[s] = shD;
+      L.ps.shL[s] = shL;
+    }
+  }
+}
+
+// Adds the wave's samples of each pixel, in sample order, to the accumulation planes.
+__global__ void kAccumulate(Launch L, float4* __restrict__ accum, float4* __restrict__ accA, float4* __restrict__ accN)
+{
+  const int n = L.pixelCount;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+  {
+    const int x = q % L.width, y = q / L.width;
+    const int idx = slotOfPixel(x, y, L.width);
+    float4 acc = accum[q];
+    float4 a = accA ? accA[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 nn = accN ? accN[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int s = 0; s < L.samples; ++s)
+    {
+      const int64_t p = (int64_t)s * L.pixelCount + idx;
+      const float4 o = L.ps.out[p];
+      acc.x += o.x;
+      acc.y += o.y;
+      acc.z += o.z;
+      acc.w += 1.f;
+      if (accA)
+      {
+        const float4 va = L.ps.aovA[p];
+        if (va.w != 0.f)
+        {
+          a.x += va.x; a.y += va.y; a.z += va.z; a.w += 1.f;
+        }
+        const float4 vn = L.ps.aovN[p];
+        if (vn.w != 0.f)
+        {
+          nn.x += vn.x; nn.y += vn.y; nn.z += vn.z; nn.w += 1.f;
+        }
+      }
+    }
+    accum[q] = acc;
+    if (accA)
+    {
+      accA[q] = a;
+      accN[q] = nn;
+    }
+  }
+}
+
+// sum * rcpSafe(weight) (image/accum_buffer.h:607-650).
+__global__ void kBlit(const float4* __restrict__ acc, int n, float* __restrict__ dst)
+{
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+  {
+    const float4 a = acc[q];
+    const float r = rcpSafe(a.w);
+    dst[3 * q + 0] = a.x * r;
+    dst[3 * q + 1] = a.y * r;
+    dst[3 * q + 2] = a.z * r;
+  }
+}
+
+// ---- launchers --------------------------------------------------------------------------------
+
+static int gridFor(const Context& ctx, int64_t n, int block = 256)
+{
+  const int64_t blocks = (n + block - 1) / block;
+  const int64_t cap = (int64_t)ctx.smCount * 16;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(blocks, cap));
+}
+
+cudaError_t launchSobol(Context& ctx, int64_t n, const uint32_t* si, const uint32_t* pid, const uint32_t* dims,
+                        int ndim, float* out)
+{
+  kSobol<<<gridFor(ctx, n), 256, 0, ctx.stream>>>(n, si, pid, dims, ndim, ctx.renderer.seed, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launchTrace(Context& ctx, int64_t n, const float* rays, int32_t* triOut, float* t, float* u, float* v)
+{
+  kTraceRays<<<gridFor(ctx, n, 128), 128, 0, ctx.stream>>>(ctx.scene, n, reinterpret_cast<const float4*>(rays),
+                                                            triOut, t, u, v, ctx.ps.err);
+  return cudaGetLastError();
+}
+
+cudaError_t launchOccluded(Context& ctx, int64_t n, const float* rays, int32_t* occ)
+{
+  kOccludedRays<<<gridFor(ctx, n, 128), 128, 0, ctx.stream>>>(ctx.scene, n, reinterpret_cast<const float4*>(rays),
+                                                               occ, ctx.ps.err);
+  return cudaGetLastError();
+}
+
+cudaError_t launchPrimary(Context& ctx, uint32_t sampleIndex, float* raysOut, int32_t* triOut, float* t)
+{
+  const int n = ctx.width * ctx.height;
+  kPrimary<<<gridFor(ctx, n, 128), 128, 0, ctx.stream>>>(ctx.scene, ctx.camera, ctx.width, ctx.height,
+                                                          ctx.renderer.seed, sampleIndex,
+                                                          reinterpret_cast<float4*>(raysOut), triOut, t, ctx.ps.err);
+  return cudaGetLastError();
+}
+
+cudaError_t launchBlit(Context& ctx, int aov, float* dst)
+{
+  const int n = ctx.width * ctx.height;
+  const float* src = aov == 0 ? ctx.accum : (aov == 1 ? ctx.accumA : ctx.accumN);
+  kBlit<<<gridFor(ctx, n), 256, 0, ctx.stream>>>(reinterpret_cast<const float4*>(src), n, dst);
+  return cudaGetLastError();
+}
+
+cudaError_t launchClear(Context& ctx)
+{
+  const size_t bytes = (size_t)ctx.width * ctx.height * sizeof(float4);
+  cudaError_t e = cudaMemsetAsync(ctx.accum, 0, bytes, ctx.stream);
+  if (e == cudaSuccess && ctx.accumA) e = cudaMemsetAsync(ctx.accumA, 0, bytes, ctx.stream);
+  if (e == cudaSuccess && ctx.accumN) e = cudaMemsetAsync(ctx.accumN, 0, bytes, ctx.stream);
+  return e;
+}
+
+cudaError_t renderSamples(Context& ctx, int spp, int64_t& rays)
+{
+  rays = 0;
+  const int pixelCount = ctx.width * ctx.height;
+  const int maxDepth = ctx.renderer.maxDepth;
+  int* counts = ctx.ps.counters;  // [2*d]: input count of bounce d, [2*d+1]: shadow count; work counters after
+  const int countSlots = 2 * (maxDepth + 2);
+  int* work = counts + countSlots;
+  std::vector<int> hostCounts(countSlots);
+  for (int done = 0; done < spp;)
+  {
+    const int S = std::min(ctx.waveSamples, spp - done);
+    Launch L;
+    L.sc = ctx.scene;
+    L.cam = ctx.camera;
+    L.rd = ctx.renderer;
+    L.ps = ctx.ps;
+    L.width = ctx.width;
+    L.height = ctx.height;
+    L.pixelCount = pixelCount;
+    L.firstSample = ctx.sampleIndex + (uint32_t)done;
+    L.samples = S;
+    L.aovMask = ctx.aovMask;
+    const int P = pixelCount * S;
+    cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(int) * 2 * countSlots, ctx.stream);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(counts, &P, sizeof(int), cudaMemcpyHostToDevice, ctx.stream);
+    if (e != cudaSuccess) return e;
+    kRaygen<<<gridFor(ctx, P), 256, 0, ctx.stream>>>(L);
+    const int persistent = ctx.smCount * 8;
+    int cur = 0;
+    for (int depth = 0; depth <= maxDepth; ++depth)
+    {
+      const int* q = depth == 0 ? nullptr : ctx.ps.queue[cur];
+      int* qOut = ctx.ps.queue[cur ^ 1];
+      kTrace<<<persistent, 256, 0, ctx.stream>>>(L, q, counts + 2 * depth, work + 2 * depth);
+      kShade<<<gridFor(ctx, P), 256, 0, ctx.stream>>>(L, q, counts + 2 * depth, depth, qOut, counts + 2 * (depth + 1),
+                                                       counts + 2 * depth + 1);
+      kShadow<<<persistent, 256, 0, ctx.stream>>>(L, counts + 2 * depth + 1, work + 2 * depth + 1);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+      cur ^= 1;
+      // Input, shadow and extension counts of this bounce; stop once no path is left.
+      int cnt[3];
+      e = cudaMemcpyAsync(cnt, counts + 2 * depth, 3 * sizeof(int), cudaMemcpyDeviceToHost, ctx.stream);
+      if (e != cudaSuccess) return e;
+      e = cudaStreamSynchronize(ctx.stream);
+      if (e != cudaSuccess) return e;
+      rays += (int64_t)cnt[0] + cnt[1];
+      if (cnt[2] == 0) break;
+    }
+    kAccumulate<<<gridFor(ctx, pixelCount), 256, 0, ctx.stream>>>(L, reinterpret_cast<float4*>(ctx.accum),
+                                                                   reinterpret_cast<float4*>(ctx.accumA),
+                                                                   reinterpret_cast<float4*>(ctx.accumN));
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    done += S;
+  }
+  ctx.sampleIndex += (uint32_t)spp;
+  return cudaSuccess;
+}
+
+} // namespace prt

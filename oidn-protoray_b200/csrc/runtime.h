@@ -1,0 +1,82 @@
+// Host runtime of the B200 render device: the context behind the C ABI and the kernel
+// launchers it drives. Shared by device.cu (C ABI, scene upload) and integrator.cu (kernels).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "bvh8.h"
+#include "device_scene.h"
+
+namespace prt {
+
+// Device memory block owned by the context.
+struct DevBuf
+{
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+// Path state of one wave, structure of arrays indexed by path slot.
+struct PathState
+{
+  int64_t capacity = 0;
+  float4* rayO = nullptr;   // origin, near
+  float4* rayD = nullptr;   // direction, far
+  float4* hit = nullptr;    // t, u, v, triangle id (int bits)
+  float4* thr = nullptr;    // throughput, lastBsdfPdf
+  float4* rad = nullptr;    // radiance L, lastBsdfType (int bits)
+  uint4* info = nullptr;    // pixelId | path flags, sample index, medium id, -
+  float4* shO = nullptr;    // shadow rays: origin, near
+  float4* shD = nullptr;    // direction, far
+  float4* shL = nullptr;    // unoccluded contribution, path slot | finish flag (int bits)
+  float4* out = nullptr;    // final radiance per path (w = 1 when written)
+  float4* aovA = nullptr;   // first-hit albedo per path (w = 1 when written)
+  float4* aovN = nullptr;   // first-hit normal per path
+  int* queue[2] = {nullptr, nullptr};
+  int* counters = nullptr;  // [0] extension count, [1] shadow count, [2] trace work, [3] shadow work
+  uint32_t* err = nullptr;
+};
+
+struct Context
+{
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string lastError;
+  int smCount = 0;
+  std::vector<DevBuf> sceneBufs;  // freed on re-upload
+  DevScene scene{};
+  bool hasScene = false;
+  Bvh8 bvh;                       // host copy (for counting and re-upload)
+  std::vector<int> meshTriOffsetHost;
+  DevRenderer renderer{100, 8, 1e-4f, 3.402823466e38f, 0u};
+  bool hasRenderer = false;
+  DevCamera camera{};
+  bool hasCamera = false;
+  int width = 0, height = 0, aovMask = 0;
+  float* accum = nullptr;         // sum rgb + weight per pixel (float4)
+  float* accumA = nullptr;        // first-hit albedo sums
+  float* accumN = nullptr;        // first-hit normal sums
+  uint32_t sampleIndex = 0;
+  PathState ps;
+  int waveSamples = 0;            // samples per pixel per wave
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+// Kernel launchers (integrator.cu). All are asynchronous on ctx.stream.
+cudaError_t launchSobol(Context& ctx, int64_t n, const uint32_t* si, const uint32_t* pid, const uint32_t* dims,
+                        int ndim, float* out);
+cudaError_t launchTrace(Context& ctx, int64_t n, const float* rays, int32_t* triOut, float* t, float* u,
+                        float* v);
+cudaError_t launchOccluded(Context& ctx, int64_t n, const float* rays, int32_t* occ);
+cudaError_t launchPrimary(Context& ctx, uint32_t sampleIndex, float* raysOut, int32_t* triOut, float* t);
+// Renders samples [ctx.sampleIndex, ctx.sampleIndex + spp) and accumulates them; returns the
+// number of closest + shadow rays traced.
+cudaError_t renderSamples(Context& ctx, int spp, int64_t& rays);
+cudaError_t launchBlit(Context& ctx, int aov, float* dst);
+cudaError_t launchClear(Context& ctx);
+
+} // namespace prt

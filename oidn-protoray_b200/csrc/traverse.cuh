@@ -1,0 +1,199 @@
+// BVH8 ray traversal on the device: closest hit and any hit.
+//
+// Replaces the reference's Embree queries (accel/embree_intersector_stream.h:66-131, called
+// from render/path_renderer_stream.h:280 and :953). The node layout is bvh8.h's compressed
+// 80-byte wide node; the walk keeps "node groups" (a base index plus the still-unvisited hit
+// children of one node) on a short per-thread stack, the scheme of Ylitie et al. 2017.
+//
+// The ray/triangle test is the fixed-operation Moller-Trumbore form shared with the host
+// oracle (crossFx/dotFx in prt_math.cuh): hit iff det != 0, u >= 0, v >= 0, u + v <= 1 and
+// near <= t <= far. The closest hit keeps the smallest t and, on equal t, the smallest
+// global triangle index, so the result does not depend on the tree or the visiting order.
+// Box tests are conservative: quantised boxes are rounded outward and the slab interval is
+// compared with a relative slack of 2e-6, so that a triangle the test accepts is never culled.
+#pragma once
+
+#include "prt_math.cuh"
+
+namespace prt {
+
+constexpr int kTraceStack = 48;           // node-group stack entries per ray
+constexpr int kTraceMaxIter = 1 << 20;    // loop cap: a corrupt tree ends the ray, not the kernel
+constexpr uint32_t kErrStackOverflow = 1u;
+constexpr uint32_t kErrIterCap = 2u;
+
+struct TraceHit
+{
+  int triId;   // global triangle index, -1 on a miss
+  float t, u, v;
+};
+
+PRT_D float expToScale(uint32_t e) { return __uint_as_float(e << 23); }
+
+PRT_D bool intersectTriFx(const float4* __restrict__ tris, uint32_t idx, f3 o, f3 d, float tnear, float tfar,
+                          float& t, float& u, float& v, int& triId)
+{
+  const float4 a = __ldg(tris + 3 * idx + 0);
+  const float4 b = __ldg(tris + 3 * idx + 1);
+  const float4 c = __ldg(tris + 3 * idx + 2);
+  const f3 v0 = mk(a.x, a.y, a.z);
+  const f3 e1 = mk(b.x, b.y, b.z);
+  const f3 e2 = mk(c.x, c.y, c.z);
+  const f3 p = crossFx(d, e2);
+  const float det = dotFx(e1, p);
+  if (!(det != 0.f)) return false;
+  const f3 s = subFx(o, v0);
+  const f3 q = crossFx(s, e1);
+  const float inv = __frcp_rn(det);
+  const float uu = __fmul_rn(dotFx(s, p), inv);
+  const float vv = __fmul_rn(dotFx(d, q), inv);
+  const float tt = __fmul_rn(dotFx(e2, q), inv);
+  if (!(uu >= 0.f) || !(vv >= 0.f) || !(__fadd_rn(uu, vv) <= 1.f)) return false;
+  if (!(tt >= tnear) || !(tt <= tfar)) return false;
+  t = tt;
+  u = uu;
+  v = vv;
+  triId = __float_as_int(a.w);
+  return true;
+}
+
+struct RayPre
+{
+  f3 o, invd;
+  uint32_t oct;   // bit k set when direction component k is negative
+};
+
+PRT_D RayPre rayPre(f3 o, f3 d)
+{
+  RayPre r;
+  r.o = o;
+  const float tiny = 8.271806e-25f;  // 2^-80: keeps 1/d finite
+  const float dx = fabsf(d.x) < tiny ? copysignf(tiny, d.x) : d.x;
+  const float dy = fabsf(d.y) < tiny ? copysignf(tiny, d.y) : d.y;
+  const float dz = fabsf(d.z) < tiny ? copysignf(tiny, d.z) : d.z;
+  r.invd = mk(__frcp_rn(dx), __frcp_rn(dy), __frcp_rn(dz));
+  r.oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+  return r;
+}
+
+PRT_D uint32_t byteOf(uint2 w, int i)
+{
+  return (i < 4 ? (w.x >> (8 * i)) : (w.y >> (8 * (i - 4)))) & 0xffu;
+}
+
+// Intersects the 8 children of one node; returns the node group of hit inner children
+// (bits 24-31: hit flags at position slot ^ oct; bits 0-7: imask) and the triangle bits.
+PRT_D void intersectNode(const uint4* __restrict__ nodes, uint32_t nodeIdx, const RayPre& r, float tnear,
+                         float tfar, uint2& ngroup, uint2& tgroup)
+{
+  const uint4 w0 = __ldg(nodes + 5 * nodeIdx + 0);
+  const uint4 w1 = __ldg(nodes + 5 * nodeIdx + 1);
+  const uint4 w2 = __ldg(nodes + 5 * nodeIdx + 2);
+  const uint4 w3 = __ldg(nodes + 5 * nodeIdx + 3);
+  const uint4 w4 = __ldg(nodes + 5 * nodeIdx + 4);
+  const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
+  const uint32_t ex = w0.w & 0xffu, ey = (w0.w >> 8) & 0xffu, ez = (w0.w >> 16) & 0xffu;
+  const uint32_t imask = (w0.w >> 24) & 0xffu;
+  const uint32_t childBase = w1.x, triBase = w1.y;
+  const uint2 meta = make_uint2(w1.z, w1.w);
+  uint2 qlox = make_uint2(w2.x, w2.y), qloy = make_uint2(w2.z, w2.w);
+  uint2 qloz = make_uint2(w3.x, w3.y), qhix = make_uint2(w3.z, w3.w);
+  uint2 qhiy = make_uint2(w4.x, w4.y), qhiz = make_uint2(w4.z, w4.w);
+  // Near plane = lo for positive directions, hi for negative ones.
+  if (r.oct & 1u) { const uint2 t = qlox; qlox = qhix; qhix = t; }
+  if (r.oct & 2u) { const uint2 t = qloy; qloy = qhiy; qhiy = t; }
+  if (r.oct & 4u) { const uint2 t = qloz; qloz = qhiz; qhiz = t; }
+  const float ax = __fmul_rn(px - r.o.x, r.invd.x);
+  const float ay = __fmul_rn(py - r.o.y, r.invd.y);
+  const float az = __fmul_rn(pz - r.o.z, r.invd.z);
+  const float bx = expToScale(ex) * r.invd.x;
+  const float by = expToScale(ey) * r.invd.y;
+  const float bz = expToScale(ez) * r.invd.z;
+  const float tmaxLimit = tfar * 1.000002f;
+  uint32_t inner = 0u, tri = 0u;
+#pragma unroll
+  for (int s = 0; s < 8; ++s)
+  {
+    const uint32_t m = byteOf(meta, s);
+    const bool isInner = (imask >> s) & 1u;
+    const float x0 = fmaf((float)byteOf(qlox, s), bx, ax), x1 = fmaf((float)byteOf(qhix, s), bx, ax);
+    const float y0 = fmaf((float)byteOf(qloy, s), by, ay), y1 = fmaf((float)byteOf(qhiy, s), by, ay);
+    const float z0 = fmaf((float)byteOf(qloz, s), bz, az), z1 = fmaf((float)byteOf(qhiz, s), bz, az);
+    const float tmin = fmaxf(fmaxf(x0, y0), fmaxf(z0, tnear));
+    const float tmax = fminf(fminf(x1, y1), z1);
+    const bool hit = (isInner || m != 0u) && tmin <= fminf(tmax * 1.000002f, tmaxLimit);
+    if (hit)
+    {
+      if (isInner) inner |= 1u << (s ^ r.oct);
+      else tri |= ((1u << (m >> 5)) - 1u) << (m & 31u);
+    }
+  }
+  ngroup = make_uint2(childBase, (inner << 24) | imask);
+  tgroup = make_uint2(triBase, tri);
+}
+
+template <bool AnyHit>
+PRT_D TraceHit traverse(const uint4* __restrict__ nodes, const float4* __restrict__ tris, f3 o, f3 d,
+                        float tnear, float tfar, uint32_t* errFlag)
+{
+  TraceHit h;
+  h.triId = -1;
+  h.t = tfar;
+  h.u = h.v = 0.f;
+  const RayPre r = rayPre(o, d);
+  uint2 stack[kTraceStack];
+  int sp = 0;
+  // The root as a one-child group: slot 0 is inner, at bit 24 + (0 ^ oct).
+  uint2 ngroup = make_uint2(0u, (1u << (24 + r.oct)) | 1u);
+  uint2 tgroup = make_uint2(0u, 0u);
+  for (int iter = 0; iter < kTraceMaxIter; ++iter)
+  {
+    while (tgroup.y != 0u)
+    {
+      const int bit = __ffs(tgroup.y) - 1;
+      tgroup.y &= tgroup.y - 1u;
+      float t, u, v;
+      int id;
+      if (intersectTriFx(tris, tgroup.x + bit, o, d, tnear, h.t, t, u, v, id))
+      {
+        if (AnyHit)
+        {
+          h.triId = id;
+          h.t = t;
+          return h;
+        }
+        if (t < h.t || h.triId < 0 || id < h.triId)
+        {
+          h.triId = id;
+          h.t = t;
+          h.u = u;
+          h.v = v;
+        }
+      }
+    }
+    if (ngroup.y <= 0x00ffffffu)
+    {
+      if (sp == 0) return h;
+      ngroup = stack[--sp];
+    }
+    const int b = 31 - __clz(ngroup.y);
+    ngroup.y &= ~(1u << b);
+    const uint32_t slot = (uint32_t)(b - 24) ^ r.oct;
+    const uint32_t imask = ngroup.y & 0xffu;
+    const uint32_t nodeIdx = ngroup.x + __popc(imask & ((1u << slot) - 1u));
+    if (ngroup.y > 0x00ffffffu)
+    {
+      if (sp == kTraceStack)
+      {
+        atomicOr(errFlag, kErrStackOverflow);
+        return h;
+      }
+      stack[sp++] = ngroup;
+    }
+    intersectNode(nodes, nodeIdx, r, tnear, h.t, ngroup, tgroup);
+  }
+  atomicOr(errFlag, kErrIterCap);
+  return h;
+}
+
+} // namespace prt

@@ -1,0 +1,206 @@
+"""Python handle on libprt_cuda.so, the B200 render device, through its C ABI.
+
+DeviceCuda mirrors the reference's Device API (render/device.h:56-114): initScene,
+initRenderer, initSampler, initCamera, initFrame, clearFrame, render, blitFrame, plus the
+ray queries. Errors come back as the exception types the reference throws
+(std::invalid_argument -> ValueError, std::logic_error -> LogicError, others -> RuntimeError).
+
+The library is built in place (make -C oidn-protoray_b200); there is no CPU fallback:
+loading fails loudly when the library or a CUDA device is missing.
+"""
+import ctypes as C
+import os
+import pathlib
+
+import numpy as np
+
+import prt_types as T
+
+LIB_PATH = pathlib.Path(__file__).resolve().parent / "libprt_cuda.so"
+
+_lib = None
+
+
+class LogicError(RuntimeError):
+    """Counterpart of std::logic_error."""
+
+
+class DeviceAbort(RuntimeError):
+    """A device loop hit its iteration cap or a bounds check."""
+
+
+def load_library():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise FileNotFoundError(f"{LIB_PATH} is not built (make -C oidn-protoray_b200)")
+    # libstdc++ must be global before a C++ library loads (see oracle/ref.py).
+    C.CDLL("libstdc++.so.6", mode=os.RTLD_GLOBAL)
+    lib = C.CDLL(str(LIB_PATH))
+    P = C.POINTER
+    vp = C.c_void_p
+    lib.prt_cuda_create.argtypes = [C.c_int, P(vp)]
+    lib.prt_cuda_destroy.argtypes = [vp]
+    lib.prt_cuda_last_error.argtypes = [vp]
+    lib.prt_cuda_last_error.restype = C.c_char_p
+    lib.prt_cuda_material_defaults.argtypes = [P(T.Material)]
+    lib.prt_cuda_material_defaults.restype = None
+    lib.prt_cuda_scene_upload.argtypes = [vp, P(T.SceneDesc)]
+    lib.prt_cuda_renderer.argtypes = [vp, P(T.RendererDesc)]
+    lib.prt_cuda_init_sampler.argtypes = [vp, C.c_uint32]
+    lib.prt_cuda_camera.argtypes = [vp, P(T.CameraDesc)]
+    lib.prt_cuda_frame.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32]
+    lib.prt_cuda_clear.argtypes = [vp]
+    lib.prt_cuda_render.argtypes = [vp, C.c_int32, P(T.RenderStats)]
+    lib.prt_cuda_blit.argtypes = [vp, C.c_int32, P(C.c_float)]
+    lib.prt_cuda_sobol.argtypes = [vp, C.c_int64, P(C.c_uint32), P(C.c_uint32), P(C.c_uint32), C.c_int32,
+                                   P(C.c_float)]
+    lib.prt_cuda_trace.argtypes = [vp, C.c_int64, P(C.c_float), P(C.c_int32), P(C.c_int32), P(C.c_float),
+                                   P(C.c_float), P(C.c_float)]
+    lib.prt_cuda_occluded.argtypes = [vp, C.c_int64, P(C.c_float), P(C.c_int32)]
+    lib.prt_cuda_query_primary.argtypes = [vp, C.c_uint32, P(C.c_float), P(C.c_int32), P(C.c_int32), P(C.c_float)]
+    lib.prt_bvh8_count.argtypes = [P(C.c_float), C.c_int64, C.c_int64, P(C.c_float), P(C.c_int32), P(C.c_float),
+                                   P(C.c_int64), P(C.c_int64), P(C.c_int64)]
+    _lib = lib
+    return lib
+
+
+def bvh8_count(tri_verts, rays):
+    """Host-only BVH8 build + counting traversal (no GPU): (tri ids, t, nodes/ray, tris/ray, node count)."""
+    lib = load_library()
+    tv = np.ascontiguousarray(tri_verts, np.float32).reshape(-1, 9)
+    r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    tri = np.zeros(r.shape[0], np.int32)
+    t = np.zeros(r.shape[0], np.float32)
+    nv, tt, nc = C.c_int64(0), C.c_int64(0), C.c_int64(0)
+    rc = lib.prt_bvh8_count(T.fptr(tv), tv.shape[0], r.shape[0], T.fptr(r), T.iptr(tri), T.fptr(t), C.byref(nv),
+                            C.byref(tt), C.byref(nc))
+    if rc != T.PRT_OK:
+        raise ValueError(f"prt_bvh8_count failed ({rc})")
+    n = max(r.shape[0], 1)
+    return tri, t, nv.value / n, tt.value / n, nc.value
+
+
+class DeviceCuda:
+    """The CUDA render device; one per host thread."""
+
+    def __init__(self, device_ordinal=0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        rc = self.lib.prt_cuda_create(device_ordinal, C.byref(h))
+        if rc != T.PRT_OK:
+            raise RuntimeError(f"prt_cuda_create failed ({rc}): no usable CUDA device")
+        self.h = h
+        self.scene = None
+        self.width = self.height = 0
+        self._keep = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.prt_cuda_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc == T.PRT_OK:
+            return
+        msg = self.lib.prt_cuda_last_error(self.h).decode()
+        if rc == T.PRT_ERR_INVALID_ARG:
+            raise ValueError(msg)
+        if rc == T.PRT_ERR_LOGIC:
+            raise LogicError(msg)
+        if rc == T.PRT_ERR_DEVICE_ABORT:
+            raise DeviceAbort(msg)
+        if rc == T.PRT_ERR_OUT_OF_MEMORY:
+            raise MemoryError(msg)
+        raise RuntimeError(f"prt_cuda error {rc}: {msg}")
+
+    # -- Device API --------------------------------------------------------------------------
+    def init_scene(self, scene):
+        desc = scene.desc()
+        self._keep = desc
+        self._check(self.lib.prt_cuda_scene_upload(self.h, C.byref(desc)))
+        self.scene = scene
+
+    def init_renderer(self, max_depth=100, rr_depth=8, min_weight=1e-4, max_radiance=3.4028234663852886e38):
+        r = T.RendererDesc(max_depth, rr_depth, min_weight, max_radiance)
+        self._check(self.lib.prt_cuda_renderer(self.h, C.byref(r)))
+
+    def init_sampler(self, seed):
+        self._check(self.lib.prt_cuda_init_sampler(self.h, seed))
+
+    def init_frame(self, width, height, aov_mask=0):
+        self._check(self.lib.prt_cuda_frame(self.h, width, height, aov_mask))
+        self.width, self.height = width, height
+
+    def init_camera(self, camera):
+        self._check(self.lib.prt_cuda_camera(self.h, C.byref(camera)))
+
+    def clear_frame(self):
+        self._check(self.lib.prt_cuda_clear(self.h))
+
+    def render(self, spp=1):
+        st = T.RenderStats()
+        self._check(self.lib.prt_cuda_render(self.h, spp, C.byref(st)))
+        return dict(mray=st.mray, rays=st.rays, spp=st.spp, render_ms=st.render_ms)
+
+    def blit_frame(self, aov=T.PRT_BLIT_HDR, out=None):
+        """Returns (height, width, 3) float32; `out` may be a CUDA torch tensor (zero copy)."""
+        if out is not None and hasattr(out, "data_ptr"):
+            self._check(self.lib.prt_cuda_blit(self.h, aov, C.cast(C.c_void_p(out.data_ptr()), C.POINTER(C.c_float))))
+            return out
+        img = np.zeros((self.height, self.width, 3), np.float32)
+        self._check(self.lib.prt_cuda_blit(self.h, aov, T.fptr(img)))
+        return img
+
+    def setup(self, scene, seed=0, aov_mask=0):
+        """initScene + initFrame + initCamera + initRenderer + initSampler for a Scene."""
+        self.init_scene(scene)
+        self.init_frame(scene.width, scene.height, aov_mask)
+        self.init_camera(scene.camera)
+        self.init_renderer(scene.max_depth, scene.rr_depth)
+        self.init_sampler(seed)
+
+    # -- queries --------------------------------------------------------------------------------
+    def sobol(self, sample_index, pixel_id, dim_set, dims):
+        n = len(sample_index)
+        si = np.ascontiguousarray(sample_index, np.uint32)
+        pi = np.ascontiguousarray(pixel_id, np.uint32)
+        ds = np.ascontiguousarray(dim_set, np.uint32)
+        out = np.zeros(n * dims, np.float32)
+        self._check(self.lib.prt_cuda_sobol(self.h, n, T.uptr(si), T.uptr(pi), T.uptr(ds), dims, T.fptr(out)))
+        return out.reshape(n, dims)
+
+    def trace(self, rays):
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        g = np.zeros(n, np.int32)
+        p = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float32)
+        u = np.zeros(n, np.float32)
+        v = np.zeros(n, np.float32)
+        self._check(self.lib.prt_cuda_trace(self.h, n, T.fptr(rays), T.iptr(g), T.iptr(p), T.fptr(t), T.fptr(u),
+                                            T.fptr(v)))
+        return g, p, t, u, v
+
+    def occluded(self, rays):
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        occ = np.zeros(rays.shape[0], np.int32)
+        self._check(self.lib.prt_cuda_occluded(self.h, rays.shape[0], T.fptr(rays), T.iptr(occ)))
+        return occ
+
+    def query_primary(self, sample_index):
+        n = self.width * self.height
+        rays = np.zeros((n, 8), np.float32)
+        g = np.zeros(n, np.int32)
+        p = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float32)
+        self._check(self.lib.prt_cuda_query_primary(self.h, sample_index, T.fptr(rays), T.iptr(g), T.iptr(p),
+                                                    T.fptr(t)))
+        return rays, g, p, t

@@ -1,0 +1,191 @@
+"""Seeded synthetic scenes for the path-tracing workloads.
+
+The reference publishes no scenes for its path tracer, so the workloads are generated here,
+deterministically from a seed, with the shapes and value distributions of each workload:
+
+* cornell():  the small plain-render scene: a Cornell-style room (5 axis-aligned quads,
+  10 triangles) with a ceiling area light (2 triangles, emission 15) and 32 icospheres of
+  subdivision 2 (320 triangles each), about 10.3k triangles, 256x256, 16 spp, depth 5.
+* terrain():  the large plain-render scene: a 1024x1024 fBm heightfield (8 octaves,
+  lacunarity 2, gain 0.5) plus 400 icospheres of subdivision 3 (1280 triangles each), about
+  2.6M triangles, four material kinds and a sun-sky light, 1920x1080, 64 spp, depth 8,
+  Russian roulette from depth 3.
+
+A Scene keeps every numpy array alive for as long as its ctypes descriptor is in use.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+
+import prt_types as T
+
+
+class Scene:
+    """Triangle meshes + Standard materials + environment lights, ready for the C ABI."""
+
+    def __init__(self):
+        self.meshes = []      # dicts: positions, normals, texcoords, indices, material
+        self.materials = []   # prt_types.Material
+        self.textures = []    # (h, w, 3) float32, row 0 at the top
+        self.env = T.EnvDesc()
+        self.env_image = None
+        self.sunsky = None    # (dir xyz, turbidity, albedo) for the reference's SunSkyLight
+        self.camera = None
+        self.width = 0
+        self.height = 0
+        self.spp = 1
+        self.max_depth = 5
+        self.rr_depth = 8
+        self._keep = []
+
+    # -- construction ---------------------------------------------------------------------
+    def add_material(self, m):
+        self.materials.append(m)
+        return len(self.materials) - 1
+
+    def add_mesh(self, positions, indices, material, normals=None, texcoords=None):
+        self.meshes.append(dict(
+            positions=np.ascontiguousarray(positions, np.float32).reshape(-1, 3),
+            indices=np.ascontiguousarray(indices, np.int32).reshape(-1, 3),
+            normals=None if normals is None else np.ascontiguousarray(normals, np.float32).reshape(-1, 3),
+            texcoords=None if texcoords is None else np.ascontiguousarray(texcoords, np.float32).reshape(-1, 2),
+            material=int(material)))
+
+    def add_texture(self, rgb):
+        self.textures.append(np.ascontiguousarray(rgb, np.float32))
+        return len(self.textures) - 1
+
+    def set_env_image(self, rgb, lut_size=0):
+        self.env_image = np.ascontiguousarray(rgb, np.float32)
+        self.env.image_width = self.env_image.shape[1]
+        self.env.image_height = self.env_image.shape[0]
+        self.env.image_lut_size = lut_size
+
+    @property
+    def tri_count(self):
+        return sum(m["indices"].shape[0] for m in self.meshes)
+
+    # -- C ABI ----------------------------------------------------------------------------
+    def desc(self):
+        meshes = (T.Mesh * len(self.meshes))()
+        for i, m in enumerate(self.meshes):
+            meshes[i].positions = T.fptr(m["positions"])
+            meshes[i].normals = T.fptr(m["normals"])
+            meshes[i].texcoords = T.fptr(m["texcoords"])
+            meshes[i].indices = T.iptr(m["indices"])
+            meshes[i].vertex_count = m["positions"].shape[0]
+            meshes[i].tri_count = m["indices"].shape[0]
+            meshes[i].material = m["material"]
+        mats = (T.Material * len(self.materials))(*self.materials)
+        texs = (T.Texture * max(len(self.textures), 1))()
+        for i, t in enumerate(self.textures):
+            texs[i].rgb = T.fptr(t)
+            texs[i].height, texs[i].width = t.shape[0], t.shape[1]
+        d = T.SceneDesc()
+        d.meshes = meshes
+        d.mesh_count = len(self.meshes)
+        d.materials = mats
+        d.material_count = len(self.materials)
+        d.textures = texs
+        d.texture_count = len(self.textures)
+        d.env = self.env
+        d.env.image_rgb = T.fptr(self.env_image)
+        self._keep = [meshes, mats, texs]
+        return d
+
+    def renderer_desc(self, max_radiance=3.4028234663852886e38, min_weight=1e-4):
+        r = T.RendererDesc()
+        r.max_depth = self.max_depth
+        r.rr_depth = self.rr_depth
+        r.min_weight = min_weight
+        r.max_radiance = max_radiance
+        return r
+
+
+def look_at(position, target, up=(0.0, 1.0, 0.0), fov_deg=40.0, near_clip=1e-3):
+    """Pinhole camera descriptor; basis (U right, V up, N back) as camera/pinhole_camera.h expects."""
+    p = np.asarray(position, np.float64)
+    f = np.asarray(target, np.float64) - p
+    f /= np.linalg.norm(f)
+    n = -f
+    u = np.cross(np.asarray(up, np.float64), n)
+    u /= np.linalg.norm(u)
+    v = np.cross(n, u)
+    c = T.CameraDesc()
+    c.position[:] = tuple(p.astype(np.float32))
+    c.basis_u[:] = tuple(u.astype(np.float32))
+    c.basis_v[:] = tuple(v.astype(np.float32))
+    c.basis_n[:] = tuple(n.astype(np.float32))
+    c.fov = float(np.float32(math.radians(fov_deg)))
+    c.near_clip = near_clip
+    return c
+
+
+def icosphere(subdiv):
+    """Unit icosphere: 20 * 4**subdiv triangles (midpoint subdivision, vertices projected)."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0),
+             (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+             (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11),
+             (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6), (7, 1, 8),
+             (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9),
+             (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    verts = [np.array(v, np.float64) / np.linalg.norm(v) for v in verts]
+    for _ in range(subdiv):
+        cache = {}
+        new_faces = []
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            new_faces += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = new_faces
+    return np.array(verts, np.float64), np.array(faces, np.int32)
+
+
+def _quad(p0, p1, p2, p3):
+    """Two triangles (p0,p1,p2), (p0,p2,p3); normal = cross(p1-p0, p2-p0)."""
+    return np.array([p0, p1, p2, p3], np.float32), np.array([[0, 1, 2], [0, 2, 3]], np.int32)
+
+
+def cornell(seed=0, width=256, height=256, spp=16, max_depth=5, n_spheres=32, sphere_subdiv=2):
+    """The small plain-render scene (about 10.3k triangles)."""
+    rng = np.random.default_rng(seed)
+    s = Scene()
+    white = s.add_material(T.material(base_color=(0.8, 0.8, 0.8), specular_weight=0.0))
+    red = s.add_material(T.material(base_color=(0.6, 0.0, 0.0), specular_weight=0.0))
+    green = s.add_material(T.material(base_color=(0.0, 0.6, 0.0), specular_weight=0.0))
+    light = s.add_material(T.material(emission_luminance=15.0, emission_color=(1.0, 1.0, 1.0),
+                                      specular_weight=0.0))
+    # Room [-1,1] x [0,2] x [-1,1], open towards +z. Quads face into the room.
+    for quad, mat in [
+        (_quad((-1, 0, 1), (1, 0, 1), (1, 0, -1), (-1, 0, -1)), white),      # floor, normal +y
+        (_quad((-1, 2, -1), (1, 2, -1), (1, 2, 1), (-1, 2, 1)), white),      # ceiling, normal -y
+        (_quad((-1, 0, -1), (1, 0, -1), (1, 2, -1), (-1, 2, -1)), white),    # back wall, normal +z
+        (_quad((-1, 0, 1), (-1, 0, -1), (-1, 2, -1), (-1, 2, 1)), red),      # left wall, normal +x
+        (_quad((1, 0, -1), (1, 0, 1), (1, 2, 1), (1, 2, -1)), green),        # right wall, normal -x
+    ]:
+        s.add_mesh(quad[0], quad[1], mat)
+    # Ceiling light just below the ceiling, facing down (emits where dot(dir, normal) < 0).
+    y = 1.99
+    lp, li = _quad((-0.25, y, -0.25), (0.25, y, -0.25), (0.25, y, 0.25), (-0.25, y, 0.25))
+    s.add_mesh(lp, li, light)
+    sv, sf = icosphere(sphere_subdiv)
+    for _ in range(n_spheres):
+        r = rng.uniform(0.05, 0.15)
+        c = np.array([rng.uniform(-1 + r, 1 - r), rng.uniform(r, 2 - r), rng.uniform(-1 + r, 1 - r)])
+        albedo = rng.uniform(0.1, 0.9, 3)
+        m = s.add_material(T.material(base_color=albedo, specular_weight=0.0))
+        s.add_mesh(sv * r + c, sf, m, normals=sv)
+    s.camera = look_at((0.0, 1.0, 3.4), (0.0, 1.0, 0.0), fov_deg=40.0)
+    s.width, s.height, s.spp, s.max_depth, s.rr_depth = width, height, spp, max_depth, 8
+    return s

@@ -1,0 +1,181 @@
+"""ctypes mirror of the structs declared in include/prt_cuda.h.
+
+These are the C-ABI scene/camera/renderer descriptors of the B200 render device. They
+flatten what the reference's Scene::loadScene builds from an rkscene file
+(render/scene.cpp:174-330) and the Props keys of the Device API (render/device.h:56-114).
+"""
+import ctypes as C
+
+import numpy as np
+
+PRT_OK = 0
+PRT_ERR_INVALID_ARG = -1
+PRT_ERR_LOGIC = -2
+PRT_ERR_OUT_OF_MEMORY = -3
+PRT_ERR_CUDA = -4
+PRT_ERR_DEVICE_ABORT = -5
+PRT_ERR_STATE = -6
+
+PRT_AOV_ALBEDO1 = 1 << 0
+PRT_AOV_NORMAL1 = 1 << 1
+
+PRT_BLIT_HDR = 0
+PRT_BLIT_ALBEDO1 = 1
+PRT_BLIT_NORMAL1 = 2
+
+F3 = C.c_float * 3
+
+
+class Mesh(C.Structure):
+    _fields_ = [
+        ("positions", C.POINTER(C.c_float)),
+        ("normals", C.POINTER(C.c_float)),
+        ("texcoords", C.POINTER(C.c_float)),
+        ("indices", C.POINTER(C.c_int32)),
+        ("vertex_count", C.c_int32),
+        ("tri_count", C.c_int32),
+        ("material", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class Material(C.Structure):
+    """Standard material parameters (material/standard.cpp:21-76)."""
+    _fields_ = [
+        ("base_weight", C.c_float),
+        ("base_color", F3),
+        ("metalness", C.c_float),
+        ("diffuse_roughness", C.c_float),
+        ("specular_weight", C.c_float),
+        ("specular_color", F3),
+        ("specular_roughness", C.c_float),
+        ("specular_ior", C.c_float),
+        ("transmission_weight", C.c_float),
+        ("transmission_color", F3),
+        ("transmission_depth", C.c_float),
+        ("subsurface_weight", C.c_float),
+        ("subsurface_color", F3),
+        ("subsurface_anisotropy", C.c_float),
+        ("coat_weight", C.c_float),
+        ("coat_color", F3),
+        ("coat_roughness", C.c_float),
+        ("coat_ior", C.c_float),
+        ("sheen_weight", C.c_float),
+        ("sheen_color", F3),
+        ("sheen_roughness", C.c_float),
+        ("emission_luminance", C.c_float),
+        ("emission_color", F3),
+        ("opacity", C.c_float),
+        ("thin_walled", C.c_int32),
+        ("base_color_texture", C.c_int32),
+        ("reserved", C.c_int32 * 2),
+    ]
+
+
+def material(**kw):
+    """A Material with the rkscene defaults (rkscene/rkscene.h:161-207), overridden by kw."""
+    m = Material()
+    m.base_weight = 1.0
+    m.base_color[:] = (0.8, 0.8, 0.8)
+    m.metalness = 0.0
+    m.diffuse_roughness = 0.0
+    m.specular_weight = 1.0
+    m.specular_color[:] = (1.0, 1.0, 1.0)
+    m.specular_roughness = 0.3
+    m.specular_ior = 1.5
+    m.transmission_weight = 0.0
+    m.transmission_color[:] = (1.0, 1.0, 1.0)
+    m.transmission_depth = 1.0
+    m.subsurface_weight = 0.0
+    m.subsurface_color[:] = (0.8, 0.8, 0.8)
+    m.subsurface_anisotropy = 0.0
+    m.coat_weight = 0.0
+    m.coat_color[:] = (1.0, 1.0, 1.0)
+    m.coat_roughness = 0.0
+    m.coat_ior = 1.6
+    m.sheen_weight = 0.0
+    m.sheen_color[:] = (1.0, 1.0, 1.0)
+    m.sheen_roughness = 0.3
+    m.emission_luminance = 0.0
+    m.emission_color[:] = (1.0, 1.0, 1.0)
+    m.opacity = 1.0
+    m.thin_walled = 0
+    m.base_color_texture = -1
+    for k, v in kw.items():
+        if isinstance(v, (tuple, list, np.ndarray)):
+            getattr(m, k)[:] = tuple(float(x) for x in v)
+        else:
+            setattr(m, k, v)
+    return m
+
+
+class Texture(C.Structure):
+    _fields_ = [("rgb", C.POINTER(C.c_float)), ("width", C.c_int32), ("height", C.c_int32)]
+
+
+class EnvDesc(C.Structure):
+    _fields_ = [
+        ("distant_color", F3),
+        ("distant_dir", F3),
+        ("distant_angle", C.c_float),
+        ("ambient_color", F3),
+        ("image_rgb", C.POINTER(C.c_float)),
+        ("image_width", C.c_int32),
+        ("image_height", C.c_int32),
+        ("image_lut_size", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("meshes", C.POINTER(Mesh)),
+        ("mesh_count", C.c_int32),
+        ("material_count", C.c_int32),
+        ("materials", C.POINTER(Material)),
+        ("textures", C.POINTER(Texture)),
+        ("texture_count", C.c_int32),
+        ("reserved", C.c_int32),
+        ("env", EnvDesc),
+    ]
+
+
+class CameraDesc(C.Structure):
+    _fields_ = [
+        ("position", F3),
+        ("basis_u", F3),
+        ("basis_v", F3),
+        ("basis_n", F3),
+        ("fov", C.c_float),
+        ("near_clip", C.c_float),
+    ]
+
+
+class RendererDesc(C.Structure):
+    _fields_ = [
+        ("max_depth", C.c_int32),
+        ("rr_depth", C.c_int32),
+        ("min_weight", C.c_float),
+        ("max_radiance", C.c_float),
+    ]
+
+
+class RenderStats(C.Structure):
+    _fields_ = [
+        ("mray", C.c_double),
+        ("rays", C.c_int64),
+        ("spp", C.c_int64),
+        ("render_ms", C.c_double),
+    ]
+
+
+def fptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None
+
+
+def iptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int32)) if a is not None else None
+
+
+def uptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_uint32)) if a is not None else None

@@ -1,0 +1,103 @@
+"""Generates the golden fixtures in tests/golden/ from the oracle.
+
+The reference has no tests and no golden data (its repository ships none), so the fixtures
+are produced by the reference's own code compiled here (oracle/_ref/libprt_ref.so, built
+by `make -C oracle` from the reference sources): its SIMD Sobol-Burley sampler, its
+PinholeCamera ray generation, its pathStream renderer, with the oracle BVH in place of
+Embree for the hit queries. Run from the repository root:
+
+    python tests/golden/make_golden.py
+
+Fixtures (small, seeded, committed):
+  sobol.npz        Sobol-Burley 1D/2D/3D draws: (seed, sampleIndex, pixelId, dimSet) grids
+  cornell_rays.npz primary rays of the small scene at 64x64 (sample indices 0 and 1) with their
+                   closest hits, plus random interior rays with closest hits and occlusion
+  cornell_img.npz  small-scene renders at 128x128: 16 spp with seeds 0 and 1, 1024 spp with
+                   seeds 0 and 1
+"""
+import pathlib
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT / "oidn-protoray_b200"))
+sys.path.insert(0, str(ROOT / "oracle"))
+import prt_scenes  # noqa: E402
+import ref  # noqa: E402
+
+OUT = pathlib.Path(__file__).resolve().parent
+
+
+def make_sobol():
+    rng = np.random.default_rng(12345)
+    out = {}
+    n = 1024
+    si = rng.integers(0, 4096, n).astype(np.uint32)
+    x = rng.integers(0, 4096, n)
+    y = rng.integers(0, 4096, n)
+    pid = (x | (y << 16)).astype(np.uint32)
+    ds = rng.integers(0, 80, n).astype(np.uint32)
+    out.update(sample_index=si, pixel_id=pid, dim_set=ds)
+    for seed in (0, 1, 0xDEADBEEF):
+        for dims in (1, 2, 3):
+            simd, scalar = ref.sobol(seed, si, pid, ds, dims)
+            out[f"s{seed}_d{dims}_simd"] = simd
+            out[f"s{seed}_d{dims}_scalar"] = scalar
+    np.savez_compressed(OUT / "sobol.npz", **out)
+
+
+def small_scene(width, height, spp):
+    s = prt_scenes.cornell(seed=0)
+    s.width, s.height, s.spp = width, height, spp
+    return s
+
+
+def make_rays():
+    s = small_scene(64, 64, 1)
+    dev = ref.RefDevice(s, seed=0)
+    out = {}
+    for si in range(2):
+        rays, g, p, t = dev.query_primary(si)
+        out[f"primary{si}_rays"] = rays
+        out[f"primary{si}_geom"] = g
+        out[f"primary{si}_prim"] = p
+        out[f"primary{si}_t"] = t
+    rng = np.random.default_rng(7)
+    n = 4096
+    org = np.stack([rng.uniform(-0.95, 0.95, n), rng.uniform(0.05, 1.95, n), rng.uniform(-0.95, 0.95, n)], 1)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    far = np.where(rng.uniform(size=n) < 0.5, 3.4028234663852886e38, rng.uniform(0.05, 2.0, n))
+    rays = np.concatenate([org, np.full((n, 1), 1e-4), d, far[:, None]], 1).astype(np.float32)
+    g, p, t, u, v = dev.trace(rays)
+    occ = dev.occluded(rays)
+    out.update(random_rays=rays, random_geom=g, random_prim=p, random_t=t, random_u=u, random_v=v, random_occ=occ)
+    np.savez_compressed(OUT / "cornell_rays.npz", **out)
+    dev.close()
+
+
+def make_images():
+    out = {}
+    for spp in (16, 1024):
+        for seed in (0, 1):
+            s = small_scene(128, 128, spp)
+            dev = ref.RefDevice(s, seed=seed)
+            t0 = time.time()
+            st = dev.render(spp)
+            out[f"spp{spp}_seed{seed}"] = dev.blit()
+            out[f"spp{spp}_seed{seed}_rays"] = np.float64(st["rays"])
+            print(f"spp {spp} seed {seed}: {time.time() - t0:.1f} s, {st['rays'] / 1e6 / st['seconds']:.1f} Mrays/s")
+            dev.close()
+    np.savez_compressed(OUT / "cornell_img.npz", **out)
+
+
+if __name__ == "__main__":
+    which = sys.argv[1:] or ["sobol", "rays", "images"]
+    if "sobol" in which:
+        make_sobol()
+    if "rays" in which:
+        make_rays()
+    if "images" in which:
+        make_images()
