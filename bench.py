@@ -1,0 +1,310 @@
+#!/usr/bin/env python
+"""Throughput of the B200 render device on the large plain-render workload.
+
+Workload (the configuration the headline metric is quoted on): the seeded terrain scene of
+prt_scenes.terrain() -- a 1024x1024 fBm heightfield plus 400 icospheres, 2,605,058
+triangles, four material kinds (Lambert, GGX gold-like conductor, rough glass, rough coat over
+Lambert) under the reference's sun-sky model -- rendered at 1920x1080, 64 spp, max depth 8,
+Russian roulette from depth 3. One step = one 64-spp frame of that workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Metric: Mrays/s = (closest + shadow rays traced) / device time, the reference's `mray`
+(render/path_renderer_stream.h:175). Timing: CUDA events on the device's stream, barrier and
+synchronize on both sides, max over ranks. The BVH (149 MB) and the path state (GBs) exceed the
+126 MB L2, so no flush is needed between steps. One process per GPU: each rank renders its own
+replica of the frame (independent sampler seed); there is no collective on the data path.
+"""
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "oidn-protoray_b200"))
+
+import numpy as np  # noqa: E402
+
+import prt_scenes  # noqa: E402
+import prt_types as T  # noqa: E402
+
+METRIC = "Mrays/s (closest + shadow rays per second), terrain workload"
+UNIT = "Mrays/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--spp", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.tmp.flush()
+        rows = [r.split(",") for r in open(self.tmp.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.tmp.name)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+                for name, v in zip(names, r[5:9]):
+                    if v.strip() == "Active":
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(spp_frames=1):
+    """The reference's own CPU path (oracle/_ref, compiled from the reference sources) on a
+    bounded sample of the same workload: one full-resolution 1-spp frame after one warm-up
+    frame, all host threads."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import ref  # test infrastructure: the CPU-baseline leg only
+
+    if not ref.ref_available():
+        return None
+    scene = prt_scenes.terrain(with_sky=False)
+    dev = ref.RefDevice(scene, seed=0)
+    dev.render(1)  # warm-up frame
+    st = dev.render(spp_frames)
+    dev.close()
+    return {"value": st["rays"] / 1e6 / st["seconds"], "unit": UNIT, "cores": ref.hardware_threads(),
+            "kind": "reference",
+            "sample": f"{spp_frames} frame(s) of the terrain workload at 1920x1080 x 1 spp after 1 warm-up frame "
+                      f"({st['rays'] / 1e6:.1f}M rays in {st['seconds']:.1f} s); reference pathStream renderer "
+                      f"compiled from its sources, oracle CPU BVH in place of Embree (not installed)"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import ref
+
+    if not ref.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libprt_ref.so is not built"}))
+        return
+    scene = prt_scenes.terrain(with_sky=False)
+    dev = ref.RefDevice(scene, seed=0)
+    for _ in range(args.warmup):
+        dev.render(1)
+    rays, secs = 0.0, 0.0
+    for _ in range(args.steps):
+        st = dev.render(1)
+        rays += st["rays"]
+        secs += st["seconds"]
+    dev.close()
+    value = rays / 1e6 / secs
+    cores = ref.hardware_threads()
+    sample = ("each step = one 1920x1080 x 1-spp frame of the terrain workload (a bounded sample of the "
+              "64-spp frame); reference pathStream + sobolBurley compiled from its sources; oracle CPU BVH in "
+              "place of Embree (not installed)")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded terrain scene)",
+        "config": {"workload": "terrain 2.6M tris, 1920x1080, 1 spp per step, depth 8, rr 3, sun-sky",
+                   "flush": "inputs larger than L2 not applicable (CPU)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def run_ours(args):
+    rank, world, local = dist_info()
+    import prt_cuda
+
+    pg = None
+    if world > 1:
+        import torch
+        import torch.distributed as torch_dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        torch_dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        pg = torch_dist
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    def max_over_ranks(x):
+        if pg is None:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if pg is None:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.SUM)
+        return float(t.item())
+
+    scene = prt_scenes.terrain(spp=args.spp)
+    dev = prt_cuda.DeviceCuda(local)
+    dev.setup(scene, seed=rank)
+
+    # Traversal counts per ray (counting variant of the kernels, one 1-spp frame, untimed).
+    dev.set_profiling(T.PRT_PROFILE_COUNTS)
+    c = dev.render(1)
+    n_closest = c["closest_nodes"] / max(c["closest_rays"], 1)
+    t_closest = c["closest_tris"] / max(c["closest_rays"], 1)
+    n_shadow = c["shadow_nodes"] / max(c["shadow_rays"], 1)
+    t_shadow = c["shadow_tris"] / max(c["shadow_rays"], 1)
+    dev.set_profiling(T.PRT_PROFILE_KERNELS)
+
+    for _ in range(args.warmup):
+        dev.render(args.spp)
+    barrier()
+    dev.clear_frame()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms = rays = closest = shadow = trace_ms = shadow_ms = launches = 0.0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        st = dev.render(args.spp)
+        ms += st["render_ms"]
+        rays += st["rays"]
+        closest += st["closest_rays"]
+        shadow += st["shadow_rays"]
+        trace_ms += st["trace_ms"]
+        shadow_ms += st["shadow_ms"]
+        launches += st["kernel_launches"]
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    barrier()
+    ms_max = max_over_ranks(ms)
+    total_rays = sum_over_ranks(rays)
+    value = total_rays / 1e6 / (ms_max * 1e-3)
+    samples_per_s = sum_over_ranks(scene.width * scene.height * args.spp * args.steps) / (ms_max * 1e-3)
+
+    # End to end through the C ABI with host buffers: camera in, 64-spp render, image out.
+    dev.set_profiling(0)
+    img = np.zeros((scene.height, scene.width, 3), np.float32)
+    e2e_steps = max(1, min(args.steps, 3))
+    barrier()
+    te = time.perf_counter()
+    e2e_rays = 0
+    for _ in range(e2e_steps):
+        dev.init_camera(scene.camera)
+        st = dev.render(args.spp)
+        e2e_rays += st["rays"]
+        dev._check(dev.lib.prt_cuda_blit(dev.h, T.PRT_BLIT_HDR, T.fptr(img)))
+    e2e_wall = max_over_ranks(time.perf_counter() - te)
+    e2e_value = sum_over_ranks(e2e_rays) / 1e6 / e2e_wall
+
+    # Roofline of the dominant kernels (closest + any-hit traversal): algorithmic bytes per ray
+    # B = ray in + hit out + 80 B per node visit + 48 B per triangle test.
+    b_closest = 32 + 16 + 80 * n_closest + 48 * t_closest
+    b_shadow = 32 + 4 + 80 * n_shadow + 48 * t_shadow
+    trav_ms = trace_ms + shadow_ms
+    achieved = (closest * b_closest + shadow * b_shadow) / (trav_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded terrain scene, reference sun-sky model output)",
+        "config": {"workload": f"terrain 2.6M tris, 1920x1080, {args.spp} spp per step, depth 8, rr 3, sun-sky",
+                   "triangles": scene.tri_count, "flush": "inputs larger than L2 (BVH 149 MB, path state GBs)",
+                   "parallelism": f"replicas x{world}"},
+        "samples_per_s": samples_per_s,
+        "wall_ms_per_step": wall * 1e3 / args.steps,
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(C_CAMERA_BYTES),
+                "d2h_bytes_per_step": int(img.nbytes)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "closest-hit + any-hit BVH8 traversal",
+                     "bytes_per_ray": {"closest": b_closest, "shadow": b_shadow},
+                     "per_ray": {"closest_nodes": n_closest, "closest_tris": t_closest, "shadow_nodes": n_shadow,
+                                 "shadow_tris": t_shadow},
+                     "kernel_ms_per_step": trav_ms / args.steps},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            out["cpu_baseline"] = cpu_baseline()
+        except Exception as exc:  # the baseline is reported, never required
+            out["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
+    dev.close()
+    if rank == 0:
+        print(json.dumps(out))
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+C_CAMERA_BYTES = 4 * 14  # prt_camera_desc: 12 floats of basis and position + fov + near clip
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -162,7 +162,23 @@ typedef struct prt_render_stats
   int64_t rays;         /* closest + shadow rays traced */
   int64_t spp;          /* samples per pixel rendered by this call */
   double  render_ms;    /* device time of the call */
+  int64_t closest_rays;
+  int64_t shadow_rays;
+  int64_t kernel_launches;  /* kernels this call launched */
+  double  trace_ms;     /* device time of the closest-hit kernels (PRT_PROFILE_KERNELS) */
+  double  shadow_ms;    /* device time of the any-hit kernels (PRT_PROFILE_KERNELS) */
+  double  shade_ms;     /* device time of the shading kernels (PRT_PROFILE_KERNELS) */
+  int64_t closest_nodes;    /* BVH8 node visits of closest-hit rays (PRT_PROFILE_COUNTS) */
+  int64_t closest_tris;     /* triangle tests of closest-hit rays (PRT_PROFILE_COUNTS) */
+  int64_t shadow_nodes;     /* node visits of shadow rays (PRT_PROFILE_COUNTS) */
+  int64_t shadow_tris;      /* triangle tests of shadow rays (PRT_PROFILE_COUNTS) */
 } prt_render_stats;
+
+/* Profiling switches for prt_cuda_set_profiling. Kernel timing records CUDA events around
+ * each traversal and shading launch; counting runs the counting variant of the traversal
+ * kernels (the reference's nodes/prims per-ray statistic, render/path_renderer_stream.h:180-184). */
+#define PRT_PROFILE_KERNELS (1 << 0)
+#define PRT_PROFILE_COUNTS  (1 << 1)
 
 /* ---- context ----------------------------------------------------------------------------- */
 
@@ -201,6 +217,9 @@ int prt_cuda_clear(prt_context* ctx);
  * (render/device_cpu.cpp:53-59), each advancing the sample index by one. */
 int prt_cuda_render(prt_context* ctx, int32_t spp, prt_render_stats* stats);
 
+/* Enables PRT_PROFILE_* instrumentation for subsequent render calls (0 = off). */
+int prt_cuda_set_profiling(prt_context* ctx, int32_t flags);
+
 /* Device::blitFrame (render/device_cpu.cpp:316-366): sum * rcpSafe(weight) per pixel, as
  * width*height*3 floats. dst may be host or device memory. */
 int prt_cuda_blit(prt_context* ctx, int32_t aov, float* dst);
@@ -225,6 +244,16 @@ int prt_cuda_occluded(prt_context* ctx, int64_t n, const float* rays, int32_t* o
  * and their closest hits: rays_out has width*height*8 floats, geom_id/prim_id width*height. */
 int prt_cuda_query_primary(prt_context* ctx, uint32_t sample_index, float* rays_out,
                            int32_t* geom_id, int32_t* prim_id, float* t);
+
+/* BSDF of one Standard material evaluated and sampled on the device for n tuples of
+ * (wo, wi, 3D sample) (9 floats each) in a canonical shading context: identity shading frame
+ * (N = z), geometric normal z, UV (0.5, 0.5), front-facing hit, path in medium `medium_id`
+ * (0 = outside; 1 = inside a transmissive material's own medium). out gets 13 floats per
+ * tuple: eval value (3), eval pdf, sample weight (3), sampled wi (3), sample pdf, sample type
+ * and BSDF flags (int bits). Mirrors Material::getBsdf + BsdfSimd::eval/sample
+ * (material/material.h:66-76, bsdf/bsdf.h:106-110); used for BSDF parity. */
+int prt_cuda_bsdf_query(prt_context* ctx, const prt_material* material, int32_t medium_id, int64_t n,
+                        const float* tuples, float* out);
 
 /* Host-only (no GPU needed): builds the BVH8 over tri_count triangles given as 9 floats each
  * (v0, v1, v2) and walks it with the counting traversal, the scalar twin of the closest-hit

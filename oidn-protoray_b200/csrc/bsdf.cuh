@@ -2,9 +2,9 @@
 //
 // StandardMaterial::getBsdfLobes (material/standard.cpp:410-620) builds, per hit, a small
 // tree: MultiBsdf{opaque base, translucent base, metal base}, optionally wrapped by a coat
-// and a sheen layer. Here the tree is a fixed struct: the per-hit parameters are resolved
-// once (resolveStandard) and eval/sample walk the same composition with the same
-// arithmetic as the reference classes, without virtual calls or an arena.
+// layer. Here the tree is a fixed struct: the per-hit parameters are resolved once
+// (resolveStandard) and eval/sample walk the same composition with the same arithmetic as
+// the reference classes, without virtual calls or a per-hit arena.
 #pragma once
 
 #include "shading.cuh"
@@ -30,21 +30,259 @@ enum : int
   kBsdfDelta = kBsdfSpecular | kBsdfContinuation,
 };
 
-// ---- DiffuseBrdf (bsdf/diffuse.h:45-82) ------------------------------------------------------
+// ---- energy-compensation tables (bsdf/albedo_tables.h; DevTables in device_scene.h) -----------
+constexpr int kGgxTableSize = 32;
+constexpr int kTableSize = 16;
+
+// math/interpolation.h interp{1,2,3,4}DLinear: clamp, floor, lerp a + s*(b - a).
+PRT_D float lerpf(float a, float b, float s) { return a + s * (b - a); }
+
+PRT_D void interpAxis(float p, int size, int& i0, int& i1, float& s)
+{
+  const float c = fminf(fmaxf(p, 0.f), (float)(size - 1));
+  s = c - floorf(c);
+  i0 = min((int)c, size - 1);
+  i1 = min(i0 + 1, size - 1);
+}
+
+PRT_D float interp1D(const float* f, int size, float x)
+{
+  int a, b;
+  float s;
+  interpAxis(x, size, a, b, s);
+  return lerpf(__ldg(f + a), __ldg(f + b), s);
+}
+
+PRT_D float interp2D(const float* f, int size, float x, float y)
+{
+  int x0, x1, y0, y1;
+  float sx, sy;
+  interpAxis(x, size, x0, x1, sx);
+  interpAxis(y, size, y0, y1, sy);
+  const float f0 = lerpf(__ldg(f + x0 + y0 * size), __ldg(f + x1 + y0 * size), sx);
+  const float f1 = lerpf(__ldg(f + x0 + y1 * size), __ldg(f + x1 + y1 * size), sx);
+  return lerpf(f0, f1, sy);
+}
+
+PRT_D float interp3D(const float* f, int size, float x, float y, float z)
+{
+  int z0, z1;
+  float sz;
+  interpAxis(z, size, z0, z1, sz);
+  const int n2 = size * size;
+  return lerpf(interp2D(f + z0 * n2, size, x, y), interp2D(f + z1 * n2, size, x, y), sz);
+}
+
+PRT_D float interp4D(const float* f, int size, float x, float y, float z, float w)
+{
+  int w0, w1;
+  float sw;
+  interpAxis(w, size, w0, w1, sw);
+  const int n3 = size * size * size;
+  return lerpf(interp3D(f + w0 * n3, size, x, y, z), interp3D(f + w1 * n3, size, x, y, z), sw);
+}
+
+// MicrofacetAlbedoTable (bsdf/albedo_tables.h:8-37)
+PRT_D float ggxAlbedo(const DevTables& t, float cosThetaO, float roughness)
+{
+  const float k = (float)(kGgxTableSize - 1);
+  return interp2D(t.ggxDir, kGgxTableSize, cosThetaO * k, roughness * k);
+}
+
+PRT_D float ggxAlbedoAvg(const DevTables& t, float roughness)
+{
+  return interp1D(t.ggxAvg, kGgxTableSize, roughness * (float)(kGgxTableSize - 1));
+}
+
+// MicrofacetDielectricAlbedoTable (bsdf/albedo_tables.h:39-130): eta <= 1 uses the eta table
+// over [1/3, 1], eta > 1 the reciprocal table over [1, 3].
+PRT_D float dielAlbedo(const DevTables& t, float cosThetaO, float eta, float roughness)
+{
+  const float k = (float)(kTableSize - 1);
+  if (eta <= 1.f)
+  {
+    const float minEta = 1.f / 3.f, maxEta = 1.f;
+    const float e = (eta - minEta) / (maxEta - minEta);
+    return interp3D(t.dielEtaDir, kTableSize, cosThetaO * k, e * k, roughness * k);
+  }
+  const float e = (eta - 1.f) / (3.f - 1.f);
+  return interp3D(t.dielRcpDir, kTableSize, cosThetaO * k, e * k, roughness * k);
+}
+
+PRT_D float dielAlbedoAvg(const DevTables& t, float eta, float roughness)
+{
+  const float k = (float)(kTableSize - 1);
+  if (eta <= 1.f)
+  {
+    const float e = (eta - 1.f / 3.f) / (1.f - 1.f / 3.f);
+    return interp2D(t.dielEtaAvg, kTableSize, e * k, roughness * k);
+  }
+  const float e = (eta - 1.f) / (3.f - 1.f);
+  return interp2D(t.dielRcpAvg, kTableSize, e * k, roughness * k);
+}
+
+// MicrofacetDielectricReflectionAlbedoTable (bsdf/albedo_tables.h:132-170)
+PRT_D float reflAlbedo(const DevTables& t, float cosThetaO, float eta, float roughness)
+{
+  const float k = (float)(kTableSize - 1);
+  const float e = (eta - 1.f / 3.f) / (1.f - 1.f / 3.f);
+  return interp3D(t.reflDir, kTableSize, cosThetaO * k, e * k, roughness * k);
+}
+
+PRT_D float reflAlbedoAvg(const DevTables& t, float eta, float roughness)
+{
+  const float k = (float)(kTableSize - 1);
+  const float e = (eta - 1.f / 3.f) / (1.f - 1.f / 3.f);
+  return interp2D(t.reflAvg, kTableSize, e * k, roughness * k);
+}
+
+// ---- microfacet distribution (bsdf/ggx_distribution.h) ---------------------------------------
+PRT_D float roughnessToAlpha(float r) { return fmaxf(r * r, 0.001f); }
+
+struct GGX
+{
+  float ax, ay;
+
+  PRT_D float eval(f3 wh) const
+  {
+    const float c2 = sqr(wh.z);
+    const float e = (sqr(wh.x / ax) + sqr(wh.y / ay)) / c2;
+    return 1.f / (kPi * ax * ay * sqr(c2 * (1.f + e)));
+  }
+
+  PRT_D float lambda(f3 w) const
+  {
+    const float c2 = sqr(w.z);
+    const float invA2 = (sqr(w.x * ax) + sqr(w.y * ay)) / c2;
+    return 0.5f * (-1.f + sqrtf(1.f + invA2));
+  }
+
+  PRT_D float G1(f3 w) const { return 1.f / (1.f + lambda(w)); }
+  PRT_D float G2(f3 wo, f3 wi) const { return 1.f / (1.f + lambda(wo) + lambda(wi)); }
+
+  PRT_D float evalVisible(f3 wh, f3 wo, float cosThetaOH, float& pdf) const
+  {
+    const float D = eval(wh);
+    pdf = G1(wo) * fabsf(cosThetaOH) * D / fabsf(wo.z);
+    return D;
+  }
+
+  // Visible-normal sampling (Heitz 2018), GGXDistribution::sampleVisible.
+  PRT_D f3 sampleVisible(f3 wo, float& pdf, float sx, float sy) const
+  {
+    const f3 V = normalize(mk(ax * wo.x, ay * wo.y, wo.z));
+    const f3 T1 = V.z < 0.9999f ? normalize(cross(V, mk(0.f, 0.f, 1.f))) : mk(1.f, 0.f, 0.f);
+    const f3 T2 = cross(T1, V);
+    const float a = 1.f / (1.f + V.z);
+    const float r = sqrtf(sx);
+    const float phi = sy < a ? sy / a * kPi : kPi + (sy - a) / (1.f - a) * kPi;
+    float sp, cp;
+    sincosf(phi, &sp, &cp);
+    const float P1 = r * cp;
+    const float P2 = r * sp * (sy < a ? 1.f : V.z);
+    f3 wh = P1 * T1 + P2 * T2 + sqrtf(fmaxf(0.f, 1.f - P1 * P1 - P2 * P2)) * V;
+    wh = normalize(mk(ax * wh.x, ay * wh.y, fmaxf(0.f, wh.z)));
+    pdf = G1(wo) * fabsf(dot(wo, wh)) * eval(wh) / fabsf(wo.z);
+    return wh;
+  }
+};
+
+// ---- Fresnel (bsdf/optics.h) -------------------------------------------------------------------
+PRT_D float fresnelDielectric(float cosI, float cosT, float eta)
+{
+  const float Rper = (eta * cosI - cosT) * (1.f / (eta * cosI + cosT));
+  const float Rpar = (cosI - eta * cosT) * (1.f / (cosI + eta * cosT));
+  return 0.5f * (Rpar * Rpar + Rper * Rper);
+}
+
+PRT_D float fresnelDielectric(float cosI, float eta)
+{
+  cosI = fmaxf(cosI, 0.f);
+  const float k = 1.f - eta * eta * (1.f - cosI * cosI);
+  if (!(k >= 0.f)) return 1.f;
+  return fresnelDielectric(cosI, sqrtf(k), eta);
+}
+
+PRT_D float fresnelDielectricEx(float cosI, float& cosT, float eta)
+{
+  cosI = fabsf(cosI);
+  const float k = 1.f - eta * eta * (1.f - cosI * cosI);
+  if (!(k >= 0.f))
+  {
+    cosT = 0.f;
+    return 1.f;
+  }
+  cosT = sqrtf(k);
+  return fresnelDielectric(cosI, cosT, eta);
+}
+
+PRT_D float fresnelDielectricAvg(float eta)
+{
+  const float r = 1.f / eta;
+  if (r >= 1.f) return (r - 1.f) / (4.08567f + 1.00071f * r);
+  const float r2 = r * r, r3 = r2 * r;
+  return 0.997118f + 0.1014f * r - 0.965241f * r2 - 0.130607f * r3;
+}
+
+PRT_D float refractCos(float cosI, float eta)
+{
+  const float k = 1.f - eta * eta * (1.f - cosI * cosI);
+  return sqrtf(fmaxf(k, 0.f));
+}
+
+PRT_D f3 refractDir(f3 I, f3 N, float cosI, float cosT, float eta) { return eta * (cosI * N - I) - cosT * N; }
+
+PRT_D float fresnelConductor(float cosI, float eta, float k)
+{
+  cosI = fabsf(cosI);
+  const float tmp = sqr(eta) + sqr(k);
+  const float c2 = sqr(cosI);
+  const float Rpar = (tmp * c2 - 2.f * eta * cosI + 1.f) * (1.f / (tmp * c2 + 2.f * eta * cosI + 1.f));
+  const float Rper = (tmp - 2.f * eta * cosI + c2) * (1.f / (tmp + 2.f * eta * cosI + c2));
+  return 0.5f * (Rpar + Rper);
+}
+
+// Gulbrandsen's artistic (reflectivity, edge tint) -> (eta, k).
+PRT_D void artisticToIor(float r, float g, float& eta, float& k)
+{
+  r = fminf(r, 0.99f);
+  const float nMin = (1.f - r) / (1.f + r);
+  const float nMax = (1.f + sqrtf(r)) / (1.f - sqrtf(r));
+  const float n = g * nMin + (1.f - g) * nMax;
+  const float k2 = (sqr(n + 1.f) * r - sqr(n - 1.f)) / (1.f - r);
+  eta = n;
+  k = sqrtf(fmaxf(k2, 0.f));
+}
+
+PRT_D float artisticAvg(float r, float g)
+{
+  const float r2 = r * r, r3 = r2 * r, g2 = g * g, g3 = g2 * g;
+  return 0.087237f + 0.0230685f * g - 0.0864902f * g2 + 0.0774594f * g3 + 0.782654f * r - 0.136432f * r2 +
+         0.278708f * r3 + 0.19744f * g * r + 0.0360605f * g2 * r - 0.2586f * g * r2;
+}
+
+PRT_D f3 powf3(f3 c, float e) { return mk(powf(c.x, e), powf(c.y, e), powf(c.z, e)); }
+PRT_D f3 lerp3(f3 a, f3 b, float s) { return a + s * (b - a); }
+
+// ---- lobes ---------------------------------------------------------------------------------------
+
+// DiffuseBrdf (bsdf/diffuse.h:45-82).
 struct DiffuseLobe
 {
   f3 color;
 
+  PRT_D int flags() const { return kDiffuseReflection; }
   PRT_D float importance() const { return reduceMax(color); }
+  PRT_D f3 albedo() const { return color; }
 
-  PRT_D f3 eval(const Frame& fr, f3 wi, float& pdf) const
+  PRT_D f3 eval(const Frame& fr, f3 Ng, f3 wo, f3 wi, float& pdf) const
   {
     const float cosThetaI = fmaxf(dot(wi, fr.N), 0.f);
     pdf = cosThetaI * kInvPi;
     return color * kInvPi * cosThetaI;
   }
 
-  PRT_D f3 sample(const Frame& fr, f3 Ng, float sx, float sy, f3& wi, float& pdf, int& type) const
+  PRT_D f3 sample(const Frame& fr, f3 Ng, f3 wo, float sx, float sy, float sc, f3& wi, float& pdf, int& type) const
   {
     wi = toWorld(fr, cosineSampleHemisphere(pdf, sx, sy));
     type = kDiffuseReflection;
@@ -52,36 +290,569 @@ struct DiffuseLobe
   }
 };
 
-// Per-hit Standard-material BSDF. Lobe slots follow the MultiBsdf order the reference adds
-// them in (opaque, translucent, metal).
+// RoughConductorBrdf / ConductorBrdf with the artistic Fresnel (bsdf/rough_conductor.h:108-225,
+// bsdf/conductor.h, bsdf/optics.h:243-268).
+struct ConductorLobe
+{
+  f3 r, g, eta, k;
+  GGX mf;
+  float roughness;
+  float Eavg;
+  f3 fmsScale;
+  bool rough;
+
+  PRT_D void init(const DevTables& t, f3 reflectivity, f3 edgeTint, float rgh, bool isRough)
+  {
+    r = reflectivity;
+    g = edgeTint;
+    artisticToIor(r.x, g.x, eta.x, k.x);
+    artisticToIor(r.y, g.y, eta.y, k.y);
+    artisticToIor(r.z, g.z, eta.z, k.z);
+    rough = isRough;
+    roughness = rgh;
+    const float a = roughnessToAlpha(rgh);
+    mf.ax = mf.ay = a;
+    if (rough)
+    {
+      Eavg = ggxAlbedoAvg(t, rgh);
+      const f3 Favg = mk(artisticAvg(r.x, g.x), artisticAvg(r.y, g.y), artisticAvg(r.z, g.z));
+      fmsScale = Favg * Favg * Eavg * mk(1.f / (1.f - Favg.x * (1.f - Eavg)), 1.f / (1.f - Favg.y * (1.f - Eavg)),
+                                         1.f / (1.f - Favg.z * (1.f - Eavg)));
+    }
+  }
+
+  PRT_D f3 F(float c) const
+  {
+    return mk(fresnelConductor(c, eta.x, k.x), fresnelConductor(c, eta.y, k.y), fresnelConductor(c, eta.z, k.z));
+  }
+
+  PRT_D int flags() const { return rough ? kGlossyReflection : kSpecularReflection; }
+  PRT_D float importance() const { return 1.f; }
+  PRT_D f3 albedo() const { return r; }
+
+  PRT_D f3 fms(const DevTables& t, float cosThetaO, float cosThetaI) const
+  {
+    const float Eo = ggxAlbedo(t, cosThetaO, roughness);
+    const float Ei = ggxAlbedo(t, cosThetaI, roughness);
+    return fmsScale * ((1.f - Eo) * (1.f - Ei) * (1.f / (kPi * (1.f - Eavg))) * cosThetaI);
+  }
+
+  PRT_D f3 eval(const DevTables& t, const Frame& fr, f3 Ng, f3 wo, f3 wi, float& pdf) const
+  {
+    pdf = 0.f;
+    if (!rough) return mk(0.f);
+    const float cosThetaO = dot(wo, fr.N);
+    const float cosThetaI = dot(wi, fr.N);
+    if (!(cosThetaO > 0.f) || !(cosThetaI > 0.f)) return mk(0.f);
+    const f3 wh = normalize(wi + wo);
+    const float cosThetaOH = dot(wo, wh);
+    const f3 wo0 = toLocal(fr, wo), wi0 = toLocal(fr, wi), wh0 = toLocal(fr, wh);
+    float whPdf;
+    const float D = mf.evalVisible(wh0, wo0, cosThetaOH, whPdf);
+    const float G = mf.G2(wo0, wi0);
+    pdf = whPdf * (1.f / (4.f * fabsf(cosThetaOH)));
+    return F(cosThetaOH) * (D * G * (1.f / (4.f * cosThetaO))) + fms(t, cosThetaO, cosThetaI);
+  }
+
+  PRT_D f3 sample(const DevTables& t, const Frame& fr, f3 Ng, f3 wo, float sx, float sy, float sc, f3& wi, float& pdf,
+                  int& type) const
+  {
+    const float cosThetaO = dot(wo, fr.N);
+    if (!rough)
+    {
+      wi = 2.f * cosThetaO * fr.N - wo;
+      if (!(cosThetaO > 0.f) || !(dot(wi, Ng) > 0.f)) return mk(0.f);
+      type = kSpecularReflection;
+      pdf = 1.f;
+      return F(cosThetaO);
+    }
+    if (!(cosThetaO > 0.f)) return mk(0.f);
+    const f3 wo0 = toLocal(fr, wo);
+    float whPdf;
+    const f3 wh = toWorld(fr, mf.sampleVisible(wo0, whPdf, sx, sy));
+    wi = reflect(wo, wh);
+    const float cosThetaI = dot(wi, fr.N);
+    if (!(cosThetaI > 0.f) || !(dot(wi, Ng) > 0.f)) return mk(0.f);
+    const float cosThetaOH = dot(wo, wh);
+    const f3 wi0 = toLocal(fr, wi);
+    const float G = mf.G2(wo0, wi0);
+    type = kGlossyReflection;
+    pdf = whPdf * (1.f / (4.f * fabsf(cosThetaOH)));
+    return F(cosThetaOH) * (G * rcpSafe(mf.G1(wo0))) + fms(t, cosThetaO, cosThetaI) * (1.f / pdf);
+  }
+};
+
+// RoughDielectricBsdf / DielectricBsdf (bsdf/rough_dielectric.h:265-550, bsdf/dielectric.h:56-131).
+// eta = etaExt / etaInt as seen from the side wo is on.
+struct DielectricLobe
+{
+  float eta;
+  GGX mf;
+  float roughness;
+  float EavgEta, EavgRcpEta, fmsRatio;
+  bool rough;
+
+  PRT_D void init(const DevTables& t, float e, float rgh, bool isRough)
+  {
+    eta = e;
+    rough = isRough;
+    roughness = rgh;
+    mf.ax = mf.ay = roughnessToAlpha(rgh);
+    if (rough)
+    {
+      EavgEta = dielAlbedoAvg(t, eta, rgh);
+      EavgRcpEta = dielAlbedoAvg(t, 1.f / eta, rgh);
+      const float FavgEta = fresnelDielectricAvg(eta);
+      const float FavgRcpEta = fresnelDielectricAvg(1.f / eta);
+      const float a = (1.f - FavgEta) * (1.f / (1.f - EavgRcpEta));
+      const float b = (1.f - FavgRcpEta) * (1.f / (1.f - EavgEta));
+      const float x = b * (1.f / (a + b));
+      fmsRatio = 1.f - x * (1.f - FavgEta);
+    }
+  }
+
+  PRT_D int flags() const
+  {
+    return rough ? (kGlossyReflection | kGlossyTransmission) : (kSpecularReflection | kSpecularTransmission);
+  }
+  PRT_D float importance() const { return 1.f; }
+  PRT_D f3 albedo() const { return mk(1.f); }
+
+  // Single-scattering part (RoughDielectricBsdfSimd::evalSingle).
+  PRT_D float evalSingle(const Frame& fr, f3 Ng, f3 wo, f3 wi, float& pdf) const
+  {
+    pdf = 0.f;
+    const float cosThetaO = dot(wo, fr.N);
+    if (!(cosThetaO > 0.f)) return 0.f;
+    const float cosThetaI = dot(wi, fr.N);
+    if (!(cosThetaI * dot(wi, Ng) > 0.f)) return 0.f;
+    const bool refl = cosThetaI > 0.f;
+    f3 wh = normalize(refl ? wi + wo : eta * wo + wi);
+    if (dot(wh, fr.N) < 0.f) wh = -wh;
+    const float cosThetaOH = dot(wo, wh);
+    const float cosThetaIH = dot(wi, wh);
+    const float F = fresnelDielectric(cosThetaOH, eta);
+    float value;
+    if (refl)
+    {
+      pdf = F * (1.f / (4.f * fabsf(cosThetaOH)));
+      value = F * (1.f / (4.f * cosThetaO));
+    }
+    else
+    {
+      pdf = (1.f - F) * (1.f / sqr(eta)) * fabsf(cosThetaIH) * (1.f / sqr(cosThetaOH + (1.f / eta) * cosThetaIH));
+      value = pdf * fabsf(cosThetaOH) * (1.f / cosThetaO);
+    }
+    const f3 wo0 = toLocal(fr, wo), wi0 = toLocal(fr, wi), wh0 = toLocal(fr, wh);
+    float whPdf;
+    const float D = mf.evalVisible(wh0, wo0, cosThetaOH, whPdf);
+    const float G = mf.G2(wo0, wi0);
+    pdf = pdf * whPdf;
+    return value * D * G;
+  }
+
+  // Multiple-scattering part for a direction on the reflection or transmission side.
+  PRT_D float evalFms(const DevTables& t, float Eo, float cosThetaI, float& fmsPdf) const
+  {
+    if (cosThetaI > 0.f)
+    {
+      const float Ei = dielAlbedo(t, cosThetaI, eta, roughness);
+      fmsPdf = fmsRatio * (cosThetaI * kInvPi);
+      return fmsRatio * (1.f - Eo) * (1.f - Ei) * (1.f / (kPi * (1.f - EavgEta))) * cosThetaI;
+    }
+    const float c = fabsf(cosThetaI);
+    const float Ei = dielAlbedo(t, c, 1.f / eta, roughness);
+    fmsPdf = (1.f - fmsRatio) * (c * kInvPi);
+    return (1.f - fmsRatio) * (1.f - Eo) * (1.f - Ei) * (1.f / (kPi * (1.f - EavgRcpEta))) * c;
+  }
+
+  PRT_D f3 eval(const DevTables& t, const Frame& fr, f3 Ng, f3 wo, f3 wi, float& pdf) const
+  {
+    pdf = 0.f;
+    if (!rough) return mk(0.f);
+    const float cosThetaO = dot(wo, fr.N);
+    if (!(cosThetaO > 0.f)) return mk(0.f);
+    const float cosThetaI = dot(wi, fr.N);
+    if (!(cosThetaI * dot(wi, Ng) > 0.f)) return mk(0.f);
+    const float Eo = dielAlbedo(t, cosThetaO, eta, roughness);
+    float fmsPdf;
+    const float fmsValue = evalFms(t, Eo, cosThetaI, fmsPdf);
+    float singlePdf;
+    const float single = evalSingle(fr, Ng, wo, wi, singlePdf);
+    pdf = Eo * singlePdf + (1.f - Eo) * fmsPdf;
+    return mk(single + fmsValue);
+  }
+
+  PRT_D f3 sample(const DevTables& t, const Frame& fr, f3 Ng, f3 wo, float sx, float sy, float sc, f3& wi, float& pdf,
+                  int& type) const
+  {
+    pdf = 0.f;
+    const float cosThetaO = dot(wo, fr.N);
+    if (!(cosThetaO > 0.f)) return mk(0.f);
+    if (!rough)
+    {
+      float cosThetaT;
+      const float F = fresnelDielectricEx(cosThetaO, cosThetaT, eta);
+      wi = mk(0.f);
+      if (sc <= F)
+      {
+        wi = 2.f * cosThetaO * fr.N - wo;
+        if (!(dot(wi, Ng) > 0.f)) return mk(0.f);
+        type = kSpecularReflection;
+        pdf = F;
+        return mk(1.f);
+      }
+      wi = refractDir(wo, fr.N, cosThetaO, cosThetaT, eta);
+      if (!(dot(wi, Ng) < 0.f)) return mk(0.f);
+      type = kSpecularTransmission;
+      pdf = 1.f - F;
+      return mk(1.f);
+    }
+    const float Eo = dielAlbedo(t, cosThetaO, eta, roughness);
+    bool ok;
+    wi = mk(0.f);
+    if (sc <= Eo)
+    {
+      const f3 wo0 = toLocal(fr, wo);
+      float whPdf;
+      const f3 wh = toWorld(fr, mf.sampleVisible(wo0, whPdf, sx, sy));
+      const float cosThetaOH = dot(wo, wh);
+      float cosThetaTH;
+      const float F = fresnelDielectricEx(cosThetaOH, cosThetaTH, eta);
+      const float sc1 = sc * (1.f / Eo);
+      if (sc1 <= F)
+      {
+        wi = 2.f * cosThetaOH * wh - wo;
+        ok = dot(wi, fr.N) > 0.f;
+      }
+      else
+      {
+        wi = refractDir(wo, wh, cosThetaOH, cosThetaTH, eta);
+        ok = dot(wi, fr.N) < 0.f;
+      }
+    }
+    else
+    {
+      const float sc1 = (sc - Eo) * (1.f / (1.f - Eo));
+      float p;
+      const f3 d = toWorld(fr, cosineSampleHemisphere(p, sx, sy));
+      wi = sc1 <= fmsRatio ? d : -d;
+      ok = true;
+    }
+    if (!ok) return mk(0.f);
+    const float cosThetaI = dot(wi, fr.N);
+    if (!(cosThetaI * dot(wi, Ng) > 0.f)) return mk(0.f);
+    type = cosThetaI > 0.f ? kGlossyReflection : kGlossyTransmission;
+    float fmsPdf;
+    const float fmsValue = evalFms(t, Eo, cosThetaI, fmsPdf);
+    float singlePdf;
+    const float single = evalSingle(fr, Ng, wo, wi, singlePdf);
+    pdf = Eo * singlePdf + (1.f - Eo) * fmsPdf;
+    return mk((single + fmsValue) * (1.f / pdf));
+  }
+};
+
+// A dielectric layer over a substrate: RoughCoatingBsdf (bsdf/rough_coating.h:271-593) when
+// rough, CoatingBsdf (bsdf/coating.h:189-417) when smooth.
+struct CoatLayer
+{
+  float eta;        // <= 1
+  f3 color;         // transmittance
+  float thickness;
+  GGX mf;
+  float roughness;
+  float avg;        // Ravg (rough) or Favg (smooth), times scale
+  float scale;
+  bool rough;
+
+  PRT_D void init(const DevTables& t, float e, f3 col, float thick, float rgh, bool isRough, float s)
+  {
+    eta = e <= 1.f ? e : 1.f / e;
+    color = col;
+    thickness = thick;
+    rough = isRough;
+    roughness = rgh;
+    mf.ax = mf.ay = roughnessToAlpha(rgh);
+    scale = s;
+    // The reference evaluates the averages with the constructor argument (before the
+    // eta <= 1 fold) and the scale.
+    avg = (rough ? reflAlbedoAvg(t, e, rgh) : fresnelDielectricAvg(e)) * s;
+  }
+
+  PRT_D int flags(int baseFlags) const { return baseFlags | (rough ? kGlossyReflection : kSpecularReflection); }
+  PRT_D float importance(float baseImportance) const { return fmaxf(1.f, baseImportance); }
+  PRT_D f3 albedo(f3 base) const { return lerp3(base, base * powf3(color, thickness), scale); }
+
+  // Attenuation of the substrate's value through the layer.
+  PRT_D f3 attenuate(const DevTables& t, f3 baseValue, float cosThetaO, float cosThetaI, float Fo, float cosThetaO1,
+                     bool diffuseBase) const
+  {
+    float Fi, lengthO1, lengthI1;
+    if (rough)
+    {
+      lengthO1 = 1.f / refractCos(cosThetaO, eta);
+      lengthI1 = 1.f / refractCos(fabsf(cosThetaI), eta);
+      Fi = reflAlbedo(t, fabsf(cosThetaI), eta, roughness) * scale;
+    }
+    else
+    {
+      float cosThetaI1;
+      Fi = fresnelDielectricEx(fabsf(cosThetaI), cosThetaI1, eta) * scale;
+      lengthO1 = 1.f / cosThetaO1;
+      lengthI1 = 1.f / cosThetaI1;
+    }
+    float length = lengthO1 + lengthI1;
+    if (cosThetaI <= 0.f) length *= 0.5f;
+    baseValue = lerp3(baseValue, baseValue * powf3(color, thickness * length), scale);
+    float T = fminf(1.f - Fo, 1.f - Fi);
+    if (diffuseBase) T = (1.f - Fo) * (1.f - Fi) * (1.f / (1.f - avg));
+    return baseValue * T;
+  }
+
+  PRT_D f3 coatValue(const Frame& fr, f3 wo, f3 wi, float cosThetaO, float& coatPdf) const
+  {
+    const f3 wh = normalize(wo + wi);
+    const float cosThetaOH = dot(wo, wh);
+    const float F = fresnelDielectric(cosThetaOH, eta) * scale;
+    const f3 wo0 = toLocal(fr, wo), wi0 = toLocal(fr, wi), wh0 = toLocal(fr, wh);
+    float whPdf;
+    const float D = mf.evalVisible(wh0, wo0, cosThetaOH, whPdf);
+    const float G = mf.G2(wo0, wi0);
+    coatPdf = whPdf * (1.f / (4.f * fabsf(cosThetaOH)));
+    return mk(F * D * G * (1.f / (4.f * cosThetaO)));
+  }
+
+  // `Sub` provides flags(), importance(), eval(wo, wi, pdf), sample(...).
+  template <class Sub>
+  PRT_D f3 eval(const DevTables& t, const Sub& base, const Frame& fr, f3 Ng, f3 wo, f3 wi, float& pdf) const
+  {
+    pdf = 0.f;
+    const float cosThetaO = dot(wo, fr.N);
+    if (!(cosThetaO > 0.f)) return mk(0.f);
+    const float cosThetaI = dot(wi, fr.N);
+    if (!(cosThetaI * dot(wi, Ng) > 0.f)) return mk(0.f);
+    float Fo, cosThetaO1 = 0.f;
+    if (rough)
+      Fo = reflAlbedo(t, cosThetaO, eta, roughness) * scale;
+    else
+      Fo = fresnelDielectricEx(cosThetaO, cosThetaO1, eta) * scale;
+    const float coatImp = Fo;
+    const float baseImp = (1.f - Fo) * base.importance();
+    const float coatPick = coatImp * (1.f / (coatImp + baseImp));
+    const float basePick = 1.f - coatPick;
+    float basePdf;
+    f3 baseValue = base.eval(t, wo, wi, basePdf);
+    const bool diffuseBase = (base.flags() & ~kBsdfDiffuse) == 0;
+    baseValue = attenuate(t, baseValue, cosThetaO, cosThetaI, Fo, cosThetaO1, diffuseBase);
+    if (rough && cosThetaI > 0.f)
+    {
+      float coatPdf;
+      const f3 cv = coatValue(fr, wo, wi, cosThetaO, coatPdf);
+      pdf = coatPick * coatPdf + basePick * basePdf;
+      return cv + baseValue;
+    }
+    pdf = basePdf * basePick;
+    return baseValue;
+  }
+
+  template <class Sub>
+  PRT_D f3 sample(const DevTables& t, const Sub& base, const Frame& fr, f3 Ng, f3 wo, float sx, float sy, float sc,
+                  f3& wi, float& pdf, int& type) const
+  {
+    pdf = 0.f;
+    type = 0;
+    wi = mk(0.f);
+    const float cosThetaO = dot(wo, fr.N);
+    if (!(cosThetaO > 0.f)) return mk(0.f);
+    const bool diffuseBase = (base.flags() & ~kBsdfDiffuse) == 0;
+    if (!rough)
+    {
+      // CoatingBsdfSimd::sample
+      float cosThetaO1;
+      const float Fo = fresnelDielectricEx(cosThetaO, cosThetaO1, eta) * scale;
+      const float coatImp = Fo;
+      const float baseImp = (1.f - Fo) * base.importance();
+      const float coatPick = coatImp * (1.f / (coatImp + baseImp));
+      const float basePick = 1.f - coatPick;
+      if (sc <= coatPick)
+      {
+        wi = 2.f * cosThetaO * fr.N - wo;
+        if (!(dot(wi, Ng) > 0.f)) return mk(0.f);
+        type = kSpecularReflection;
+        pdf = coatPick;
+        return mk(Fo * (1.f / coatPick));
+      }
+      const float s1 = (sc - coatPick) * (1.f / basePick);
+      float basePdf;
+      int baseType;
+      f3 bw = base.sample(t, wo, sx, sy, s1, wi, basePdf, baseType);
+      type = baseType;
+      const float cosThetaI = dot(wi, fr.N);
+      if (!(reduceMax(bw) > 0.f) || !(cosThetaI * dot(wi, Ng) > 0.f)) return mk(0.f);
+      float cosThetaI1;
+      const float Fi = fresnelDielectricEx(fabsf(cosThetaI), cosThetaI1, eta) * scale;
+      float length = 1.f / cosThetaO1 + 1.f / cosThetaI1;
+      if (cosThetaI <= 0.f) length *= 0.5f;
+      bw = lerp3(bw, bw * powf3(color, thickness * length), scale);
+      float T = fminf(1.f - Fo, 1.f - Fi);
+      if (diffuseBase) T = (1.f - Fo) * (1.f - Fi) * (1.f / (1.f - avg));
+      pdf = basePdf * basePick;
+      return bw * (T * (1.f / basePick));
+    }
+    // RoughCoatingBsdfSimd::sample
+    const f3 wo0 = toLocal(fr, wo);
+    const float Ro = reflAlbedo(t, cosThetaO, eta, roughness) * scale;
+    const float coatImp = Ro;
+    const float baseImp = (1.f - Ro) * base.importance();
+    const float coatPick = coatImp * (1.f / (coatImp + baseImp));
+    const float basePick = 1.f - coatPick;
+    f3 wh = mk(0.f);
+    float basePdf = 0.f;
+    f3 baseValue = mk(0.f);
+    if (sc <= coatPick)
+    {
+      float whPdf;
+      wh = toWorld(fr, mf.sampleVisible(wo0, whPdf, sx, sy));
+      const float cosThetaOH = dot(wo, wh);
+      wi = 2.f * cosThetaOH * wh - wo;
+      if (!(dot(wi, fr.N) > 0.f)) return mk(0.f);
+      type = kGlossyReflection;
+      baseValue = base.eval(t, wo, wi, basePdf);
+    }
+    else
+    {
+      const float s1 = (sc - coatPick) * (1.f / basePick);
+      f3 baseWi;
+      float basePdf2;
+      int baseType;
+      const f3 bw = base.sample(t, wo, sx, sy, s1, baseWi, basePdf2, baseType);
+      if (!(reduceMax(bw) > 0.f)) return mk(0.f);
+      wi = baseWi;
+      basePdf = basePdf2;
+      type = baseType;
+      baseValue = bw * ((type & kBsdfDelta) != 0 ? 1.f : basePdf);
+      wh = normalize(wo + wi);
+    }
+    const float cosThetaI = dot(wi, fr.N);
+    if (!(cosThetaI * dot(wi, Ng) > 0.f)) return mk(0.f);
+    const float cosThetaOH = dot(wo, wh);
+    baseValue = attenuate(t, baseValue, cosThetaO, cosThetaI, Ro, 0.f, diffuseBase);
+    if (type & kBsdfDelta)
+    {
+      pdf = basePdf;
+      return baseValue * (1.f / basePick);
+    }
+    if (cosThetaI <= 0.f)
+    {
+      pdf = basePick * basePdf;
+      return baseValue * (1.f / pdf);
+    }
+    const float F = fresnelDielectric(cosThetaOH, eta) * scale;
+    const f3 wi0 = toLocal(fr, wi), wh0 = toLocal(fr, wh);
+    float whPdf;
+    const float D = mf.evalVisible(wh0, wo0, cosThetaOH, whPdf);
+    const float G = mf.G2(wo0, wi0);
+    const float coatPdf = whPdf * (1.f / (4.f * fabsf(cosThetaOH)));
+    const f3 cv = mk(F * D * G * (1.f / (4.f * cosThetaO)));
+    pdf = coatPick * coatPdf + basePick * basePdf;
+    return (cv + baseValue) * (1.f / pdf);
+  }
+};
+
+// ---- Standard material composition -----------------------------------------------------------
+
+enum : int
+{
+  kSlotOpaque = 0,
+  kSlotDielectric = 1,
+  kSlotConductor = 2,
+};
+
+// The opaque base: a Lambertian lobe, optionally under the specular dielectric layer
+// (material/standard.cpp:441-502).
+struct OpaqueBase
+{
+  DiffuseLobe diff;
+  CoatLayer spec;
+  bool hasSpec;
+};
+
+struct StdBsdf;
+
+// Substrate adaptor for the specular layer: the diffuse lobe.
+struct DiffuseSub
+{
+  const DiffuseLobe* d;
+  const Frame* fr;
+  f3 Ng;
+  PRT_D int flags() const { return kDiffuseReflection; }
+  PRT_D float importance() const { return d->importance(); }
+  PRT_D f3 eval(const DevTables& t, f3 wo, f3 wi, float& pdf) const { return d->eval(*fr, Ng, wo, wi, pdf); }
+  PRT_D f3 sample(const DevTables& t, f3 wo, float sx, float sy, float sc, f3& wi, float& pdf, int& type) const
+  {
+    return d->sample(*fr, Ng, wo, sx, sy, sc, wi, pdf, type);
+  }
+};
+
+// MultiBsdf over the base lobes (bsdf/multi_bsdf.h:151-270) and the outer coat.
 struct StdBsdf
 {
   Frame fr;
   f3 Ng;
-  int flags;
   int nLobes;
+  int kind[3];
   float scale[3];
   float imp[3];
   float impSum;
-  int kind[3];       // lobe kind per slot
-  DiffuseLobe diffuse;
-  f3 albedo;
+  int baseFlags;
+  OpaqueBase opaque;
+  DielectricLobe diel;
+  ConductorLobe cond;
+  CoatLayer coat;
+  bool hasCoat;
+  f3 albedoV;
 
-  PRT_D f3 evalLobe(int i, f3 wo, f3 wi, float& pdf) const
+  PRT_D int flags() const { return hasCoat ? coat.flags(baseFlags) : baseFlags; }
+
+  PRT_D float slotImportance(int k) const
   {
-    (void)wo;
-    return diffuse.eval(fr, wi, pdf);
+    if (k == kSlotOpaque) return opaque.hasSpec ? opaque.spec.importance(opaque.diff.importance()) : opaque.diff.importance();
+    return 1.f;
   }
 
-  PRT_D f3 sampleLobe(int i, f3 wo, float sx, float sy, float sz, f3& wi, float& pdf, int& type) const
+  PRT_D f3 evalSlot(const DevTables& t, int k, f3 wo, f3 wi, float& pdf) const
   {
-    (void)wo;
-    (void)sz;
-    return diffuse.sample(fr, Ng, sx, sy, wi, pdf, type);
+    if (k == kSlotOpaque)
+    {
+      if (opaque.hasSpec)
+      {
+        const DiffuseSub sub{&opaque.diff, &fr, Ng};
+        return opaque.spec.eval(t, sub, fr, Ng, wo, wi, pdf);
+      }
+      return opaque.diff.eval(fr, Ng, wo, wi, pdf);
+    }
+    if (k == kSlotDielectric) return diel.eval(t, fr, Ng, wo, wi, pdf);
+    return cond.eval(t, fr, Ng, wo, wi, pdf);
   }
 
-  // MultiBsdfSimd::eval (bsdf/multi_bsdf.h:173-190).
-  PRT_D f3 eval(f3 wo, f3 wi, float& pdf) const
+  PRT_D f3 sampleSlot(const DevTables& t, int k, f3 wo, float sx, float sy, float sc, f3& wi, float& pdf,
+                      int& type) const
+  {
+    if (k == kSlotOpaque)
+    {
+      if (opaque.hasSpec)
+      {
+        const DiffuseSub sub{&opaque.diff, &fr, Ng};
+        return opaque.spec.sample(t, sub, fr, Ng, wo, sx, sy, sc, wi, pdf, type);
+      }
+      return opaque.diff.sample(fr, Ng, wo, sx, sy, sc, wi, pdf, type);
+    }
+    if (k == kSlotDielectric) return diel.sample(t, fr, Ng, wo, sx, sy, sc, wi, pdf, type);
+    return cond.sample(t, fr, Ng, wo, sx, sy, sc, wi, pdf, type);
+  }
+
+  // MultiBsdfSimd::eval
+  PRT_D f3 evalBase(const DevTables& t, f3 wo, f3 wi, float& pdf) const
   {
     f3 value = mk(0.f);
     pdf = 0.f;
@@ -89,7 +860,7 @@ struct StdBsdf
     {
       if (!(imp[i] > 0.f)) continue;
       float p;
-      const f3 v = evalLobe(i, wo, wi, p);
+      const f3 v = evalSlot(t, kind[i], wo, wi, p);
       value += v * scale[i];
       pdf += p * imp[i];
     }
@@ -97,37 +868,35 @@ struct StdBsdf
     return value;
   }
 
-  // MultiBsdfSimd::sample (bsdf/multi_bsdf.h:192-270).
-  PRT_D f3 sample(f3 wo, float sx, float sy, float sz, f3& wi, float& pdf, int& type) const
+  // MultiBsdfSimd::sample
+  PRT_D f3 sampleBase(const DevTables& t, f3 wo, float sx, float sy, float sc, f3& wi, float& pdf, int& type) const
   {
     pdf = 0.f;
     type = 0;
+    wi = mk(0.f);
     if (!(impSum > 0.f)) return mk(0.f);
-    if (nLobes == 1)
-    {
-      const f3 w = sampleLobe(0, wo, sx, sy, sz, wi, pdf, type);
-      return w * scale[0];
-    }
-    const float x = sz * impSum;
+    if (nLobes == 1) return sampleSlot(t, kind[0], wo, sx, sy, sc, wi, pdf, type) * scale[0];
+    const float x = sc * impSum;
     int choice = 0;
-    float prefix = imp[0], importance = imp[0], sc = scale[0];
+    float prefix = imp[0], importance = imp[0], sc0 = scale[0];
     for (int i = 1; i < nLobes; ++i)
     {
       if (!(x > prefix)) break;
       choice = i;
       prefix += imp[i];
       importance = imp[i];
-      sc = scale[i];
+      sc0 = scale[i];
     }
     const float s1 = (x + importance - prefix) * (1.f / importance);
-    f3 weight = sampleLobe(choice, wo, sx, sy, s1, wi, pdf, type);
+    f3 weight = sampleSlot(t, kind[choice], wo, sx, sy, s1, wi, pdf, type);
     if (!(reduceMax(weight) > 0.f))
     {
       weight = mk(0.f);
       pdf = 0.f;
       type = 0;
+      wi = mk(0.f);
     }
-    weight *= sc;
+    weight *= sc0;
     if (!(reduceMax(weight) > 0.f) || !(pdf > 0.f)) return mk(0.f);
     if (type & kBsdfDelta) return weight * impSum * (1.f / importance);
     f3 value = weight * pdf;
@@ -136,13 +905,42 @@ struct StdBsdf
     {
       if (i == choice || !(imp[i] > 0.f)) continue;
       float p;
-      const f3 v = evalLobe(i, wo, wi, p);
+      const f3 v = evalSlot(t, kind[i], wo, wi, p);
       value += v * scale[i];
       pdf += p * imp[i];
     }
     pdf *= 1.f / impSum;
     return value * (1.f / pdf);
   }
+
+  PRT_D int baseFlagsFn() const { return baseFlags; }
+
+  struct BaseSub
+  {
+    const StdBsdf* b;
+    PRT_D int flags() const { return b->baseFlags; }
+    PRT_D float importance() const { return b->impSum; }
+    PRT_D f3 eval(const DevTables& t, f3 wo, f3 wi, float& pdf) const { return b->evalBase(t, wo, wi, pdf); }
+    PRT_D f3 sample(const DevTables& t, f3 wo, float sx, float sy, float sc, f3& wi, float& pdf, int& type) const
+    {
+      return b->sampleBase(t, wo, sx, sy, sc, wi, pdf, type);
+    }
+  };
+
+  PRT_D f3 eval(const DevTables& t, f3 wo, f3 wi, float& pdf) const
+  {
+    if (hasCoat) return coat.eval(t, BaseSub{this}, fr, Ng, wo, wi, pdf);
+    return evalBase(t, wo, wi, pdf);
+  }
+
+  PRT_D f3 sample(const DevTables& t, f3 wo, float sx, float sy, float sz, f3& wi, float& pdf, int& type) const
+  {
+    if (hasCoat) return coat.sample(t, BaseSub{this}, fr, Ng, wo, sx, sy, sz, wi, pdf, type);
+    return sampleBase(t, wo, sx, sy, sz, wi, pdf, type);
+  }
+
+  PRT_D f3 albedo() const { return albedoV; }
+  PRT_D f3 normal() const { return fr.N; }
 };
 
 // Material texture lookup: repeat in both directions (image/image_texture.h:197-226).
@@ -151,37 +949,89 @@ PRT_D f3 textureRgb(const DevTexture& t, float u, float v)
   return texLookup(t.rgb, t.width, t.height, u, v, true);
 }
 
-// StandardMaterial::getBsdfLobes (material/standard.cpp:410-620), the lobes implemented on
-// the device: Lambertian base without specular, subsurface, coat or sheen layers.
-PRT_D void resolveStandard(const DevScene& sc, const DevMaterial& m, const ShadeCtx& ctx, f3 wo, StdBsdf& b)
+PRT_D void addSlot(StdBsdf& b, int kind, float scale, float importance, int flags)
+{
+  const int i = b.nLobes++;
+  b.kind[i] = kind;
+  b.scale[i] = scale;
+  b.imp[i] = importance * scale;
+  b.impSum += b.imp[i];
+  b.baseFlags |= flags;
+}
+
+// StandardMaterial::getBsdfLobes (material/standard.cpp:410-620) for the lobes the device
+// implements: Lambertian base with an optional specular layer, rough or smooth dielectric
+// transmission, rough or smooth artistic conductor, rough or smooth coat. `backfacing` is the
+// medium-interface orientation (material/material.h:66-76).
+PRT_D void resolveStandard(const DevScene& sc, const DevTables& t, const DevMaterial& m, const ShadeCtx& ctx, f3 wo,
+                           bool backfacing, StdBsdf& b)
 {
   b.fr = makeShadingFrame(ctx, wo);
   b.Ng = ctx.Ng;
-  b.flags = 0;
   b.nLobes = 0;
   b.impSum = 0.f;
+  b.baseFlags = 0;
+  b.hasCoat = false;
+  b.opaque.hasSpec = false;
   const float base = clamp01(m.baseWeight);
   f3 baseColor = mk(m.baseColor[0], m.baseColor[1], m.baseColor[2]);
   if (m.baseColorTex >= 0) baseColor = textureRgb(sc.textures[m.baseColorTex], ctx.uvx, ctx.uvy) * baseColor;
   baseColor = clamp01(baseColor);
   const float metalness = clamp01(m.metalness);
+  const float specular = clamp01(m.specularWeight);
+  const float specularRoughness = clamp01(m.specularRoughness);
+  const bool fromOutside = m.thinWalled ? true : !backfacing;
+  f3 albedo = mk(0.f);
   const float dielectric = 1.f - metalness;
   if (dielectric > kMatEps)
   {
     const float transmission = clamp01(m.transmissionWeight);
+    float eta = fromOutside ? m.ambientIor * (1.f / m.specularIor) : m.specularIor * (1.f / m.ambientIor);
+    eta = fminf(fmaxf(eta, 1.f / 3.f), 3.f);
     const float opaque = dielectric * (1.f - transmission);
     if (opaque > kMatEps)
     {
-      b.diffuse.color = baseColor * base;
-      const int i = b.nLobes++;
-      b.kind[i] = 0;
-      b.scale[i] = opaque;
-      b.imp[i] = b.diffuse.importance() * opaque;
-      b.impSum += b.imp[i];
-      b.flags |= kDiffuseReflection;
+      b.opaque.diff.color = baseColor * base;
+      f3 a = b.opaque.diff.color;
+      int fl = kDiffuseReflection;
+      if (fabsf(m.specularIor - m.ambientIor) > kMatEps && specular > kMatEps)
+      {
+        b.opaque.hasSpec = true;
+        b.opaque.spec.init(t, eta, mk(1.f), 1.f, specularRoughness, m.hasSpecularRoughness != 0, specular);
+        fl = b.opaque.spec.flags(fl);
+        a = b.opaque.spec.albedo(a);
+      }
+      const float impo = b.opaque.hasSpec ? b.opaque.spec.importance(b.opaque.diff.importance()) : b.opaque.diff.importance();
+      addSlot(b, kSlotOpaque, opaque, impo, fl);
+      albedo += a * opaque;
+    }
+    const float translucent = dielectric * transmission * specular;
+    if (translucent > kMatEps)
+    {
+      b.diel.init(t, eta, specularRoughness, m.hasSpecularRoughness != 0);
+      addSlot(b, kSlotDielectric, translucent, 1.f, b.diel.flags());
+      albedo += mk(translucent);
     }
   }
-  b.albedo = b.diffuse.color;
+  const float metal = metalness * specular;
+  if (metal > kMatEps)
+  {
+    const f3 specColor = clamp01(mk(m.specularColor[0], m.specularColor[1], m.specularColor[2]));
+    b.cond.init(t, baseColor * base, specColor, specularRoughness, m.hasSpecularRoughness != 0);
+    addSlot(b, kSlotConductor, metal, 1.f, b.cond.flags());
+    albedo += b.cond.albedo() * metal;
+  }
+  const float coat = clamp01(m.coatWeight);
+  if (coat > kMatEps && fabsf(m.coatIor - m.ambientIor) > kMatEps)
+  {
+    float coatEta = fromOutside ? m.ambientIor * (1.f / m.coatIor) : m.coatIor * (1.f / m.ambientIor);
+    coatEta = fminf(fmaxf(coatEta, 1.f / 3.f), 3.f);
+    const f3 coatColor = clamp01(mk(m.coatColor[0], m.coatColor[1], m.coatColor[2]));
+    b.coat.init(t, coatEta, coatColor, 0.5f, clamp01(m.coatRoughness), m.hasCoatRoughness != 0, coat);
+    b.hasCoat = true;
+    albedo = b.coat.albedo(albedo);
+  }
+  b.albedoV = albedo;
 }
 
 } // namespace prt

@@ -212,9 +212,9 @@ DevMaterial resolveMaterial(const prt_material& m, std::vector<float>& media, in
     }
   }
   // Lobes the device implements: see resolveStandard (bsdf.cuh).
-  const bool unsupported = (d.metalness != 0.f) || (d.specularWeight != 0.f && std::fabs(d.specularIor - 1.f) > 1e-4f) ||
-                           d.transmissionWeight != 0.f || d.subsurfaceWeight != 0.f || d.coatWeight != 0.f ||
-                           d.sheenWeight != 0.f || d.opacity != 1.f || d.hasDiffuseRoughness;
+  const bool unsupported = d.subsurfaceWeight != 0.f || d.sheenWeight != 0.f || d.opacity != 1.f ||
+                           d.hasDiffuseRoughness || (d.thinWalled && d.transmissionWeight != 0.f) ||
+                           (d.transmissionWeight != 0.f && std::fabs(d.specularIor - d.ambientIor) <= 1e-4f);
   if (unsupported && !(d.type & kMatEmissive))
     throw std::invalid_argument("material uses lobes not yet supported by the CUDA device");
   return d;
@@ -588,8 +588,10 @@ int prt_cuda_create(int device_ordinal, prt_context** out_ctx)
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c.smCount, cudaDevAttrMultiProcessorCount, device_ordinal);
   if (e == cudaSuccess) e = cudaMalloc(&c.ps.err, sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMemset(c.ps.err, 0, sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&c.ps.travCounts, 4 * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaEventCreate(&c.ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&c.ev1);
+  if (e == cudaSuccess) e = buildAlbedoTables(c.tables, &c.tableStorage);
   if (e != cudaSuccess)
   {
     delete ctx;
@@ -608,6 +610,8 @@ int prt_cuda_destroy(prt_context* ctx)
   freeFrame(c);
   if (c.ps.counters) cudaFree(c.ps.counters);
   if (c.ps.err) cudaFree(c.ps.err);
+  if (c.ps.travCounts) cudaFree(c.ps.travCounts);
+  if (c.tableStorage) cudaFree(c.tableStorage);
   if (c.ev0) cudaEventDestroy(c.ev0);
   if (c.ev1) cudaEventDestroy(c.ev1);
   if (c.stream) cudaStreamDestroy(c.stream);
@@ -717,8 +721,9 @@ int prt_cuda_render(prt_context* ctx, int32_t spp, prt_render_stats* stats)
     if (spp < 0) throw std::invalid_argument("spp must be >= 0");
     cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
     cuCheck(cudaEventRecord(c.ev0, c.stream), "event");
-    int64_t rays = 0;
-    cuCheck(renderSamples(c, spp, rays), "render");
+    RenderCounters rc;
+    cuCheck(renderSamples(c, spp, rc), "render");
+    const int64_t rays = rc.closestRays + rc.shadowRays;
     cuCheck(cudaEventRecord(c.ev1, c.stream), "event");
     cuCheck(cudaEventSynchronize(c.ev1), "render sync");
     checkDeviceErrors(c);
@@ -730,7 +735,25 @@ int prt_cuda_render(prt_context* ctx, int32_t spp, prt_render_stats* stats)
       stats->spp = spp;
       stats->render_ms = ms;
       stats->mray = ms > 0.f ? (double)rays / 1e6 / (ms * 1e-3) : 0.0;
+      stats->closest_rays = rc.closestRays;
+      stats->shadow_rays = rc.shadowRays;
+      stats->kernel_launches = rc.launches;
+      stats->trace_ms = rc.traceMs;
+      stats->shadow_ms = rc.shadowMs;
+      stats->shade_ms = rc.shadeMs;
+      stats->closest_nodes = (int64_t)rc.trav[0];
+      stats->closest_tris = (int64_t)rc.trav[1];
+      stats->shadow_nodes = (int64_t)rc.trav[2];
+      stats->shadow_tris = (int64_t)rc.trav[3];
     }
+  });
+}
+
+int prt_cuda_set_profiling(prt_context* ctx, int32_t flags)
+{
+  return guarded(ctx, [&](Context& c) {
+    if (flags & ~3) throw std::invalid_argument("unknown profiling flags");
+    c.profileFlags = flags;
   });
 }
 
@@ -876,6 +899,23 @@ int prt_bvh8_count(const float* tri_verts, int64_t tri_count, int64_t n, const f
   {
     return PRT_ERR_LOGIC;
   }
+}
+
+int prt_cuda_bsdf_query(prt_context* ctx, const prt_material* material, int32_t medium_id, int64_t n,
+                        const float* tuples, float* out)
+{
+  return guarded(ctx, [&](Context& c) {
+    if (!material || n < 0 || (n > 0 && (!tuples || !out))) throw std::invalid_argument("invalid BSDF query");
+    if (material->base_color_texture >= 0) throw std::invalid_argument("BSDF queries take untextured materials");
+    std::vector<float> media = {1.f, 1.f, 1.f, 1.f};
+    const DevMaterial m = resolveMaterial(*material, media, 0);
+    if (n == 0) return;
+    Staged in(c, tuples, (size_t)n * 9 * sizeof(float), true);
+    Staged o(c, out, (size_t)n * 13 * sizeof(float), false);
+    cuCheck(launchBsdfQuery(c, m, medium_id, n, (const float*)in.dev, (float*)o.dev), "bsdf query");
+    o.copyOut();
+    cuCheck(cudaStreamSynchronize(c.stream), "bsdf sync");
+  });
 }
 
 } // extern "C"

@@ -124,6 +124,25 @@ struct DevScene
   float sceneRadius;
 };
 
+// BSDF energy-compensation tables (bsdf/albedo_tables.h), computed on the device at context
+// creation (albedo.cu) with the integrators of bsdf/albedo.h; sizes and parameterisations are
+// the reference's.
+struct DevTables
+{
+  const float* ggxDir;        // 32 x 32   (cosThetaO, roughness)
+  const float* ggxAvg;        // 32        (roughness)
+  const float* dielEtaDir;    // 16^3      (cosThetaO, eta in [1/3, 1], roughness)
+  const float* dielEtaAvg;    // 16^2
+  const float* dielRcpDir;    // 16^3      (cosThetaO, eta in [1, 3], roughness)
+  const float* dielRcpAvg;    // 16^2
+  const float* reflDir;       // 16^3      dielectric reflection only, eta in [1/3, 1]
+  const float* reflAvg;       // 16^2
+  const float* reflEcDir;     // 16^3      with multi-scattering (specular-albedo AOV only)
+  const float* reflEcAvg;     // 16^2
+  const float* condEcDir;     // 16^4      (cosThetaO, r, g, roughness) (specular-albedo AOV only)
+  const float* sheenDir;      // 16^2
+};
+
 struct DevCamera
 {
   float org[3];

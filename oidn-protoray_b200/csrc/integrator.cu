@@ -18,6 +18,7 @@
 #include "bsdf.cuh"
 
 #include <algorithm>
+#include <cstring>
 
 namespace prt {
 
@@ -34,6 +35,7 @@ constexpr uint32_t kDimBsdf = 0, kDimLight = 3, kDimTerminate = 6, kDimBounce = 
 struct Launch
 {
   DevScene sc;
+  DevTables tab;
   DevCamera cam;
   DevRenderer rd;
   PathState ps;
@@ -169,6 +171,44 @@ __global__ void kPrimary(DevScene sc, DevCamera cam, int width, int height, uint
   }
 }
 
+// BSDF parity queries in a canonical shading context (see prt_cuda_bsdf_query).
+__global__ void kBsdfQuery(DevTables tab, DevMaterial m, int mediumId, int64_t n, const float* __restrict__ tuples,
+                           float* __restrict__ out)
+{
+  DevScene sc;
+  sc.textures = nullptr;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+  {
+    const float* t = tuples + 9 * i;
+    const f3 wo = mk(t[0], t[1], t[2]), wi = mk(t[3], t[4], t[5]);
+    ShadeCtx ctx;
+    ctx.p = mk(0.f);
+    ctx.eps = 1e-6f;
+    ctx.f.U = mk(1.f, 0.f, 0.f);
+    ctx.f.V = mk(0.f, 1.f, 0.f);
+    ctx.f.N = mk(0.f, 0.f, 1.f);
+    ctx.Ng = ctx.f.N;
+    ctx.uvx = ctx.uvy = 0.5f;
+    ctx.backfacing = false;
+    const bool backfacing = (m.type & kMatMediaInterface) ? mediumId == m.mediumInt : false;
+    StdBsdf b;
+    resolveStandard(sc, tab, m, ctx, wo, backfacing, b);
+    float evalPdf;
+    const f3 ev = b.eval(tab, wo, wi, evalPdf);
+    f3 swi = mk(0.f);
+    float spdf = 0.f;
+    int stype = 0;
+    const f3 sw = b.sample(tab, wo, t[6], t[7], t[8], swi, spdf, stype);
+    float* o = out + 13 * i;
+    o[0] = ev.x; o[1] = ev.y; o[2] = ev.z; o[3] = evalPdf;
+    o[4] = sw.x; o[5] = sw.y; o[6] = sw.z;
+    o[7] = swi.x; o[8] = swi.y; o[9] = swi.z;
+    o[10] = spdf;
+    o[11] = __int_as_float(stype);
+    o[12] = __int_as_float(b.flags());
+  }
+}
+
 // ---- wavefront kernels -----------------------------------------------------------------------
 
 // Path initialisation (render/path_renderer_stream.h:209-262).
@@ -203,39 +243,61 @@ __global__ void kRaygen(Launch L)
   }
 }
 
+// Adds one warp's traversal counts to the global totals (counting variant only).
+PRT_D void addCounts(unsigned long long* dst, const TraceCount& c)
+{
+  unsigned long long n = (unsigned long long)c.nodes, t = (unsigned long long)c.tris;
+  for (int o = 16; o > 0; o >>= 1)
+  {
+    n += __shfl_down_sync(0xffffffffu, n, o);
+    t += __shfl_down_sync(0xffffffffu, t, o);
+  }
+  if (laneId() == 0)
+  {
+    atomicAdd(dst, n);
+    atomicAdd(dst + 1, t);
+  }
+}
+
 // Closest-hit traversal of the queued rays; persistent warps take 32 rays at a time.
+template <bool Count>
 __global__ void __launch_bounds__(256) kTrace(Launch L, const int* __restrict__ queue, const int* __restrict__ count,
                                               int* __restrict__ work)
 {
   const int n = *count;
+  TraceCount tc;
   for (;;)
   {
     int base = 0;
     if (laneId() == 0) base = atomicAdd(work, 32);
     base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= n) return;
+    if (base >= n) break;
     const int i = base + laneId();
     if (i < n)
     {
       const int p = queue ? __ldg(queue + i) : i;
       const float4 a = L.ps.rayO[p], b = L.ps.rayD[p];
-      const TraceHit h = traverse<false>(L.sc.nodes, L.sc.tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w, L.ps.err);
+      const TraceHit h = traverse<false, Count>(L.sc.nodes, L.sc.tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w,
+                                                L.ps.err, &tc);
       L.ps.hit[p] = make_float4(h.t, h.u, h.v, __int_as_float(h.triId));
     }
   }
+  if (Count) addCounts(L.ps.travCounts, tc);
 }
 
 // Any-hit test of the queued shadow rays; adds the unoccluded NEE contribution and
 // finishes paths that ended at this bounce (render/path_renderer_stream.h:953-1010).
+template <bool Count>
 __global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__ count, int* __restrict__ work)
 {
   const int n = *count;
+  TraceCount tc;
   for (;;)
   {
     int base = 0;
     if (laneId() == 0) base = atomicAdd(work, 32);
     base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= n) return;
+    if (base >= n) break;
     const int i = base + laneId();
     if (i < n)
     {
@@ -245,7 +307,8 @@ __global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__
       bool unoccluded = b.w > 0.f;
       if (unoccluded)
       {
-        const TraceHit h = traverse<true>(L.sc.nodes, L.sc.tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w, L.ps.err);
+        const TraceHit h = traverse<true, Count>(L.sc.nodes, L.sc.tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w,
+                                                 L.ps.err, &tc);
         unoccluded = h.triId < 0;
       }
       float4 r = L.ps.rad[p];
@@ -263,6 +326,7 @@ __global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__
       }
     }
   }
+  if (Count) addCounts(L.ps.travCounts + 2, tc);
 }
 
 PRT_D void finishPath(const Launch& L, int p, f3 rad)
@@ -346,13 +410,23 @@ __global__ void __launch_bounds__(256) kShade(Launch L, const int* __restrict__ 
           ShadeCtx ctx;
           postIntersect(L.sc, org, dir, hh.x, triId, hh.y, hh.z, ctx);
           const f3 wo = -dir;
+          uint32_t mediumId = info.z & 0xffffu;
+          // Material::getBsdf orientation: media interfaces take it from the medium the path
+          // is in, every other material is treated as front-facing (material/material.h:66-76).
+          const bool backfacing = (mat.type & kMatMediaInterface) ? (int)mediumId == mat.mediumInt : false;
           StdBsdf bsdf;
-          resolveStandard(L.sc, mat, ctx, wo, bsdf);
+          resolveStandard(L.sc, L.tab, mat, ctx, wo, backfacing, bsdf);
           const SobolState st = sobolSetSample(L.rd.seed, info.y, pixelId & kPixelIdMask);
           const bool aov2 = (pixelId & kPathAov2Flag) == 0u;
           const bool rr = !(aov1 || aov2);
+          // Volume transmission (Beer's law) inside a medium.
+          if (mediumId > 0u)
+          {
+            const f3 mc = ld3(L.sc.mediaColor + 3 * mediumId);
+            T *= powf3(mc, hh.x);
+          }
           // Direct light (NEE)
-          if (bsdf.flags & kBsdfSmooth)
+          if (bsdf.flags() & kBsdfSmooth)
           {
             float lx, ly, lz;
             sobolGet3D(st, sampleDim + kDimLight, lx, ly, lz);
@@ -362,7 +436,7 @@ __global__ void __launch_bounds__(256) kShade(Launch L, const int* __restrict__ 
             if (reduceMax(Lw) > 0.f && lightPdf > 0.f)
             {
               float bsdfPdf;
-              const f3 bv = bsdf.eval(wo, wi, bsdfPdf);
+              const f3 bv = bsdf.eval(L.tab, wo, wi, bsdfPdf);
               if (reduceMax(bv) > 0.f)
               {
                 const f3 dirT = T * bv;
@@ -385,15 +459,16 @@ __global__ void __launch_bounds__(256) kShade(Launch L, const int* __restrict__ 
           f3 wi;
           float bsdfPdf;
           int bsdfType;
-          const f3 bw = bsdf.sample(wo, bx, by, bz, wi, bsdfPdf, bsdfType);
+          const f3 bw = bsdf.sample(L.tab, wo, bx, by, bz, wi, bsdfPdf, bsdfType);
           extend = reduceMax(bw) > 0.f && bsdfPdf > 0.f;
           const int extType = extend ? bsdfType : 0;
           if (aov1)
           {
             if (L.aovMask)
             {
-              L.ps.aovA[p] = make_float4(bsdf.albedo.x, bsdf.albedo.y, bsdf.albedo.z, 1.f);
-              L.ps.aovN[p] = make_float4(bsdf.fr.N.x, bsdf.fr.N.y, bsdf.fr.N.z, 1.f);
+              const f3 a = bsdf.albedo(), nn = bsdf.normal();
+              L.ps.aovA[p] = make_float4(a.x, a.y, a.z, 1.f);
+              L.ps.aovN[p] = make_float4(nn.x, nn.y, nn.z, 1.f);
             }
             pixelId |= kPathAov1Flag;
           }
@@ -414,6 +489,10 @@ __global__ void __launch_bounds__(256) kShade(Launch L, const int* __restrict__ 
             const bool update = (bsdfType & kBsdfContinuation) == 0;
             L.ps.thr[p] = make_float4(T.x, T.y, T.z, update ? bsdfPdf : lastPdf);
             ra.w = __int_as_float(update ? bsdfType : lastType);
+            // Material::nextMedium (material/material.h:84-93).
+            if ((mat.type & kMatMediaInterface) && dot(wo, ctx.Ng) * dot(wi, ctx.Ng) < 0.f)
+              mediumId = (int)mediumId == mat.mediumInt ? (uint32_t)mat.mediumExt : (uint32_t)mat.mediumInt;
+            info.z = mediumId;
           }
           info.x = pixelId;
           L.ps.info[p] = info;
@@ -532,6 +611,12 @@ cudaError_t launchPrimary(Context& ctx, uint32_t sampleIndex, float* raysOut, in
   return cudaGetLastError();
 }
 
+cudaError_t launchBsdfQuery(Context& ctx, const DevMaterial& m, int mediumId, int64_t n, const float* tuples, float* out)
+{
+  kBsdfQuery<<<gridFor(ctx, n, 128), 128, 0, ctx.stream>>>(ctx.tables, m, mediumId, n, tuples, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launchBlit(Context& ctx, int aov, float* dst)
 {
   const int n = ctx.width * ctx.height;
@@ -549,20 +634,45 @@ cudaError_t launchClear(Context& ctx)
   return e;
 }
 
-cudaError_t renderSamples(Context& ctx, int spp, int64_t& rays)
+// Event pair recorded around one launch when kernel timing is on.
+struct TimedLaunch
 {
-  rays = 0;
+  cudaEvent_t a, b;
+  int kind;  // 0 trace, 1 shadow, 2 shade
+};
+
+cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
+{
+  rc = RenderCounters();
   const int pixelCount = ctx.width * ctx.height;
   const int maxDepth = ctx.renderer.maxDepth;
-  int* counts = ctx.ps.counters;  // [2*d]: input count of bounce d, [2*d+1]: shadow count; work counters after
+  int* counts = ctx.ps.counters;  // [2*d]: input count of bounce d, [2*d+1]: its shadow count
   const int countSlots = 2 * (maxDepth + 2);
   int* work = counts + countSlots;
-  std::vector<int> hostCounts(countSlots);
+  const bool timing = (ctx.profileFlags & 1) != 0;
+  const bool counting = (ctx.profileFlags & 2) != 0;
+  std::vector<TimedLaunch> timed;
+  auto begin = [&](int kind) {
+    if (!timing) return;
+    TimedLaunch t;
+    cudaEventCreate(&t.a);
+    cudaEventCreate(&t.b);
+    t.kind = kind;
+    cudaEventRecord(t.a, ctx.stream);
+    timed.push_back(t);
+  };
+  auto end = [&]() {
+    if (timing) cudaEventRecord(timed.back().b, ctx.stream);
+  };
+  cudaError_t e = cudaSuccess;
+  if (counting) e = cudaMemsetAsync(ctx.ps.travCounts, 0, 4 * sizeof(unsigned long long), ctx.stream);
+  if (e != cudaSuccess) return e;
   for (int done = 0; done < spp;)
   {
     const int S = std::min(ctx.waveSamples, spp - done);
     Launch L;
     L.sc = ctx.scene;
+    L.tab = ctx.tables;
     L.cam = ctx.camera;
     L.rd = ctx.renderer;
     L.ps = ctx.ps;
@@ -573,21 +683,35 @@ cudaError_t renderSamples(Context& ctx, int spp, int64_t& rays)
     L.samples = S;
     L.aovMask = ctx.aovMask;
     const int P = pixelCount * S;
-    cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(int) * 2 * countSlots, ctx.stream);
+    e = cudaMemsetAsync(counts, 0, sizeof(int) * 2 * countSlots, ctx.stream);
     if (e != cudaSuccess) return e;
     e = cudaMemcpyAsync(counts, &P, sizeof(int), cudaMemcpyHostToDevice, ctx.stream);
     if (e != cudaSuccess) return e;
     kRaygen<<<gridFor(ctx, P), 256, 0, ctx.stream>>>(L);
+    rc.launches++;
     const int persistent = ctx.smCount * 8;
     int cur = 0;
     for (int depth = 0; depth <= maxDepth; ++depth)
     {
       const int* q = depth == 0 ? nullptr : ctx.ps.queue[cur];
       int* qOut = ctx.ps.queue[cur ^ 1];
-      kTrace<<<persistent, 256, 0, ctx.stream>>>(L, q, counts + 2 * depth, work + 2 * depth);
+      begin(0);
+      if (counting)
+        kTrace<true><<<persistent, 256, 0, ctx.stream>>>(L, q, counts + 2 * depth, work + 2 * depth);
+      else
+        kTrace<false><<<persistent, 256, 0, ctx.stream>>>(L, q, counts + 2 * depth, work + 2 * depth);
+      end();
+      begin(2);
       kShade<<<gridFor(ctx, P), 256, 0, ctx.stream>>>(L, q, counts + 2 * depth, depth, qOut, counts + 2 * (depth + 1),
                                                        counts + 2 * depth + 1);
-      kShadow<<<persistent, 256, 0, ctx.stream>>>(L, counts + 2 * depth + 1, work + 2 * depth + 1);
+      end();
+      begin(1);
+      if (counting)
+        kShadow<true><<<persistent, 256, 0, ctx.stream>>>(L, counts + 2 * depth + 1, work + 2 * depth + 1);
+      else
+        kShadow<false><<<persistent, 256, 0, ctx.stream>>>(L, counts + 2 * depth + 1, work + 2 * depth + 1);
+      end();
+      rc.launches += 3;
       e = cudaGetLastError();
       if (e != cudaSuccess) return e;
       cur ^= 1;
@@ -597,17 +721,37 @@ cudaError_t renderSamples(Context& ctx, int spp, int64_t& rays)
       if (e != cudaSuccess) return e;
       e = cudaStreamSynchronize(ctx.stream);
       if (e != cudaSuccess) return e;
-      rays += (int64_t)cnt[0] + cnt[1];
+      rc.closestRays += cnt[0];
+      rc.shadowRays += cnt[1];
       if (cnt[2] == 0) break;
     }
     kAccumulate<<<gridFor(ctx, pixelCount), 256, 0, ctx.stream>>>(L, reinterpret_cast<float4*>(ctx.accum),
                                                                    reinterpret_cast<float4*>(ctx.accumA),
                                                                    reinterpret_cast<float4*>(ctx.accumN));
+    rc.launches++;
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     done += S;
   }
   ctx.sampleIndex += (uint32_t)spp;
+  if (timing || counting)
+  {
+    e = cudaStreamSynchronize(ctx.stream);
+    if (e != cudaSuccess) return e;
+  }
+  for (auto& t : timed)
+  {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t.a, t.b);
+    (t.kind == 0 ? rc.traceMs : t.kind == 1 ? rc.shadowMs : rc.shadeMs) += ms;
+    cudaEventDestroy(t.a);
+    cudaEventDestroy(t.b);
+  }
+  if (counting)
+  {
+    e = cudaMemcpy(rc.trav, ctx.ps.travCounts, sizeof(rc.trav), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return e;
+  }
   return cudaSuccess;
 }
 

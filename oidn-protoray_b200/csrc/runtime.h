@@ -37,7 +37,8 @@ struct PathState
   float4* aovA = nullptr;   // first-hit albedo per path (w = 1 when written)
   float4* aovN = nullptr;   // first-hit normal per path
   int* queue[2] = {nullptr, nullptr};
-  int* counters = nullptr;  // [0] extension count, [1] shadow count, [2] trace work, [3] shadow work
+  int* counters = nullptr;  // per bounce: input and shadow counts, then the work counters
+  unsigned long long* travCounts = nullptr;  // closest nodes, closest tris, shadow nodes, shadow tris
   uint32_t* err = nullptr;
 };
 
@@ -64,6 +65,17 @@ struct Context
   PathState ps;
   int waveSamples = 0;            // samples per pixel per wave
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  DevTables tables{};             // energy-compensation tables (albedo.cu)
+  float* tableStorage = nullptr;
+  int profileFlags = 0;
+};
+
+// Per-call statistics gathered by renderSamples.
+struct RenderCounters
+{
+  int64_t closestRays = 0, shadowRays = 0, launches = 0;
+  double traceMs = 0.0, shadowMs = 0.0, shadeMs = 0.0;
+  unsigned long long trav[4] = {0, 0, 0, 0};
 };
 
 // Kernel launchers (integrator.cu). All are asynchronous on ctx.stream.
@@ -75,8 +87,11 @@ cudaError_t launchOccluded(Context& ctx, int64_t n, const float* rays, int32_t* 
 cudaError_t launchPrimary(Context& ctx, uint32_t sampleIndex, float* raysOut, int32_t* triOut, float* t);
 // Renders samples [ctx.sampleIndex, ctx.sampleIndex + spp) and accumulates them; returns the
 // number of closest + shadow rays traced.
-cudaError_t renderSamples(Context& ctx, int spp, int64_t& rays);
+cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc);
 cudaError_t launchBlit(Context& ctx, int aov, float* dst);
 cudaError_t launchClear(Context& ctx);
+cudaError_t launchBsdfQuery(Context& ctx, const DevMaterial& m, int mediumId, int64_t n, const float* tuples, float* out);
+// Builds the BSDF energy-compensation tables on the current device (albedo.cu).
+cudaError_t buildAlbedoTables(DevTables& t, float** storage);
 
 } // namespace prt

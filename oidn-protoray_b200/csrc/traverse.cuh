@@ -132,9 +132,16 @@ PRT_D void intersectNode(const uint4* __restrict__ nodes, uint32_t nodeIdx, cons
   tgroup = make_uint2(triBase, tri);
 }
 
-template <bool AnyHit>
+// Node visits and triangle tests of one ray (counting variant only).
+struct TraceCount
+{
+  int nodes = 0;
+  int tris = 0;
+};
+
+template <bool AnyHit, bool Count = false>
 PRT_D TraceHit traverse(const uint4* __restrict__ nodes, const float4* __restrict__ tris, f3 o, f3 d,
-                        float tnear, float tfar, uint32_t* errFlag)
+                        float tnear, float tfar, uint32_t* errFlag, TraceCount* count = nullptr)
 {
   TraceHit h;
   h.triId = -1;
@@ -152,6 +159,7 @@ PRT_D TraceHit traverse(const uint4* __restrict__ nodes, const float4* __restric
     {
       const int bit = __ffs(tgroup.y) - 1;
       tgroup.y &= tgroup.y - 1u;
+      if (Count) count->tris++;
       float t, u, v;
       int id;
       if (intersectTriFx(tris, tgroup.x + bit, o, d, tnear, h.t, t, u, v, id))
@@ -190,6 +198,7 @@ PRT_D TraceHit traverse(const uint4* __restrict__ nodes, const float4* __restric
       }
       stack[sp++] = ngroup;
     }
+    if (Count) count->nodes++;
     intersectNode(nodes, nodeIdx, r, tnear, h.t, ngroup, tgroup);
   }
   atomicOr(errFlag, kErrIterCap);

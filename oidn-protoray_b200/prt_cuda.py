@@ -53,6 +53,7 @@ def load_library():
     lib.prt_cuda_frame.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32]
     lib.prt_cuda_clear.argtypes = [vp]
     lib.prt_cuda_render.argtypes = [vp, C.c_int32, P(T.RenderStats)]
+    lib.prt_cuda_set_profiling.argtypes = [vp, C.c_int32]
     lib.prt_cuda_blit.argtypes = [vp, C.c_int32, P(C.c_float)]
     lib.prt_cuda_sobol.argtypes = [vp, C.c_int64, P(C.c_uint32), P(C.c_uint32), P(C.c_uint32), C.c_int32,
                                    P(C.c_float)]
@@ -60,6 +61,7 @@ def load_library():
                                    P(C.c_float), P(C.c_float)]
     lib.prt_cuda_occluded.argtypes = [vp, C.c_int64, P(C.c_float), P(C.c_int32)]
     lib.prt_cuda_query_primary.argtypes = [vp, C.c_uint32, P(C.c_float), P(C.c_int32), P(C.c_int32), P(C.c_float)]
+    lib.prt_cuda_bsdf_query.argtypes = [vp, P(T.Material), C.c_int32, C.c_int64, P(C.c_float), P(C.c_float)]
     lib.prt_bvh8_count.argtypes = [P(C.c_float), C.c_int64, C.c_int64, P(C.c_float), P(C.c_int32), P(C.c_float),
                                    P(C.c_int64), P(C.c_int64), P(C.c_int64)]
     _lib = lib
@@ -148,7 +150,10 @@ class DeviceCuda:
     def render(self, spp=1):
         st = T.RenderStats()
         self._check(self.lib.prt_cuda_render(self.h, spp, C.byref(st)))
-        return dict(mray=st.mray, rays=st.rays, spp=st.spp, render_ms=st.render_ms)
+        return {name: getattr(st, name) for name, _ in T.RenderStats._fields_}
+
+    def set_profiling(self, flags):
+        self._check(self.lib.prt_cuda_set_profiling(self.h, flags))
 
     def blit_frame(self, aov=T.PRT_BLIT_HDR, out=None):
         """Returns (height, width, 3) float32; `out` may be a CUDA torch tensor (zero copy)."""
@@ -188,6 +193,14 @@ class DeviceCuda:
         self._check(self.lib.prt_cuda_trace(self.h, n, T.fptr(rays), T.iptr(g), T.iptr(p), T.fptr(t), T.fptr(u),
                                             T.fptr(v)))
         return g, p, t, u, v
+
+    def bsdf_query(self, material, tuples, medium_id=0):
+        """(n, 13) float32: eval value, eval pdf, sample weight, sampled wi, sample pdf, type, flags."""
+        t = np.ascontiguousarray(tuples, np.float32).reshape(-1, 9)
+        out = np.zeros((t.shape[0], 13), np.float32)
+        self._check(self.lib.prt_cuda_bsdf_query(self.h, C.byref(material), medium_id, t.shape[0], T.fptr(t),
+                                                 T.fptr(out)))
+        return out
 
     def occluded(self, rays):
         rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)

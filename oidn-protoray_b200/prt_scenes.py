@@ -15,6 +15,7 @@ A Scene keeps every numpy array alive for as long as its ctypes descriptor is in
 """
 import ctypes as C
 import math
+import pathlib
 
 import numpy as np
 
@@ -67,7 +68,9 @@ class Scene:
         return sum(m["indices"].shape[0] for m in self.meshes)
 
     # -- C ABI ----------------------------------------------------------------------------
-    def desc(self):
+    def desc(self, oracle=False):
+        """The C-ABI scene descriptor. With oracle=True and a sun-sky light, the sun/sky
+        products are left out: the reference builds them itself from `sunsky`."""
         meshes = (T.Mesh * len(self.meshes))()
         for i, m in enumerate(self.meshes):
             meshes[i].positions = T.fptr(m["positions"])
@@ -91,6 +94,9 @@ class Scene:
         d.texture_count = len(self.textures)
         d.env = self.env
         d.env.image_rgb = T.fptr(self.env_image)
+        if oracle and self.sunsky is not None:
+            d.env.distant_color[:] = (0.0, 0.0, 0.0)
+            d.env.image_rgb = None
         self._keep = [meshes, mats, texs]
         return d
 
@@ -188,4 +194,114 @@ def cornell(seed=0, width=256, height=256, spp=16, max_depth=5, n_spheres=32, sp
         s.add_mesh(sv * r + c, sf, m, normals=sv)
     s.camera = look_at((0.0, 1.0, 3.4), (0.0, 1.0, 0.0), fov_deg=40.0)
     s.width, s.height, s.spp, s.max_depth, s.rr_depth = width, height, spp, max_depth, 8
+    return s
+
+
+# ---- large plain-render scene: fBm terrain + icospheres under a sun-sky ----------------------
+
+SUNSKY_FIXTURE = pathlib.Path(__file__).resolve().parent.parent / "tests" / "golden" / "sunsky_t3_e30.npz"
+SUN_ELEVATION_DEG = 30.0
+SUN_AZIMUTH_DEG = 45.0
+SUN_TURBIDITY = 3.0
+SUN_GROUND_ALBEDO = 0.2
+
+
+def sun_direction(elevation_deg=SUN_ELEVATION_DEG, azimuth_deg=SUN_AZIMUTH_DEG):
+    """Unit vector toward the sun; y is up (light/sun_sky_light.cpp:34-36 uses acos(dir.y))."""
+    el, az = math.radians(elevation_deg), math.radians(azimuth_deg)
+    return np.array([math.cos(el) * math.sin(az), math.sin(el), -math.cos(el) * math.cos(az)], np.float32)
+
+
+def value_noise_fbm(x, z, rng_seed, octaves=8, lacunarity=2.0, gain=0.5, base_freq=4.0, lattice=256):
+    """Seeded value-noise fBm in [-1, 1]-ish, vectorised over arrays x, z in [0, 1]."""
+    rng = np.random.default_rng(rng_seed)
+    table = rng.uniform(-1.0, 1.0, (lattice, lattice)).astype(np.float64)
+    total = np.zeros_like(x, dtype=np.float64)
+    amp, freq = 1.0, base_freq
+    for o in range(octaves):
+        px = x * freq + o * 17.31
+        pz = z * freq + o * 9.73
+        ix, iz = np.floor(px).astype(np.int64), np.floor(pz).astype(np.int64)
+        fx, fz = px - ix, pz - iz
+        sx, sz = fx * fx * (3 - 2 * fx), fz * fz * (3 - 2 * fz)
+        a = table[ix % lattice, iz % lattice]
+        b = table[(ix + 1) % lattice, iz % lattice]
+        c = table[ix % lattice, (iz + 1) % lattice]
+        d = table[(ix + 1) % lattice, (iz + 1) % lattice]
+        total += amp * ((a * (1 - sx) + b * sx) * (1 - sz) + (c * (1 - sx) + d * sx) * sz)
+        amp *= gain
+        freq *= lacunarity
+    return total
+
+
+def load_sunsky():
+    """Sun (radiance, angular diameter) and sky image of the reference's sun-sky model for the
+    terrain's sun, produced by the oracle (tests/golden/make_golden.py)."""
+    z = np.load(SUNSKY_FIXTURE)
+    return z["sun_color"], float(z["sun_angle"]), z["sky"]
+
+
+def terrain(seed=0, grid=1024, n_spheres=400, sphere_subdiv=3, width=1920, height=1080, spp=64, max_depth=8,
+            rr_depth=3, extent=50.0, relief=10.0, with_sky=True):
+    """The large plain-render scene: grid^2 fBm heightfield (2 (grid-1)^2 triangles) plus
+    n_spheres icospheres; spheres get one of four materials uniformly at random."""
+    rng = np.random.default_rng(seed)
+    s = Scene()
+    # Heightfield over [-extent, extent]^2 in xz, UVs = grid coordinates in [0, 1].
+    u = np.linspace(0.0, 1.0, grid)
+    U, V = np.meshgrid(u, u, indexing="xy")
+    H = value_noise_fbm(U, V, seed) * relief
+    X = (U * 2.0 - 1.0) * extent
+    Z = (V * 2.0 - 1.0) * extent
+    pos = np.stack([X, H, Z], -1).reshape(-1, 3).astype(np.float32)
+    # Smooth vertex normals from central differences of the height.
+    dx = 2.0 * extent / (grid - 1)
+    gx = np.gradient(H, dx, axis=1)
+    gz = np.gradient(H, dx, axis=0)
+    nrm = np.stack([-gx, np.ones_like(H), -gz], -1)
+    nrm /= np.linalg.norm(nrm, axis=-1, keepdims=True)
+    i = np.arange(grid - 1)
+    I, J = np.meshgrid(i, i, indexing="xy")
+    v00 = (J * grid + I).ravel()
+    v10 = v00 + 1
+    v01 = v00 + grid
+    v11 = v01 + 1
+    # Counter-clockwise seen from +y.
+    tris = np.concatenate([np.stack([v00, v01, v10], 1), np.stack([v10, v01, v11], 1)]).astype(np.int32)
+    ground = s.add_material(T.material(base_color=(0.45, 0.42, 0.36), specular_weight=0.0))
+    uvs = np.stack([U, V], -1).reshape(-1, 2).astype(np.float32)
+    s.add_mesh(pos, tris, ground, normals=nrm.reshape(-1, 3).astype(np.float32), texcoords=uvs)
+    # Spheres resting on the terrain.
+    sv, sf = icosphere(sphere_subdiv)
+    gold_r = (1.0, 0.766, 0.336)   # reflectivity (F0) of gold
+    gold_g = (1.0, 0.95, 0.75)     # edge tint
+    for _ in range(n_spheres):
+        r = rng.uniform(0.3, 1.5)
+        cx, cz = rng.uniform(-0.9 * extent, 0.9 * extent, 2)
+        hy = float(value_noise_fbm(np.array([(cx / extent + 1) / 2]), np.array([(cz / extent + 1) / 2]), seed)[0] * relief)
+        kind = int(rng.integers(0, 4))
+        if kind == 0:
+            m = T.material(base_color=rng.uniform(0.1, 0.9, 3), specular_weight=0.0)
+        elif kind == 1:
+            m = T.material(metalness=1.0, base_color=gold_r, specular_color=gold_g,
+                           specular_roughness=rng.uniform(0.05, 0.5))
+        elif kind == 2:
+            m = T.material(transmission_weight=1.0, specular_ior=1.5, specular_roughness=rng.uniform(0.0, 0.3))
+        else:
+            m = T.material(base_color=rng.uniform(0.1, 0.9, 3), specular_weight=0.0, coat_weight=1.0,
+                           coat_roughness=rng.uniform(0.05, 0.5))
+        mid = s.add_material(m)
+        s.add_mesh(sv * r + np.array([cx, hy + r * 0.9, cz]), sf, mid, normals=sv)
+    # Sun-sky light: the reference computes it from (direction, turbidity, albedo); the device
+    # takes its two products, the sun as a distant light and the sky as an image light.
+    d = sun_direction()
+    s.sunsky = np.array([d[0], d[1], d[2], SUN_TURBIDITY, SUN_GROUND_ALBEDO], np.float32)
+    if with_sky:
+        sun_color, sun_angle, sky = load_sunsky()
+        s.env.distant_color[:] = tuple(float(c) for c in sun_color)
+        s.env.distant_dir[:] = tuple(float(c) for c in d)
+        s.env.distant_angle = sun_angle
+        s.set_env_image(sky, lut_size=128)
+    s.camera = look_at((0.0, 28.0, 62.0), (0.0, 0.0, -5.0), fov_deg=45.0)
+    s.width, s.height, s.spp, s.max_depth, s.rr_depth = width, height, spp, max_depth, rr_depth
     return s

@@ -166,7 +166,21 @@ class RenderStats(C.Structure):
         ("rays", C.c_int64),
         ("spp", C.c_int64),
         ("render_ms", C.c_double),
+        ("closest_rays", C.c_int64),
+        ("shadow_rays", C.c_int64),
+        ("kernel_launches", C.c_int64),
+        ("trace_ms", C.c_double),
+        ("shadow_ms", C.c_double),
+        ("shade_ms", C.c_double),
+        ("closest_nodes", C.c_int64),
+        ("closest_tris", C.c_int64),
+        ("shadow_nodes", C.c_int64),
+        ("shadow_tris", C.c_int64),
     ]
+
+
+PRT_PROFILE_KERNELS = 1 << 0
+PRT_PROFILE_COUNTS = 1 << 1
 
 
 def fptr(a):

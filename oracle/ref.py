@@ -65,6 +65,34 @@ def _check(rc):
         raise RuntimeError("oracle: " + _lib().ref_last_error().decode())
 
 
+def sunsky(direction, turbidity, albedo):
+    """The reference's sun-sky products: (sun radiance, sun angular diameter, sky image)."""
+    lib = _lib()
+    P = C.POINTER(C.c_float)
+    d = np.ascontiguousarray(direction, np.float32)
+    sun = np.zeros(3, np.float32)
+    ang = C.c_float()
+    w, h = C.c_int(), C.c_int()
+    lib.ref_sunsky.argtypes = [P, C.c_float, C.c_float, P, P, P, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    _check(lib.ref_sunsky(T.fptr(d), turbidity, albedo, T.fptr(sun), C.byref(ang), None, C.byref(w), C.byref(h)))
+    sky = np.zeros((h.value, w.value, 3), np.float32)
+    _check(lib.ref_sunsky(T.fptr(d), turbidity, albedo, T.fptr(sun), C.byref(ang), T.fptr(sky), C.byref(w),
+                          C.byref(h)))
+    return sun, ang.value, sky
+
+
+def bsdf_query(material, tuples, medium_id=0):
+    """The reference's Standard material BSDF on (wo, wi, sample) tuples: (n, 13) float32."""
+    lib = _lib()
+    t = np.ascontiguousarray(tuples, np.float32).reshape(-1, 9)
+    out = np.zeros((t.shape[0], 13), np.float32)
+    lib.ref_bsdf_query.argtypes = [C.POINTER(T.Material), C.c_int, C.c_int64, C.POINTER(C.c_float),
+                                   C.POINTER(C.c_float)]
+    if lib.ref_bsdf_query(C.byref(material), medium_id, t.shape[0], T.fptr(t), T.fptr(out)) != 0:
+        raise RuntimeError("oracle BSDF query failed")
+    return out
+
+
 def hardware_threads():
     return _lib().ref_hardware_threads()
 
@@ -87,7 +115,7 @@ class RefDevice:
 
     def __init__(self, scene, seed=0, aov_mask=0, sunsky=None):
         self.scene = scene
-        self.desc = scene.desc()
+        self.desc = scene.desc(oracle=True)
         self.rdesc = scene.renderer_desc()
         self.tmp = tempfile.TemporaryDirectory(prefix="prt_oracle_")
         ss = None

@@ -1,3 +1,127 @@
 // Test infrastructure (oracle only): batched BSDF queries through the reference's own
-// BsdfSimd classes. Filled in with the BSDF parity tuples.
+// Standard material (material/standard.cpp:410-620) and BsdfSimd classes.
+//
+// Each query is a (wo, wi, 3D sample) tuple in a canonical shading context: the shading
+// frame is the identity (U = x, V = y, N = z), the geometric normal is z, UV = (0.5, 0.5),
+// the hit is front-facing and the path is in medium `mediumId`. For each tuple the output is
+//   eval value (3), eval pdf, sample weight (3), sampled wi (3), sample pdf, sample type,
+//   BSDF flags                                                        -> 13 floats
+// computed with Material::getBsdf (material/material.h:66-76) then BsdfSimd::eval / ::sample,
+// eight lanes at a time exactly as the stream renderer calls them.
+#define RKSCENE_FLOAT2   prt::Vec2f
+#define RKSCENE_FLOAT3   prt::Vec3f
+#define RKSCENE_FLOAT4   prt::Vec4f
+#define RKSCENE_FLOAT3X4 prt::Affine3f
+
+#include <cstring>
+#include <memory>
+#include <string>
+
 #include "bsdf/albedo_tables.h"
+#include "material/material_factory.h"
+#include "material/material.h"
+#include "core/shading_context.h"
+#include "bsdf/bsdf.h"
+
+#include "../include/prt_cuda.h"
+
+using namespace prt;
+
+namespace {
+
+Props standardProps(const prt_material& m)
+{
+  // The keys Scene::loadScene sets for an rkscene material (render/scene.cpp:180-212).
+  Props p;
+  auto v3 = [](const float* a) { return Vec3f(a[0], a[1], a[2]); };
+  p.set("type", "Standard");
+  p.set("baseWeight", m.base_weight);
+  p.set("baseColor", v3(m.base_color));
+  p.set("metalness", m.metalness);
+  p.set("diffuseRoughness", m.diffuse_roughness);
+  p.set("specularWeight", m.specular_weight);
+  p.set("specularColor", v3(m.specular_color));
+  p.set("specularRoughness", m.specular_roughness);
+  p.set("specularIOR", m.specular_ior);
+  p.set("transmissionWeight", m.transmission_weight);
+  p.set("transmissionColor", v3(m.transmission_color));
+  p.set("transmissionDepth", m.transmission_depth);
+  p.set("subsurfaceWeight", m.subsurface_weight);
+  p.set("subsurfaceColor", v3(m.subsurface_color));
+  p.set("subsurfaceAnisotropy", m.subsurface_anisotropy);
+  p.set("coatWeight", m.coat_weight);
+  p.set("coatColor", v3(m.coat_color));
+  p.set("coatRoughness", m.coat_roughness);
+  p.set("coatIOR", m.coat_ior);
+  p.set("sheenWeight", m.sheen_weight);
+  p.set("sheenColor", v3(m.sheen_color));
+  p.set("sheenRoughness", m.sheen_roughness);
+  p.set("emissionLuminance", m.emission_luminance);
+  p.set("emissionColor", v3(m.emission_color));
+  p.set("thinWalled", m.thin_walled);
+  p.set("opacity", m.opacity);
+  return p;
+}
+
+} // namespace
+
+extern "C" {
+
+int ref_bsdf_query(const prt_material* mat, int mediumId, int64_t n, const float* tuples, float* out)
+{
+  try
+  {
+    precomputeAlbedoTables();
+    MaterialFactory factory("", Props());
+    std::shared_ptr<Material> material = factory.make(standardProps(*mat));
+    for (int64_t base = 0; base < n; base += simdSize)
+    {
+      const int lanes = (int)std::min<int64_t>(simdSize, n - base);
+      vbool m = vint(step) < lanes;
+      Vec3vf wo, wi, s;
+      for (int k = 0; k < simdSize; ++k)
+      {
+        const float* t = tuples + 9 * (base + std::min(k, lanes - 1));
+        wo.x[k] = t[0]; wo.y[k] = t[1]; wo.z[k] = t[2];
+        wi.x[k] = t[3]; wi.y[k] = t[4]; wi.z[k] = t[5];
+        s.x[k] = t[6]; s.y[k] = t[7]; s.z[k] = t[8];
+      }
+      ShadingContextSimd ctx;
+      ctx.p = Vec3vf(zero);
+      ctx.f.U = Vec3vf(1.f, 0.f, 0.f);
+      ctx.f.V = Vec3vf(0.f, 1.f, 0.f);
+      ctx.f.N = Vec3vf(0.f, 0.f, 1.f);
+      ctx.Ng = Vec3vf(0.f, 0.f, 1.f);
+      for (int u = 0; u < maxNumUVs; ++u) ctx.uv[u] = Vec2vf(0.5f);
+      ctx.backfacing = vbool(zero);
+      ctx.eps = vfloat(1e-6f);
+      const BsdfSimd* bsdf = material->getBsdf(m, ctx, wo, vint(mediumId));
+      vfloat evalPdf;
+      Vec3vf evalValue = bsdf->eval(m, ctx, wo, wi, evalPdf);
+      Vec3vf sWi = zero;
+      vfloat sPdf = zero;
+      vint sType = zero;
+      Vec3vf sWeight = bsdf->sample(m, ctx, wo, sWi, sPdf, sType, BsdfSampleSimd(s));
+      vint flags = bsdf->getFlags();
+      for (int k = 0; k < lanes; ++k)
+      {
+        float* o = out + 13 * (base + k);
+        o[0] = evalValue.x[k]; o[1] = evalValue.y[k]; o[2] = evalValue.z[k]; o[3] = evalPdf[k];
+        o[4] = sWeight.x[k]; o[5] = sWeight.y[k]; o[6] = sWeight.z[k];
+        o[7] = sWi.x[k]; o[8] = sWi.y[k]; o[9] = sWi.z[k];
+        o[10] = sPdf[k];
+        int ty = sType[k];
+        int fl = flags[k];
+        std::memcpy(&o[11], &ty, 4);
+        std::memcpy(&o[12], &fl, 4);
+      }
+    }
+    return 0;
+  }
+  catch (const std::exception&)
+  {
+    return -1;
+  }
+}
+
+} // extern "C"

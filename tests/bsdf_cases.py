@@ -1,0 +1,63 @@
+"""Seeded BSDF parity tuples and the Standard-material cases they are evaluated on.
+
+Shared by the BSDF parity tests and the fixture generator: tuples are (wo, wi, 3D sample) in
+the canonical shading frame (N = z); wo is drawn mostly from the upper hemisphere (the side the
+renderer shades from) with some grazing and below-horizon directions, wi from the full sphere.
+"""
+import numpy as np
+
+import prt_types as T
+
+GOLD_R = (1.0, 0.766, 0.336)
+GOLD_G = (1.0, 0.95, 0.75)
+
+
+def cases():
+    """(name, material, medium id) for every lobe combination the device implements."""
+    return [
+        ("lambert", T.material(base_color=(0.7, 0.4, 0.2), specular_weight=0.0), 0),
+        ("plastic_rough", T.material(base_color=(0.5, 0.6, 0.7), specular_roughness=0.3), 0),
+        ("plastic_smooth", T.material(base_color=(0.5, 0.6, 0.7), specular_roughness=0.0), 0),
+        ("gold_rough", T.material(metalness=1.0, base_color=GOLD_R, specular_color=GOLD_G, specular_roughness=0.25), 0),
+        ("gold_smooth", T.material(metalness=1.0, base_color=GOLD_R, specular_color=GOLD_G, specular_roughness=0.0), 0),
+        ("half_metal", T.material(metalness=0.5, base_color=(0.9, 0.5, 0.3), specular_roughness=0.4), 0),
+        ("glass_rough_out", T.material(transmission_weight=1.0, specular_roughness=0.2), 0),
+        ("glass_rough_in", T.material(transmission_weight=1.0, specular_roughness=0.2), 1),
+        ("glass_smooth", T.material(transmission_weight=1.0, specular_roughness=0.0), 0),
+        ("coat_rough_lambert", T.material(base_color=(0.3, 0.6, 0.3), specular_weight=0.0, coat_weight=1.0,
+                                          coat_roughness=0.2), 0),
+        ("coat_smooth_lambert", T.material(base_color=(0.3, 0.6, 0.3), specular_weight=0.0, coat_weight=1.0,
+                                           coat_roughness=0.0), 0),
+        ("coat_tinted_plastic", T.material(base_color=(0.8, 0.2, 0.2), coat_weight=0.7, coat_roughness=0.35,
+                                           coat_color=(0.9, 0.8, 0.6)), 0),
+    ]
+
+
+def tuples(n, seed):
+    rng = np.random.default_rng(seed)
+    wo = rng.normal(size=(n, 3))
+    wo /= np.linalg.norm(wo, axis=1, keepdims=True)
+    flip = rng.uniform(size=n) < 0.9
+    wo[flip, 2] = np.abs(wo[flip, 2])
+    wi = rng.normal(size=(n, 3))
+    wi /= np.linalg.norm(wi, axis=1, keepdims=True)
+    s = rng.uniform(size=(n, 3))
+    return np.concatenate([wo, wi, s], 1).astype(np.float32)
+
+
+def compare(gpu, ref, rel=1e-5, floor=1e-6):
+    """Per-quantity agreement: |a - b| <= rel * max(|a|, |b|) + floor, on the outputs that are
+    defined on both sides (sample outputs only where both samplings succeeded)."""
+    out = {}
+    ev_ok = np.abs(gpu[:, 0:4] - ref[:, 0:4]) <= rel * np.maximum(np.abs(gpu[:, 0:4]), np.abs(ref[:, 0:4])) + floor
+    out["eval"] = ev_ok.all(1)
+    both = (np.max(gpu[:, 4:7], 1) > 0) & (np.max(ref[:, 4:7], 1) > 0)
+    succ_same = (np.max(gpu[:, 4:7], 1) > 0) == (np.max(ref[:, 4:7], 1) > 0)
+    smp = np.concatenate([gpu[:, 4:11], ref[:, 4:11]], 1)
+    a, b = gpu[:, 4:11], ref[:, 4:11]
+    s_ok = np.abs(a - b) <= rel * np.maximum(np.abs(a), np.abs(b)) + floor
+    type_ok = gpu[:, 11].view(np.int32) == ref[:, 11].view(np.int32)
+    out["sample"] = succ_same & (~both | (s_ok.all(1) & type_ok))
+    out["flags"] = gpu[:, 12].view(np.int32) == ref[:, 12].view(np.int32)
+    del smp
+    return out

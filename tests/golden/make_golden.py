@@ -14,6 +14,8 @@ Fixtures (small, seeded, committed):
                    closest hits, plus random interior rays with closest hits and occlusion
   cornell_img.npz  small-scene renders at 128x128: 16 spp with seeds 0 and 1, 1024 spp with
                    seeds 0 and 1
+  sunsky_t3_e30.npz the reference's sun-sky products (sun radiance and angle, 512x256 sky) for
+                   the terrain scene's sun (elevation 30 deg, turbidity 3, ground albedo 0.2)
 """
 import pathlib
 import sys
@@ -93,8 +95,17 @@ def make_images():
     np.savez_compressed(OUT / "cornell_img.npz", **out)
 
 
+def make_sunsky():
+    d = prt_scenes.sun_direction()
+    sun, angle, sky = ref.sunsky(d, prt_scenes.SUN_TURBIDITY, prt_scenes.SUN_GROUND_ALBEDO)
+    np.savez_compressed(prt_scenes.SUNSKY_FIXTURE, sun_color=sun, sun_angle=np.float32(angle), sky=sky,
+                        direction=d)
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["sobol", "rays", "images"]
+    which = sys.argv[1:] or ["sobol", "rays", "images", "sunsky"]
+    if "sunsky" in which:
+        make_sunsky()
     if "sobol" in which:
         make_sobol()
     if "rays" in which:
