@@ -255,6 +255,13 @@ int prt_cuda_query_primary(prt_context* ctx, uint32_t sample_index, float* rays_
 int prt_cuda_bsdf_query(prt_context* ctx, const prt_material* material, int32_t medium_id, int64_t n,
                         const float* tuples, float* out);
 
+/* Copies the BSDF energy-compensation tables the context computed at creation (the
+ * reference's precomputeAlbedoTables, bsdf/albedo_tables.cpp:173-188) to out, concatenated in
+ * the order GGX dir (32x32), GGX avg (32), dielectric eta dir (16^3), eta avg (16^2), dielectric
+ * 1/eta dir (16^3), avg (16^2), dielectric reflection dir (16^3), avg (16^2). Writes at most
+ * `capacity` floats and returns the total count through *count. */
+int prt_cuda_albedo_tables(prt_context* ctx, float* out, int64_t capacity, int64_t* count);
+
 /* Host-only (no GPU needed): builds the BVH8 over tri_count triangles given as 9 floats each
  * (v0, v1, v2) and walks it with the counting traversal, the scalar twin of the closest-hit
  * kernel. For each of the n rays (8 floats) writes the global triangle index (-1 on a miss)

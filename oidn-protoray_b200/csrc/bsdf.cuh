@@ -175,9 +175,10 @@ struct GGX
     const f3 T2 = cross(T1, V);
     const float a = 1.f / (1.f + V.z);
     const float r = sqrtf(sx);
-    const float phi = sy < a ? sy / a * kPi : kPi + (sy - a) / (1.f - a) * kPi;
+    // phi = sy < a ? sy / a * pi : pi + (sy - a) / (1 - a) * pi
+    const float phiOverPi = sy < a ? sy / a : 1.f + (sy - a) / (1.f - a);
     float sp, cp;
-    sincosf(phi, &sp, &cp);
+    sincospif(phiOverPi, &sp, &cp);
     const float P1 = r * cp;
     const float P2 = r * sp * (sy < a ? 1.f : V.z);
     f3 wh = P1 * T1 + P2 * T2 + sqrtf(fmaxf(0.f, 1.f - P1 * P1 - P2 * P2)) * V;
@@ -768,6 +769,7 @@ enum : int
   kSlotConductor = 2,
 };
 
+
 // The opaque base: a Lambertian lobe, optionally under the specular dielectric layer
 // (material/standard.cpp:441-502).
 struct OpaqueBase
@@ -777,25 +779,25 @@ struct OpaqueBase
   bool hasSpec;
 };
 
-struct StdBsdf;
-
 // Substrate adaptor for the specular layer: the diffuse lobe.
 struct DiffuseSub
 {
-  const DiffuseLobe* d;
-  const Frame* fr;
+  DiffuseLobe d;
+  Frame fr;
   f3 Ng;
   PRT_D int flags() const { return kDiffuseReflection; }
-  PRT_D float importance() const { return d->importance(); }
-  PRT_D f3 eval(const DevTables& t, f3 wo, f3 wi, float& pdf) const { return d->eval(*fr, Ng, wo, wi, pdf); }
+  PRT_D float importance() const { return d.importance(); }
+  PRT_D f3 eval(const DevTables& t, f3 wo, f3 wi, float& pdf) const { return d.eval(fr, Ng, wo, wi, pdf); }
   PRT_D f3 sample(const DevTables& t, f3 wo, float sx, float sy, float sc, f3& wi, float& pdf, int& type) const
   {
-    return d->sample(*fr, Ng, wo, sx, sy, sc, wi, pdf, type);
+    return d.sample(fr, Ng, wo, sx, sy, sc, wi, pdf, type);
   }
 };
 
-// MultiBsdf over the base lobes (bsdf/multi_bsdf.h:151-270) and the outer coat.
-struct StdBsdf
+// MultiBsdf over the base lobes (bsdf/multi_bsdf.h:151-270) and the outer coat. F is the
+// feature set the instance may contain (branches outside F are compiled out).
+template <int F>
+struct StdBsdfT
 {
   Frame fr;
   f3 Ng;
@@ -812,43 +814,41 @@ struct StdBsdf
   bool hasCoat;
   f3 albedoV;
 
-  PRT_D int flags() const { return hasCoat ? coat.flags(baseFlags) : baseFlags; }
-
-  PRT_D float slotImportance(int k) const
-  {
-    if (k == kSlotOpaque) return opaque.hasSpec ? opaque.spec.importance(opaque.diff.importance()) : opaque.diff.importance();
-    return 1.f;
-  }
+  PRT_D int flags() const { return ((F & kFeatCoat) && hasCoat) ? coat.flags(baseFlags) : baseFlags; }
 
   PRT_D f3 evalSlot(const DevTables& t, int k, f3 wo, f3 wi, float& pdf) const
   {
-    if (k == kSlotOpaque)
+    if ((F & kFeatOpaque) && k == kSlotOpaque)
     {
-      if (opaque.hasSpec)
+      if ((F & kFeatSpecular) && opaque.hasSpec)
       {
-        const DiffuseSub sub{&opaque.diff, &fr, Ng};
+        const DiffuseSub sub{opaque.diff, fr, Ng};
         return opaque.spec.eval(t, sub, fr, Ng, wo, wi, pdf);
       }
       return opaque.diff.eval(fr, Ng, wo, wi, pdf);
     }
-    if (k == kSlotDielectric) return diel.eval(t, fr, Ng, wo, wi, pdf);
-    return cond.eval(t, fr, Ng, wo, wi, pdf);
+    if ((F & kFeatDielectric) && k == kSlotDielectric) return diel.eval(t, fr, Ng, wo, wi, pdf);
+    if (F & kFeatConductor) return cond.eval(t, fr, Ng, wo, wi, pdf);
+    pdf = 0.f;
+    return mk(0.f);
   }
 
   PRT_D f3 sampleSlot(const DevTables& t, int k, f3 wo, float sx, float sy, float sc, f3& wi, float& pdf,
                       int& type) const
   {
-    if (k == kSlotOpaque)
+    if ((F & kFeatOpaque) && k == kSlotOpaque)
     {
-      if (opaque.hasSpec)
+      if ((F & kFeatSpecular) && opaque.hasSpec)
       {
-        const DiffuseSub sub{&opaque.diff, &fr, Ng};
+        const DiffuseSub sub{opaque.diff, fr, Ng};
         return opaque.spec.sample(t, sub, fr, Ng, wo, sx, sy, sc, wi, pdf, type);
       }
       return opaque.diff.sample(fr, Ng, wo, sx, sy, sc, wi, pdf, type);
     }
-    if (k == kSlotDielectric) return diel.sample(t, fr, Ng, wo, sx, sy, sc, wi, pdf, type);
-    return cond.sample(t, fr, Ng, wo, sx, sy, sc, wi, pdf, type);
+    if ((F & kFeatDielectric) && k == kSlotDielectric) return diel.sample(t, fr, Ng, wo, sx, sy, sc, wi, pdf, type);
+    if (F & kFeatConductor) return cond.sample(t, fr, Ng, wo, sx, sy, sc, wi, pdf, type);
+    pdf = 0.f;
+    return mk(0.f);
   }
 
   // MultiBsdfSimd::eval
@@ -917,7 +917,7 @@ struct StdBsdf
 
   struct BaseSub
   {
-    const StdBsdf* b;
+    const StdBsdfT* b;
     PRT_D int flags() const { return b->baseFlags; }
     PRT_D float importance() const { return b->impSum; }
     PRT_D f3 eval(const DevTables& t, f3 wo, f3 wi, float& pdf) const { return b->evalBase(t, wo, wi, pdf); }
@@ -929,13 +929,13 @@ struct StdBsdf
 
   PRT_D f3 eval(const DevTables& t, f3 wo, f3 wi, float& pdf) const
   {
-    if (hasCoat) return coat.eval(t, BaseSub{this}, fr, Ng, wo, wi, pdf);
+    if ((F & kFeatCoat) && hasCoat) return coat.eval(t, BaseSub{this}, fr, Ng, wo, wi, pdf);
     return evalBase(t, wo, wi, pdf);
   }
 
   PRT_D f3 sample(const DevTables& t, f3 wo, float sx, float sy, float sz, f3& wi, float& pdf, int& type) const
   {
-    if (hasCoat) return coat.sample(t, BaseSub{this}, fr, Ng, wo, sx, sy, sz, wi, pdf, type);
+    if ((F & kFeatCoat) && hasCoat) return coat.sample(t, BaseSub{this}, fr, Ng, wo, sx, sy, sz, wi, pdf, type);
     return sampleBase(t, wo, sx, sy, sz, wi, pdf, type);
   }
 
@@ -949,7 +949,10 @@ PRT_D f3 textureRgb(const DevTexture& t, float u, float v)
   return texLookup(t.rgb, t.width, t.height, u, v, true);
 }
 
-PRT_D void addSlot(StdBsdf& b, int kind, float scale, float importance, int flags)
+using StdBsdf = StdBsdfT<kFeatAll>;
+
+template <int F>
+PRT_D void addSlot(StdBsdfT<F>& b, int kind, float scale, float importance, int flags)
 {
   const int i = b.nLobes++;
   b.kind[i] = kind;
@@ -963,8 +966,9 @@ PRT_D void addSlot(StdBsdf& b, int kind, float scale, float importance, int flag
 // implements: Lambertian base with an optional specular layer, rough or smooth dielectric
 // transmission, rough or smooth artistic conductor, rough or smooth coat. `backfacing` is the
 // medium-interface orientation (material/material.h:66-76).
+template <int F>
 PRT_D void resolveStandard(const DevScene& sc, const DevTables& t, const DevMaterial& m, const ShadeCtx& ctx, f3 wo,
-                           bool backfacing, StdBsdf& b)
+                           bool backfacing, StdBsdfT<F>& b)
 {
   b.fr = makeShadingFrame(ctx, wo);
   b.Ng = ctx.Ng;
@@ -983,18 +987,18 @@ PRT_D void resolveStandard(const DevScene& sc, const DevTables& t, const DevMate
   const bool fromOutside = m.thinWalled ? true : !backfacing;
   f3 albedo = mk(0.f);
   const float dielectric = 1.f - metalness;
-  if (dielectric > kMatEps)
+  if ((F & (kFeatOpaque | kFeatDielectric)) && dielectric > kMatEps)
   {
     const float transmission = clamp01(m.transmissionWeight);
     float eta = fromOutside ? m.ambientIor * (1.f / m.specularIor) : m.specularIor * (1.f / m.ambientIor);
     eta = fminf(fmaxf(eta, 1.f / 3.f), 3.f);
     const float opaque = dielectric * (1.f - transmission);
-    if (opaque > kMatEps)
+    if ((F & kFeatOpaque) && opaque > kMatEps)
     {
       b.opaque.diff.color = baseColor * base;
       f3 a = b.opaque.diff.color;
       int fl = kDiffuseReflection;
-      if (fabsf(m.specularIor - m.ambientIor) > kMatEps && specular > kMatEps)
+      if ((F & kFeatSpecular) && fabsf(m.specularIor - m.ambientIor) > kMatEps && specular > kMatEps)
       {
         b.opaque.hasSpec = true;
         b.opaque.spec.init(t, eta, mk(1.f), 1.f, specularRoughness, m.hasSpecularRoughness != 0, specular);
@@ -1006,7 +1010,7 @@ PRT_D void resolveStandard(const DevScene& sc, const DevTables& t, const DevMate
       albedo += a * opaque;
     }
     const float translucent = dielectric * transmission * specular;
-    if (translucent > kMatEps)
+    if ((F & kFeatDielectric) && translucent > kMatEps)
     {
       b.diel.init(t, eta, specularRoughness, m.hasSpecularRoughness != 0);
       addSlot(b, kSlotDielectric, translucent, 1.f, b.diel.flags());
@@ -1014,7 +1018,7 @@ PRT_D void resolveStandard(const DevScene& sc, const DevTables& t, const DevMate
     }
   }
   const float metal = metalness * specular;
-  if (metal > kMatEps)
+  if ((F & kFeatConductor) && metal > kMatEps)
   {
     const f3 specColor = clamp01(mk(m.specularColor[0], m.specularColor[1], m.specularColor[2]));
     b.cond.init(t, baseColor * base, specColor, specularRoughness, m.hasSpecularRoughness != 0);
@@ -1022,7 +1026,7 @@ PRT_D void resolveStandard(const DevScene& sc, const DevTables& t, const DevMate
     albedo += b.cond.albedo() * metal;
   }
   const float coat = clamp01(m.coatWeight);
-  if (coat > kMatEps && fabsf(m.coatIor - m.ambientIor) > kMatEps)
+  if ((F & kFeatCoat) && coat > kMatEps && fabsf(m.coatIor - m.ambientIor) > kMatEps)
   {
     float coatEta = fromOutside ? m.ambientIor * (1.f / m.coatIor) : m.coatIor * (1.f / m.ambientIor);
     coatEta = fminf(fmaxf(coatEta, 1.f / 3.f), 3.f);

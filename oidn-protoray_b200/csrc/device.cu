@@ -110,7 +110,7 @@ void freeFrame(Context& c)
   PathState& s = c.ps;
   f(s.rayO); f(s.rayD); f(s.hit); f(s.thr); f(s.rad); f(s.info);
   f(s.shO); f(s.shD); f(s.shL); f(s.out); f(s.aovA); f(s.aovN);
-  f(s.queue[0]); f(s.queue[1]);
+  f(s.queue[0]); f(s.queue[1]); f(s.classQueues);
   s.capacity = 0;
 }
 
@@ -217,6 +217,29 @@ DevMaterial resolveMaterial(const prt_material& m, std::vector<float>& media, in
                            (d.transmissionWeight != 0.f && std::fabs(d.specularIor - d.ambientIor) <= 1e-4f);
   if (unsupported && !(d.type & kMatEmissive))
     throw std::invalid_argument("material uses lobes not yet supported by the CUDA device");
+  // Static lobe features (StandardMaterial::getBsdfLobes branch conditions with the
+  // material's constant parameters; only the base colour can be textured).
+  auto c01 = [](float x) { return std::min(std::max(x, 0.f), 1.f); };
+  const float eps = 1e-4f;
+  const float metal = c01(d.metalness), spec = c01(d.specularWeight), trans = c01(d.transmissionWeight);
+  const float diel = 1.f - metal;
+  d.features = 0;
+  if (diel > eps && diel * (1.f - trans) > eps)
+  {
+    d.features |= kFeatOpaque;
+    if (std::fabs(d.specularIor - d.ambientIor) > eps && spec > eps) d.features |= kFeatSpecular;
+  }
+  if (diel > eps && diel * trans * spec > eps) d.features |= kFeatDielectric;
+  if (metal * spec > eps) d.features |= kFeatConductor;
+  if (c01(d.coatWeight) > eps && std::fabs(d.coatIor - d.ambientIor) > eps) d.features |= kFeatCoat;
+  d.shadeClass = kShadeClasses - 1;
+  for (int k = 1; k < kShadeClasses; ++k)
+    if (kShadeClassFeatures[k] == d.features)
+    {
+      d.shadeClass = k;
+      break;
+    }
+  if (d.type & kMatEmissive) d.shadeClass = 0;
   return d;
 }
 
@@ -364,6 +387,9 @@ void uploadScene(Context& c, const prt_scene_desc* s)
   }
   sc.areaLightCount = (int)areaOff.size();
   sc.meshLight = upload(c, meshLight);
+  std::vector<int> meshClass(s->mesh_count);
+  for (int g = 0; g < s->mesh_count; ++g) meshClass[g] = mats[s->meshes[g].material].shadeClass;
+  sc.meshClass = upload(c, meshClass);
   sc.areaTriOffset = upload(c, areaOff);
   sc.areaTriCount = upload(c, areaCnt);
   sc.areaCdfOffset = upload(c, areaCdfOff);
@@ -501,14 +527,15 @@ void allocFrame(Context& c, int width, int height, int aovMask)
   }
   s.queue[0] = (int*)devAlloc(c, cap * sizeof(int), nullptr);
   s.queue[1] = (int*)devAlloc(c, cap * sizeof(int), nullptr);
+  s.classQueues = (int*)devAlloc(c, (size_t)cap * kShadeClasses * sizeof(int), nullptr);
   cuCheck(launchClear(c), "clear");
   cuCheck(cudaStreamSynchronize(c.stream), "frame");
 }
 
-// Per-bounce queue counters: 2 * (maxDepth + 2) counts followed by as many work counters.
+// Per-bounce counter blocks of 16 ints (see renderSamples), maxDepth + 2 of them.
 void ensureCounters(Context& c)
 {
-  const size_t need = sizeof(int) * 4 * (size_t)(c.renderer.maxDepth + 2);
+  const size_t need = sizeof(int) * 16 * (size_t)(c.renderer.maxDepth + 2);
   cudaStreamSynchronize(c.stream);
   if (c.ps.counters) cudaFree(c.ps.counters);
   c.ps.counters = (int*)devAlloc(c, need, nullptr);
@@ -915,6 +942,19 @@ int prt_cuda_bsdf_query(prt_context* ctx, const prt_material* material, int32_t 
     cuCheck(launchBsdfQuery(c, m, medium_id, n, (const float*)in.dev, (float*)o.dev), "bsdf query");
     o.copyOut();
     cuCheck(cudaStreamSynchronize(c.stream), "bsdf sync");
+  });
+}
+
+int prt_cuda_albedo_tables(prt_context* ctx, float* out, int64_t capacity, int64_t* count)
+{
+  return guarded(ctx, [&](Context& c) {
+    if (!count || capacity < 0 || (capacity > 0 && !out)) throw std::invalid_argument("invalid table query");
+    const int64_t total = 32 * 32 + 32 + 3 * (16 * 16 * 16 + 16 * 16);
+    *count = total;
+    if (capacity == 0) return;
+    // The tables were allocated back to back from one buffer in this order (albedo.cu).
+    cuCheck(cudaMemcpy(out, c.tableStorage, sizeof(float) * std::min(capacity, total), cudaMemcpyDeviceToHost),
+            "table copy");
   });
 }
 

@@ -15,12 +15,41 @@ enum : int
   kMatTransparent = 1 << 3,
 };
 
+// Lobe features of a Standard material, known per material at upload. A shading kernel
+// instantiated for a feature set compiles only those lobes; kFeatAll keeps every branch.
+enum : int
+{
+  kFeatOpaque = 1 << 0,     // Lambertian opaque base
+  kFeatSpecular = 1 << 1,   // dielectric specular layer over the opaque base
+  kFeatDielectric = 1 << 2, // transmissive dielectric base
+  kFeatConductor = 1 << 3,  // metal base
+  kFeatCoat = 1 << 4,       // outer coat layer
+  kFeatAll = 31,
+};
+
+// Shading classes: 0 ends the path (miss, area-light hit, maxDepth); 1.. shade a surface with
+// the lobe features listed here. Materials whose features match no specialised class use the
+// last (general) class.
+constexpr int kShadeClasses = 8;
+constexpr int kShadeClassFeatures[kShadeClasses] = {
+  0,
+  kFeatOpaque,
+  kFeatOpaque | kFeatSpecular,
+  kFeatConductor,
+  kFeatDielectric,
+  kFeatOpaque | kFeatCoat,
+  kFeatOpaque | kFeatSpecular | kFeatCoat,
+  kFeatAll,
+};
+
 // A Standard material with its parameters read and clamped as StandardMaterial::getBsdfLobes
 // reads them (material/standard.cpp:410-620). "has*" flags mirror the MaterialParam truth
 // tests that pick rough versus smooth lobes (material/material_param.h:49,181).
 struct DevMaterial
 {
   int type;
+  int features;          // kFeat* lobes the material can produce
+  int shadeClass;        // index into kShadeClassFeatures (0 for emissive materials)
   int baseColorTex;      // texture index or -1
   int mediumInt, mediumExt;
   float baseWeight;
@@ -102,6 +131,7 @@ struct DevScene
   const int* meshMaterial;   // material index per mesh
   const int* meshTriOffset;  // first global triangle of each mesh
   const int* meshLight;      // area light index per mesh, -1 if not emissive
+  const int* meshClass;      // shading class per mesh (its material's)
   int meshCount;
   const DevMaterial* materials;
   int materialCount;

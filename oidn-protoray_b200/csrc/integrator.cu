@@ -47,6 +47,13 @@ struct Launch
 
 PRT_D int laneId() { return threadIdx.x & 31; }
 
+template <int... Fs>
+struct ShadeLaunch;
+// Surface classes 1..kShadeClasses-1 in kShadeClassFeatures order.
+#define PRT_SHADE_CLASS_LIST                                                                          \
+  kFeatOpaque, kFeatOpaque | kFeatSpecular, kFeatConductor, kFeatDielectric, kFeatOpaque | kFeatCoat, \
+    kFeatOpaque | kFeatSpecular | kFeatCoat, kFeatAll
+
 // Appends `pred` lanes of the calling (converged) warp to a queue; returns the slot or -1.
 PRT_D int warpAppend(int* counter, bool pred)
 {
@@ -259,10 +266,14 @@ PRT_D void addCounts(unsigned long long* dst, const TraceCount& c)
   }
 }
 
-// Closest-hit traversal of the queued rays; persistent warps take 32 rays at a time.
+// Closest-hit traversal of the queued rays; persistent warps take 32 rays at a time. Each hit
+// is then binned by the shading it needs (the GPU form of the reference's material sort,
+// render/renderer_stream.h:108-181): class 0 ends the path (miss, area light, maxDepth),
+// classes 1.. are the material feature classes.
 template <bool Count>
 __global__ void __launch_bounds__(256) kTrace(Launch L, const int* __restrict__ queue, const int* __restrict__ count,
-                                              int* __restrict__ work)
+                                              int* __restrict__ work, int depth, int* __restrict__ classQueues,
+                                              int* __restrict__ classCounts)
 {
   const int n = *count;
   TraceCount tc;
@@ -273,13 +284,21 @@ __global__ void __launch_bounds__(256) kTrace(Launch L, const int* __restrict__ 
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= n) break;
     const int i = base + laneId();
+    int cls = -1, p = 0;
     if (i < n)
     {
-      const int p = queue ? __ldg(queue + i) : i;
+      p = queue ? __ldg(queue + i) : i;
       const float4 a = L.ps.rayO[p], b = L.ps.rayD[p];
       const TraceHit h = traverse<false, Count>(L.sc.nodes, L.sc.tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w,
                                                 L.ps.err, &tc);
       L.ps.hit[p] = make_float4(h.t, h.u, h.v, __int_as_float(h.triId));
+      cls = 0;
+      if (h.triId >= 0 && depth < L.rd.maxDepth) cls = __ldg(L.sc.meshClass + __ldg(L.sc.triVerts + h.triId).w);
+    }
+    for (int c = 0; c < kShadeClasses; ++c)
+    {
+      const int slot = warpAppend(classCounts + c, cls == c);
+      if (cls == c) classQueues[(int64_t)c * L.ps.capacity + slot] = p;
     }
   }
   if (Count) addCounts(L.ps.travCounts, tc);
@@ -335,10 +354,71 @@ PRT_D void finishPath(const Launch& L, int p, f3 rad)
   L.ps.out[p] = make_float4(c.x, c.y, c.z, 1.f);
 }
 
-// Shading of one bounce (render/path_renderer_stream.h:276-949).
-__global__ void __launch_bounds__(256) kShade(Launch L, const int* __restrict__ queue, const int* __restrict__ count,
-                                              int depth, int* __restrict__ queueOut, int* __restrict__ extCount,
-                                              int* __restrict__ shadowCount)
+// Paths that end at this bounce without shading a surface (render/path_renderer_stream.h:287-582
+// and the depth cut-off at :612): misses (environment lights), area-light hits, and surface
+// hits at maxDepth.
+__global__ void __launch_bounds__(256) kShadeEnd(Launch L, const int* __restrict__ queue, const int* __restrict__ count,
+                                                 int depth)
+{
+  const int n = *count;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+  {
+    const int p = __ldg(queue + i);
+    const float4 rd = L.ps.rayD[p], hh = L.ps.hit[p];
+    const float4 tp = L.ps.thr[p];
+    float4 ra = L.ps.rad[p];
+    const uint32_t pixelId = L.ps.info[p].x;
+    const f3 dir = mk(rd.x, rd.y, rd.z);
+    const int triId = __float_as_int(hh.w);
+    const f3 T = mk(tp.x, tp.y, tp.z);
+    f3 Lr = mk(ra.x, ra.y, ra.z);
+    const float lastPdf = tp.w;
+    const int lastType = __float_as_int(ra.w);
+    const bool aov1 = (pixelId & kPathAov1Flag) == 0u;
+    if (triId < 0)
+    {
+      float lightPdf;
+      const f3 Le = evalEnvLights(L.sc, dir, lightPdf);
+      const float w = (lastType & kBsdfSmooth) == 0 ? 1.f : misWeight(lastPdf, lightPdf);
+      Lr += T * w * Le;
+      if (aov1 && L.aovMask)
+      {
+        L.ps.aovA[p] = make_float4(0.f, 0.f, 0.f, 1.f);
+        L.ps.aovN[p] = make_float4(0.f, 0.f, 0.f, 1.f);
+      }
+    }
+    else
+    {
+      const int4 tv = __ldg(L.sc.triVerts + triId);
+      const int mesh = tv.w;
+      const int matId = __ldg(L.sc.meshMaterial + mesh);
+      if (L.sc.materials[matId].type & kMatEmissive)
+      {
+        float lightPdf;
+        const int prim = triId - __ldg(L.sc.meshTriOffset + mesh);
+        const f3 Le = evalAreaLight(L.sc, mesh, prim, dir, hh.x, lightPdf);
+        const float w = (lastType & kBsdfSmooth) == 0 ? 1.f : misWeight(lastPdf, lightPdf);
+        Lr += T * w * Le;
+        if (aov1 && L.aovMask)
+        {
+          const f3 N = normalize(-dir);
+          L.ps.aovA[p] = make_float4(1.f, 1.f, 1.f, 1.f);
+          L.ps.aovN[p] = make_float4(N.x, N.y, N.z, 1.f);
+        }
+      }
+      // else: a surface at maxDepth ends the path with its current radiance.
+    }
+    finishPath(L, p, Lr);
+  }
+}
+
+// Surface shading of one bounce (render/path_renderer_stream.h:592-949) for materials whose
+// lobes lie in feature set F: NEE with MIS, BSDF sampling, Russian roulette, medium tracking.
+template <int F>
+__global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __restrict__ queue,
+                                                     const int* __restrict__ count, int depth,
+                                                     int* __restrict__ queueOut, int* __restrict__ extCount,
+                                                     int* __restrict__ shadowCount)
 {
   const int n = *count;
   const uint32_t sampleDim = kDimBase + kDimBounce * (uint32_t)depth;
@@ -346,173 +426,126 @@ __global__ void __launch_bounds__(256) kShade(Launch L, const int* __restrict__ 
   {
     const int i = base + threadIdx.x;
     const bool active = i < n;
-    const int p = active ? (queue ? __ldg(queue + i) : i) : 0;
+    const int p = active ? __ldg(queue + i) : 0;
     bool extend = false;
     bool shadow = false;
     float4 shO = make_float4(0.f, 0.f, 0.f, 0.f), shD = shO, shL = shO;
     if (active)
     {
       const float4 ro = L.ps.rayO[p], rd = L.ps.rayD[p], hh = L.ps.hit[p];
-      float4 tp = L.ps.thr[p];
+      const float4 tp = L.ps.thr[p];
       float4 ra = L.ps.rad[p];
       uint4 info = L.ps.info[p];
       const f3 org = mk(ro.x, ro.y, ro.z), dir = mk(rd.x, rd.y, rd.z);
       const int triId = __float_as_int(hh.w);
       f3 T = mk(tp.x, tp.y, tp.z);
-      f3 Lr = mk(ra.x, ra.y, ra.z);
+      const f3 Lr = mk(ra.x, ra.y, ra.z);
       const float lastPdf = tp.w;
       const int lastType = __float_as_int(ra.w);
       uint32_t pixelId = info.x;
       const bool aov1 = (pixelId & kPathAov1Flag) == 0u;
-      if (triId < 0)
+      ShadeCtx ctx;
+      postIntersect(L.sc, org, dir, hh.x, triId, hh.y, hh.z, ctx);
+      const DevMaterial& mat = L.sc.materials[ctx.material];
+      const f3 wo = -dir;
+      uint32_t mediumId = info.z & 0xffffu;
+      // Material::getBsdf orientation: media interfaces take it from the medium the path
+      // is in, every other material is treated as front-facing (material/material.h:66-76).
+      const bool backfacing = (mat.type & kMatMediaInterface) ? (int)mediumId == mat.mediumInt : false;
+      StdBsdfT<F> bsdf;
+      resolveStandard<F>(L.sc, L.tab, mat, ctx, wo, backfacing, bsdf);
+      const SobolState st = sobolSetSample(L.rd.seed, info.y, pixelId & kPixelIdMask);
+      const bool aov2 = (pixelId & kPathAov2Flag) == 0u;
+      const bool rr = !(aov1 || aov2);
+      // Volume transmission (Beer's law) inside a medium.
+      if (mediumId > 0u)
       {
-        // Miss: environment lights (render/path_renderer_stream.h:287-415).
-        float lightPdf;
-        const f3 Le = evalEnvLights(L.sc, dir, lightPdf);
-        const float w = (lastType & kBsdfSmooth) == 0 ? 1.f : misWeight(lastPdf, lightPdf);
-        Lr += T * w * Le;
-        finishPath(L, p, Lr);
-        if (aov1 && L.aovMask)
-        {
-          L.ps.aovA[p] = make_float4(0.f, 0.f, 0.f, 1.f);
-          L.ps.aovN[p] = make_float4(0.f, 0.f, 0.f, 1.f);
-        }
+        const f3 mc = ld3(L.sc.mediaColor + 3 * mediumId);
+        T *= powf3(mc, hh.x);
       }
-      else
+      // Direct light (NEE)
+      if (bsdf.flags() & kBsdfSmooth)
       {
-        const int4 tv = __ldg(L.sc.triVerts + triId);
-        const int mesh = tv.w;
-        const int matId = __ldg(L.sc.meshMaterial + mesh);
-        const DevMaterial& mat = L.sc.materials[matId];
-        if (mat.type & kMatEmissive)
+        float lx, ly, lz;
+        sobolGet3D(st, sampleDim + kDimLight, lx, ly, lz);
+        f3 wi;
+        float lightPdf, dist;
+        const f3 Lw = sampleLight(L.sc, ctx.p, lx, ly, lz, wi, lightPdf, dist);
+        if (reduceMax(Lw) > 0.f && lightPdf > 0.f)
         {
-          // Area light hit (render/path_renderer_stream.h:421-582).
-          float lightPdf;
-          const int prim = triId - __ldg(L.sc.meshTriOffset + mesh);
-          const f3 Le = evalAreaLight(L.sc, mesh, prim, dir, hh.x, lightPdf);
-          const float w = (lastType & kBsdfSmooth) == 0 ? 1.f : misWeight(lastPdf, lightPdf);
-          Lr += T * w * Le;
-          finishPath(L, p, Lr);
-          if (aov1 && L.aovMask)
-          {
-            const f3 N = normalize(-dir);
-            L.ps.aovA[p] = make_float4(1.f, 1.f, 1.f, 1.f);
-            L.ps.aovN[p] = make_float4(N.x, N.y, N.z, 1.f);
-          }
-        }
-        else if (depth >= L.rd.maxDepth)
-        {
-          finishPath(L, p, Lr);
-        }
-        else
-        {
-          // Surface hit (render/path_renderer_stream.h:592-949).
-          ShadeCtx ctx;
-          postIntersect(L.sc, org, dir, hh.x, triId, hh.y, hh.z, ctx);
-          const f3 wo = -dir;
-          uint32_t mediumId = info.z & 0xffffu;
-          // Material::getBsdf orientation: media interfaces take it from the medium the path
-          // is in, every other material is treated as front-facing (material/material.h:66-76).
-          const bool backfacing = (mat.type & kMatMediaInterface) ? (int)mediumId == mat.mediumInt : false;
-          StdBsdf bsdf;
-          resolveStandard(L.sc, L.tab, mat, ctx, wo, backfacing, bsdf);
-          const SobolState st = sobolSetSample(L.rd.seed, info.y, pixelId & kPixelIdMask);
-          const bool aov2 = (pixelId & kPathAov2Flag) == 0u;
-          const bool rr = !(aov1 || aov2);
-          // Volume transmission (Beer's law) inside a medium.
-          if (mediumId > 0u)
-          {
-            const f3 mc = ld3(L.sc.mediaColor + 3 * mediumId);
-            T *= powf3(mc, hh.x);
-          }
-          // Direct light (NEE)
-          if (bsdf.flags() & kBsdfSmooth)
-          {
-            float lx, ly, lz;
-            sobolGet3D(st, sampleDim + kDimLight, lx, ly, lz);
-            f3 wi;
-            float lightPdf, dist;
-            const f3 Lw = sampleLight(L.sc, ctx.p, lx, ly, lz, wi, lightPdf, dist);
-            if (reduceMax(Lw) > 0.f && lightPdf > 0.f)
-            {
-              float bsdfPdf;
-              const f3 bv = bsdf.eval(L.tab, wo, wi, bsdfPdf);
-              if (reduceMax(bv) > 0.f)
-              {
-                const f3 dirT = T * bv;
-                if (depth >= L.rd.rrDepth)
-                {
-                  const float contProb = rr ? fminf(luminance(dirT * (1.f / bsdfPdf)), 0.95f) : 1.f;
-                  bsdfPdf *= contProb;
-                }
-                const f3 dirL = dirT * misWeight(lightPdf, bsdfPdf) * Lw;
-                shadow = true;
-                shO = make_float4(ctx.p.x, ctx.p.y, ctx.p.z, ctx.eps);
-                shD = make_float4(wi.x, wi.y, wi.z, dist - ctx.eps);
-                shL = make_float4(dirL.x, dirL.y, dirL.z, 0.f);
-              }
-            }
-          }
-          // BSDF sampling
-          float bx, by, bz;
-          sobolGet3D(st, sampleDim + kDimBsdf, bx, by, bz);
-          f3 wi;
           float bsdfPdf;
-          int bsdfType;
-          const f3 bw = bsdf.sample(L.tab, wo, bx, by, bz, wi, bsdfPdf, bsdfType);
-          extend = reduceMax(bw) > 0.f && bsdfPdf > 0.f;
-          const int extType = extend ? bsdfType : 0;
-          if (aov1)
+          const f3 bv = bsdf.eval(L.tab, wo, wi, bsdfPdf);
+          if (reduceMax(bv) > 0.f)
           {
-            if (L.aovMask)
+            const f3 dirT = T * bv;
+            if (depth >= L.rd.rrDepth)
             {
-              const f3 a = bsdf.albedo(), nn = bsdf.normal();
-              L.ps.aovA[p] = make_float4(a.x, a.y, a.z, 1.f);
-              L.ps.aovN[p] = make_float4(nn.x, nn.y, nn.z, 1.f);
+              const float contProb = rr ? fminf(luminance(dirT * (1.f / bsdfPdf)), 0.95f) : 1.f;
+              bsdfPdf *= contProb;
             }
-            pixelId |= kPathAov1Flag;
+            const f3 dirL = dirT * misWeight(lightPdf, bsdfPdf) * Lw;
+            shadow = true;
+            shO = make_float4(ctx.p.x, ctx.p.y, ctx.p.z, ctx.eps);
+            shD = make_float4(wi.x, wi.y, wi.z, dist - ctx.eps);
+            shL = make_float4(dirL.x, dirL.y, dirL.z, 0.f);
           }
-          if (aov2 && (extType & kBsdfDelta) == 0) pixelId |= kPathAov2Flag;
-          T *= bw;
-          extend = extend && reduceMax(T) >= L.rd.minWeight;
-          if (depth >= L.rd.rrDepth)
-          {
-            const float contProb = rr ? fminf(luminance(T), 0.95f) : 1.f;
-            extend = extend && sobolGet1D(st, sampleDim + kDimTerminate) <= contProb;
-            T *= 1.f / contProb;
-            bsdfPdf *= contProb;
-          }
-          if (extend)
-          {
-            L.ps.rayO[p] = make_float4(ctx.p.x, ctx.p.y, ctx.p.z, ctx.eps);
-            L.ps.rayD[p] = make_float4(wi.x, wi.y, wi.z, kPosMax);
-            const bool update = (bsdfType & kBsdfContinuation) == 0;
-            L.ps.thr[p] = make_float4(T.x, T.y, T.z, update ? bsdfPdf : lastPdf);
-            ra.w = __int_as_float(update ? bsdfType : lastType);
-            // Material::nextMedium (material/material.h:84-93).
-            if ((mat.type & kMatMediaInterface) && dot(wo, ctx.Ng) * dot(wi, ctx.Ng) < 0.f)
-              mediumId = (int)mediumId == mat.mediumInt ? (uint32_t)mat.mediumExt : (uint32_t)mat.mediumInt;
-            info.z = mediumId;
-          }
-          info.x = pixelId;
-          L.ps.info[p] = info;
-          if (!extend && !shadow) finishPath(L, p, Lr);
-          if (shadow) shL.w = __uint_as_float((uint32_t)p | (extend ? 0u : kShadowFinish));
-          ra.x = Lr.x;
-          ra.y = Lr.y;
-          ra.z = Lr.z;
-          L.ps.rad[p] = ra;
         }
       }
+      // BSDF sampling
+      float bx, by, bz;
+      sobolGet3D(st, sampleDim + kDimBsdf, bx, by, bz);
+      f3 wi;
+      float bsdfPdf;
+      int bsdfType;
+      const f3 bw = bsdf.sample(L.tab, wo, bx, by, bz, wi, bsdfPdf, bsdfType);
+      extend = reduceMax(bw) > 0.f && bsdfPdf > 0.f;
+      const int extType = extend ? bsdfType : 0;
+      if (aov1)
+      {
+        if (L.aovMask)
+        {
+          const f3 a = bsdf.albedo(), nn = bsdf.normal();
+          L.ps.aovA[p] = make_float4(a.x, a.y, a.z, 1.f);
+          L.ps.aovN[p] = make_float4(nn.x, nn.y, nn.z, 1.f);
+        }
+        pixelId |= kPathAov1Flag;
+      }
+      if (aov2 && (extType & kBsdfDelta) == 0) pixelId |= kPathAov2Flag;
+      T *= bw;
+      extend = extend && reduceMax(T) >= L.rd.minWeight;
+      if (depth >= L.rd.rrDepth)
+      {
+        const float contProb = rr ? fminf(luminance(T), 0.95f) : 1.f;
+        extend = extend && sobolGet1D(st, sampleDim + kDimTerminate) <= contProb;
+        T *= 1.f / contProb;
+        bsdfPdf *= contProb;
+      }
+      if (extend)
+      {
+        L.ps.rayO[p] = make_float4(ctx.p.x, ctx.p.y, ctx.p.z, ctx.eps);
+        L.ps.rayD[p] = make_float4(wi.x, wi.y, wi.z, kPosMax);
+        const bool update = (bsdfType & kBsdfContinuation) == 0;
+        L.ps.thr[p] = make_float4(T.x, T.y, T.z, update ? bsdfPdf : lastPdf);
+        ra.w = __int_as_float(update ? bsdfType : lastType);
+        // Material::nextMedium (material/material.h:84-93).
+        if ((mat.type & kMatMediaInterface) && dot(wo, ctx.Ng) * dot(wi, ctx.Ng) < 0.f)
+          mediumId = (int)mediumId == mat.mediumInt ? (uint32_t)mat.mediumExt : (uint32_t)mat.mediumInt;
+        info.z = mediumId;
+        L.ps.rad[p] = ra;
+      }
+      info.x = pixelId;
+      L.ps.info[p] = info;
+      if (!extend && !shadow) finishPath(L, p, Lr);
+      if (shadow) shL.w = __uint_as_float((uint32_t)p | (extend ? 0u : kShadowFinish));
     }
     const int e = warpAppend(extCount, extend);
     if (extend) queueOut[e] = p;
-    const int s = warpAppend(shadowCount, shadow);
+    const int sidx = warpAppend(shadowCount, shadow);
     if (shadow)
     {
-      L.ps.shO[s] = shO;
-      L.ps.shD[s] = shD;
-      L.ps.shL[s] = shL;
+      L.ps.shO[sidx] = shO;
+      L.ps.shD[sidx] = shD;
+      L.ps.shL[sidx] = shL;
     }
   }
 }
@@ -634,6 +667,9 @@ cudaError_t launchClear(Context& ctx)
   return e;
 }
 
+using ShadeClassList = ShadeLaunch<PRT_SHADE_CLASS_LIST>;
+static_assert(kShadeClassFeatures[1] == kFeatOpaque && kShadeClassFeatures[7] == kFeatAll, "class list");
+
 // Event pair recorded around one launch when kernel timing is on.
 struct TimedLaunch
 {
@@ -641,14 +677,47 @@ struct TimedLaunch
   int kind;  // 0 trace, 1 shadow, 2 shade
 };
 
+// Per-bounce counter block (ints): [0] paths entering the bounce, [1..kShadeClasses] paths per
+// shading class, [kCntShadow] shadow rays, [kCntWorkTrace], [kCntWorkShadow] work counters.
+constexpr int kCntShadow = 1 + kShadeClasses;
+constexpr int kCntWorkTrace = kCntShadow + 1;
+constexpr int kCntWorkShadow = kCntShadow + 2;
+constexpr int kCntStride = 16;
+static_assert(kCntWorkShadow < kCntStride, "counter block");
+
+// Launches one surface-shading kernel per feature class (the class list is kShadeClassFeatures).
+template <int... Fs>
+struct ShadeLaunch;
+
+template <>
+struct ShadeLaunch<>
+{
+  static void run(int, const Launch&, cudaStream_t, int, int*, int*, int, int*, int*, int*) {}
+};
+
+template <int F0, int... Fs>
+struct ShadeLaunch<F0, Fs...>
+{
+  static void run(int cls, const Launch& L, cudaStream_t st, int grid, int* classQueues, int* cnt, int depth,
+                  int* queueOut, int* nextCount, int* shadowCount)
+  {
+    kShadeSurface<F0><<<grid, 256, 0, st>>>(L, classQueues + (int64_t)cls * L.ps.capacity, cnt + 1 + cls, depth,
+                                            queueOut, nextCount, shadowCount);
+    ShadeLaunch<Fs...>::run(cls + 1, L, st, grid, classQueues, cnt, depth, queueOut, nextCount, shadowCount);
+  }
+};
+
+using ShadeClassList = ShadeLaunch<PRT_SHADE_CLASS_LIST>;
+static_assert(kShadeClassFeatures[1] == kFeatOpaque && kShadeClassFeatures[7] == kFeatAll, "class list");
+
+
 cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
 {
   rc = RenderCounters();
   const int pixelCount = ctx.width * ctx.height;
   const int maxDepth = ctx.renderer.maxDepth;
-  int* counts = ctx.ps.counters;  // [2*d]: input count of bounce d, [2*d+1]: its shadow count
-  const int countSlots = 2 * (maxDepth + 2);
-  int* work = counts + countSlots;
+  int* counts = ctx.ps.counters;
+  const int blocks = maxDepth + 2;
   const bool timing = (ctx.profileFlags & 1) != 0;
   const bool counting = (ctx.profileFlags & 2) != 0;
   std::vector<TimedLaunch> timed;
@@ -667,6 +736,7 @@ cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
   cudaError_t e = cudaSuccess;
   if (counting) e = cudaMemsetAsync(ctx.ps.travCounts, 0, 4 * sizeof(unsigned long long), ctx.stream);
   if (e != cudaSuccess) return e;
+  const int persistent = ctx.smCount * 8;
   for (int done = 0; done < spp;)
   {
     const int S = std::min(ctx.waveSamples, spp - done);
@@ -683,47 +753,47 @@ cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
     L.samples = S;
     L.aovMask = ctx.aovMask;
     const int P = pixelCount * S;
-    e = cudaMemsetAsync(counts, 0, sizeof(int) * 2 * countSlots, ctx.stream);
+    e = cudaMemsetAsync(counts, 0, sizeof(int) * kCntStride * blocks, ctx.stream);
     if (e != cudaSuccess) return e;
     e = cudaMemcpyAsync(counts, &P, sizeof(int), cudaMemcpyHostToDevice, ctx.stream);
     if (e != cudaSuccess) return e;
     kRaygen<<<gridFor(ctx, P), 256, 0, ctx.stream>>>(L);
     rc.launches++;
-    const int persistent = ctx.smCount * 8;
-    int cur = 0;
     for (int depth = 0; depth <= maxDepth; ++depth)
     {
-      const int* q = depth == 0 ? nullptr : ctx.ps.queue[cur];
-      int* qOut = ctx.ps.queue[cur ^ 1];
+      int* cnt = counts + kCntStride * depth;
+      int* next = counts + kCntStride * (depth + 1);
+      const int* q = depth == 0 ? nullptr : ctx.ps.queue[depth & 1];
+      int* qOut = ctx.ps.queue[(depth + 1) & 1];
       begin(0);
       if (counting)
-        kTrace<true><<<persistent, 256, 0, ctx.stream>>>(L, q, counts + 2 * depth, work + 2 * depth);
+        kTrace<true><<<persistent, 256, 0, ctx.stream>>>(L, q, cnt, cnt + kCntWorkTrace, depth, ctx.ps.classQueues, cnt + 1);
       else
-        kTrace<false><<<persistent, 256, 0, ctx.stream>>>(L, q, counts + 2 * depth, work + 2 * depth);
+        kTrace<false><<<persistent, 256, 0, ctx.stream>>>(L, q, cnt, cnt + kCntWorkTrace, depth, ctx.ps.classQueues, cnt + 1);
       end();
       begin(2);
-      kShade<<<gridFor(ctx, P), 256, 0, ctx.stream>>>(L, q, counts + 2 * depth, depth, qOut, counts + 2 * (depth + 1),
-                                                       counts + 2 * depth + 1);
+      kShadeEnd<<<persistent, 256, 0, ctx.stream>>>(L, ctx.ps.classQueues, cnt + 1, depth);
+      ShadeClassList::run(1, L, ctx.stream, persistent, ctx.ps.classQueues, cnt, depth, qOut, next, cnt + kCntShadow);
       end();
       begin(1);
       if (counting)
-        kShadow<true><<<persistent, 256, 0, ctx.stream>>>(L, counts + 2 * depth + 1, work + 2 * depth + 1);
+        kShadow<true><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow);
       else
-        kShadow<false><<<persistent, 256, 0, ctx.stream>>>(L, counts + 2 * depth + 1, work + 2 * depth + 1);
+        kShadow<false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow);
       end();
-      rc.launches += 3;
+      rc.launches += 3 + kShadeClasses;
       e = cudaGetLastError();
       if (e != cudaSuccess) return e;
-      cur ^= 1;
-      // Input, shadow and extension counts of this bounce; stop once no path is left.
-      int cnt[3];
-      e = cudaMemcpyAsync(cnt, counts + 2 * depth, 3 * sizeof(int), cudaMemcpyDeviceToHost, ctx.stream);
+      // Paths in, shadow rays and paths out of this bounce; stop once no path is left.
+      int in = 0, shadow = 0, out = 0;
+      e = cudaMemcpyAsync(&in, cnt, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(&shadow, cnt + kCntShadow, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(&out, next, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(ctx.stream);
       if (e != cudaSuccess) return e;
-      e = cudaStreamSynchronize(ctx.stream);
-      if (e != cudaSuccess) return e;
-      rc.closestRays += cnt[0];
-      rc.shadowRays += cnt[1];
-      if (cnt[2] == 0) break;
+      rc.closestRays += in;
+      rc.shadowRays += shadow;
+      if (out == 0) break;
     }
     kAccumulate<<<gridFor(ctx, pixelCount), 256, 0, ctx.stream>>>(L, reinterpret_cast<float4*>(ctx.accum),
                                                                    reinterpret_cast<float4*>(ctx.accumA),

@@ -37,6 +37,7 @@ struct PathState
   float4* aovA = nullptr;   // first-hit albedo per path (w = 1 when written)
   float4* aovN = nullptr;   // first-hit normal per path
   int* queue[2] = {nullptr, nullptr};
+  int* classQueues = nullptr;  // kShadeClasses queues of `capacity` entries each
   int* counters = nullptr;  // per bounce: input and shadow counts, then the work counters
   unsigned long long* travCounts = nullptr;  // closest nodes, closest tris, shadow nodes, shadow tris
   uint32_t* err = nullptr;

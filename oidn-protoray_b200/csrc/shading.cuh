@@ -173,9 +173,8 @@ PRT_D f3 cosineSampleHemisphere(float& pdf, float sx, float sy)
 {
   const float cosTheta = sqrtf(sx);
   const float sinTheta = sqrtf(1.f - sx);
-  const float phi = 2.f * kPi * sy;
   float sinPhi, cosPhi;
-  sincosf(phi, &sinPhi, &cosPhi);
+  sincospif(2.f * sy, &sinPhi, &cosPhi);  // phi = 2 pi sy
   pdf = cosTheta * kInvPi;
   return mk(cosPhi * sinTheta, sinPhi * sinTheta, cosTheta);
 }
@@ -184,9 +183,8 @@ PRT_D f3 uniformSampleSphere(float& pdf, float sx, float sy)
 {
   const float cosTheta = 1.f - 2.f * sx;
   const float sinTheta = 2.f * sqrtf(sx * (1.f - sx));
-  const float phi = 2.f * kPi * sy;
   float sinPhi, cosPhi;
-  sincosf(phi, &sinPhi, &cosPhi);
+  sincospif(2.f * sy, &sinPhi, &cosPhi);
   pdf = 1.f / (4.f * kPi);
   return mk(cosPhi * sinTheta, sinPhi * sinTheta, cosTheta);
 }
@@ -197,9 +195,8 @@ PRT_D f3 uniformSampleCone(float& pdf, float sx, float sy, float angle, float co
 {
   const float cosTheta = 1.f - sx * (1.f - cosAngle);
   const float sinTheta = cos2sin(cosTheta);
-  const float phi = 2.f * kPi * sy;
   float sinPhi, cosPhi;
-  sincosf(phi, &sinPhi, &cosPhi);
+  sincospif(2.f * sy, &sinPhi, &cosPhi);
   pdf = conePdf;
   (void)angle;
   return mk(cosPhi * sinTheta, sinPhi * sinTheta, cosTheta);
@@ -375,11 +372,10 @@ PRT_D f3 sampleOneLight(const DevScene& sc, int l, f3 p, float sx, float sy, flo
   const int ix = cdfSampleReuse(im.xCdfs + (size_t)iy * (im.lutW + 1), im.lutW, xPdf, s0);
   const float u = ((float)ix + s0) * (1.f / (float)im.lutW);
   const float v = ((float)iy + s1) * (1.f / (float)im.lutH);
-  const float theta = (1.f - v) * kPi;
-  const float phi = (u - 0.5f) * (2.f * kPi);
+  // theta = (1 - v) pi, phi = (u - 0.5) 2 pi
   float sinPhi, cosPhi, sinTheta, cosTheta;
-  sincosf(phi, &sinPhi, &cosPhi);
-  sincosf(theta, &sinTheta, &cosTheta);
+  sincospif((u - 0.5f) * 2.f, &sinPhi, &cosPhi);
+  sincospif(1.f - v, &sinTheta, &cosTheta);
   wi = mk(sinPhi * sinTheta, cosTheta, -cosPhi * sinTheta);
   pdf = xPdf * yPdf * (float)im.lutW * (float)im.lutH * (1.f / (2.f * kPi * kPi * sinTheta));
   return texLookup(im.rgb, im.width, im.height, u, v, false) * (1.f / pdf);

@@ -62,6 +62,7 @@ def load_library():
     lib.prt_cuda_occluded.argtypes = [vp, C.c_int64, P(C.c_float), P(C.c_int32)]
     lib.prt_cuda_query_primary.argtypes = [vp, C.c_uint32, P(C.c_float), P(C.c_int32), P(C.c_int32), P(C.c_float)]
     lib.prt_cuda_bsdf_query.argtypes = [vp, P(T.Material), C.c_int32, C.c_int64, P(C.c_float), P(C.c_float)]
+    lib.prt_cuda_albedo_tables.argtypes = [vp, P(C.c_float), C.c_int64, P(C.c_int64)]
     lib.prt_bvh8_count.argtypes = [P(C.c_float), C.c_int64, C.c_int64, P(C.c_float), P(C.c_int32), P(C.c_float),
                                    P(C.c_int64), P(C.c_int64), P(C.c_int64)]
     _lib = lib
@@ -200,6 +201,13 @@ class DeviceCuda:
         out = np.zeros((t.shape[0], 13), np.float32)
         self._check(self.lib.prt_cuda_bsdf_query(self.h, C.byref(material), medium_id, t.shape[0], T.fptr(t),
                                                  T.fptr(out)))
+        return out
+
+    def albedo_tables(self):
+        n = C.c_int64(0)
+        self._check(self.lib.prt_cuda_albedo_tables(self.h, None, 0, C.byref(n)))
+        out = np.zeros(n.value, np.float32)
+        self._check(self.lib.prt_cuda_albedo_tables(self.h, T.fptr(out), n.value, C.byref(n)))
         return out
 
     def occluded(self, rays):

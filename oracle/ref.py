@@ -93,6 +93,16 @@ def bsdf_query(material, tuples, medium_id=0):
     return out
 
 
+def albedo_tables():
+    lib = _lib()
+    lib.ref_albedo_tables.restype = C.c_int64
+    lib.ref_albedo_tables.argtypes = [C.POINTER(C.c_float)]
+    n = lib.ref_albedo_tables(None)
+    out = np.zeros(n, np.float32)
+    lib.ref_albedo_tables(T.fptr(out))
+    return out
+
+
 def hardware_threads():
     return _lib().ref_hardware_threads()
 

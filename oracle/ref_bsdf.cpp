@@ -124,4 +124,24 @@ int ref_bsdf_query(const prt_material* mat, int mediumId, int64_t n, const float
   }
 }
 
+// The reference's energy-compensation tables in the order of prt_cuda_albedo_tables.
+int64_t ref_albedo_tables(float* out)
+{
+  precomputeAlbedoTables();
+  float* o = out;
+  auto put = [&](const float* src, int n) {
+    if (out) std::memcpy(o, src, sizeof(float) * n);
+    o += n;
+  };
+  put(MicrofacetAlbedoTable::dir, 32 * 32);
+  put(MicrofacetAlbedoTable::avg, 32);
+  put(MicrofacetDielectricAlbedoTable::etaDir, 16 * 16 * 16);
+  put(MicrofacetDielectricAlbedoTable::etaAvg, 16 * 16);
+  put(MicrofacetDielectricAlbedoTable::rcpEtaDir, 16 * 16 * 16);
+  put(MicrofacetDielectricAlbedoTable::rcpEtaAvg, 16 * 16);
+  put(MicrofacetDielectricReflectionAlbedoTable::etaDir, 16 * 16 * 16);
+  put(MicrofacetDielectricReflectionAlbedoTable::etaAvg, 16 * 16);
+  return (int64_t)(o - out);
+}
+
 } // extern "C"
