@@ -217,6 +217,26 @@ int prt_cuda_clear(prt_context* ctx);
  * (render/device_cpu.cpp:53-59), each advancing the sample index by one. */
 int prt_cuda_render(prt_context* ctx, int32_t spp, prt_render_stats* stats);
 
+/* Launch tuning of the wavefront kernels; 0 in a field keeps the current value.
+ * trace_blocks / shade_blocks: persistent blocks of 256 threads per SM for the traversal and
+ *   shading kernels;
+ * wave_paths: upper bound on paths in flight per wave (path state is ~170 bytes per path). */
+typedef struct prt_tuning
+{
+  int32_t trace_blocks;
+  int32_t shade_blocks;
+  int32_t wave_paths;
+} prt_tuning;
+
+int prt_cuda_set_tuning(prt_context* ctx, const prt_tuning* tuning);
+int prt_cuda_get_tuning(prt_context* ctx, prt_tuning* tuning);
+
+/* Picks the tuning that renders the current scene, camera and frame fastest: each candidate
+ * renders `spp` samples per pixel once (after one warm-up), device-timed. The frame is cleared
+ * and the sample index reset afterwards. Writes the chosen tuning (also made current) and its
+ * Mrays/s. */
+int prt_cuda_autotune(prt_context* ctx, int32_t spp, prt_tuning* chosen, double* mrays);
+
 /* Enables PRT_PROFILE_* instrumentation for subsequent render calls (0 = off). */
 int prt_cuda_set_profiling(prt_context* ctx, int32_t flags);
 

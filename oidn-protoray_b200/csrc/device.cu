@@ -510,17 +510,41 @@ void allocFrame(Context& c, int width, int height, int aovMask)
     c.accumA = (float*)devAlloc(c, px * sizeof(float4), nullptr);
     c.accumN = (float*)devAlloc(c, px * sizeof(float4), nullptr);
   }
-  // Wave capacity: whole samples of the frame, up to ~16M paths (about 3 GB of path state).
-  const int64_t target = 16ll << 20;
-  c.waveSamples = (int)std::max<int64_t>(1, target / (int64_t)px);
-  const int64_t cap = (int64_t)c.waveSamples * px;
+  cuCheck(launchClear(c), "clear");
+  cuCheck(cudaStreamSynchronize(c.stream), "frame");
+}
+
+// Per-bounce counter blocks of 16 ints (see renderSamples), maxDepth + 2 of them.
+// Path state for waves of `samples` whole-frame samples (at least one), capped at ~16M paths
+// (about 3.5 GB). Allocated on the first render and grown when a call needs more.
+void ensurePathState(Context& c, int spp)
+{
+  const int64_t px = (int64_t)c.width * c.height;
+  const int64_t target = c.wavePaths;
+  const int maxWave = (int)std::max<int64_t>(1, target / px);
+  const int want = std::max(1, std::min(spp, maxWave));
+  if (c.ps.capacity >= want * px && c.ps.capacity <= std::max<int64_t>(target, px))
+  {
+    c.waveSamples = (int)(c.ps.capacity / px);
+    return;
+  }
+  cudaStreamSynchronize(c.stream);
   PathState& s = c.ps;
+  auto f = [](auto*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+  };
+  f(s.rayO); f(s.rayD); f(s.hit); f(s.thr); f(s.rad); f(s.info);
+  f(s.shO); f(s.shD); f(s.shL); f(s.out); f(s.aovA); f(s.aovN);
+  f(s.queue[0]); f(s.queue[1]); f(s.classQueues);
+  c.waveSamples = want;
+  const int64_t cap = (int64_t)want * px;
   s.capacity = cap;
   auto a4 = [&](size_t n) { return (float4*)devAlloc(c, n * sizeof(float4), nullptr); };
   s.rayO = a4(cap); s.rayD = a4(cap); s.hit = a4(cap); s.thr = a4(cap); s.rad = a4(cap);
   s.info = (uint4*)devAlloc(c, cap * sizeof(uint4), nullptr);
   s.shO = a4(cap); s.shD = a4(cap); s.shL = a4(cap); s.out = a4(cap);
-  if (aovMask)
+  if (c.aovMask)
   {
     s.aovA = a4(cap);
     s.aovN = a4(cap);
@@ -528,11 +552,8 @@ void allocFrame(Context& c, int width, int height, int aovMask)
   s.queue[0] = (int*)devAlloc(c, cap * sizeof(int), nullptr);
   s.queue[1] = (int*)devAlloc(c, cap * sizeof(int), nullptr);
   s.classQueues = (int*)devAlloc(c, (size_t)cap * kShadeClasses * sizeof(int), nullptr);
-  cuCheck(launchClear(c), "clear");
-  cuCheck(cudaStreamSynchronize(c.stream), "frame");
 }
 
-// Per-bounce counter blocks of 16 ints (see renderSamples), maxDepth + 2 of them.
 void ensureCounters(Context& c)
 {
   const size_t need = sizeof(int) * 16 * (size_t)(c.renderer.maxDepth + 2);
@@ -747,6 +768,7 @@ int prt_cuda_render(prt_context* ctx, int32_t spp, prt_render_stats* stats)
     if (!c.hasRenderer || !c.hasCamera || !c.accum) throw ApiError{PRT_ERR_STATE, "renderer, camera and frame are required"};
     if (spp < 0) throw std::invalid_argument("spp must be >= 0");
     cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+    ensurePathState(c, spp);
     cuCheck(cudaEventRecord(c.ev0, c.stream), "event");
     RenderCounters rc;
     cuCheck(renderSamples(c, spp, rc), "render");
@@ -955,6 +977,89 @@ int prt_cuda_albedo_tables(prt_context* ctx, float* out, int64_t capacity, int64
     // The tables were allocated back to back from one buffer in this order (albedo.cu).
     cuCheck(cudaMemcpy(out, c.tableStorage, sizeof(float) * std::min(capacity, total), cudaMemcpyDeviceToHost),
             "table copy");
+  });
+}
+
+int prt_cuda_set_tuning(prt_context* ctx, const prt_tuning* t)
+{
+  return guarded(ctx, [&](Context& c) {
+    if (!t) throw std::invalid_argument("null tuning");
+    if (t->trace_blocks < 0 || t->trace_blocks > 32 || t->shade_blocks < 0 || t->shade_blocks > 32 || t->wave_paths < 0)
+      throw std::invalid_argument("tuning out of range");
+    if (t->trace_blocks) c.traceBlocks = t->trace_blocks;
+    if (t->shade_blocks) c.shadeBlocks = t->shade_blocks;
+    if (t->wave_paths) c.wavePaths = t->wave_paths;
+  });
+}
+
+int prt_cuda_get_tuning(prt_context* ctx, prt_tuning* t)
+{
+  return guarded(ctx, [&](Context& c) {
+    if (!t) throw std::invalid_argument("null tuning");
+    t->trace_blocks = c.traceBlocks;
+    t->shade_blocks = c.shadeBlocks;
+    t->wave_paths = (int32_t)std::min<int64_t>(c.wavePaths, 0x7fffffff);
+  });
+}
+
+int prt_cuda_autotune(prt_context* ctx, int32_t spp, prt_tuning* chosen, double* mrays)
+{
+  return guarded(ctx, [&](Context& c) {
+    requireScene(c);
+    if (!c.hasRenderer || !c.hasCamera || !c.accum) throw ApiError{PRT_ERR_STATE, "renderer, camera and frame are required"};
+    if (spp <= 0) throw std::invalid_argument("spp must be > 0");
+    cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+    auto timeOne = [&](int tb, int sb, int64_t wave) {
+      c.traceBlocks = tb;
+      c.shadeBlocks = sb;
+      c.wavePaths = wave;
+      ensurePathState(c, spp);
+      RenderCounters rc;
+      cuCheck(cudaEventRecord(c.ev0, c.stream), "event");
+      cuCheck(renderSamples(c, spp, rc), "autotune render");
+      cuCheck(cudaEventRecord(c.ev1, c.stream), "event");
+      cuCheck(cudaEventSynchronize(c.ev1), "autotune sync");
+      float ms = 0.f;
+      cuCheck(cudaEventElapsedTime(&ms, c.ev0, c.ev1), "event time");
+      return (double)(rc.closestRays + rc.shadowRays) / 1e6 / (ms * 1e-3);
+    };
+    const int profile = c.profileFlags;
+    c.profileFlags = 0;
+    int bT = c.traceBlocks, bS = c.shadeBlocks;
+    int64_t bW = c.wavePaths;
+    timeOne(bT, bS, bW);  // warm-up
+    double best = -1.0;
+    // One axis at a time: wave size (paths in flight), then traversal and shading grids.
+    for (int64_t w : {8ll << 20, 16ll << 20, 32ll << 20})
+    {
+      const double v = timeOne(bT, bS, w);
+      if (v > best) { best = v; bW = w; }
+    }
+    for (int tb : {4, 6, 8, 12})
+    {
+      const double v = timeOne(tb, bS, bW);
+      if (v > best) { best = v; bT = tb; }
+    }
+    for (int sb : {2, 4, 8})
+    {
+      const double v = timeOne(bT, sb, bW);
+      if (v > best) { best = v; bS = sb; }
+    }
+    c.traceBlocks = bT;
+    c.shadeBlocks = bS;
+    c.wavePaths = bW;
+    c.profileFlags = profile;
+    checkDeviceErrors(c);
+    cuCheck(launchClear(c), "clear");
+    c.sampleIndex = 0;
+    cuCheck(cudaStreamSynchronize(c.stream), "sync");
+    if (chosen)
+    {
+      chosen->trace_blocks = bT;
+      chosen->shade_blocks = bS;
+      chosen->wave_paths = (int32_t)bW;
+    }
+    if (mrays) *mrays = best;
   });
 }
 

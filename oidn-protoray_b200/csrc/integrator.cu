@@ -266,10 +266,11 @@ PRT_D void addCounts(unsigned long long* dst, const TraceCount& c)
   }
 }
 
-// Closest-hit traversal of the queued rays; persistent warps take 32 rays at a time. Each hit
-// is then binned by the shading it needs (the GPU form of the reference's material sort,
+// Closest-hit traversal of the queued rays. Persistent warps keep one ray per lane; when at
+// least L.refill lanes are idle the warp retires their finished rays -- writing the hit
+// and binning it by the shading it needs (the GPU form of the reference's material sort,
 // render/renderer_stream.h:108-181): class 0 ends the path (miss, area light, maxDepth),
-// classes 1.. are the material feature classes.
+// classes 1.. are the material feature classes -- and fetches new rays for them.
 template <bool Count>
 __global__ void __launch_bounds__(256) kTrace(Launch L, const int* __restrict__ queue, const int* __restrict__ count,
                                               int* __restrict__ work, int depth, int* __restrict__ classQueues,
@@ -736,7 +737,8 @@ cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
   cudaError_t e = cudaSuccess;
   if (counting) e = cudaMemsetAsync(ctx.ps.travCounts, 0, 4 * sizeof(unsigned long long), ctx.stream);
   if (e != cudaSuccess) return e;
-  const int persistent = ctx.smCount * 8;
+  const int persistent = ctx.smCount * ctx.traceBlocks;
+  const int shadeGrid = ctx.smCount * ctx.shadeBlocks;
   for (int done = 0; done < spp;)
   {
     const int S = std::min(ctx.waveSamples, spp - done);
@@ -772,8 +774,8 @@ cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
         kTrace<false><<<persistent, 256, 0, ctx.stream>>>(L, q, cnt, cnt + kCntWorkTrace, depth, ctx.ps.classQueues, cnt + 1);
       end();
       begin(2);
-      kShadeEnd<<<persistent, 256, 0, ctx.stream>>>(L, ctx.ps.classQueues, cnt + 1, depth);
-      ShadeClassList::run(1, L, ctx.stream, persistent, ctx.ps.classQueues, cnt, depth, qOut, next, cnt + kCntShadow);
+      kShadeEnd<<<shadeGrid, 256, 0, ctx.stream>>>(L, ctx.ps.classQueues, cnt + 1, depth);
+      ShadeClassList::run(1, L, ctx.stream, shadeGrid, ctx.ps.classQueues, cnt, depth, qOut, next, cnt + kCntShadow);
       end();
       begin(1);
       if (counting)

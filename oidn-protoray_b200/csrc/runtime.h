@@ -69,6 +69,9 @@ struct Context
   DevTables tables{};             // energy-compensation tables (albedo.cu)
   float* tableStorage = nullptr;
   int profileFlags = 0;
+  int traceBlocks = 8;            // launch tuning (prt_tuning)
+  int shadeBlocks = 8;
+  int64_t wavePaths = 32ll << 20;
 };
 
 // Per-call statistics gathered by renderSamples.

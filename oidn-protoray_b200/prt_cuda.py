@@ -54,6 +54,9 @@ def load_library():
     lib.prt_cuda_clear.argtypes = [vp]
     lib.prt_cuda_render.argtypes = [vp, C.c_int32, P(T.RenderStats)]
     lib.prt_cuda_set_profiling.argtypes = [vp, C.c_int32]
+    lib.prt_cuda_set_tuning.argtypes = [vp, P(T.Tuning)]
+    lib.prt_cuda_get_tuning.argtypes = [vp, P(T.Tuning)]
+    lib.prt_cuda_autotune.argtypes = [vp, C.c_int32, P(T.Tuning), P(C.c_double)]
     lib.prt_cuda_blit.argtypes = [vp, C.c_int32, P(C.c_float)]
     lib.prt_cuda_sobol.argtypes = [vp, C.c_int64, P(C.c_uint32), P(C.c_uint32), P(C.c_uint32), C.c_int32,
                                    P(C.c_float)]
@@ -152,6 +155,22 @@ class DeviceCuda:
         st = T.RenderStats()
         self._check(self.lib.prt_cuda_render(self.h, spp, C.byref(st)))
         return {name: getattr(st, name) for name, _ in T.RenderStats._fields_}
+
+    def set_tuning(self, trace_blocks=0, shade_blocks=0, wave_paths=0):
+        t = T.Tuning(trace_blocks, shade_blocks, wave_paths)
+        self._check(self.lib.prt_cuda_set_tuning(self.h, C.byref(t)))
+
+    def get_tuning(self):
+        t = T.Tuning()
+        self._check(self.lib.prt_cuda_get_tuning(self.h, C.byref(t)))
+        return {name: getattr(t, name) for name, _ in T.Tuning._fields_}
+
+    def autotune(self, spp=4):
+        """Picks the fastest launch tuning for the current scene/frame; clears the frame."""
+        t = T.Tuning()
+        m = C.c_double()
+        self._check(self.lib.prt_cuda_autotune(self.h, spp, C.byref(t), C.byref(m)))
+        return {name: getattr(t, name) for name, _ in T.Tuning._fields_}, m.value
 
     def set_profiling(self, flags):
         self._check(self.lib.prt_cuda_set_profiling(self.h, flags))

@@ -273,8 +273,12 @@ def terrain(seed=0, grid=1024, n_spheres=400, sphere_subdiv=3, width=1920, heigh
     s.add_mesh(pos, tris, ground, normals=nrm.reshape(-1, 3).astype(np.float32), texcoords=uvs)
     # Spheres resting on the terrain.
     sv, sf = icosphere(sphere_subdiv)
-    gold_r = (1.0, 0.766, 0.336)   # reflectivity (F0) of gold
-    gold_g = (1.0, 0.95, 0.75)     # edge tint
+    # Gold-like conductor through the Standard material's artistic Fresnel: reflectivity (F0)
+    # of gold and a white edge tint. The edge tint stays (1, 1, 1) because the reference's
+    # scene format does not store a metal's specular colour (rkscene/rkscene.h:626-627), so a
+    # metal loaded by the reference always has that tint.
+    gold_r = (1.0, 0.766, 0.336)
+    gold_g = (1.0, 1.0, 1.0)
     for _ in range(n_spheres):
         r = rng.uniform(0.3, 1.5)
         cx, cz = rng.uniform(-0.9 * extent, 0.9 * extent, 2)
@@ -302,6 +306,6 @@ def terrain(seed=0, grid=1024, n_spheres=400, sphere_subdiv=3, width=1920, heigh
         s.env.distant_dir[:] = tuple(float(c) for c in d)
         s.env.distant_angle = sun_angle
         s.set_env_image(sky, lut_size=128)
-    s.camera = look_at((0.0, 28.0, 62.0), (0.0, 0.0, -5.0), fov_deg=45.0)
+    s.camera = look_at((0.0, 0.56 * extent, 1.24 * extent), (0.0, 0.0, -0.1 * extent), fov_deg=45.0)
     s.width, s.height, s.spp, s.max_depth, s.rr_depth = width, height, spp, max_depth, rr_depth
     return s

@@ -179,6 +179,14 @@ class RenderStats(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [
+        ("trace_blocks", C.c_int32),
+        ("shade_blocks", C.c_int32),
+        ("wave_paths", C.c_int32),
+    ]
+
+
 PRT_PROFILE_KERNELS = 1 << 0
 PRT_PROFILE_COUNTS = 1 << 1
 

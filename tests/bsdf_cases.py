@@ -46,18 +46,23 @@ def tuples(n, seed):
 
 
 def compare(gpu, ref, rel=1e-5, floor=1e-6):
-    """Per-quantity agreement: |a - b| <= rel * max(|a|, |b|) + floor, on the outputs that are
-    defined on both sides (sample outputs only where both samplings succeeded)."""
+    """Per-tuple agreement of the 13 outputs.
+
+    eval value and pdf, sample weight and pdf: |a - b| <= rel * max(|a|, |b|) + floor;
+    sampled direction (a unit vector): |a - b| <= max(rel, 2e-5) per component; sample type:
+    equal; and both sides must agree on whether sampling succeeded. Sample outputs are
+    compared only where both succeeded. Returns boolean arrays {"eval", "sample", "flags"}."""
+    def close(a, b):
+        return np.abs(a - b) <= rel * np.maximum(np.abs(a), np.abs(b)) + floor
+
     out = {}
-    ev_ok = np.abs(gpu[:, 0:4] - ref[:, 0:4]) <= rel * np.maximum(np.abs(gpu[:, 0:4]), np.abs(ref[:, 0:4])) + floor
-    out["eval"] = ev_ok.all(1)
-    both = (np.max(gpu[:, 4:7], 1) > 0) & (np.max(ref[:, 4:7], 1) > 0)
-    succ_same = (np.max(gpu[:, 4:7], 1) > 0) == (np.max(ref[:, 4:7], 1) > 0)
-    smp = np.concatenate([gpu[:, 4:11], ref[:, 4:11]], 1)
-    a, b = gpu[:, 4:11], ref[:, 4:11]
-    s_ok = np.abs(a - b) <= rel * np.maximum(np.abs(a), np.abs(b)) + floor
+    out["eval"] = close(gpu[:, 0:4], ref[:, 0:4]).all(1)
+    gs = np.max(gpu[:, 4:7], 1) > 0
+    rs = np.max(ref[:, 4:7], 1) > 0
+    both = gs & rs
+    w_ok = close(gpu[:, 4:7], ref[:, 4:7]).all(1) & close(gpu[:, 10], ref[:, 10])
+    wi_ok = (np.abs(gpu[:, 7:10] - ref[:, 7:10]) <= max(rel, 2e-5)).all(1)
     type_ok = gpu[:, 11].view(np.int32) == ref[:, 11].view(np.int32)
-    out["sample"] = succ_same & (~both | (s_ok.all(1) & type_ok))
+    out["sample"] = (gs == rs) & (~both | (w_ok & wi_ok & type_ok))
     out["flags"] = gpu[:, 12].view(np.int32) == ref[:, 12].view(np.int32)
-    del smp
     return out

@@ -14,6 +14,10 @@ Fixtures (small, seeded, committed):
                    closest hits, plus random interior rays with closest hits and occlusion
   cornell_img.npz  small-scene renders at 128x128: 16 spp with seeds 0 and 1, 1024 spp with
                    seeds 0 and 1
+  terrain_img.npz  small terrain renders (96^2 heightfield, 24 spheres of all four material
+                   kinds, sun-sky) at 128x64: 16 spp and 256 spp, seeds 0 and 1
+  bsdf.npz         the reference's Standard-material BSDF (eval, sample) on 512 seeded tuples
+                   for each case of tests/bsdf_cases.py
   sunsky_t3_e30.npz the reference's sun-sky products (sun radiance and angle, 512x256 sky) for
                    the terrain scene's sun (elevation 30 deg, turbidity 3, ground albedo 0.2)
 """
@@ -95,6 +99,32 @@ def make_images():
     np.savez_compressed(OUT / "cornell_img.npz", **out)
 
 
+def make_bsdf():
+    sys.path.insert(0, str(ROOT / "tests"))
+    import bsdf_cases
+
+    tup = bsdf_cases.tuples(512, 1)
+    out = {name: ref.bsdf_query(m, tup, med) for name, m, med in bsdf_cases.cases()}
+    np.savez_compressed(OUT / "bsdf.npz", **out)
+
+
+def small_terrain(spp):
+    return prt_scenes.terrain(seed=1, grid=96, n_spheres=24, width=128, height=64, spp=spp, extent=12.0, relief=3.0,
+                              with_sky=False)
+
+
+def make_terrain_images():
+    out = {}
+    for spp in (16, 256):
+        for seed in (0, 1):
+            dev = ref.RefDevice(small_terrain(spp), seed=seed)
+            st = dev.render(spp)
+            out[f"spp{spp}_seed{seed}"] = dev.blit()
+            out[f"spp{spp}_seed{seed}_rays"] = np.float64(st["rays"])
+            dev.close()
+    np.savez_compressed(OUT / "terrain_img.npz", **out)
+
+
 def make_sunsky():
     d = prt_scenes.sun_direction()
     sun, angle, sky = ref.sunsky(d, prt_scenes.SUN_TURBIDITY, prt_scenes.SUN_GROUND_ALBEDO)
@@ -103,7 +133,11 @@ def make_sunsky():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["sobol", "rays", "images", "sunsky"]
+    which = sys.argv[1:] or ["sobol", "rays", "images", "sunsky", "bsdf", "terrain"]
+    if "terrain" in which:
+        make_terrain_images()
+    if "bsdf" in which:
+        make_bsdf()
     if "sunsky" in which:
         make_sunsky()
     if "sobol" in which:

@@ -142,3 +142,28 @@ def test_restated_sobol_matches_reference_fixture(golden, seed, dims):
     diff = out.view(np.uint32) != scalar.view(np.uint32)
     assert diff.mean() < 0.15
     assert np.all(np.abs(out[diff] - scalar[diff]) <= 2.5e-7)
+
+
+def test_cpp_wrapper_compiles_and_links(tmp_path):
+    """The C++ Device mirror (host/device_cuda.hpp) compiles against the C ABI and links with
+    libprt_cuda.so; a host-only entry point runs without a GPU."""
+    import shutil
+    import subprocess
+
+    if shutil.which("g++") is None:
+        pytest.skip("no C++ compiler")
+    src = tmp_path / "wrapper.cpp"
+    src.write_text(
+        '#include "device_cuda.hpp"\n'
+        "#include <cstdio>\n"
+        "int main() {\n"
+        "  prt_material m; prt_cuda_material_defaults(&m);\n"
+        '  std::printf("%g %g %g\\n", m.base_color[0], m.specular_ior, m.coat_ior);\n'
+        "  return (m.base_color_texture == -1 && m.opacity == 1.f) ? 0 : 1;\n"
+        "}\n")
+    exe = tmp_path / "wrapper"
+    pkg = ROOT / "oidn-protoray_b200"
+    subprocess.run(["g++", "-std=c++17", "-I", str(pkg / "host"), str(src), "-o", str(exe), "-L", str(pkg),
+                    "-lprt_cuda", f"-Wl,-rpath,{pkg}"], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    assert [float(x) for x in out] == [0.8, 1.5, 1.6]
