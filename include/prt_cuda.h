@@ -217,6 +217,23 @@ int prt_cuda_clear(prt_context* ctx);
  * (render/device_cpu.cpp:53-59), each advancing the sample index by one. */
 int prt_cuda_render(prt_context* ctx, int32_t spp, prt_render_stats* stats);
 
+/* No counterpart in the reference. Rendering for callers that must not allocate device memory:
+ * hosts whose device memory is owned by their own pool or budget, and hosts that may not take the
+ * device-wide synchronisation a cudaMalloc/cudaFree can cause in the middle of their work.
+ * Renders `spp` samples per pixel numbered from `first_sample` (the same samples prt_cuda_render
+ * draws at that sample index) with the current scene, camera, renderer and seed, and writes
+ * their average to `hdr_out`: width*height RGB floats, row-major, in device or managed memory the
+ * caller owns. The frame and sample index of prt_cuda_render are left untouched.
+ * No device memory is allocated or freed: path state, queues, counters and sums live in one
+ * scratch area compiled into the library (about 18 MB, present on every GPU that loads it until
+ * the process exits), sized for frames of at most 65,536 pixels (e.g. 256x256) and
+ * maxDepth <= 1000; larger frames are rejected with PRT_ERR_INVALID_ARG.
+ * The first call on a device looks up the area's device address; make that first call before
+ * any stream capture. All calls on a device share the one area (each call zeroes what must start
+ * at zero), so calls whose GPU work overlaps -- from several contexts or threads on one device --
+ * race and must be serialised by the caller. */
+int prt_cuda_render_static(prt_context* ctx, uint32_t first_sample, int32_t spp, float* hdr_out);
+
 /* Launch tuning of the wavefront kernels; 0 in a field keeps the current value.
  * trace_blocks / shade_blocks: persistent blocks of 256 threads per SM for the traversal and
  *   shading kernels;

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -1060,6 +1061,143 @@ int prt_cuda_autotune(prt_context* ctx, int32_t spp, prt_tuning* chosen, double*
       chosen->wave_paths = (int32_t)bW;
     }
     if (mrays) *mrays = best;
+  });
+}
+
+} // extern "C"
+
+// ---- Rendering without device allocation ------------------------------------------------------
+//
+// prt_cuda_render_static renders from a fixed scratch area compiled into this library instead of
+// the path state that prt_cuda_render allocates on demand. The area holds the path state of at
+// most kStaticPaths paths, three accumulation planes of as many pixels, and the per-bounce
+// counters for maxDepth <= kStaticMaxDepth: about 18 MB on every GPU that loads the library,
+// held until the process exits.
+
+namespace {
+
+constexpr int64_t kStaticPaths = 1 << 16;  // paths in flight = largest frame, in pixels
+constexpr int kStaticMaxDepth = 1000;      // the deepest renderer prt_cuda_renderer accepts
+constexpr size_t kStaticAlign = 256;
+
+constexpr size_t staticRound(size_t n) { return (n + kStaticAlign - 1) / kStaticAlign * kStaticAlign; }
+
+// Byte offsets of the carved buffers.
+constexpr size_t kStaticPlane = staticRound(sizeof(float4) * kStaticPaths);  // one float4 per path
+constexpr size_t kStaticQueue = staticRound(sizeof(int) * kStaticPaths);
+constexpr size_t kStaticPathPlanes = 12;  // rayO rayD hit thr rad info shO shD shL out aovA aovN
+constexpr size_t kStaticOffQueues = kStaticPathPlanes * kStaticPlane;
+constexpr size_t kStaticOffAccum = kStaticOffQueues + (2 + kShadeClasses) * kStaticQueue;
+constexpr size_t kStaticOffCounters = kStaticOffAccum + 3 * kStaticPlane;
+constexpr size_t kStaticOffTrav = kStaticOffCounters + staticRound(sizeof(int) * 16 * (kStaticMaxDepth + 2));
+constexpr size_t kStaticOffErr = kStaticOffTrav + staticRound(4 * sizeof(unsigned long long));
+constexpr size_t kStaticBytes = kStaticOffErr + kStaticAlign;
+
+// The scratch area itself. Host code must not pass `gStaticScratch` to a kernel: on the host the
+// name denotes a host-side shadow, not the device address. staticScratchOf() looks the device
+// address up once per device.
+static __device__ __align__(256) unsigned char gStaticScratch[kStaticBytes];
+
+constexpr int kStaticMaxDevices = 64;
+std::mutex gStaticMutex;
+unsigned char* gStaticAddr[kStaticMaxDevices] = {};
+
+// Device address of the scratch area on device `dev`, which must be the current device.
+unsigned char* staticScratchOf(int dev)
+{
+  if (dev < 0 || dev >= kStaticMaxDevices) throw ApiError{PRT_ERR_INVALID_ARG, "device ordinal out of range"};
+  std::lock_guard<std::mutex> lock(gStaticMutex);
+  if (!gStaticAddr[dev])
+  {
+    void* p = nullptr;
+    cuCheck(cudaGetSymbolAddress(&p, gStaticScratch), "cudaGetSymbolAddress(static scratch)");
+    gStaticAddr[dev] = static_cast<unsigned char*>(p);
+  }
+  return gStaticAddr[dev];
+}
+
+// Restores the context's own path state, frame and sample index when the static render returns
+// or throws.
+struct StaticSwap
+{
+  Context& c;
+  PathState ps;
+  float *accum, *accumA, *accumN;
+  int waveSamples, profileFlags;
+  uint32_t sampleIndex;
+  explicit StaticSwap(Context& ctx)
+      : c(ctx), ps(ctx.ps), accum(ctx.accum), accumA(ctx.accumA), accumN(ctx.accumN), waveSamples(ctx.waveSamples),
+        profileFlags(ctx.profileFlags), sampleIndex(ctx.sampleIndex)
+  {
+  }
+  ~StaticSwap()
+  {
+    c.ps = ps;
+    c.accum = accum;
+    c.accumA = accumA;
+    c.accumN = accumN;
+    c.waveSamples = waveSamples;
+    c.profileFlags = profileFlags;
+    c.sampleIndex = sampleIndex;
+  }
+};
+
+} // namespace
+
+extern "C" {
+
+int prt_cuda_render_static(prt_context* ctx, uint32_t first_sample, int32_t spp, float* hdr_out)
+{
+  return guarded(ctx, [&](Context& c) {
+    requireScene(c);
+    if (!c.hasRenderer || !c.hasCamera || !c.accum) throw ApiError{PRT_ERR_STATE, "renderer, camera and frame are required"};
+    if (spp <= 0) throw std::invalid_argument("spp must be > 0");
+    if (!hdr_out) throw std::invalid_argument("null output");
+    const int64_t px = (int64_t)c.width * c.height;
+    if (px > kStaticPaths)
+      throw std::invalid_argument("frame of " + std::to_string(c.width) + "x" + std::to_string(c.height) + " = " +
+                                  std::to_string(px) + " pixels exceeds the static scratch limit of " +
+                                  std::to_string(kStaticPaths) + " pixels");
+    if (c.renderer.maxDepth > kStaticMaxDepth) throw std::invalid_argument("maxDepth exceeds the static scratch limit");
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, hdr_out) != cudaSuccess ||
+        (attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged))
+    {
+      cudaGetLastError();
+      throw std::invalid_argument("hdr_out must be device or managed memory");
+    }
+    cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+    unsigned char* base = staticScratchOf(c.device);
+
+    StaticSwap keep(c);
+    PathState s;
+    s.capacity = kStaticPaths;
+    float4* planes[kStaticPathPlanes];
+    for (size_t k = 0; k < kStaticPathPlanes; ++k) planes[k] = reinterpret_cast<float4*>(base + k * kStaticPlane);
+    s.rayO = planes[0]; s.rayD = planes[1]; s.hit = planes[2]; s.thr = planes[3]; s.rad = planes[4];
+    s.info = reinterpret_cast<uint4*>(planes[5]);
+    s.shO = planes[6]; s.shD = planes[7]; s.shL = planes[8]; s.out = planes[9];
+    s.aovA = planes[10]; s.aovN = planes[11];
+    s.queue[0] = reinterpret_cast<int*>(base + kStaticOffQueues);
+    s.queue[1] = reinterpret_cast<int*>(base + kStaticOffQueues + kStaticQueue);
+    s.classQueues = reinterpret_cast<int*>(base + kStaticOffQueues + 2 * kStaticQueue);
+    s.counters = reinterpret_cast<int*>(base + kStaticOffCounters);
+    s.travCounts = reinterpret_cast<unsigned long long*>(base + kStaticOffTrav);
+    s.err = reinterpret_cast<uint32_t*>(base + kStaticOffErr);
+    c.ps = s;
+    c.accum = reinterpret_cast<float*>(base + kStaticOffAccum);
+    c.accumA = c.aovMask ? reinterpret_cast<float*>(base + kStaticOffAccum + kStaticPlane) : nullptr;
+    c.accumN = c.aovMask ? reinterpret_cast<float*>(base + kStaticOffAccum + 2 * kStaticPlane) : nullptr;
+    c.waveSamples = (int)(kStaticPaths / px);
+    c.sampleIndex = first_sample;
+    c.profileFlags = 0;
+    // The area keeps the previous call's contents: zero the sums and the error flag.
+    cuCheck(cudaMemsetAsync(base + kStaticOffAccum, 0, 3 * kStaticPlane, c.stream), "clear static sums");
+    cuCheck(cudaMemsetAsync(s.err, 0, sizeof(uint32_t), c.stream), "clear static error flag");
+    RenderCounters rc;
+    cuCheck(renderSamples(c, spp, rc), "static render");
+    cuCheck(launchBlit(c, 0, hdr_out), "static blit");
+    checkDeviceErrors(c);
   });
 }
 
