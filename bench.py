@@ -109,10 +109,10 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(spp_frames=1):
+def cpu_baseline(min_seconds=10.0):
     """The reference's own CPU path (oracle/_ref, compiled from the reference sources) on a
-    bounded sample of the same workload: one full-resolution 1-spp frame after one warm-up
-    frame, all host threads."""
+    bounded sample of the same workload: full-resolution 1-spp frames of the terrain scene,
+    after one warm-up frame, until at least `min_seconds` of render time; all host threads."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import ref  # test infrastructure: the CPU-baseline leg only
 
@@ -121,13 +121,18 @@ def cpu_baseline(spp_frames=1):
     scene = prt_scenes.terrain(with_sky=False)
     dev = ref.RefDevice(scene, seed=0)
     dev.render(1)  # warm-up frame
-    st = dev.render(spp_frames)
+    rays, secs, frames = 0.0, 0.0, 0
+    while secs < min_seconds:
+        st = dev.render(1)
+        rays += st["rays"]
+        secs += st["seconds"]
+        frames += 1
     dev.close()
-    return {"value": st["rays"] / 1e6 / st["seconds"], "unit": UNIT, "cores": ref.hardware_threads(),
+    return {"value": rays / 1e6 / secs, "unit": UNIT, "cores": ref.hardware_threads(),
             "kind": "reference",
-            "sample": f"{spp_frames} frame(s) of the terrain workload at 1920x1080 x 1 spp after 1 warm-up frame "
-                      f"({st['rays'] / 1e6:.1f}M rays in {st['seconds']:.1f} s); reference pathStream renderer "
-                      f"compiled from its sources, oracle CPU BVH in place of Embree (not installed)"}
+            "sample": f"{frames} frames of the terrain workload at 1920x1080 x 1 spp (samples 1..{frames} of the "
+                      f"64-spp frame) after 1 warm-up frame ({rays / 1e6:.1f}M rays in {secs:.1f} s); reference "
+                      f"pathStream renderer compiled from its sources, oracle CPU BVH in place of Embree (not installed)"}
 
 
 def run_reference(args):
@@ -221,7 +226,7 @@ def run_ours(args):
     dev.clear_frame()
     sampler = ClockSampler(local)
     sampler.start()
-    ms = rays = closest = shadow = trace_ms = shadow_ms = launches = 0.0
+    ms = rays = closest = shadow = trace_ms = shadow_ms = shade_ms = launches = trace_launches = 0.0
     t0 = time.perf_counter()
     for _ in range(args.steps):
         st = dev.render(args.spp)
@@ -231,7 +236,9 @@ def run_ours(args):
         shadow += st["shadow_rays"]
         trace_ms += st["trace_ms"]
         shadow_ms += st["shadow_ms"]
+        shade_ms += st["shade_ms"]
         launches += st["kernel_launches"]
+        trace_launches += st["trace_launches"]
     wall = time.perf_counter() - t0
     clocks = sampler.stop()
     barrier()
@@ -255,12 +262,16 @@ def run_ours(args):
     e2e_wall = max_over_ranks(time.perf_counter() - te)
     e2e_value = sum_over_ranks(e2e_rays) / 1e6 / e2e_wall
 
-    # Roofline of the dominant kernels (closest + any-hit traversal): algorithmic bytes per ray
-    # B = ray in + hit out + 80 B per node visit + 48 B per triangle test.
+    # Roofline of the dominant kernel, the closest-hit BVH8 traversal (kTrace, ~60% of the
+    # frame): algorithmic bytes per ray B = ray in + hit out + 80 B per node visit + 48 B per
+    # triangle test, over its CUDA-event time. Measured DRAM traffic: NCU_TRACE_DRAM_BYTES of
+    # one 1-spp frame's kTrace launches (profiles/kTrace_terrain_1spp.md), per closest ray of
+    # that frame, times the closest rays of an average launch here.
     b_closest = 32 + 16 + 80 * n_closest + 48 * t_closest
     b_shadow = 32 + 4 + 80 * n_shadow + 48 * t_shadow
-    trav_ms = trace_ms + shadow_ms
-    achieved = (closest * b_closest + shadow * b_shadow) / (trav_ms * 1e-3) / 1e9
+    achieved = closest * b_closest / (trace_ms * 1e-3) / 1e9
+    per_launch_rays = closest / max(trace_launches, 1)
+    traffic = NCU_TRACE_DRAM_BYTES / max(c["closest_rays"], 1) * per_launch_rays
     peak, peak_kind = measured_peaks()
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -276,12 +287,18 @@ def run_ours(args):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(C_CAMERA_BYTES),
                 "d2h_bytes_per_step": int(img.nbytes)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "peak_kind": peak_kind,
-                     "kernel": "closest-hit + any-hit BVH8 traversal",
+                     "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "kTrace (closest-hit BVH8 traversal + hit binning)",
+                     "algorithmic_bytes_per_launch": per_launch_rays * b_closest,
+                     "launch_ms": trace_ms / max(trace_launches, 1),
+                     "launches_per_step": trace_launches / args.steps,
                      "bytes_per_ray": {"closest": b_closest, "shadow": b_shadow},
                      "per_ray": {"closest_nodes": n_closest, "closest_tris": t_closest, "shadow_nodes": n_shadow,
                                  "shadow_tris": t_shadow},
-                     "kernel_ms_per_step": trav_ms / args.steps},
+                     "traffic_note": "ncu DRAM bytes of a 1-spp frame's kTrace launches, scaled per closest ray"},
+        "kernel_ms_per_step": {"trace": trace_ms / args.steps, "shadow": shadow_ms / args.steps,
+                               "shade": shade_ms / args.steps},
+        "rays_per_step": {"closest": closest / args.steps, "shadow": shadow / args.steps},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -294,6 +311,10 @@ def run_ours(args):
     if pg is not None:
         pg.destroy_process_group()
 
+
+# DRAM bytes (read + write) of the 9 kTrace launches of one 1920x1080 x 1-spp terrain frame,
+# from ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum (profiles/kTrace_terrain_1spp.md).
+NCU_TRACE_DRAM_BYTES = 781_850_368
 
 C_CAMERA_BYTES = 4 * 14  # prt_camera_desc: 12 floats of basis and position + fov + near clip
 

@@ -172,6 +172,7 @@ typedef struct prt_render_stats
   int64_t closest_tris;     /* triangle tests of closest-hit rays (PRT_PROFILE_COUNTS) */
   int64_t shadow_nodes;     /* node visits of shadow rays (PRT_PROFILE_COUNTS) */
   int64_t shadow_tris;      /* triangle tests of shadow rays (PRT_PROFILE_COUNTS) */
+  int64_t trace_launches;   /* closest-hit traversal launches (one per bounce per wave) */
 } prt_render_stats;
 
 /* Profiling switches for prt_cuda_set_profiling. Kernel timing records CUDA events around

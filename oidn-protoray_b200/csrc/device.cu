@@ -795,6 +795,7 @@ int prt_cuda_render(prt_context* ctx, int32_t spp, prt_render_stats* stats)
       stats->closest_tris = (int64_t)rc.trav[1];
       stats->shadow_nodes = (int64_t)rc.trav[2];
       stats->shadow_tris = (int64_t)rc.trav[3];
+      stats->trace_launches = rc.traceLaunches;
     }
   });
 }

@@ -784,6 +784,7 @@ cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
         kShadow<false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow);
       end();
       rc.launches += 3 + kShadeClasses;
+      rc.traceLaunches++;
       e = cudaGetLastError();
       if (e != cudaSuccess) return e;
       // Paths in, shadow rays and paths out of this bounce; stop once no path is left.

@@ -77,7 +77,7 @@ struct Context
 // Per-call statistics gathered by renderSamples.
 struct RenderCounters
 {
-  int64_t closestRays = 0, shadowRays = 0, launches = 0;
+  int64_t closestRays = 0, shadowRays = 0, launches = 0, traceLaunches = 0;
   double traceMs = 0.0, shadowMs = 0.0, shadeMs = 0.0;
   unsigned long long trav[4] = {0, 0, 0, 0};
 };

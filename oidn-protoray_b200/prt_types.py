@@ -176,6 +176,7 @@ class RenderStats(C.Structure):
         ("closest_tris", C.c_int64),
         ("shadow_nodes", C.c_int64),
         ("shadow_tris", C.c_int64),
+        ("trace_launches", C.c_int64),
     ]
 
 
