@@ -255,6 +255,39 @@ int prt_cuda_get_tuning(prt_context* ctx, prt_tuning* tuning);
  * Mrays/s. */
 int prt_cuda_autotune(prt_context* ctx, int32_t spp, prt_tuning* chosen, double* mrays);
 
+/* ---- batch rendering -------------------------------------------------------------------
+ * No counterpart in the reference, whose Device renders one scene per call. A batch holds many
+ * independent frames -- each with its own scene, camera, renderer settings, sampler seed,
+ * size, sample count and AOVs -- and renders all of them in one persistent wavefront: the
+ * frames' paths share one path pool, terminated paths are replaced by new camera paths of any
+ * frame (path regeneration), and the bounce loop is a CUDA graph replayed until every frame
+ * has all its samples. Each frame gets the image that prt_cuda_render would produce for it
+ * (samples 0..spp-1 of its seed), up to the order of floating-point additions per pixel. */
+typedef struct prt_batch prt_batch;
+
+typedef struct prt_batch_item
+{
+  const prt_scene_desc* scene;   /* borrowed for prt_cuda_batch_create only */
+  prt_camera_desc       camera;
+  prt_renderer_desc     renderer;
+  int32_t               width;   /* multiple of 32, like prt_cuda_frame */
+  int32_t               height;  /* multiple of 8 */
+  int32_t               spp;
+  int32_t               aov_mask;  /* PRT_AOV_* */
+  uint32_t              seed;      /* sampler seed (Device::initSampler) */
+  int32_t               reserved;
+} prt_batch_item;
+
+/* Uploads every item's scene (BVH8 build, materials, lights) and allocates the frames and the
+ * shared path pool (prt_tuning.wave_paths slots at most). */
+int prt_cuda_batch_create(prt_context* ctx, const prt_batch_item* items, int32_t count, prt_batch** out_batch);
+/* Clears the frames and renders every item to completion; stats count all items' rays
+ * (stats->spp is 0: the items' sample counts differ). */
+int prt_cuda_batch_render(prt_batch* batch, prt_render_stats* stats);
+/* Device::blitFrame of one item: width*height RGB floats (host or device memory). */
+int prt_cuda_batch_blit(prt_batch* batch, int32_t item, int32_t aov, float* dst);
+int prt_cuda_batch_destroy(prt_batch* batch);
+
 /* Enables PRT_PROFILE_* instrumentation for subsequent render calls (0 = off). */
 int prt_cuda_set_profiling(prt_context* ctx, int32_t flags);
 

@@ -615,6 +615,24 @@ void checkDeviceErrors(Context& c)
   }
 }
 
+// PinholeCamera constructor (camera/pinhole_camera.h:20-36) for a width x height frame.
+DevCamera makeCamera(const prt_camera_desc& cam, int width, int height)
+{
+  DevCamera d;
+  const float aspect = float(width) / float(height);
+  const float hh = std::tan(0.5f * cam.fov);
+  const float hw = hh * aspect;
+  auto basis = [&](float x, float y, float z, float* out) {
+    for (int k = 0; k < 3; ++k) out[k] = x * cam.basis_u[k] + y * cam.basis_v[k] + z * cam.basis_n[k];
+  };
+  for (int k = 0; k < 3; ++k) d.org[k] = cam.position[k];
+  basis(-hw, hh, -1.f, d.imageO);
+  basis(2.f * hw, 0.f, 0.f, d.imageDx);
+  basis(0.f, -2.f * hh, 0.f, d.imageDy);
+  d.nearClip = cam.near_clip;
+  return d;
+}
+
 void requireScene(Context& c)
 {
   if (!c.hasScene) throw ApiError{PRT_ERR_STATE, "no scene uploaded"};
@@ -730,18 +748,7 @@ int prt_cuda_camera(prt_context* ctx, const prt_camera_desc* cam)
   return guarded(ctx, [&](Context& c) {
     if (!cam) throw std::invalid_argument("null camera");
     if (c.width <= 0) throw ApiError{PRT_ERR_STATE, "initialise the frame before the camera"};
-    // PinholeCamera constructor (camera/pinhole_camera.h:20-36).
-    const float aspect = float(c.width) / float(c.height);
-    const float hh = std::tan(0.5f * cam->fov);
-    const float hw = hh * aspect;
-    auto basis = [&](float x, float y, float z, float* out) {
-      for (int k = 0; k < 3; ++k) out[k] = x * cam->basis_u[k] + y * cam->basis_v[k] + z * cam->basis_n[k];
-    };
-    for (int k = 0; k < 3; ++k) c.camera.org[k] = cam->position[k];
-    basis(-hw, hh, -1.f, c.camera.imageO);
-    basis(2.f * hw, 0.f, 0.f, c.camera.imageDx);
-    basis(0.f, -2.f * hh, 0.f, c.camera.imageDy);
-    c.camera.nearClip = cam->near_clip;
+    c.camera = makeCamera(*cam, c.width, c.height);
     c.hasCamera = true;
   });
 }
@@ -1200,6 +1207,175 @@ int prt_cuda_render_static(prt_context* ctx, uint32_t first_sample, int32_t spp,
     cuCheck(launchBlit(c, 0, hdr_out), "static blit");
     checkDeviceErrors(c);
   });
+}
+
+} // extern "C"
+
+// ---- batch rendering ----------------------------------------------------------------------------
+
+struct prt_batch
+{
+  prt_context* ctx;
+  BatchState b;
+};
+
+namespace {
+
+void freeBatch(BatchState& b)
+{
+  if (b.exec) cudaGraphExecDestroy(b.exec);
+  b.exec = nullptr;
+  for (auto& x : b.bufs) cudaFree(x.ptr);
+  b.bufs.clear();
+}
+
+} // namespace
+
+extern "C" {
+
+int prt_cuda_batch_create(prt_context* ctx, const prt_batch_item* items, int32_t count, prt_batch** out)
+{
+  if (out) *out = nullptr;
+  return guarded(ctx, [&](Context& c) {
+    if (!out || !items || count <= 0) throw std::invalid_argument("invalid batch description");
+    cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+    std::unique_ptr<prt_batch> bp(new prt_batch{ctx, BatchState()});
+    BatchState& B = bp->b;
+    try
+    {
+      for (int i = 0; i < count; ++i)
+      {
+        const prt_batch_item& it = items[i];
+        if (!it.scene) throw std::invalid_argument("batch item without a scene");
+        if (it.width <= 0 || it.height <= 0 || it.spp <= 0) throw std::invalid_argument("invalid batch item frame");
+        if (it.width % 32 != 0 || it.height % 8 != 0)
+          throw std::logic_error("image size is not divisible by the tile size");
+        if (it.width > 4096 || it.height > 4096) throw std::logic_error("image size is too large");
+        if (it.renderer.max_depth < 0 || it.renderer.max_depth > 1000) throw std::invalid_argument("invalid renderer settings");
+        if (it.aov_mask & ~(PRT_AOV_ALBEDO1 | PRT_AOV_NORMAL1)) throw std::invalid_argument("unknown AOV bits");
+        // Scene upload through the frame form's path, into buffers the batch owns.
+        Context tmp;
+        tmp.device = c.device;
+        tmp.stream = c.stream;
+        tmp.smCount = c.smCount;
+        uploadScene(tmp, it.scene);
+        B.bufs.insert(B.bufs.end(), tmp.sceneBufs.begin(), tmp.sceneBufs.end());
+        tmp.sceneBufs.clear();
+        BatchItem bi;
+        std::memset(&bi, 0, sizeof(bi));
+        bi.sc = tmp.scene;
+        bi.cam = makeCamera(it.camera, it.width, it.height);
+        bi.rd = DevRenderer{it.renderer.max_depth, it.renderer.rr_depth, it.renderer.min_weight, it.renderer.max_radiance,
+                            it.seed};
+        bi.width = it.width;
+        bi.height = it.height;
+        bi.pixelCount = it.width * it.height;
+        bi.aovMask = it.aov_mask;
+        bi.workBase = B.workTotal;
+        bi.workCount = (long long)bi.pixelCount * it.spp;
+        B.workTotal += bi.workCount;
+        const size_t plane = (size_t)bi.pixelCount * sizeof(float4);
+        bi.accum = (float4*)devAlloc(c, plane, &B.bufs);
+        if (it.aov_mask)
+        {
+          bi.accA = (float4*)devAlloc(c, plane, &B.bufs);
+          bi.accN = (float4*)devAlloc(c, plane, &B.bufs);
+          B.anyAov = true;
+        }
+        B.maxDepth = std::max(B.maxDepth, it.renderer.max_depth);
+        B.items.push_back(bi);
+      }
+      // Shared path pool: as many slots as the frame form's wave, at most the whole batch.
+      const int64_t C = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(c.wavePaths, B.workTotal), 1ll << 30));
+      PathState& s = B.ps;
+      s.capacity = C;
+      auto a4 = [&](int64_t n) { return (float4*)devAlloc(c, (size_t)n * sizeof(float4), &B.bufs); };
+      s.rayO = a4(C); s.rayD = a4(C); s.hit = a4(C); s.thr = a4(C); s.rad = a4(C);
+      s.info = (uint4*)a4(C);
+      s.shO = a4(C); s.shD = a4(C); s.shL = a4(C);
+      if (B.anyAov)
+      {
+        s.aovA = a4(C);
+        s.aovN = a4(C);
+      }
+      s.queue[0] = (int*)devAlloc(c, (size_t)C * sizeof(int), &B.bufs);
+      s.queue[1] = (int*)devAlloc(c, (size_t)C * sizeof(int), &B.bufs);
+      s.classQueues = (int*)devAlloc(c, (size_t)C * kShadeClasses * sizeof(int), &B.bufs);
+      s.err = c.ps.err;
+      s.travCounts = c.ps.travCounts;
+      B.freeList[0] = (int*)devAlloc(c, (size_t)C * sizeof(int), &B.bufs);
+      B.freeList[1] = (int*)devAlloc(c, (size_t)C * sizeof(int), &B.bufs);
+      B.ctl = (BatchCtl*)devAlloc(c, sizeof(BatchCtl), &B.bufs);
+      B.dItems = (BatchItem*)devAlloc(c, B.items.size() * sizeof(BatchItem), &B.bufs);
+      cuCheck(cudaMemcpyAsync(B.dItems, B.items.data(), B.items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice,
+                              c.stream), "batch items");
+      cuCheck(cudaStreamSynchronize(c.stream), "batch upload");
+    }
+    catch (...)
+    {
+      freeBatch(B);
+      throw;
+    }
+    *out = bp.release();
+  });
+}
+
+int prt_cuda_batch_render(prt_batch* batch, prt_render_stats* stats)
+{
+  if (!batch) return PRT_ERR_INVALID_ARG;
+  return guarded(batch->ctx, [&](Context& c) {
+    BatchState& B = batch->b;
+    cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+    RenderCounters rc;
+    cuCheck(cudaEventRecord(c.ev0, c.stream), "event");
+    const cudaError_t e = renderBatch(c, B, rc);
+    if (e == cudaErrorLaunchTimeout)
+      throw ApiError{PRT_ERR_DEVICE_ABORT, "batch render did not finish within its iteration bound"};
+    cuCheck(e, "batch render");
+    cuCheck(cudaEventRecord(c.ev1, c.stream), "event");
+    cuCheck(cudaEventSynchronize(c.ev1), "batch sync");
+    checkDeviceErrors(c);
+    float ms = 0.f;
+    cuCheck(cudaEventElapsedTime(&ms, c.ev0, c.ev1), "event time");
+    if (stats)
+    {
+      std::memset(stats, 0, sizeof(*stats));
+      stats->rays = rc.closestRays + rc.shadowRays;
+      stats->spp = 0;
+      stats->render_ms = ms;
+      stats->mray = ms > 0.f ? (double)stats->rays / 1e6 / (ms * 1e-3) : 0.0;
+      stats->closest_rays = rc.closestRays;
+      stats->shadow_rays = rc.shadowRays;
+      stats->kernel_launches = rc.launches;
+      stats->trace_launches = rc.traceLaunches;
+    }
+  });
+}
+
+int prt_cuda_batch_blit(prt_batch* batch, int32_t item, int32_t aov, float* dst)
+{
+  if (!batch) return PRT_ERR_INVALID_ARG;
+  return guarded(batch->ctx, [&](Context& c) {
+    BatchState& B = batch->b;
+    if (item < 0 || item >= (int)B.items.size() || !dst) throw std::invalid_argument("invalid batch item or destination");
+    const BatchItem& it = B.items[item];
+    if (aov < 0 || aov > 2 || (aov > 0 && !it.accA)) throw std::invalid_argument("AOV not enabled");
+    const float4* plane = aov == 0 ? it.accum : (aov == 1 ? it.accA : it.accN);
+    Staged o(c, dst, (size_t)it.pixelCount * 3 * sizeof(float), false);
+    cuCheck(launchBlitPlane(c, plane, it.pixelCount, (float*)o.dev), "batch blit");
+    o.copyOut();
+    cuCheck(cudaStreamSynchronize(c.stream), "batch blit sync");
+  });
+}
+
+int prt_cuda_batch_destroy(prt_batch* batch)
+{
+  if (!batch) return PRT_ERR_INVALID_ARG;
+  cudaSetDevice(batch->ctx->c.device);
+  cudaStreamSynchronize(batch->ctx->c.stream);
+  freeBatch(batch->b);
+  delete batch;
+  return PRT_OK;
 }
 
 } // extern "C"

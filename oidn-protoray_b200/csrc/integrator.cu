@@ -18,6 +18,7 @@
 #include "bsdf.cuh"
 
 #include <algorithm>
+#include <cstddef>
 #include <cstring>
 
 namespace prt {
@@ -43,6 +44,11 @@ struct Launch
   uint32_t firstSample;
   int samples;       // samples in this wave
   int aovMask;
+  // Batch form only (nullptr / 0 in the frame form).
+  const BatchItem* items;
+  int itemCount;
+  BatchCtl* ctl;
+  int* freeList[2];
 };
 
 PRT_D int laneId() { return threadIdx.x & 31; }
@@ -217,36 +223,131 @@ __global__ void kBsdfQuery(DevTables tab, DevMaterial m, int mediumId, int64_t n
 }
 
 // ---- wavefront kernels -----------------------------------------------------------------------
+//
+// Every wavefront kernel exists in two forms, selected by the template flag `Batch`:
+//  * frame form (Batch = false): one scene and frame per launch (Launch::sc, ::cam, ::rd);
+//    the bounce depth is uniform per launch and finished paths write ps.out, which
+//    kAccumulate adds per pixel in sample order after the wave;
+//  * batch form (Batch = true): paths of many scenes share the queues. info.w of a path is its
+//    batch item (scene, camera, renderer, frame), info.z carries the bounce depth in bits
+//    16-31, finished paths add themselves to their item's accumulation planes and return their
+//    slot to the free list, and kBatchRegen refills free slots with new camera paths.
 
-// Path initialisation (render/path_renderer_stream.h:209-262).
+// Per-path view of the scene, renderer and frame a path belongs to.
+template <bool Batch>
+struct PathEnv;
+
+template <>
+struct PathEnv<false>
+{
+  const DevScene& sc;
+  const DevRenderer& rd;
+  int aovMask;
+  PRT_D PathEnv(const Launch& L, uint32_t) : sc(L.sc), rd(L.rd), aovMask(L.aovMask) {}
+};
+
+template <>
+struct PathEnv<true>
+{
+  const BatchItem& it;
+  const DevScene& sc;
+  const DevRenderer& rd;
+  int aovMask;
+  PRT_D PathEnv(const Launch& L, uint32_t item) : it(L.items[item]), sc(it.sc), rd(it.rd), aovMask(it.aovMask) {}
+};
+
+constexpr uint32_t kDepthShift = 16;
+constexpr uint32_t kMediumMask = 0xffffu;
+
+// Camera path of (sample, Morton index) in slot p (render/path_renderer_stream.h:209-262).
+PRT_D void initPath(const PathState& ps, int64_t p, const DevCamera& cam, const DevRenderer& rd, int width, int height,
+                    int idx, uint32_t sampleIndex, uint32_t item, bool aov)
+{
+  int x, y;
+  pixelOf(idx, width, x, y);
+  const uint32_t pixelId = (uint32_t)x | ((uint32_t)y << 16);
+  const SobolState st = sobolSetSample(rd.seed, sampleIndex, pixelId);
+  float sx, sy;
+  sobolGet2D(st, kDimPixel, sx, sy);
+  f3 org, dir;
+  float tnear;
+  cameraRay(cam, ((float)x + sx) * (1.f / (float)width), ((float)y + sy) * (1.f / (float)height), org, dir, tnear);
+  ps.rayO[p] = make_float4(org.x, org.y, org.z, tnear);
+  ps.rayD[p] = make_float4(dir.x, dir.y, dir.z, kPosMax);
+  ps.thr[p] = make_float4(1.f, 1.f, 1.f, 1.f);
+  ps.rad[p] = make_float4(0.f, 0.f, 0.f, __int_as_float(kSpecularReflection));
+  ps.info[p] = make_uint4(pixelId, sampleIndex, 0u, item);
+  if (aov)
+  {
+    ps.aovA[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    ps.aovN[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
+// Path initialisation of a frame-form wave.
 __global__ void kRaygen(Launch L)
 {
   const int64_t P = (int64_t)L.pixelCount * L.samples;
-  const float invW = 1.f / (float)L.width, invH = 1.f / (float)L.height;
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P; p += (int64_t)gridDim.x * blockDim.x)
   {
     const int s = (int)(p / L.pixelCount);
     const int idx = (int)(p - (int64_t)s * L.pixelCount);
-    int x, y;
-    pixelOf(idx, L.width, x, y);
-    const uint32_t pixelId = (uint32_t)x | ((uint32_t)y << 16);
-    const uint32_t sampleIndex = L.firstSample + (uint32_t)s;
-    const SobolState st = sobolSetSample(L.rd.seed, sampleIndex, pixelId);
-    float sx, sy;
-    sobolGet2D(st, kDimPixel, sx, sy);
-    f3 org, dir;
-    float tnear;
-    cameraRay(L.cam, ((float)x + sx) * invW, ((float)y + sy) * invH, org, dir, tnear);
-    L.ps.rayO[p] = make_float4(org.x, org.y, org.z, tnear);
-    L.ps.rayD[p] = make_float4(dir.x, dir.y, dir.z, kPosMax);
-    L.ps.thr[p] = make_float4(1.f, 1.f, 1.f, 1.f);
-    L.ps.rad[p] = make_float4(0.f, 0.f, 0.f, __int_as_float(kSpecularReflection));
-    L.ps.info[p] = make_uint4(pixelId, sampleIndex, 0u, 0u);
-    if (L.aovMask)
+    initPath(L.ps, p, L.cam, L.rd, L.width, L.height, idx, L.firstSample + (uint32_t)s, 0u, L.aovMask != 0);
+  }
+}
+
+// Batch form: the control step at the start of an iteration (one thread). `a` is the parity
+// of the iteration: it reads queue[a], free list a and counter block a, and the paths it
+// extends or frees go to queue[a ^ 1] and free list a ^ 1.
+__global__ void kBatchStep(BatchCtl* ctl, int a)
+{
+  const int b = a ^ 1;
+  int* ca = ctl->counts[a];
+  int* cb = ctl->counts[b];
+  ctl->rays[1] += (unsigned long long)cb[kBatchCntShadow];  // shadow rays of the previous iteration
+  const long long remaining = ctl->workTotal - ctl->workNext;
+  const long long freeSlots = ctl->freeCount[a];
+  const int n = (int)(remaining < freeSlots ? remaining : freeSlots);
+  ctl->regenCount = n;
+  ctl->regenBase = ctl->workNext;
+  ctl->regenOffset = ca[0];
+  ctl->workNext += n;
+  ca[0] += n;
+  ctl->rays[0] += (unsigned long long)ca[0];
+  for (int k = 1; k < kBatchCntStride; ++k) ca[k] = 0;
+  cb[0] = 0;
+  ctl->freeCount[b] = 0;
+  ctl->iterations += 1;
+  if (ca[0] == 0 && ctl->workNext >= ctl->workTotal) ctl->done = 1;
+}
+
+// Batch form: fills the slots on free list `a` with new camera paths (path regeneration) and
+// appends them to queue[a] after the paths extended by the previous iteration.
+__global__ void kBatchRegen(Launch L, int a, int* __restrict__ queue)
+{
+  const BatchCtl* ctl = L.ctl;
+  const int n = ctl->regenCount;
+  const long long base = ctl->regenBase;
+  const int offset = ctl->regenOffset;
+  const int* freeList = L.freeList[a];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+  {
+    const long long w = base + i;
+    // The item whose work range holds w (items are in work order).
+    int lo = 0, hi = L.itemCount - 1;
+    while (lo < hi)
     {
-      L.ps.aovA[p] = make_float4(0.f, 0.f, 0.f, 0.f);
-      L.ps.aovN[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+      const int mid = (lo + hi + 1) >> 1;
+      if (L.items[mid].workBase <= w) lo = mid;
+      else hi = mid - 1;
     }
+    const BatchItem& it = L.items[lo];
+    const long long local = w - it.workBase;
+    const int s = (int)(local / it.pixelCount);
+    const int idx = (int)(local - (long long)s * it.pixelCount);
+    const int slot = freeList[i];
+    initPath(L.ps, slot, it.cam, it.rd, it.width, it.height, idx, (uint32_t)s, (uint32_t)lo, it.aovMask != 0);
+    queue[offset + i] = slot;
   }
 }
 
@@ -266,12 +367,11 @@ PRT_D void addCounts(unsigned long long* dst, const TraceCount& c)
   }
 }
 
-// Closest-hit traversal of the queued rays. Persistent warps keep one ray per lane; when at
-// least L.refill lanes are idle the warp retires their finished rays -- writing the hit
-// and binning it by the shading it needs (the GPU form of the reference's material sort,
-// render/renderer_stream.h:108-181): class 0 ends the path (miss, area light, maxDepth),
-// classes 1.. are the material feature classes -- and fetches new rays for them.
-template <bool Count>
+// Closest-hit traversal of the queued rays. Persistent warps fetch 32 rays at a time, write
+// the hit and bin the path by the shading it needs (the GPU form of the reference's material
+// sort, render/renderer_stream.h:108-181): class 0 ends the path (miss, area light, maxDepth),
+// classes 1.. are the material feature classes.
+template <bool Count, bool Batch>
 __global__ void __launch_bounds__(256) kTrace(Launch L, const int* __restrict__ queue, const int* __restrict__ count,
                                               int* __restrict__ work, int depth, int* __restrict__ classQueues,
                                               int* __restrict__ classCounts)
@@ -290,11 +390,20 @@ __global__ void __launch_bounds__(256) kTrace(Launch L, const int* __restrict__ 
     {
       p = queue ? __ldg(queue + i) : i;
       const float4 a = L.ps.rayO[p], b = L.ps.rayD[p];
-      const TraceHit h = traverse<false, Count>(L.sc.nodes, L.sc.tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w,
+      uint32_t item = 0u;
+      int pathDepth = depth;
+      if (Batch)
+      {
+        const uint4 info = L.ps.info[p];
+        item = info.w;
+        pathDepth = (int)(info.z >> kDepthShift);
+      }
+      const PathEnv<Batch> E(L, item);
+      const TraceHit h = traverse<false, Count>(E.sc.nodes, E.sc.tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w,
                                                 L.ps.err, &tc);
       L.ps.hit[p] = make_float4(h.t, h.u, h.v, __int_as_float(h.triId));
       cls = 0;
-      if (h.triId >= 0 && depth < L.rd.maxDepth) cls = __ldg(L.sc.meshClass + __ldg(L.sc.triVerts + h.triId).w);
+      if (h.triId >= 0 && pathDepth < E.rd.maxDepth) cls = __ldg(E.sc.meshClass + __ldg(E.sc.triVerts + h.triId).w);
     }
     for (int c = 0; c < kShadeClasses; ++c)
     {
@@ -305,10 +414,46 @@ __global__ void __launch_bounds__(256) kTrace(Launch L, const int* __restrict__ 
   if (Count) addCounts(L.ps.travCounts, tc);
 }
 
+// Ends path p with radiance `rad`. Frame form: ps.out, summed later by kAccumulate. Batch
+// form: added to the item's accumulation planes at once (with the first-hit AOVs); the
+// caller returns the slot to the free list.
+template <bool Batch>
+PRT_D void finishPath(const Launch& L, int p, f3 rad, const uint4& info)
+{
+  if (!Batch)
+  {
+    const f3 c = clampL(rad, L.rd.maxRadiance);
+    L.ps.out[p] = make_float4(c.x, c.y, c.z, 1.f);
+    return;
+  }
+  const BatchItem& it = L.items[info.w];
+  const f3 c = clampL(rad, it.rd.maxRadiance);
+  const uint32_t pid = info.x;
+  const int q = (int)((pid >> 16) & 0x0fffu) * it.width + (int)(pid & 0x0fffu);
+  atomicAdd(it.accum + q, make_float4(c.x, c.y, c.z, 1.f));
+  if (it.aovMask)
+  {
+    const float4 va = L.ps.aovA[p], vn = L.ps.aovN[p];
+    if (va.w != 0.f) atomicAdd(it.accA + q, make_float4(va.x, va.y, va.z, 1.f));
+    if (vn.w != 0.f) atomicAdd(it.accN + q, make_float4(vn.x, vn.y, vn.z, 1.f));
+  }
+}
+
+// Batch form: returns the slots of the lanes with `freed` set to free list `b` (converged
+// warp, like warpAppend).
+template <bool Batch>
+PRT_D void freeSlots(const Launch& L, int b, bool freed, int p)
+{
+  if (!Batch) return;
+  const int f = warpAppend(&L.ctl->freeCount[b], freed);
+  if (freed) L.freeList[b][f] = p;
+}
+
 // Any-hit test of the queued shadow rays; adds the unoccluded NEE contribution and
 // finishes paths that ended at this bounce (render/path_renderer_stream.h:953-1010).
-template <bool Count>
-__global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__ count, int* __restrict__ work)
+template <bool Count, bool Batch>
+__global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__ count, int* __restrict__ work,
+                                               int parity)
 {
   const int n = *count;
   TraceCount tc;
@@ -319,15 +464,20 @@ __global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= n) break;
     const int i = base + laneId();
+    bool freed = false;
+    int p = 0;
     if (i < n)
     {
       const float4 a = L.ps.shO[i], b = L.ps.shD[i], c = L.ps.shL[i];
       const uint32_t tag = __float_as_uint(c.w);
-      const int p = (int)(tag & 0x7fffffffu);
+      p = (int)(tag & 0x7fffffffu);
+      uint4 info = make_uint4(0u, 0u, 0u, 0u);
+      if (Batch) info = L.ps.info[p];
+      const PathEnv<Batch> E(L, info.w);
       bool unoccluded = b.w > 0.f;
       if (unoccluded)
       {
-        const TraceHit h = traverse<true, Count>(L.sc.nodes, L.sc.tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w,
+        const TraceHit h = traverse<true, Count>(E.sc.nodes, E.sc.tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w,
                                                  L.ps.err, &tc);
         unoccluded = h.triId < 0;
       }
@@ -341,88 +491,91 @@ __global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__
       }
       if (tag & kShadowFinish)
       {
-        const f3 cl = clampL(mk(r.x, r.y, r.z), L.rd.maxRadiance);
-        L.ps.out[p] = make_float4(cl.x, cl.y, cl.z, 1.f);
+        finishPath<Batch>(L, p, mk(r.x, r.y, r.z), info);
+        freed = true;
       }
     }
+    freeSlots<Batch>(L, parity ^ 1, freed, p);
   }
   if (Count) addCounts(L.ps.travCounts + 2, tc);
-}
-
-PRT_D void finishPath(const Launch& L, int p, f3 rad)
-{
-  const f3 c = clampL(rad, L.rd.maxRadiance);
-  L.ps.out[p] = make_float4(c.x, c.y, c.z, 1.f);
 }
 
 // Paths that end at this bounce without shading a surface (render/path_renderer_stream.h:287-582
 // and the depth cut-off at :612): misses (environment lights), area-light hits, and surface
 // hits at maxDepth.
+template <bool Batch>
 __global__ void __launch_bounds__(256) kShadeEnd(Launch L, const int* __restrict__ queue, const int* __restrict__ count,
-                                                 int depth)
+                                                 int depth, int parity)
 {
   const int n = *count;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+  for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x)
   {
-    const int p = __ldg(queue + i);
-    const float4 rd = L.ps.rayD[p], hh = L.ps.hit[p];
-    const float4 tp = L.ps.thr[p];
-    float4 ra = L.ps.rad[p];
-    const uint32_t pixelId = L.ps.info[p].x;
-    const f3 dir = mk(rd.x, rd.y, rd.z);
-    const int triId = __float_as_int(hh.w);
-    const f3 T = mk(tp.x, tp.y, tp.z);
-    f3 Lr = mk(ra.x, ra.y, ra.z);
-    const float lastPdf = tp.w;
-    const int lastType = __float_as_int(ra.w);
-    const bool aov1 = (pixelId & kPathAov1Flag) == 0u;
-    if (triId < 0)
+    const int i = base + threadIdx.x;
+    const bool active = i < n;
+    const int p = active ? __ldg(queue + i) : 0;
+    if (active)
     {
-      float lightPdf;
-      const f3 Le = evalEnvLights(L.sc, dir, lightPdf);
-      const float w = (lastType & kBsdfSmooth) == 0 ? 1.f : misWeight(lastPdf, lightPdf);
-      Lr += T * w * Le;
-      if (aov1 && L.aovMask)
-      {
-        L.ps.aovA[p] = make_float4(0.f, 0.f, 0.f, 1.f);
-        L.ps.aovN[p] = make_float4(0.f, 0.f, 0.f, 1.f);
-      }
-    }
-    else
-    {
-      const int4 tv = __ldg(L.sc.triVerts + triId);
-      const int mesh = tv.w;
-      const int matId = __ldg(L.sc.meshMaterial + mesh);
-      if (L.sc.materials[matId].type & kMatEmissive)
+      const float4 rd = L.ps.rayD[p], hh = L.ps.hit[p];
+      const float4 tp = L.ps.thr[p];
+      float4 ra = L.ps.rad[p];
+      const uint4 info = L.ps.info[p];
+      const PathEnv<Batch> E(L, info.w);
+      const uint32_t pixelId = info.x;
+      const f3 dir = mk(rd.x, rd.y, rd.z);
+      const int triId = __float_as_int(hh.w);
+      const f3 T = mk(tp.x, tp.y, tp.z);
+      f3 Lr = mk(ra.x, ra.y, ra.z);
+      const float lastPdf = tp.w;
+      const int lastType = __float_as_int(ra.w);
+      const bool aov1 = (pixelId & kPathAov1Flag) == 0u;
+      if (triId < 0)
       {
         float lightPdf;
-        const int prim = triId - __ldg(L.sc.meshTriOffset + mesh);
-        const f3 Le = evalAreaLight(L.sc, mesh, prim, dir, hh.x, lightPdf);
+        const f3 Le = evalEnvLights(E.sc, dir, lightPdf);
         const float w = (lastType & kBsdfSmooth) == 0 ? 1.f : misWeight(lastPdf, lightPdf);
         Lr += T * w * Le;
-        if (aov1 && L.aovMask)
+        if (aov1 && E.aovMask)
         {
-          const f3 N = normalize(-dir);
-          L.ps.aovA[p] = make_float4(1.f, 1.f, 1.f, 1.f);
-          L.ps.aovN[p] = make_float4(N.x, N.y, N.z, 1.f);
+          L.ps.aovA[p] = make_float4(0.f, 0.f, 0.f, 1.f);
+          L.ps.aovN[p] = make_float4(0.f, 0.f, 0.f, 1.f);
         }
       }
-      // else: a surface at maxDepth ends the path with its current radiance.
+      else
+      {
+        const int4 tv = __ldg(E.sc.triVerts + triId);
+        const int mesh = tv.w;
+        const int matId = __ldg(E.sc.meshMaterial + mesh);
+        if (E.sc.materials[matId].type & kMatEmissive)
+        {
+          float lightPdf;
+          const int prim = triId - __ldg(E.sc.meshTriOffset + mesh);
+          const f3 Le = evalAreaLight(E.sc, mesh, prim, dir, hh.x, lightPdf);
+          const float w = (lastType & kBsdfSmooth) == 0 ? 1.f : misWeight(lastPdf, lightPdf);
+          Lr += T * w * Le;
+          if (aov1 && E.aovMask)
+          {
+            const f3 N = normalize(-dir);
+            L.ps.aovA[p] = make_float4(1.f, 1.f, 1.f, 1.f);
+            L.ps.aovN[p] = make_float4(N.x, N.y, N.z, 1.f);
+          }
+        }
+        // else: a surface at maxDepth ends the path with its current radiance.
+      }
+      finishPath<Batch>(L, p, Lr, info);
     }
-    finishPath(L, p, Lr);
+    freeSlots<Batch>(L, parity ^ 1, active, p);
   }
 }
 
 // Surface shading of one bounce (render/path_renderer_stream.h:592-949) for materials whose
 // lobes lie in feature set F: NEE with MIS, BSDF sampling, Russian roulette, medium tracking.
-template <int F>
+template <int F, bool Batch>
 __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __restrict__ queue,
-                                                     const int* __restrict__ count, int depth,
+                                                     const int* __restrict__ count, int launchDepth,
                                                      int* __restrict__ queueOut, int* __restrict__ extCount,
-                                                     int* __restrict__ shadowCount)
+                                                     int* __restrict__ shadowCount, int parity)
 {
   const int n = *count;
-  const uint32_t sampleDim = kDimBase + kDimBounce * (uint32_t)depth;
   for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x)
   {
     const int i = base + threadIdx.x;
@@ -430,6 +583,7 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
     const int p = active ? __ldg(queue + i) : 0;
     bool extend = false;
     bool shadow = false;
+    bool freed = false;
     float4 shO = make_float4(0.f, 0.f, 0.f, 0.f), shD = shO, shL = shO;
     if (active)
     {
@@ -437,6 +591,9 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
       const float4 tp = L.ps.thr[p];
       float4 ra = L.ps.rad[p];
       uint4 info = L.ps.info[p];
+      const PathEnv<Batch> E(L, info.w);
+      const int depth = Batch ? (int)(info.z >> kDepthShift) : launchDepth;
+      const uint32_t sampleDim = kDimBase + kDimBounce * (uint32_t)depth;
       const f3 org = mk(ro.x, ro.y, ro.z), dir = mk(rd.x, rd.y, rd.z);
       const int triId = __float_as_int(hh.w);
       f3 T = mk(tp.x, tp.y, tp.z);
@@ -446,22 +603,22 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
       uint32_t pixelId = info.x;
       const bool aov1 = (pixelId & kPathAov1Flag) == 0u;
       ShadeCtx ctx;
-      postIntersect(L.sc, org, dir, hh.x, triId, hh.y, hh.z, ctx);
-      const DevMaterial& mat = L.sc.materials[ctx.material];
+      postIntersect(E.sc, org, dir, hh.x, triId, hh.y, hh.z, ctx);
+      const DevMaterial& mat = E.sc.materials[ctx.material];
       const f3 wo = -dir;
-      uint32_t mediumId = info.z & 0xffffu;
+      uint32_t mediumId = info.z & kMediumMask;
       // Material::getBsdf orientation: media interfaces take it from the medium the path
       // is in, every other material is treated as front-facing (material/material.h:66-76).
       const bool backfacing = (mat.type & kMatMediaInterface) ? (int)mediumId == mat.mediumInt : false;
       StdBsdfT<F> bsdf;
-      resolveStandard<F>(L.sc, L.tab, mat, ctx, wo, backfacing, bsdf);
-      const SobolState st = sobolSetSample(L.rd.seed, info.y, pixelId & kPixelIdMask);
+      resolveStandard<F>(E.sc, L.tab, mat, ctx, wo, backfacing, bsdf);
+      const SobolState st = sobolSetSample(E.rd.seed, info.y, pixelId & kPixelIdMask);
       const bool aov2 = (pixelId & kPathAov2Flag) == 0u;
       const bool rr = !(aov1 || aov2);
       // Volume transmission (Beer's law) inside a medium.
       if (mediumId > 0u)
       {
-        const f3 mc = ld3(L.sc.mediaColor + 3 * mediumId);
+        const f3 mc = ld3(E.sc.mediaColor + 3 * mediumId);
         T *= powf3(mc, hh.x);
       }
       // Direct light (NEE)
@@ -471,7 +628,7 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
         sobolGet3D(st, sampleDim + kDimLight, lx, ly, lz);
         f3 wi;
         float lightPdf, dist;
-        const f3 Lw = sampleLight(L.sc, ctx.p, lx, ly, lz, wi, lightPdf, dist);
+        const f3 Lw = sampleLight(E.sc, ctx.p, lx, ly, lz, wi, lightPdf, dist);
         if (reduceMax(Lw) > 0.f && lightPdf > 0.f)
         {
           float bsdfPdf;
@@ -479,7 +636,7 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
           if (reduceMax(bv) > 0.f)
           {
             const f3 dirT = T * bv;
-            if (depth >= L.rd.rrDepth)
+            if (depth >= E.rd.rrDepth)
             {
               const float contProb = rr ? fminf(luminance(dirT * (1.f / bsdfPdf)), 0.95f) : 1.f;
               bsdfPdf *= contProb;
@@ -503,7 +660,7 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
       const int extType = extend ? bsdfType : 0;
       if (aov1)
       {
-        if (L.aovMask)
+        if (E.aovMask)
         {
           const f3 a = bsdf.albedo(), nn = bsdf.normal();
           L.ps.aovA[p] = make_float4(a.x, a.y, a.z, 1.f);
@@ -513,8 +670,8 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
       }
       if (aov2 && (extType & kBsdfDelta) == 0) pixelId |= kPathAov2Flag;
       T *= bw;
-      extend = extend && reduceMax(T) >= L.rd.minWeight;
-      if (depth >= L.rd.rrDepth)
+      extend = extend && reduceMax(T) >= E.rd.minWeight;
+      if (depth >= E.rd.rrDepth)
       {
         const float contProb = rr ? fminf(luminance(T), 0.95f) : 1.f;
         extend = extend && sobolGet1D(st, sampleDim + kDimTerminate) <= contProb;
@@ -531,12 +688,16 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
         // Material::nextMedium (material/material.h:84-93).
         if ((mat.type & kMatMediaInterface) && dot(wo, ctx.Ng) * dot(wi, ctx.Ng) < 0.f)
           mediumId = (int)mediumId == mat.mediumInt ? (uint32_t)mat.mediumExt : (uint32_t)mat.mediumInt;
-        info.z = mediumId;
+        info.z = Batch ? (mediumId | ((uint32_t)(depth + 1) << kDepthShift)) : mediumId;
         L.ps.rad[p] = ra;
       }
       info.x = pixelId;
       L.ps.info[p] = info;
-      if (!extend && !shadow) finishPath(L, p, Lr);
+      if (!extend && !shadow)
+      {
+        finishPath<Batch>(L, p, Lr, info);
+        freed = true;
+      }
       if (shadow) shL.w = __uint_as_float((uint32_t)p | (extend ? 0u : kShadowFinish));
     }
     const int e = warpAppend(extCount, extend);
@@ -548,6 +709,7 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
       L.ps.shD[sidx] = shD;
       L.ps.shL[sidx] = shL;
     }
+    freeSlots<Batch>(L, parity ^ 1, freed, p);
   }
 }
 
@@ -693,18 +855,23 @@ struct ShadeLaunch;
 template <>
 struct ShadeLaunch<>
 {
-  static void run(int, const Launch&, cudaStream_t, int, int*, int*, int, int*, int*, int*) {}
+  template <bool Batch>
+  static void run(int, const Launch&, cudaStream_t, int, int*, int*, int, int*, int*, int*, int)
+  {
+  }
 };
 
 template <int F0, int... Fs>
 struct ShadeLaunch<F0, Fs...>
 {
+  template <bool Batch>
   static void run(int cls, const Launch& L, cudaStream_t st, int grid, int* classQueues, int* cnt, int depth,
-                  int* queueOut, int* nextCount, int* shadowCount)
+                  int* queueOut, int* nextCount, int* shadowCount, int parity)
   {
-    kShadeSurface<F0><<<grid, 256, 0, st>>>(L, classQueues + (int64_t)cls * L.ps.capacity, cnt + 1 + cls, depth,
-                                            queueOut, nextCount, shadowCount);
-    ShadeLaunch<Fs...>::run(cls + 1, L, st, grid, classQueues, cnt, depth, queueOut, nextCount, shadowCount);
+    kShadeSurface<F0, Batch><<<grid, 256, 0, st>>>(L, classQueues + (int64_t)cls * L.ps.capacity, cnt + 1 + cls,
+                                                   depth, queueOut, nextCount, shadowCount, parity);
+    ShadeLaunch<Fs...>::template run<Batch>(cls + 1, L, st, grid, classQueues, cnt, depth, queueOut, nextCount,
+                                            shadowCount, parity);
   }
 };
 
@@ -754,6 +921,10 @@ cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
     L.firstSample = ctx.sampleIndex + (uint32_t)done;
     L.samples = S;
     L.aovMask = ctx.aovMask;
+    L.items = nullptr;
+    L.itemCount = 0;
+    L.ctl = nullptr;
+    L.freeList[0] = L.freeList[1] = nullptr;
     const int P = pixelCount * S;
     e = cudaMemsetAsync(counts, 0, sizeof(int) * kCntStride * blocks, ctx.stream);
     if (e != cudaSuccess) return e;
@@ -769,19 +940,22 @@ cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
       int* qOut = ctx.ps.queue[(depth + 1) & 1];
       begin(0);
       if (counting)
-        kTrace<true><<<persistent, 256, 0, ctx.stream>>>(L, q, cnt, cnt + kCntWorkTrace, depth, ctx.ps.classQueues, cnt + 1);
+        kTrace<true, false><<<persistent, 256, 0, ctx.stream>>>(L, q, cnt, cnt + kCntWorkTrace, depth,
+                                                                ctx.ps.classQueues, cnt + 1);
       else
-        kTrace<false><<<persistent, 256, 0, ctx.stream>>>(L, q, cnt, cnt + kCntWorkTrace, depth, ctx.ps.classQueues, cnt + 1);
+        kTrace<false, false><<<persistent, 256, 0, ctx.stream>>>(L, q, cnt, cnt + kCntWorkTrace, depth,
+                                                                 ctx.ps.classQueues, cnt + 1);
       end();
       begin(2);
-      kShadeEnd<<<shadeGrid, 256, 0, ctx.stream>>>(L, ctx.ps.classQueues, cnt + 1, depth);
-      ShadeClassList::run(1, L, ctx.stream, shadeGrid, ctx.ps.classQueues, cnt, depth, qOut, next, cnt + kCntShadow);
+      kShadeEnd<false><<<shadeGrid, 256, 0, ctx.stream>>>(L, ctx.ps.classQueues, cnt + 1, depth, 0);
+      ShadeClassList::run<false>(1, L, ctx.stream, shadeGrid, ctx.ps.classQueues, cnt, depth, qOut, next,
+                                 cnt + kCntShadow, 0);
       end();
       begin(1);
       if (counting)
-        kShadow<true><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow);
+        kShadow<true, false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0);
       else
-        kShadow<false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow);
+        kShadow<false, false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0);
       end();
       rc.launches += 3 + kShadeClasses;
       rc.traceLaunches++;
@@ -825,6 +999,137 @@ cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
     e = cudaMemcpy(rc.trav, ctx.ps.travCounts, sizeof(rc.trav), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return e;
   }
+  return cudaSuccess;
+}
+
+
+
+// ---- batch form ---------------------------------------------------------------------------------
+
+__global__ void kIota(int* __restrict__ dst, int n)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = i;
+}
+
+cudaError_t launchBlitPlane(Context& ctx, const float4* plane, int n, float* dst)
+{
+  kBlit<<<gridFor(ctx, n), 256, 0, ctx.stream>>>(plane, n, dst);
+  return cudaGetLastError();
+}
+
+namespace {
+
+constexpr int kGraphIterations = 8;  // bounce iterations per graph launch (even: parities alternate)
+
+int* batchCounts(BatchCtl* ctl, int parity)
+{
+  return reinterpret_cast<int*>(reinterpret_cast<char*>(ctl) + offsetof(BatchCtl, counts)) + parity * kBatchCntStride;
+}
+
+// One bounce iteration of the batch: control step, regeneration, closest hit, shading by
+// class, shadow rays. Every count is read on the device, so the sequence can be captured once
+// and replayed.
+int batchIteration(const Context& ctx, const Launch& L, int a, int persistent, int shadeGrid, int regenGrid)
+{
+  const int b = a ^ 1;
+  int* ca = batchCounts(L.ctl, a);
+  int* cb = batchCounts(L.ctl, b);
+  cudaStream_t st = ctx.stream;
+  kBatchStep<<<1, 1, 0, st>>>(L.ctl, a);
+  kBatchRegen<<<regenGrid, 256, 0, st>>>(L, a, L.ps.queue[a]);
+  kTrace<false, true><<<persistent, 256, 0, st>>>(L, L.ps.queue[a], ca, ca + kBatchCntShadow + 1, 0,
+                                                  L.ps.classQueues, ca + 1);
+  kShadeEnd<true><<<shadeGrid, 256, 0, st>>>(L, L.ps.classQueues, ca + 1, 0, a);
+  ShadeClassList::run<true>(1, L, st, shadeGrid, L.ps.classQueues, ca, 0, L.ps.queue[b], cb, ca + kBatchCntShadow, a);
+  kShadow<false, true><<<persistent, 256, 0, st>>>(L, ca + kBatchCntShadow, ca + kBatchCntShadow + 2, a);
+  return 5 + (kShadeClasses - 1);
+}
+
+} // namespace
+
+cudaError_t renderBatch(Context& ctx, BatchState& B, RenderCounters& rc)
+{
+  rc = RenderCounters();
+  cudaError_t e = cudaSuccess;
+  const int64_t C = B.ps.capacity;
+  for (const BatchItem& it : B.items)
+  {
+    const size_t bytes = (size_t)it.pixelCount * sizeof(float4);
+    e = cudaMemsetAsync(it.accum, 0, bytes, ctx.stream);
+    if (e == cudaSuccess && it.accA) e = cudaMemsetAsync(it.accA, 0, bytes, ctx.stream);
+    if (e == cudaSuccess && it.accN) e = cudaMemsetAsync(it.accN, 0, bytes, ctx.stream);
+    if (e != cudaSuccess) return e;
+  }
+  BatchCtl h;
+  std::memset(&h, 0, sizeof(h));
+  h.workTotal = B.workTotal;
+  h.freeCount[0] = (int)C;
+  e = cudaMemcpyAsync(B.ctl, &h, sizeof(h), cudaMemcpyHostToDevice, ctx.stream);
+  if (e != cudaSuccess) return e;
+  kIota<<<gridFor(ctx, C), 256, 0, ctx.stream>>>(B.freeList[0], (int)C);
+  rc.launches++;
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+
+  if (!B.exec)
+  {
+    Launch L;
+    std::memset(&L, 0, sizeof(L));
+    L.tab = ctx.tables;
+    L.ps = B.ps;
+    L.items = B.dItems;
+    L.itemCount = (int)B.items.size();
+    L.ctl = B.ctl;
+    L.freeList[0] = B.freeList[0];
+    L.freeList[1] = B.freeList[1];
+    const int persistent = ctx.smCount * ctx.traceBlocks;
+    const int shadeGrid = ctx.smCount * ctx.shadeBlocks;
+    const int regenGrid = gridFor(ctx, C);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    int kernels = 0;
+    for (int k = 0; k < kGraphIterations; ++k) kernels += batchIteration(ctx, L, k & 1, persistent, shadeGrid, regenGrid);
+    cudaError_t launchErr = cudaGetLastError();
+    e = cudaStreamEndCapture(ctx.stream, &graph);
+    if (e == cudaSuccess) e = launchErr;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&B.exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return e;
+    B.graphKernels = kernels;
+  }
+
+  // Each slot finishes a path at least every maxDepth + 1 iterations while work remains.
+  const long long rounds = (B.workTotal + C - 1) / C;
+  const long long maxIterations = (rounds + 2) * (long long)(B.maxDepth + 2) + 2 * kGraphIterations;
+  int* done = nullptr;
+  e = cudaMallocHost(&done, sizeof(int));
+  if (e != cudaSuccess) return e;
+  long long iterations = 0;
+  *done = 0;
+  while (!*done)
+  {
+    if (iterations > maxIterations)
+    {
+      cudaFreeHost(done);
+      return cudaErrorLaunchTimeout;
+    }
+    e = cudaGraphLaunch(B.exec, ctx.stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(done, reinterpret_cast<char*>(B.ctl) + offsetof(BatchCtl, done), sizeof(int),
+                          cudaMemcpyDeviceToHost, ctx.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx.stream);
+    if (e != cudaSuccess) break;
+    iterations += kGraphIterations;
+    rc.launches += B.graphKernels;
+  }
+  cudaFreeHost(done);
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpy(&h, B.ctl, sizeof(h), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return e;
+  rc.closestRays = (int64_t)h.rays[0];
+  rc.shadowRays = (int64_t)h.rays[1];
+  rc.traceLaunches = iterations;
   return cudaSuccess;
 }
 

@@ -43,6 +43,56 @@ struct PathState
   uint32_t* err = nullptr;
 };
 
+// One frame of a batch render: its scene, camera, renderer settings, frame and range of
+// work items (pixel-samples) in the batch's global work order.
+struct BatchItem
+{
+  DevScene sc;
+  DevCamera cam;
+  DevRenderer rd;
+  int width, height, pixelCount, aovMask;
+  long long workBase;   // first work item of this frame
+  long long workCount;  // pixelCount * spp
+  float4* accum;        // sum rgb + weight per pixel
+  float4* accA;         // first-hit albedo sums (aovMask != 0)
+  float4* accN;         // first-hit normal sums
+};
+
+// Counter block of one batch iteration (ints): [0] paths to trace, [1..kShadeClasses] paths
+// per shading class, [kBatchCntShadow] shadow rays, then the two work counters.
+constexpr int kBatchCntShadow = 1 + kShadeClasses;
+constexpr int kBatchCntStride = 16;
+
+// Device-side control block of a batch render (kBatchStep advances it every iteration).
+struct BatchCtl
+{
+  long long workNext, workTotal;
+  long long regenBase;
+  int regenCount, regenOffset;
+  int counts[2][kBatchCntStride];
+  int freeCount[2];
+  int done;
+  int iterations;
+  unsigned long long rays[2];  // closest-hit rays, shadow rays
+};
+
+// Host state of a batch render (prt_batch): the frames, their uploaded scenes, a shared
+// path pool with its queues and free lists, and the captured bounce-loop graph.
+struct BatchState
+{
+  std::vector<DevBuf> bufs;        // scene buffers and accumulation planes of every item
+  std::vector<BatchItem> items;    // host copy of the items (device pointers inside)
+  BatchItem* dItems = nullptr;
+  long long workTotal = 0;
+  int maxDepth = 0;
+  bool anyAov = false;
+  PathState ps;                    // path pool; ps.err is the context's error flag
+  BatchCtl* ctl = nullptr;
+  int* freeList[2] = {nullptr, nullptr};
+  cudaGraphExec_t exec = nullptr;  // kGraphIterations bounce iterations
+  int graphKernels = 0;
+};
+
 struct Context
 {
   int device = 0;
@@ -93,6 +143,10 @@ cudaError_t launchPrimary(Context& ctx, uint32_t sampleIndex, float* raysOut, in
 // number of closest + shadow rays traced.
 cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc);
 cudaError_t launchBlit(Context& ctx, int aov, float* dst);
+// Renders every item of a batch to completion (path regeneration over one shared path pool,
+// bounce loop replayed as a CUDA graph) into the items' accumulation planes.
+cudaError_t renderBatch(Context& ctx, BatchState& b, RenderCounters& rc);
+cudaError_t launchBlitPlane(Context& ctx, const float4* plane, int n, float* dst);
 cudaError_t launchClear(Context& ctx);
 cudaError_t launchBsdfQuery(Context& ctx, const DevMaterial& m, int mediumId, int64_t n, const float* tuples, float* out);
 // Builds the BSDF energy-compensation tables on the current device (albedo.cu).

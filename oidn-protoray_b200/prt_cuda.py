@@ -55,6 +55,10 @@ def load_library():
     lib.prt_cuda_render.argtypes = [vp, C.c_int32, P(T.RenderStats)]
     lib.prt_cuda_set_profiling.argtypes = [vp, C.c_int32]
     lib.prt_cuda_set_tuning.argtypes = [vp, P(T.Tuning)]
+    lib.prt_cuda_batch_create.argtypes = [vp, P(T.BatchItem), C.c_int32, P(vp)]
+    lib.prt_cuda_batch_render.argtypes = [vp, P(T.RenderStats)]
+    lib.prt_cuda_batch_blit.argtypes = [vp, C.c_int32, C.c_int32, P(C.c_float)]
+    lib.prt_cuda_batch_destroy.argtypes = [vp]
     lib.prt_cuda_get_tuning.argtypes = [vp, P(T.Tuning)]
     lib.prt_cuda_autotune.argtypes = [vp, C.c_int32, P(T.Tuning), P(C.c_double)]
     lib.prt_cuda_blit.argtypes = [vp, C.c_int32, P(C.c_float)]
@@ -244,3 +248,50 @@ class DeviceCuda:
         self._check(self.lib.prt_cuda_query_primary(self.h, sample_index, T.fptr(rays), T.iptr(g), T.iptr(p),
                                                     T.fptr(t)))
         return rays, g, p, t
+
+
+class Batch:
+    """Many frames rendered in one persistent wavefront (prt_cuda_batch_*).
+
+    `frames` is a list of (Scene, seed, aov_mask); each Scene carries its own width, height,
+    spp, max_depth, rr_depth and camera.
+    """
+
+    def __init__(self, device, frames):
+        self.dev = device
+        self.frames = [(sc, seed, aov) for sc, seed, aov in frames]
+        descs = [sc.desc() for sc, _, _ in self.frames]
+        items = (T.BatchItem * len(descs))()
+        for k, ((sc, seed, aov), d) in enumerate(zip(self.frames, descs)):
+            it = items[k]
+            it.scene = C.pointer(d)
+            it.camera = sc.camera
+            it.renderer = T.RendererDesc(sc.max_depth, sc.rr_depth, 1e-4, 3.4028234663852886e38)
+            it.width, it.height, it.spp, it.aov_mask, it.seed = sc.width, sc.height, sc.spp, aov, seed
+        h = C.c_void_p()
+        device._check(device.lib.prt_cuda_batch_create(device.h, items, len(descs), C.byref(h)))
+        self.h = h
+        self.samples = sum(sc.width * sc.height * sc.spp for sc, _, _ in self.frames)
+
+    def render(self):
+        st = T.RenderStats()
+        self.dev._check(self.dev.lib.prt_cuda_batch_render(self.h, C.byref(st)))
+        return {name: getattr(st, name) for name, _ in T.RenderStats._fields_}
+
+    def blit(self, item, aov=T.PRT_BLIT_HDR):
+        sc = self.frames[item][0]
+        img = np.zeros((sc.height, sc.width, 3), np.float32)
+        self.dev._check(self.dev.lib.prt_cuda_batch_blit(self.h, item, aov, T.fptr(img)))
+        return img
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.dev.lib.prt_cuda_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

@@ -309,3 +309,29 @@ def terrain(seed=0, grid=1024, n_spheres=400, sphere_subdiv=3, width=1920, heigh
     s.camera = look_at((0.0, 0.56 * extent, 1.24 * extent), (0.0, 0.0, -0.1 * extent), fov_deg=45.0)
     s.width, s.height, s.spp, s.max_depth, s.rr_depth = width, height, spp, max_depth, rr_depth
     return s
+
+
+BATCH_SIZES = (64, 96, 128, 192, 256, 384, 512)   # square frames, all multiples of 32
+BATCH_SPPS = (4, 8, 16, 32, 64)
+
+
+def batch_frames(count=64, seed=0, tri_range=(1e3, 5e5), sizes=BATCH_SIZES, spps=BATCH_SPPS, depth_range=(3, 10),
+                 aov_mask=T.PRT_AOV_ALBEDO1 | T.PRT_AOV_NORMAL1):
+    """The batched workload: `count` independent terrain scenes whose triangle count is
+    log-uniform in tri_range (about 80% heightfield, 20% icospheres), each with a square
+    frame from `sizes`, spp from `spps`, max depth uniform in depth_range and its own scene and
+    sampler seed. Returns a list of (Scene, sampler seed, aov_mask)."""
+    rng = np.random.default_rng(seed)
+    frames = []
+    for k in range(count):
+        tris = float(np.exp(rng.uniform(np.log(tri_range[0]), np.log(tri_range[1]))))
+        n_spheres = int(0.2 * tris / 1280)
+        grid = max(8, int(np.sqrt(max(tris - 1280 * n_spheres, 128) / 2.0)) + 1)
+        size = int(rng.choice(sizes))
+        spp = int(rng.choice(spps))
+        depth = int(rng.integers(depth_range[0], depth_range[1] + 1))
+        scene_seed = int(rng.integers(0, 2**31 - 1))
+        s = terrain(seed=scene_seed, grid=grid, n_spheres=n_spheres, width=size, height=size, spp=spp,
+                    max_depth=depth, rr_depth=3)
+        frames.append((s, int(rng.integers(0, 2**31 - 1)), aov_mask))
+    return frames

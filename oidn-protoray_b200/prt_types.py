@@ -180,6 +180,20 @@ class RenderStats(C.Structure):
     ]
 
 
+class BatchItem(C.Structure):
+    _fields_ = [
+        ("scene", C.POINTER(SceneDesc)),
+        ("camera", CameraDesc),
+        ("renderer", RendererDesc),
+        ("width", C.c_int32),
+        ("height", C.c_int32),
+        ("spp", C.c_int32),
+        ("aov_mask", C.c_int32),
+        ("seed", C.c_uint32),
+        ("reserved", C.c_int32),
+    ]
+
+
 class Tuning(C.Structure):
     _fields_ = [
         ("trace_blocks", C.c_int32),
