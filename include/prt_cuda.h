@@ -288,6 +288,31 @@ int prt_cuda_batch_render(prt_batch* batch, prt_render_stats* stats);
 int prt_cuda_batch_blit(prt_batch* batch, int32_t item, int32_t aov, float* dst);
 int prt_cuda_batch_destroy(prt_batch* batch);
 
+/* ---- differentiation -------------------------------------------------------------------
+ * No counterpart in the reference. Path-replay adjoint of the image prt_cuda_render produces:
+ * given dLoss/dImage (width*height RGB floats, row-major, row 0 at the top; host or device
+ * memory), writes
+ *   grad_textures: dLoss/d(texel) of every scene texture used as a Lambertian base colour,
+ *                  textures concatenated in scene order, each width*height*3 floats with row 0
+ *                  at the top (the layout of prt_texture); at least grad_texture_count floats;
+ *   grad_roughness: dLoss/d(specular_roughness) of every material (0 for materials without a
+ *                  specular layer); grad_roughness_count >= material_count.
+ * Either output may be NULL. The estimate uses samples [first_sample, first_sample + spp) of the
+ * current seed; each path is walked twice from its Sobol seed (primal, then replay), so nothing
+ * is stored per path. Supported materials: Lambertian, optionally under a specular layer, plus
+ * emitters (other lobes return PRT_ERR_INVALID_ARG). stats->render_ms is the device time. */
+int prt_cuda_adjoint(prt_context* ctx, uint32_t first_sample, int32_t spp, const float* d_loss_d_image,
+                     float* grad_textures, int64_t grad_texture_count, float* grad_roughness,
+                     int32_t grad_roughness_count, prt_render_stats* stats);
+
+/* Parameter updates between renders without re-uploading the scene (no BVH rebuild).
+ * prt_cuda_update_texture: new contents of texture `texture` (same size; row 0 at the top;
+ * host or device memory). prt_cuda_update_material: new parameters of material `material`,
+ * which must keep its lobe set, emission and medium. No counterpart in the reference, which
+ * reloads the scene. */
+int prt_cuda_update_texture(prt_context* ctx, int32_t texture, const float* rgb);
+int prt_cuda_update_material(prt_context* ctx, int32_t material, const prt_material* m);
+
 /* Enables PRT_PROFILE_* instrumentation for subsequent render calls (0 = off). */
 int prt_cuda_set_profiling(prt_context* ctx, int32_t flags);
 

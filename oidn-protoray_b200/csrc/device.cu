@@ -492,6 +492,8 @@ void uploadScene(Context& c, const prt_scene_desc* s)
   cuCheck(cudaStreamSynchronize(c.stream), "scene upload");
   c.scene = sc;
   c.hasScene = true;
+  c.materialsHost = mats;
+  c.texturesHost = texs;
 }
 
 void allocFrame(Context& c, int width, int height, int aovMask)
@@ -573,6 +575,8 @@ struct Staged
   bool owned = false;
   Context* c = nullptr;
 
+  Staged(const Staged&) = delete;
+  Staged& operator=(const Staged&) = delete;
   Staged(Context& ctx, const void* p, size_t n, bool copyIn) : bytes(n), c(&ctx)
   {
     cudaPointerAttributes attr;
@@ -1376,6 +1380,94 @@ int prt_cuda_batch_destroy(prt_batch* batch)
   freeBatch(batch->b);
   delete batch;
   return PRT_OK;
+}
+
+} // extern "C"
+
+// ---- differentiation ----------------------------------------------------------------------------
+
+extern "C" {
+
+int prt_cuda_adjoint(prt_context* ctx, uint32_t first_sample, int32_t spp, const float* d_loss_d_image,
+                     float* grad_textures, int64_t grad_texture_count, float* grad_roughness,
+                     int32_t grad_roughness_count, prt_render_stats* stats)
+{
+  return guarded(ctx, [&](Context& c) {
+    requireScene(c);
+    if (!c.hasRenderer || !c.hasCamera || !c.accum) throw ApiError{PRT_ERR_STATE, "renderer, camera and frame are required"};
+    if (spp <= 0 || !d_loss_d_image) throw std::invalid_argument("invalid adjoint request");
+    for (const DevMaterial& m : c.materialsHost)
+      if (!(m.type & kMatEmissive) && (m.features & ~(kFeatOpaque | kFeatSpecular)))
+        throw std::invalid_argument("the adjoint supports Lambertian materials with an optional specular layer");
+    if (c.texturesHost.size() > 32) throw std::invalid_argument("the adjoint supports at most 32 textures");
+    int64_t texFloats = 0;
+    for (const DevTexture& t : c.texturesHost) texFloats += 3ll * t.width * t.height;
+    const int64_t mats = (int64_t)c.materialsHost.size();
+    if ((grad_textures && grad_texture_count < texFloats) || (grad_roughness && grad_roughness_count < mats))
+      throw std::invalid_argument("gradient buffers are too small");
+    cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+    const size_t px = (size_t)c.width * c.height;
+    Staged dl(c, d_loss_d_image, px * 3 * sizeof(float), true);
+    // Gradients are always accumulated on the device; host outputs are copied at the end.
+    Staged gt(c, grad_textures, (size_t)std::max<int64_t>(texFloats, 1) * sizeof(float), false);
+    Staged gr(c, grad_roughness, (size_t)std::max<int64_t>(mats, 1) * sizeof(float), false);
+    cuCheck(cudaMemsetAsync(gt.dev, 0, (size_t)std::max<int64_t>(texFloats, 1) * sizeof(float), c.stream), "clear");
+    cuCheck(cudaMemsetAsync(gr.dev, 0, (size_t)std::max<int64_t>(mats, 1) * sizeof(float), c.stream), "clear");
+    cuCheck(cudaEventRecord(c.ev0, c.stream), "event");
+    cuCheck(launchAdjoint(c, first_sample, spp, (const float*)dl.dev, (float*)gt.dev, (float*)gr.dev, 1e-3f), "adjoint");
+    cuCheck(cudaEventRecord(c.ev1, c.stream), "event");
+    if (grad_textures) gt.copyOut();
+    if (grad_roughness) gr.copyOut();
+    cuCheck(cudaStreamSynchronize(c.stream), "adjoint sync");
+    checkDeviceErrors(c);
+    float ms = 0.f;
+    cuCheck(cudaEventElapsedTime(&ms, c.ev0, c.ev1), "event time");
+    if (stats)
+    {
+      std::memset(stats, 0, sizeof(*stats));
+      stats->spp = spp;
+      stats->render_ms = ms;
+      stats->kernel_launches = 1;
+    }
+  });
+}
+
+int prt_cuda_update_texture(prt_context* ctx, int32_t texture, const float* rgb)
+{
+  return guarded(ctx, [&](Context& c) {
+    requireScene(c);
+    if (texture < 0 || texture >= (int)c.texturesHost.size() || !rgb) throw std::invalid_argument("invalid texture update");
+    cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+    const DevTexture& t = c.texturesHost[texture];
+    Staged src(c, rgb, 3ull * t.width * t.height * sizeof(float), true);
+    cuCheck(launchTextureUpdate(c, t, (const float*)src.dev), "texture update");
+    cuCheck(cudaStreamSynchronize(c.stream), "texture update sync");
+  });
+}
+
+int prt_cuda_update_material(prt_context* ctx, int32_t material, const prt_material* m)
+{
+  return guarded(ctx, [&](Context& c) {
+    requireScene(c);
+    if (material < 0 || material >= (int)c.materialsHost.size() || !m) throw std::invalid_argument("invalid material update");
+    std::vector<float> media = {1.f, 1.f, 1.f, 1.f};
+    DevMaterial d = resolveMaterial(*m, media, (int)c.texturesHost.size());
+    const DevMaterial& old = c.materialsHost[material];
+    if (d.type != old.type || d.features != old.features || d.shadeClass != old.shadeClass)
+      throw std::invalid_argument("a material update must keep the material's lobes (re-upload the scene instead)");
+    if ((d.type & kMatMediaInterface) && (d.specularIor != old.specularIor || d.transmissionDepth != old.transmissionDepth ||
+                                          std::memcmp(d.transmissionColor, old.transmissionColor, sizeof(float) * 3) != 0))
+      throw std::invalid_argument("a material update must keep the medium of a transmissive material");
+    if (std::memcmp(d.emission, old.emission, sizeof(float) * 3) != 0)
+      throw std::invalid_argument("a material update must keep the emission (re-upload the scene instead)");
+    d.mediumInt = old.mediumInt;
+    d.mediumExt = old.mediumExt;
+    cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+    cuCheck(cudaMemcpyAsync(const_cast<DevMaterial*>(c.scene.materials) + material, &d, sizeof(d), cudaMemcpyHostToDevice,
+                            c.stream), "material update");
+    cuCheck(cudaStreamSynchronize(c.stream), "material update sync");
+    c.materialsHost[material] = d;
+  });
 }
 
 } // extern "C"

@@ -104,6 +104,8 @@ struct Context
   bool hasScene = false;
   Bvh8 bvh;                       // host copy (for counting and re-upload)
   std::vector<int> meshTriOffsetHost;
+  std::vector<DevMaterial> materialsHost;  // host copies of the uploaded material records
+  std::vector<DevTexture> texturesHost;    // device pointers and sizes of the scene's textures
   DevRenderer renderer{100, 8, 1e-4f, 3.402823466e38f, 0u};
   bool hasRenderer = false;
   DevCamera camera{};
@@ -147,6 +149,12 @@ cudaError_t launchBlit(Context& ctx, int aov, float* dst);
 // bounce loop replayed as a CUDA graph) into the items' accumulation planes.
 cudaError_t renderBatch(Context& ctx, BatchState& b, RenderCounters& rc);
 cudaError_t launchBlitPlane(Context& ctx, const float4* plane, int n, float* dst);
+// Path-replay adjoint (adjoint.cu): dLoss/d(texel) of every scene texture and dLoss/d(specular
+// roughness) of every material for the image gradient dLdI (W*H*3, device memory).
+cudaError_t launchAdjoint(Context& ctx, uint32_t firstSample, int spp, const float* dLdI, float* gradTex,
+                          float* gradRough, float roughnessStep);
+// Copies a caller-order (row 0 at the top) RGB image into a device texture (row 0 at the bottom).
+cudaError_t launchTextureUpdate(Context& ctx, const DevTexture& t, const float* rgb);
 cudaError_t launchClear(Context& ctx);
 cudaError_t launchBsdfQuery(Context& ctx, const DevMaterial& m, int mediumId, int64_t n, const float* tuples, float* out);
 // Builds the BSDF energy-compensation tables on the current device (albedo.cu).

@@ -55,6 +55,9 @@ def load_library():
     lib.prt_cuda_render.argtypes = [vp, C.c_int32, P(T.RenderStats)]
     lib.prt_cuda_set_profiling.argtypes = [vp, C.c_int32]
     lib.prt_cuda_set_tuning.argtypes = [vp, P(T.Tuning)]
+    lib.prt_cuda_adjoint.argtypes = [vp, C.c_uint32, C.c_int32, vp, vp, C.c_int64, vp, C.c_int32, P(T.RenderStats)]
+    lib.prt_cuda_update_texture.argtypes = [vp, C.c_int32, vp]
+    lib.prt_cuda_update_material.argtypes = [vp, C.c_int32, P(T.Material)]
     lib.prt_cuda_batch_create.argtypes = [vp, P(T.BatchItem), C.c_int32, P(vp)]
     lib.prt_cuda_batch_render.argtypes = [vp, P(T.RenderStats)]
     lib.prt_cuda_batch_blit.argtypes = [vp, C.c_int32, C.c_int32, P(C.c_float)]
@@ -175,6 +178,42 @@ class DeviceCuda:
         m = C.c_double()
         self._check(self.lib.prt_cuda_autotune(self.h, spp, C.byref(t), C.byref(m)))
         return {name: getattr(t, name) for name, _ in T.Tuning._fields_}, m.value
+
+    # -- differentiation -------------------------------------------------------------------
+    @staticmethod
+    def _ptr(a):
+        if a is None:
+            return None
+        if hasattr(a, "data_ptr"):
+            return C.c_void_p(a.data_ptr())
+        return a.ctypes.data_as(C.c_void_p)
+
+    def adjoint(self, d_loss_d_image, spp, first_sample=0, grad_textures=None, grad_roughness=None):
+        """Path-replay adjoint: accumulates dLoss/d(texel) into grad_textures (all scene textures
+        concatenated, each (h, w, 3), row 0 at the top) and dLoss/d(specular roughness) into
+        grad_roughness (one per material). Arrays may be numpy or CUDA torch tensors (float32);
+        numpy outputs are created when None. Returns (grad_textures, grad_roughness, stats)."""
+        sc = self.scene
+        tex_floats = sum(int(t.size) for t in sc.textures)
+        if grad_textures is None:
+            grad_textures = np.zeros(max(tex_floats, 1), np.float32)
+        if grad_roughness is None:
+            grad_roughness = np.zeros(len(sc.materials), np.float32)
+        if not hasattr(d_loss_d_image, "data_ptr"):
+            d_loss_d_image = np.ascontiguousarray(d_loss_d_image, np.float32)
+        st = T.RenderStats()
+        self._check(self.lib.prt_cuda_adjoint(self.h, first_sample, spp, self._ptr(d_loss_d_image),
+                                              self._ptr(grad_textures), tex_floats, self._ptr(grad_roughness),
+                                              len(sc.materials), C.byref(st)))
+        return grad_textures, grad_roughness, {name: getattr(st, name) for name, _ in T.RenderStats._fields_}
+
+    def update_texture(self, index, rgb):
+        if not hasattr(rgb, "data_ptr"):
+            rgb = np.ascontiguousarray(rgb, np.float32)
+        self._check(self.lib.prt_cuda_update_texture(self.h, index, self._ptr(rgb)))
+
+    def update_material(self, index, material):
+        self._check(self.lib.prt_cuda_update_material(self.h, index, C.byref(material)))
 
     def set_profiling(self, flags):
         self._check(self.lib.prt_cuda_set_profiling(self.h, flags))

@@ -197,6 +197,88 @@ def cornell(seed=0, width=256, height=256, spp=16, max_depth=5, n_spheres=32, sp
     return s
 
 
+def smooth_noise_texture(size, seed, lo=0.1, hi=0.9):
+    """(size, size, 3) smooth value noise in [lo, hi], one seeded noise per channel."""
+    u = (np.arange(size) + 0.5) / size
+    U, V = np.meshgrid(u, u, indexing="xy")
+    out = np.empty((size, size, 3), np.float32)
+    for c in range(3):
+        n = value_noise_fbm(U, V, seed * 3 + c, octaves=4, base_freq=3.0)
+        n = (n - n.min()) / max(n.max() - n.min(), 1e-9)
+        out[..., c] = lo + (hi - lo) * n
+    return out
+
+
+def cornell_inverse(seed=0, target=False, tex_size=256, width=256, height=256, spp=16, max_depth=5, n_spheres=32,
+                    albedo_init=0.5, roughness_init=0.3):
+    """The inverse-rendering scene: the small scene with the floor and the back wall textured by
+    tex_size^2 RGB albedo textures and every sphere given a specular layer whose roughness is a
+    parameter. target=False: textures at albedo_init, roughness roughness_init. target=True:
+    textures from seeded smooth noise in [0.1, 0.9], roughness uniform in [0.05, 0.6].
+    Returns (scene, params) with params = {"textures": [ids], "roughness": [material ids]}."""
+    rng = np.random.default_rng(seed)
+    trng = np.random.default_rng(seed + 1000)
+    s = Scene()
+    if target:
+        floor_tex = s.add_texture(smooth_noise_texture(tex_size, seed + 1))
+        back_tex = s.add_texture(smooth_noise_texture(tex_size, seed + 2))
+    else:
+        floor_tex = s.add_texture(np.full((tex_size, tex_size, 3), albedo_init, np.float32))
+        back_tex = s.add_texture(np.full((tex_size, tex_size, 3), albedo_init, np.float32))
+    floor_m = s.add_material(T.material(base_color=(1.0, 1.0, 1.0), base_color_texture=floor_tex, specular_weight=0.0))
+    back_m = s.add_material(T.material(base_color=(1.0, 1.0, 1.0), base_color_texture=back_tex, specular_weight=0.0))
+    white = s.add_material(T.material(base_color=(0.8, 0.8, 0.8), specular_weight=0.0))
+    red = s.add_material(T.material(base_color=(0.6, 0.0, 0.0), specular_weight=0.0))
+    green = s.add_material(T.material(base_color=(0.0, 0.6, 0.0), specular_weight=0.0))
+    light = s.add_material(T.material(emission_luminance=15.0, emission_color=(1.0, 1.0, 1.0), specular_weight=0.0))
+    uv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+    for quad, mat, tex in [
+        (_quad((-1, 0, 1), (1, 0, 1), (1, 0, -1), (-1, 0, -1)), floor_m, True),
+        (_quad((-1, 2, -1), (1, 2, -1), (1, 2, 1), (-1, 2, 1)), white, False),
+        (_quad((-1, 0, -1), (1, 0, -1), (1, 2, -1), (-1, 2, -1)), back_m, True),
+        (_quad((-1, 0, 1), (-1, 0, -1), (-1, 2, -1), (-1, 2, 1)), red, False),
+        (_quad((1, 0, -1), (1, 0, 1), (1, 2, 1), (1, 2, -1)), green, False),
+    ]:
+        s.add_mesh(quad[0], quad[1], mat, texcoords=uv if tex else None)
+    y = 1.99
+    lp, li = _quad((-0.25, y, -0.25), (0.25, y, -0.25), (0.25, y, 0.25), (-0.25, y, 0.25))
+    s.add_mesh(lp, li, light)
+    sv, sf = icosphere(2)
+    rough_ids = []
+    for _ in range(n_spheres):
+        r = rng.uniform(0.05, 0.15)
+        c = np.array([rng.uniform(-1 + r, 1 - r), rng.uniform(r, 2 - r), rng.uniform(-1 + r, 1 - r)])
+        albedo = rng.uniform(0.1, 0.9, 3)
+        rough = float(trng.uniform(0.05, 0.6)) if target else roughness_init
+        m = s.add_material(T.material(base_color=albedo, specular_weight=1.0, specular_roughness=rough,
+                                      specular_ior=1.5))
+        rough_ids.append(m)
+        s.add_mesh(sv * r + c, sf, m, normals=sv)
+    s.camera = look_at((0.0, 1.0, 3.4), (0.0, 1.0, 0.0), fov_deg=40.0)
+    s.width, s.height, s.spp, s.max_depth, s.rr_depth = width, height, spp, max_depth, 8
+    return s, {"textures": [floor_tex, back_tex], "roughness": rough_ids}
+
+
+def lit_plane(albedo=(0.5, 0.5, 0.5), width=128, height=128, spp=64, sun_elevation_deg=50.0, sun_angle=0.1,
+              sun_color=250.0):
+    """A single Lambertian plane (y = 0, albedo from a 1x1 texture) under a distant light, seen
+    from above so that it fills the frame; max depth 1. Each pixel's expected value is
+    albedo * sun_color * sin^2(sun_angle / 2) * cos(zenith angle of the sun)."""
+    s = Scene()
+    tex = s.add_texture(np.array(albedo, np.float32).reshape(1, 1, 3))
+    m = s.add_material(T.material(base_color=(1.0, 1.0, 1.0), base_color_texture=tex, specular_weight=0.0))
+    q = _quad((-4, 0, 4), (4, 0, 4), (4, 0, -4), (-4, 0, -4))
+    s.add_mesh(q[0], q[1], m, texcoords=np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32))
+    d = sun_direction(sun_elevation_deg, 30.0)
+    s.env.distant_color[:] = (sun_color, sun_color, sun_color)
+    s.env.distant_dir[:] = tuple(float(c) for c in d)
+    s.env.distant_angle = sun_angle
+    s.camera = look_at((0.0, 2.0, 0.0), (0.0, 0.0, 0.0), up=(0.0, 0.0, -1.0), fov_deg=60.0)
+    s.width, s.height, s.spp, s.max_depth, s.rr_depth = width, height, spp, 1, 8
+    k = sun_color * math.sin(sun_angle / 2) ** 2 * math.sin(math.radians(sun_elevation_deg))
+    return s, k
+
+
 # ---- large plain-render scene: fBm terrain + icospheres under a sun-sky ----------------------
 
 SUNSKY_FIXTURE = pathlib.Path(__file__).resolve().parent.parent / "tests" / "golden" / "sunsky_t3_e30.npz"
