@@ -45,6 +45,8 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--spp", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="skip the small-scene, batched and adjoint measurements")
     return ap.parse_args()
 
 
@@ -300,6 +302,11 @@ def run_ours(args):
                                "shade": shade_ms / args.steps},
         "rays_per_step": {"closest": closest / args.steps, "shadow": shadow / args.steps},
     }
+    if not args.headline_only:
+        barrier()
+        out["small_scene"] = small_scene_bench(dev)
+        out["batched"] = batched_bench(dev)
+        out["adjoint"] = adjoint_bench(dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             out["cpu_baseline"] = cpu_baseline()
@@ -315,6 +322,85 @@ def run_ours(args):
 # DRAM bytes (read + write) of the 9 kTrace launches of one 1920x1080 x 1-spp terrain frame,
 # from ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum (profiles/kTrace_terrain_1spp.md).
 NCU_TRACE_DRAM_BYTES = 781_850_368
+
+def small_scene_bench(dev, repeats=5):
+    """The small plain-render workload: the Cornell-style room with 32 icospheres (10.3k
+    triangles), 256x256, 16 spp, max depth 5, seed 0. Best of `repeats` device-timed frames."""
+    scene = prt_scenes.cornell(seed=0)
+    dev.setup(scene, seed=0)
+    dev.render(scene.spp)
+    best = None
+    for _ in range(repeats):
+        dev.init_sampler(0)
+        dev.clear_frame()
+        st = dev.render(scene.spp)
+        if best is None or st["render_ms"] < best["render_ms"]:
+            best = st
+    return {"workload": "room + 32 icospheres, 10,252 tris, 256x256, 16 spp, depth 5", "mrays_per_s": best["mray"],
+            "samples_per_s": scene.width * scene.height * scene.spp / (best["render_ms"] * 1e-3),
+            "ms_per_frame": best["render_ms"], "rays": best["rays"]}
+
+
+def batched_bench(dev, count=64, repeats=3):
+    """64 independent terrain frames (triangles log-uniform in [1k, 500k], square sizes 64..512,
+    spp in {4..64}, depth 3..10, beauty + albedo1 + normal1): one batch render (persistent
+    wavefront, path regeneration, graph-captured bounce loop) against 64 frame-form renders of
+    the same frames with the same seeds. Device time; scene upload outside both."""
+    import prt_cuda
+
+    frames = prt_scenes.batch_frames(count=count, seed=0)
+    samples = sum(s.width * s.height * s.spp for s, _, _ in frames)
+    batch = prt_cuda.Batch(dev, frames)
+    batch.render()
+    b_ms, b_rays, launches = None, 0, 0
+    for _ in range(repeats):
+        st = batch.render()
+        if b_ms is None or st["render_ms"] < b_ms:
+            b_ms, b_rays, launches = st["render_ms"], st["rays"], st["kernel_launches"]
+    batch.close()
+    p_ms, p_rays = 0.0, 0
+    for scene, seed, aov in frames:
+        dev.init_scene(scene)
+        dev.init_frame(scene.width, scene.height, aov)
+        dev.init_camera(scene.camera)
+        dev.init_renderer(scene.max_depth, scene.rr_depth)
+        dev.init_sampler(seed)
+        dev.render(scene.spp)  # warm-up (path state allocation)
+        dev.init_sampler(seed)
+        dev.clear_frame()
+        st = dev.render(scene.spp)
+        p_ms += st["render_ms"]
+        p_rays += st["rays"]
+    return {"workload": f"{count} terrain frames, {sum(s.tri_count for s, _, _ in frames):,} tris in total, "
+                        f"{samples:,} pixel-samples, 3 AOVs",
+            "batched_ms": b_ms, "plain_ms": p_ms, "speedup": p_ms / b_ms,
+            "batched_mrays_per_s": b_rays / 1e6 / (b_ms * 1e-3), "plain_mrays_per_s": p_rays / 1e6 / (p_ms * 1e-3),
+            "batched_samples_per_s": samples / (b_ms * 1e-3), "rays_equal": b_rays == p_rays,
+            "batched_kernel_launches": launches}
+
+
+def adjoint_bench(dev, repeats=3):
+    """Inverse-rendering workload: the room with textured floor and back wall (256^2 RGB
+    albedo textures) and rough specular spheres, 256x256, 16 spp per gradient. Cost of one
+    path-replay adjoint (all texel and roughness gradients) against one forward render."""
+    scene, params = prt_scenes.cornell_inverse(seed=0)
+    dev.setup(scene, seed=0)
+    dl = np.full((scene.height, scene.width, 3), 1e-3, np.float32)
+    dev.render(scene.spp)
+    dev.adjoint(dl, scene.spp)
+    f_ms = a_ms = None
+    for _ in range(repeats):
+        dev.init_sampler(0)
+        dev.clear_frame()
+        f = dev.render(scene.spp)["render_ms"]
+        a = dev.adjoint(dl, scene.spp)[2]["render_ms"]
+        f_ms = f if f_ms is None else min(f_ms, f)
+        a_ms = a if a_ms is None else min(a_ms, a)
+    n_params = sum(int(scene.textures[t].size) for t in params["textures"]) + len(params["roughness"])
+    return {"workload": "room, 2 x 256^2 RGB albedo textures + 32 roughnesses, 256x256, 16 spp",
+            "forward_ms": f_ms, "adjoint_ms": a_ms, "cost_ratio": a_ms / f_ms,
+            "gradients_per_s": 1e3 / a_ms, "parameters": n_params}
+
 
 C_CAMERA_BYTES = 4 * 14  # prt_camera_desc: 12 floats of basis and position + fov + near clip
 

@@ -1413,8 +1413,11 @@ int prt_cuda_adjoint(prt_context* ctx, uint32_t first_sample, int32_t spp, const
     Staged gr(c, grad_roughness, (size_t)std::max<int64_t>(mats, 1) * sizeof(float), false);
     cuCheck(cudaMemsetAsync(gt.dev, 0, (size_t)std::max<int64_t>(texFloats, 1) * sizeof(float), c.stream), "clear");
     cuCheck(cudaMemsetAsync(gr.dev, 0, (size_t)std::max<int64_t>(mats, 1) * sizeof(float), c.stream), "clear");
+    ensurePathState(c, spp);
+    RenderCounters rc;
     cuCheck(cudaEventRecord(c.ev0, c.stream), "event");
-    cuCheck(launchAdjoint(c, first_sample, spp, (const float*)dl.dev, (float*)gt.dev, (float*)gr.dev, 1e-3f), "adjoint");
+    cuCheck(launchAdjoint(c, first_sample, spp, (const float*)dl.dev, (float*)gt.dev, (float*)gr.dev, 1e-3f, rc),
+            "adjoint");
     cuCheck(cudaEventRecord(c.ev1, c.stream), "event");
     if (grad_textures) gt.copyOut();
     if (grad_roughness) gr.copyOut();
@@ -1427,7 +1430,11 @@ int prt_cuda_adjoint(prt_context* ctx, uint32_t first_sample, int32_t spp, const
       std::memset(stats, 0, sizeof(*stats));
       stats->spp = spp;
       stats->render_ms = ms;
-      stats->kernel_launches = 1;
+      stats->rays = rc.closestRays + rc.shadowRays;
+      stats->closest_rays = rc.closestRays;
+      stats->shadow_rays = rc.shadowRays;
+      stats->kernel_launches = rc.launches;
+      stats->trace_launches = rc.traceLaunches;
     }
   });
 }

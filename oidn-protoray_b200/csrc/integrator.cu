@@ -13,6 +13,7 @@
 // accumulation planes, reproducing AccumBuffer3f::addSerial (image/accum_buffer.h:439-486)
 // without atomics, so the image does not depend on scheduling.
 #include "wavefront.cuh"
+#include "adjoint.cuh"
 
 #include <algorithm>
 #include <cstddef>
@@ -36,6 +37,8 @@ struct Launch
   int itemCount;
   BatchCtl* ctl;
   int* freeList[2];
+  // Replay form of the adjoint only.
+  AdjointView adj;
 };
 
 template <int... Fs>
@@ -499,7 +502,7 @@ __global__ void __launch_bounds__(256) kShadeEnd(Launch L, const int* __restrict
 
 // Surface shading of one bounce (render/path_renderer_stream.h:592-949) for materials whose
 // lobes lie in feature set F: NEE with MIS, BSDF sampling, Russian roulette, medium tracking.
-template <int F, bool Batch>
+template <int F, bool Batch, bool Adj = false>
 __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __restrict__ queue,
                                                      const int* __restrict__ count, int launchDepth,
                                                      int* __restrict__ queueOut, int* __restrict__ extCount,
@@ -552,6 +555,8 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
         T *= powf3(mc, hh.x);
       }
       // Direct light (NEE)
+      bool neeVisible = false;
+      f3 neeL = mk(0.f), neeWi = mk(0.f);
       if (bsdf.flags() & kBsdfSmooth)
       {
         float lx, ly, lz;
@@ -572,10 +577,22 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
               bsdfPdf *= contProb;
             }
             const f3 dirL = dirT * misWeight(lightPdf, bsdfPdf) * Lw;
-            shadow = true;
-            shO = make_float4(ctx.p.x, ctx.p.y, ctx.p.z, ctx.eps);
-            shD = make_float4(wi.x, wi.y, wi.z, dist - ctx.eps);
-            shL = make_float4(dirL.x, dirL.y, dirL.z, 0.f);
+            if (Adj)
+            {
+              // Replay: the shadow ray is traced here, its visibility is part of the vertex.
+              const float far = dist - ctx.eps;
+              neeVisible = far > 0.f ? traverse<true>(E.sc.nodes, E.sc.tris, ctx.p, wi, ctx.eps, far, L.ps.err).triId < 0
+                                     : true;
+              neeL = neeVisible ? dirL : mk(0.f);
+              neeWi = wi;
+            }
+            else
+            {
+              shadow = true;
+              shO = make_float4(ctx.p.x, ctx.p.y, ctx.p.z, ctx.eps);
+              shD = make_float4(wi.x, wi.y, wi.z, dist - ctx.eps);
+              shL = make_float4(dirL.x, dirL.y, dirL.z, 0.f);
+            }
           }
         }
       }
@@ -590,7 +607,7 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
       const int extType = extend ? bsdfType : 0;
       if (aov1)
       {
-        if (E.aovMask)
+        if (!Adj && E.aovMask)
         {
           const f3 a = bsdf.albedo(), nn = bsdf.normal();
           L.ps.aovA[p] = make_float4(a.x, a.y, a.z, 1.f);
@@ -608,6 +625,18 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
         T *= 1.f / contProb;
         bsdfPdf *= contProb;
       }
+      if (Adj)
+      {
+        // Replay: out[p] holds the radiance still to come at this vertex.
+        const float4 o = L.ps.out[p];
+        const f3 rest = mk(o.x, o.y, o.z) - neeL;
+        const uint32_t px = pixelId & kPixelIdMask;
+        const float* g = L.adj.dLdI + 3 * ((size_t)(px >> 16) * L.width + (px & 0xffffu));
+        const f3 delta = mk(g[0], g[1], g[2]) * L.adj.invSpp;
+        adjointVertex<F>(L.adj, E.sc, L.tab, mat, ctx, bsdf, wo, wi, neeWi, extend, neeVisible, neeL,
+                         extend ? rest : mk(0.f), delta);
+        if (extend) L.ps.out[p] = make_float4(rest.x, rest.y, rest.z, o.w);
+      }
       if (extend)
       {
         L.ps.rayO[p] = make_float4(ctx.p.x, ctx.p.y, ctx.p.z, ctx.eps);
@@ -623,7 +652,7 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
       }
       info.x = pixelId;
       L.ps.info[p] = info;
-      if (!extend && !shadow)
+      if (!Adj && !extend && !shadow)
       {
         finishPath<Batch>(L, p, Lr, info);
         freed = true;
@@ -809,13 +838,105 @@ using ShadeClassList = ShadeLaunch<PRT_SHADE_CLASS_LIST>;
 static_assert(kShadeClassFeatures[1] == kFeatOpaque && kShadeClassFeatures[7] == kFeatAll, "class list");
 
 
+// Traces one frame-form wave (kRaygen, then per bounce: closest hit, shading by class, shadow
+// rays) until no path is left. replay = true runs the adjoint's replay instead: the same paths
+// with the replay form of the shading kernels (classes 1 and 2, the adjoint's material set),
+// which trace their shadow rays inline and scatter gradients.
+template <class Begin, class End>
+static cudaError_t bounceLoop(Context& ctx, const Launch& L, int P, bool replay, bool counting, Begin begin, End end,
+                              RenderCounters& rc)
+{
+  const int maxDepth = ctx.renderer.maxDepth;
+  int* counts = ctx.ps.counters;
+  const int persistent = ctx.smCount * ctx.traceBlocks;
+  const int shadeGrid = ctx.smCount * ctx.shadeBlocks;
+  cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(int) * kCntStride * (maxDepth + 2), ctx.stream);
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpyAsync(counts, &P, sizeof(int), cudaMemcpyHostToDevice, ctx.stream);
+  if (e != cudaSuccess) return e;
+  kRaygen<<<gridFor(ctx, P), 256, 0, ctx.stream>>>(L);
+  rc.launches++;
+  for (int depth = 0; depth <= maxDepth; ++depth)
+  {
+    int* cnt = counts + kCntStride * depth;
+    int* next = counts + kCntStride * (depth + 1);
+    const int* q = depth == 0 ? nullptr : ctx.ps.queue[depth & 1];
+    int* qOut = ctx.ps.queue[(depth + 1) & 1];
+    begin(0);
+    if (counting)
+      kTrace<true, false><<<persistent, 256, 0, ctx.stream>>>(L, q, cnt, cnt + kCntWorkTrace, depth,
+                                                              ctx.ps.classQueues, cnt + 1);
+    else
+      kTrace<false, false><<<persistent, 256, 0, ctx.stream>>>(L, q, cnt, cnt + kCntWorkTrace, depth,
+                                                               ctx.ps.classQueues, cnt + 1);
+    end();
+    begin(2);
+    if (replay)
+    {
+      // Paths of class 0 (misses, emitters, maxDepth) carry no parameters: they are dropped.
+      kShadeSurface<kShadeClassFeatures[1], false, true><<<shadeGrid, 256, 0, ctx.stream>>>(
+        L, ctx.ps.classQueues + (int64_t)1 * ctx.ps.capacity, cnt + 2, depth, qOut, next, cnt + kCntShadow, 0);
+      kShadeSurface<kShadeClassFeatures[2], false, true><<<shadeGrid, 256, 0, ctx.stream>>>(
+        L, ctx.ps.classQueues + (int64_t)2 * ctx.ps.capacity, cnt + 3, depth, qOut, next, cnt + kCntShadow, 0);
+      rc.launches += 3;
+    }
+    else
+    {
+      kShadeEnd<false><<<shadeGrid, 256, 0, ctx.stream>>>(L, ctx.ps.classQueues, cnt + 1, depth, 0);
+      ShadeClassList::run<false>(1, L, ctx.stream, shadeGrid, ctx.ps.classQueues, cnt, depth, qOut, next,
+                                 cnt + kCntShadow, 0);
+      rc.launches += 1 + kShadeClasses;
+    }
+    end();
+    if (!replay)
+    {
+      begin(1);
+      if (counting)
+        kShadow<true, false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0);
+      else
+        kShadow<false, false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0);
+      end();
+      rc.launches++;
+    }
+    rc.traceLaunches++;
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    // Paths in, shadow rays and paths out of this bounce; stop once no path is left.
+    int in = 0, shadow = 0, out = 0;
+    e = cudaMemcpyAsync(&in, cnt, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&shadow, cnt + kCntShadow, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&out, next, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx.stream);
+    if (e != cudaSuccess) return e;
+    rc.closestRays += in;
+    rc.shadowRays += shadow;
+    if (out == 0) break;
+  }
+  return cudaSuccess;
+}
+
+static Launch frameLaunch(const Context& ctx, uint32_t firstSample, int samples)
+{
+  Launch L;
+  std::memset(&L, 0, sizeof(L));
+  L.sc = ctx.scene;
+  L.tab = ctx.tables;
+  L.cam = ctx.camera;
+  L.rd = ctx.renderer;
+  L.ps = ctx.ps;
+  L.width = ctx.width;
+  L.height = ctx.height;
+  L.pixelCount = ctx.width * ctx.height;
+  L.firstSample = firstSample;
+  L.samples = samples;
+  L.aovMask = ctx.aovMask;
+  return L;
+}
+
 cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
 {
   rc = RenderCounters();
   const int pixelCount = ctx.width * ctx.height;
-  const int maxDepth = ctx.renderer.maxDepth;
-  int* counts = ctx.ps.counters;
-  const int blocks = maxDepth + 2;
   const bool timing = (ctx.profileFlags & 1) != 0;
   const bool counting = (ctx.profileFlags & 2) != 0;
   std::vector<TimedLaunch> timed;
@@ -834,74 +955,12 @@ cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
   cudaError_t e = cudaSuccess;
   if (counting) e = cudaMemsetAsync(ctx.ps.travCounts, 0, 4 * sizeof(unsigned long long), ctx.stream);
   if (e != cudaSuccess) return e;
-  const int persistent = ctx.smCount * ctx.traceBlocks;
-  const int shadeGrid = ctx.smCount * ctx.shadeBlocks;
   for (int done = 0; done < spp;)
   {
     const int S = std::min(ctx.waveSamples, spp - done);
-    Launch L;
-    L.sc = ctx.scene;
-    L.tab = ctx.tables;
-    L.cam = ctx.camera;
-    L.rd = ctx.renderer;
-    L.ps = ctx.ps;
-    L.width = ctx.width;
-    L.height = ctx.height;
-    L.pixelCount = pixelCount;
-    L.firstSample = ctx.sampleIndex + (uint32_t)done;
-    L.samples = S;
-    L.aovMask = ctx.aovMask;
-    L.items = nullptr;
-    L.itemCount = 0;
-    L.ctl = nullptr;
-    L.freeList[0] = L.freeList[1] = nullptr;
-    const int P = pixelCount * S;
-    e = cudaMemsetAsync(counts, 0, sizeof(int) * kCntStride * blocks, ctx.stream);
+    const Launch L = frameLaunch(ctx, ctx.sampleIndex + (uint32_t)done, S);
+    e = bounceLoop(ctx, L, pixelCount * S, false, counting, begin, end, rc);
     if (e != cudaSuccess) return e;
-    e = cudaMemcpyAsync(counts, &P, sizeof(int), cudaMemcpyHostToDevice, ctx.stream);
-    if (e != cudaSuccess) return e;
-    kRaygen<<<gridFor(ctx, P), 256, 0, ctx.stream>>>(L);
-    rc.launches++;
-    for (int depth = 0; depth <= maxDepth; ++depth)
-    {
-      int* cnt = counts + kCntStride * depth;
-      int* next = counts + kCntStride * (depth + 1);
-      const int* q = depth == 0 ? nullptr : ctx.ps.queue[depth & 1];
-      int* qOut = ctx.ps.queue[(depth + 1) & 1];
-      begin(0);
-      if (counting)
-        kTrace<true, false><<<persistent, 256, 0, ctx.stream>>>(L, q, cnt, cnt + kCntWorkTrace, depth,
-                                                                ctx.ps.classQueues, cnt + 1);
-      else
-        kTrace<false, false><<<persistent, 256, 0, ctx.stream>>>(L, q, cnt, cnt + kCntWorkTrace, depth,
-                                                                 ctx.ps.classQueues, cnt + 1);
-      end();
-      begin(2);
-      kShadeEnd<false><<<shadeGrid, 256, 0, ctx.stream>>>(L, ctx.ps.classQueues, cnt + 1, depth, 0);
-      ShadeClassList::run<false>(1, L, ctx.stream, shadeGrid, ctx.ps.classQueues, cnt, depth, qOut, next,
-                                 cnt + kCntShadow, 0);
-      end();
-      begin(1);
-      if (counting)
-        kShadow<true, false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0);
-      else
-        kShadow<false, false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0);
-      end();
-      rc.launches += 3 + kShadeClasses;
-      rc.traceLaunches++;
-      e = cudaGetLastError();
-      if (e != cudaSuccess) return e;
-      // Paths in, shadow rays and paths out of this bounce; stop once no path is left.
-      int in = 0, shadow = 0, out = 0;
-      e = cudaMemcpyAsync(&in, cnt, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(&shadow, cnt + kCntShadow, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(&out, next, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(ctx.stream);
-      if (e != cudaSuccess) return e;
-      rc.closestRays += in;
-      rc.shadowRays += shadow;
-      if (out == 0) break;
-    }
     kAccumulate<<<gridFor(ctx, pixelCount), 256, 0, ctx.stream>>>(L, reinterpret_cast<float4*>(ctx.accum),
                                                                    reinterpret_cast<float4*>(ctx.accumA),
                                                                    reinterpret_cast<float4*>(ctx.accumN));
@@ -932,7 +991,43 @@ cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
   return cudaSuccess;
 }
 
-
+// Path-replay adjoint of samples [firstSample, firstSample + spp): per wave, a forward pass
+// that leaves each path's radiance in ps.out (nothing is accumulated into the frame), then the
+// replay pass over the same paths.
+cudaError_t launchAdjoint(Context& ctx, uint32_t firstSample, int spp, const float* dLdI, float* gradTex,
+                          float* gradRough, float roughnessStep, RenderCounters& rc)
+{
+  rc = RenderCounters();
+  AdjointView A;
+  std::memset(&A, 0, sizeof(A));
+  A.dLdI = dLdI;
+  A.gradTex = gradTex;
+  A.gradRough = gradRough;
+  long long off = 0;
+  for (size_t i = 0; i < ctx.texturesHost.size() && i < (size_t)kAdjointMaxTextures; ++i)
+  {
+    A.texOffset[i] = off;
+    off += 3ll * ctx.texturesHost[i].width * ctx.texturesHost[i].height;
+  }
+  A.step = roughnessStep;
+  A.invSpp = 1.f / (float)spp;
+  auto none = [](int) {};
+  auto none0 = []() {};
+  const int pixelCount = ctx.width * ctx.height;
+  for (int done = 0; done < spp;)
+  {
+    const int S = std::min(ctx.waveSamples, spp - done);
+    Launch L = frameLaunch(ctx, firstSample + (uint32_t)done, S);
+    L.aovMask = 0;
+    cudaError_t e = bounceLoop(ctx, L, pixelCount * S, false, false, none, none0, rc);
+    if (e != cudaSuccess) return e;
+    L.adj = A;
+    e = bounceLoop(ctx, L, pixelCount * S, true, false, none, none0, rc);
+    if (e != cudaSuccess) return e;
+    done += S;
+  }
+  return cudaSuccess;
+}
 
 // ---- batch form ---------------------------------------------------------------------------------
 

@@ -152,7 +152,7 @@ cudaError_t launchBlitPlane(Context& ctx, const float4* plane, int n, float* dst
 // Path-replay adjoint (adjoint.cu): dLoss/d(texel) of every scene texture and dLoss/d(specular
 // roughness) of every material for the image gradient dLdI (W*H*3, device memory).
 cudaError_t launchAdjoint(Context& ctx, uint32_t firstSample, int spp, const float* dLdI, float* gradTex,
-                          float* gradRough, float roughnessStep);
+                          float* gradRough, float roughnessStep, RenderCounters& rc);
 // Copies a caller-order (row 0 at the top) RGB image into a device texture (row 0 at the bottom).
 cudaError_t launchTextureUpdate(Context& ctx, const DevTexture& t, const float* rgb);
 cudaError_t launchClear(Context& ctx);
