@@ -137,6 +137,48 @@ def cpu_baseline(min_seconds=10.0):
                       f"pathStream renderer compiled from its sources, oracle CPU BVH in place of Embree (not installed)"}
 
 
+class Ranks:
+    """Process-group plumbing of the replica runs: barrier, max and sum over ranks (a no-op
+    with one process). `device` is where the reduction tensor lives ("cuda:N" for NCCL, "cpu"
+    for gloo)."""
+
+    def __init__(self, pg, device):
+        self.pg = pg
+        self.device = device
+
+    @classmethod
+    def init(cls, backend, local_rank, timeout_s=120):
+        import torch
+        import torch.distributed as torch_dist
+        from datetime import timedelta
+
+        device = "cpu"
+        if backend == "nccl":
+            torch.cuda.set_device(local_rank)
+            device = f"cuda:{local_rank}"
+        torch_dist.init_process_group(backend, timeout=timedelta(seconds=timeout_s))
+        return cls(torch_dist, device)
+
+    def barrier(self):
+        if self.pg is not None:
+            self.pg.barrier()
+
+    def _reduce(self, x, op):
+        if self.pg is None:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.pg.all_reduce(t, op=op)
+        return float(t.item())
+
+    def max(self, x):
+        return x if self.pg is None else self._reduce(x, self.pg.ReduceOp.MAX)
+
+    def sum(self, x):
+        return x if self.pg is None else self._reduce(x, self.pg.ReduceOp.SUM)
+
+
 def run_reference(args):
     rank, world, _ = dist_info()
     if rank != 0:
@@ -177,37 +219,9 @@ def run_ours(args):
     rank, world, local = dist_info()
     import prt_cuda
 
-    pg = None
-    if world > 1:
-        import torch
-        import torch.distributed as torch_dist
-        from datetime import timedelta
-
-        torch.cuda.set_device(local)
-        torch_dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-        pg = torch_dist
-
-    def barrier():
-        if pg is not None:
-            pg.barrier()
-
-    def max_over_ranks(x):
-        if pg is None:
-            return x
-        import torch
-
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x):
-        if pg is None:
-            return x
-        import torch
-
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.SUM)
-        return float(t.item())
+    ranks = Ranks.init("nccl", local) if world > 1 else Ranks(None, None)
+    barrier, max_over_ranks, sum_over_ranks = ranks.barrier, ranks.max, ranks.sum
+    pg = ranks.pg
 
     scene = prt_scenes.terrain(spp=args.spp)
     dev = prt_cuda.DeviceCuda(local)
