@@ -244,6 +244,8 @@ typedef struct prt_tuning
   int32_t trace_blocks;
   int32_t shade_blocks;
   int32_t wave_paths;
+  int32_t top_stage;   /* 1: traversal reads the top 3 BVH levels from shared memory; 2: from
+                          global memory (the default); 0 keeps the current value */
 } prt_tuning;
 
 int prt_cuda_set_tuning(prt_context* ctx, const prt_tuning* tuning);

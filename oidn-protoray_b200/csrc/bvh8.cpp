@@ -2,6 +2,8 @@
 // assignment and 8-bit child-box quantisation. See bvh8.h for the node format.
 #include "bvh8.h"
 
+#include <deque>
+
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -363,8 +365,30 @@ struct WideBuilder
     out.nodes.resize(out.nodes.size() + innerN);
     out.nodes[wideIndex] = node;
     const uint32_t base = node.childBase;
+    // Children in the top levels are emitted breadth-first (queued), deeper ones depth-first.
     for (int i = 0; i < innerN; ++i)
-      emit((int)base + i, innerSlots[i], depth + 1);
+    {
+      if (depth + 1 < kBvh8TopLevels) pending.push_back({(int)base + i, innerSlots[i], depth + 1});
+      else emit((int)base + i, innerSlots[i], depth + 1);
+    }
+  }
+
+  struct Pending
+  {
+    int wideIndex, binIndex, depth;
+  };
+  std::deque<Pending> pending;
+
+  // Emits the whole tree: the top levels level by level, then each subtree depth-first.
+  void emitAll()
+  {
+    emit(0, 0, 0);
+    while (!pending.empty())
+    {
+      const Pending p = pending.front();
+      pending.pop_front();
+      emit(p.wideIndex, p.binIndex, p.depth);
+    }
   }
 };
 
@@ -410,8 +434,21 @@ void buildBvh8(const float* triVerts, int64_t triCount, Bvh8& out, int threads)
   out.nodes.reserve(n / 2 + 1);
   out.nodes.resize(1);
   WideBuilder wb(bb, triVerts, out);
-  wb.emit(0, 0, 0);
+  wb.emitAll();
   out.maxDepth = wb.maxDepth;
+  // Nodes of the top levels: the root, then every node whose parent is in the top levels.
+  {
+    int count = 1, levelBegin = 0, levelEnd = 1;
+    for (int level = 1; level < kBvh8TopLevels; ++level)
+    {
+      int next = 0;
+      for (int i = levelBegin; i < levelEnd; ++i) next += __builtin_popcount(out.nodes[i].imask);
+      levelBegin = levelEnd;
+      levelEnd += next;
+      count += next;
+    }
+    out.topCount = std::min(count, (int)out.nodes.size());
+  }
   for (int k = 0; k < 3; ++k) { out.lo[k] = bb.nodes[0].box.lo[k]; out.hi[k] = bb.nodes[0].box.hi[k]; }
   out.buildMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }

@@ -38,12 +38,19 @@ struct alignas(16) Bvh8Tri
 };
 static_assert(sizeof(Bvh8Tri) == 48, "Bvh8Tri must be 48 bytes");
 
+// The first kBvh8TopLevels levels of the tree are stored breadth-first at the start of the
+// node array (at most 1 + 8 + 64 = kBvh8TopNodes nodes), so that a kernel can stage them in
+// shared memory; deeper levels are stored depth-first, each subtree contiguous.
+constexpr int kBvh8TopLevels = 3;
+constexpr int kBvh8TopNodes = 73;
+
 struct Bvh8
 {
   std::vector<Bvh8Node> nodes;
   std::vector<Bvh8Tri> tris;
   float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};  // scene bounds
   int maxDepth = 0;                             // wide levels
+  int topCount = 1;                             // nodes of the first kBvh8TopLevels levels (stored first)
   double buildMs = 0.0;
 };
 

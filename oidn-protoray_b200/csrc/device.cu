@@ -338,6 +338,7 @@ void uploadScene(Context& c, const prt_scene_desc* s)
   buildBvh8(triPos.data(), totalTris, c.bvh);
   sc.nodes = reinterpret_cast<const uint4*>(upload(c, c.bvh.nodes));
   sc.tris = reinterpret_cast<const float4*>(upload(c, c.bvh.tris));
+  sc.topNodes = std::min(c.bvh.topCount, kBvh8TopNodes);
   sc.triCount = totalTris;
   sc.triVerts = upload(c, triVerts);
   sc.pos = upload(c, pos);
@@ -997,8 +998,10 @@ int prt_cuda_set_tuning(prt_context* ctx, const prt_tuning* t)
 {
   return guarded(ctx, [&](Context& c) {
     if (!t) throw std::invalid_argument("null tuning");
-    if (t->trace_blocks < 0 || t->trace_blocks > 32 || t->shade_blocks < 0 || t->shade_blocks > 32 || t->wave_paths < 0)
+    if (t->trace_blocks < 0 || t->trace_blocks > 32 || t->shade_blocks < 0 || t->shade_blocks > 32 || t->wave_paths < 0 ||
+        t->top_stage < 0 || t->top_stage > 2)
       throw std::invalid_argument("tuning out of range");
+    if (t->top_stage) c.topStage = t->top_stage == 1 ? 1 : 0;
     if (t->trace_blocks) c.traceBlocks = t->trace_blocks;
     if (t->shade_blocks) c.shadeBlocks = t->shade_blocks;
     if (t->wave_paths) c.wavePaths = t->wave_paths;
@@ -1012,6 +1015,7 @@ int prt_cuda_get_tuning(prt_context* ctx, prt_tuning* t)
     t->trace_blocks = c.traceBlocks;
     t->shade_blocks = c.shadeBlocks;
     t->wave_paths = (int32_t)std::min<int64_t>(c.wavePaths, 0x7fffffff);
+    t->top_stage = c.topStage ? 1 : 2;
   });
 }
 
@@ -1022,10 +1026,11 @@ int prt_cuda_autotune(prt_context* ctx, int32_t spp, prt_tuning* chosen, double*
     if (!c.hasRenderer || !c.hasCamera || !c.accum) throw ApiError{PRT_ERR_STATE, "renderer, camera and frame are required"};
     if (spp <= 0) throw std::invalid_argument("spp must be > 0");
     cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
-    auto timeOne = [&](int tb, int sb, int64_t wave) {
+    auto timeOne = [&](int tb, int sb, int64_t wave, int top) {
       c.traceBlocks = tb;
       c.shadeBlocks = sb;
       c.wavePaths = wave;
+      c.topStage = top;
       ensurePathState(c, spp);
       RenderCounters rc;
       cuCheck(cudaEventRecord(c.ev0, c.stream), "event");
@@ -1038,26 +1043,33 @@ int prt_cuda_autotune(prt_context* ctx, int32_t spp, prt_tuning* chosen, double*
     };
     const int profile = c.profileFlags;
     c.profileFlags = 0;
-    int bT = c.traceBlocks, bS = c.shadeBlocks;
+    int bT = c.traceBlocks, bS = c.shadeBlocks, bTop = c.topStage;
     int64_t bW = c.wavePaths;
-    timeOne(bT, bS, bW);  // warm-up
+    timeOne(bT, bS, bW, bTop);  // warm-up
     double best = -1.0;
-    // One axis at a time: wave size (paths in flight), then traversal and shading grids.
+    // One axis at a time: wave size (paths in flight), traversal and shading grids, staging
+    // of the top BVH levels in shared memory.
     for (int64_t w : {8ll << 20, 16ll << 20, 32ll << 20})
     {
-      const double v = timeOne(bT, bS, w);
+      const double v = timeOne(bT, bS, w, bTop);
       if (v > best) { best = v; bW = w; }
     }
     for (int tb : {4, 6, 8, 12})
     {
-      const double v = timeOne(tb, bS, bW);
+      const double v = timeOne(tb, bS, bW, bTop);
       if (v > best) { best = v; bT = tb; }
     }
     for (int sb : {2, 4, 8})
     {
-      const double v = timeOne(bT, sb, bW);
+      const double v = timeOne(bT, sb, bW, bTop);
       if (v > best) { best = v; bS = sb; }
     }
+    for (int top : {0, 1})
+    {
+      const double v = timeOne(bT, bS, bW, top);
+      if (v > best) { best = v; bTop = top; }
+    }
+    c.topStage = bTop;
     c.traceBlocks = bT;
     c.shadeBlocks = bS;
     c.wavePaths = bW;
@@ -1071,6 +1083,7 @@ int prt_cuda_autotune(prt_context* ctx, int32_t spp, prt_tuning* chosen, double*
       chosen->trace_blocks = bT;
       chosen->shade_blocks = bS;
       chosen->wave_paths = (int32_t)bW;
+      chosen->top_stage = bTop ? 1 : 2;
     }
     if (mrays) *mrays = best;
   });

@@ -152,6 +152,7 @@ struct DevScene
   const float* mediaColor;       // 3 per medium
   int mediaCount;
   float sceneRadius;
+  int topNodes;          // BVH nodes stored breadth-first at the start (shared-memory staging)
 };
 
 // BSDF energy-compensation tables (bsdf/albedo_tables.h), computed on the device at context

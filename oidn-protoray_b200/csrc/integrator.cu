@@ -284,6 +284,18 @@ __global__ void kBatchRegen(Launch L, int a, int* __restrict__ queue)
   }
 }
 
+// Copies the breadth-first top levels of the frame's BVH into shared memory (Top = true; frame
+// form only, the batch form mixes scenes). Returns the number of staged nodes.
+template <bool Top>
+PRT_D int stageTopNodes(const Launch& L)
+{
+  if (!Top) return 0;
+  const int n = min(L.sc.topNodes, kBvh8TopNodes);
+  for (int i = threadIdx.x; i < 5 * n; i += blockDim.x) gTopNodes[i] = __ldg(L.sc.nodes + i);
+  __syncthreads();
+  return n;
+}
+
 // Adds one warp's traversal counts to the global totals (counting variant only).
 PRT_D void addCounts(unsigned long long* dst, const TraceCount& c)
 {
@@ -304,12 +316,13 @@ PRT_D void addCounts(unsigned long long* dst, const TraceCount& c)
 // the hit and bin the path by the shading it needs (the GPU form of the reference's material
 // sort, render/renderer_stream.h:108-181): class 0 ends the path (miss, area light, maxDepth),
 // classes 1.. are the material feature classes.
-template <bool Count, bool Batch>
+template <bool Count, bool Batch, bool Top = false>
 __global__ void __launch_bounds__(256) kTrace(Launch L, const int* __restrict__ queue, const int* __restrict__ count,
                                               int* __restrict__ work, int depth, int* __restrict__ classQueues,
                                               int* __restrict__ classCounts)
 {
   const int n = *count;
+  const int top = stageTopNodes<Top && !Batch>(L);
   TraceCount tc;
   for (;;)
   {
@@ -332,8 +345,8 @@ __global__ void __launch_bounds__(256) kTrace(Launch L, const int* __restrict__ 
         pathDepth = (int)(info.z >> kDepthShift);
       }
       const PathEnv<Batch> E(L, item);
-      const TraceHit h = traverse<false, Count>(E.sc.nodes, E.sc.tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w,
-                                                L.ps.err, &tc);
+      const TraceHit h = traverse<false, Count, Top && !Batch>(E.sc.nodes, E.sc.tris, mk(a.x, a.y, a.z),
+                                                               mk(b.x, b.y, b.z), a.w, b.w, L.ps.err, &tc, top);
       L.ps.hit[p] = make_float4(h.t, h.u, h.v, __int_as_float(h.triId));
       cls = 0;
       if (h.triId >= 0 && pathDepth < E.rd.maxDepth) cls = __ldg(E.sc.meshClass + __ldg(E.sc.triVerts + h.triId).w);
@@ -384,11 +397,12 @@ PRT_D void freeSlots(const Launch& L, int b, bool freed, int p)
 
 // Any-hit test of the queued shadow rays; adds the unoccluded NEE contribution and
 // finishes paths that ended at this bounce (render/path_renderer_stream.h:953-1010).
-template <bool Count, bool Batch>
+template <bool Count, bool Batch, bool Top = false>
 __global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__ count, int* __restrict__ work,
                                                int parity)
 {
   const int n = *count;
+  const int top = stageTopNodes<Top && !Batch>(L);
   TraceCount tc;
   for (;;)
   {
@@ -410,8 +424,8 @@ __global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__
       bool unoccluded = b.w > 0.f;
       if (unoccluded)
       {
-        const TraceHit h = traverse<true, Count>(E.sc.nodes, E.sc.tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w,
-                                                 L.ps.err, &tc);
+        const TraceHit h = traverse<true, Count, Top && !Batch>(E.sc.nodes, E.sc.tris, mk(a.x, a.y, a.z),
+                                                                mk(b.x, b.y, b.z), a.w, b.w, L.ps.err, &tc, top);
         unoccluded = h.triId < 0;
       }
       float4 r = L.ps.rad[p];
@@ -866,6 +880,9 @@ static cudaError_t bounceLoop(Context& ctx, const Launch& L, int P, bool replay,
     if (counting)
       kTrace<true, false><<<persistent, 256, 0, ctx.stream>>>(L, q, cnt, cnt + kCntWorkTrace, depth,
                                                               ctx.ps.classQueues, cnt + 1);
+    else if (ctx.topStage)
+      kTrace<false, false, true><<<persistent, 256, 0, ctx.stream>>>(L, q, cnt, cnt + kCntWorkTrace, depth,
+                                                                     ctx.ps.classQueues, cnt + 1);
     else
       kTrace<false, false><<<persistent, 256, 0, ctx.stream>>>(L, q, cnt, cnt + kCntWorkTrace, depth,
                                                                ctx.ps.classQueues, cnt + 1);
@@ -893,6 +910,8 @@ static cudaError_t bounceLoop(Context& ctx, const Launch& L, int P, bool replay,
       begin(1);
       if (counting)
         kShadow<true, false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0);
+      else if (ctx.topStage)
+        kShadow<false, false, true><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0);
       else
         kShadow<false, false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0);
       end();

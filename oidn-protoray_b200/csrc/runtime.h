@@ -124,6 +124,7 @@ struct Context
   int traceBlocks = 8;            // launch tuning (prt_tuning)
   int shadeBlocks = 8;
   int64_t wavePaths = 32ll << 20;
+  int topStage = 0;               // stage the top BVH levels in shared memory (frame form)
 };
 
 // Per-call statistics gathered by renderSamples.

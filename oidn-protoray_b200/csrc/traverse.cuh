@@ -14,6 +14,7 @@
 #pragma once
 
 #include "prt_math.cuh"
+#include "bvh8.h"
 
 namespace prt {
 
@@ -83,14 +84,31 @@ PRT_D uint32_t byteOf(uint2 w, int i)
 
 // Intersects the 8 children of one node; returns the node group of hit inner children
 // (bits 24-31: hit flags at position slot ^ oct; bits 0-7: imask) and the triangle bits.
+// Shared-memory copy of the breadth-first top levels of the BVH (bvh8.h), filled by a
+// traversal kernel that stages them; with Top = true node i < topCount is read from here.
+static __shared__ uint4 gTopNodes[5 * kBvh8TopNodes];
+
+template <bool Top>
 PRT_D void intersectNode(const uint4* __restrict__ nodes, uint32_t nodeIdx, const RayPre& r, float tnear,
-                         float tfar, uint2& ngroup, uint2& tgroup)
+                         float tfar, uint2& ngroup, uint2& tgroup, int topCount = 0)
 {
-  const uint4 w0 = __ldg(nodes + 5 * nodeIdx + 0);
-  const uint4 w1 = __ldg(nodes + 5 * nodeIdx + 1);
-  const uint4 w2 = __ldg(nodes + 5 * nodeIdx + 2);
-  const uint4 w3 = __ldg(nodes + 5 * nodeIdx + 3);
-  const uint4 w4 = __ldg(nodes + 5 * nodeIdx + 4);
+  uint4 w0, w1, w2, w3, w4;
+  if (Top && nodeIdx < (uint32_t)topCount)
+  {
+    w0 = gTopNodes[5 * nodeIdx + 0];
+    w1 = gTopNodes[5 * nodeIdx + 1];
+    w2 = gTopNodes[5 * nodeIdx + 2];
+    w3 = gTopNodes[5 * nodeIdx + 3];
+    w4 = gTopNodes[5 * nodeIdx + 4];
+  }
+  else
+  {
+    w0 = __ldg(nodes + 5 * nodeIdx + 0);
+    w1 = __ldg(nodes + 5 * nodeIdx + 1);
+    w2 = __ldg(nodes + 5 * nodeIdx + 2);
+    w3 = __ldg(nodes + 5 * nodeIdx + 3);
+    w4 = __ldg(nodes + 5 * nodeIdx + 4);
+  }
   const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
   const uint32_t ex = w0.w & 0xffu, ey = (w0.w >> 8) & 0xffu, ez = (w0.w >> 16) & 0xffu;
   const uint32_t imask = (w0.w >> 24) & 0xffu;
@@ -139,9 +157,10 @@ struct TraceCount
   int tris = 0;
 };
 
-template <bool AnyHit, bool Count = false>
+template <bool AnyHit, bool Count = false, bool Top = false>
 PRT_D TraceHit traverse(const uint4* __restrict__ nodes, const float4* __restrict__ tris, f3 o, f3 d,
-                        float tnear, float tfar, uint32_t* errFlag, TraceCount* count = nullptr)
+                        float tnear, float tfar, uint32_t* errFlag, TraceCount* count = nullptr,
+                        int topCount = 0)
 {
   TraceHit h;
   h.triId = -1;
@@ -199,7 +218,7 @@ PRT_D TraceHit traverse(const uint4* __restrict__ nodes, const float4* __restric
       stack[sp++] = ngroup;
     }
     if (Count) count->nodes++;
-    intersectNode(nodes, nodeIdx, r, tnear, h.t, ngroup, tgroup);
+    intersectNode<Top>(nodes, nodeIdx, r, tnear, h.t, ngroup, tgroup, topCount);
   }
   atomicOr(errFlag, kErrIterCap);
   return h;

@@ -199,6 +199,7 @@ class Tuning(C.Structure):
         ("trace_blocks", C.c_int32),
         ("shade_blocks", C.c_int32),
         ("wave_paths", C.c_int32),
+        ("top_stage", C.c_int32),
     ]
 
 

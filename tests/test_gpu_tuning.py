@@ -1,0 +1,70 @@
+"""Launch tuning (prt_cuda_set_tuning / prt_cuda_autotune) changes speed, never the image.
+
+Every tuning axis -- path-pool size (samples per wave), traversal and shading blocks per SM,
+staging of the top BVH levels in shared memory -- leaves each path's samples and shading
+unchanged and the accumulation adds each pixel's samples in sample order, so images are
+bit-identical across tunings.
+"""
+import numpy as np
+import pytest
+
+import prt_cuda
+import prt_scenes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dev():
+    d = prt_cuda.DeviceCuda(0)
+    s = prt_scenes.terrain(seed=3, grid=128, n_spheres=40, width=256, height=128, spp=8)
+    d.setup(s, seed=5)
+    d.test_scene = s
+    yield d
+    d.close()
+
+
+def render(dev, spp):
+    dev.init_sampler(5)
+    dev.clear_frame()
+    st = dev.render(spp)
+    return dev.blit_frame(), st["rays"]
+
+
+@pytest.mark.parametrize("tuning", [
+    dict(top_stage=1),
+    dict(top_stage=2, trace_blocks=4, shade_blocks=2),
+    dict(wave_paths=256 * 128 * 3),          # 3 samples per wave: waves of 3, 3, 2 samples
+    dict(trace_blocks=12, shade_blocks=16, top_stage=1),
+])
+def test_tuning_keeps_the_image(dev, tuning):
+    default = dev.get_tuning()
+    ref, rays = render(dev, 8)
+    try:
+        dev.set_tuning(**tuning)
+        img, rays2 = render(dev, 8)
+    finally:
+        dev.set_tuning(**default)
+    assert rays2 == rays
+    assert np.array_equal(img, ref)
+
+
+def test_autotune_returns_a_valid_tuning(dev):
+    default = dev.get_tuning()
+    ref, _ = render(dev, 4)
+    try:
+        chosen, mrays = dev.autotune(2)
+        assert mrays > 0
+        assert chosen["top_stage"] in (1, 2) and 1 <= chosen["trace_blocks"] <= 32
+        assert dev.get_tuning() == chosen
+        img, _ = render(dev, 4)
+        assert np.array_equal(img, ref)
+    finally:
+        dev.set_tuning(**default)
+
+
+def test_tuning_rejects_out_of_range(dev):
+    with pytest.raises(ValueError):
+        dev.set_tuning(trace_blocks=64)
+    with pytest.raises(ValueError):
+        dev.set_tuning(top_stage=3)
