@@ -356,7 +356,8 @@ int prt_cuda_bsdf_query(prt_context* ctx, const prt_material* material, int32_t 
 /* Copies the BSDF energy-compensation tables the context computed at creation (the
  * reference's precomputeAlbedoTables, bsdf/albedo_tables.cpp:173-188) to out, concatenated in
  * the order GGX dir (32x32), GGX avg (32), dielectric eta dir (16^3), eta avg (16^2), dielectric
- * 1/eta dir (16^3), avg (16^2), dielectric reflection dir (16^3), avg (16^2). Writes at most
+ * 1/eta dir (16^3), avg (16^2), dielectric reflection dir (16^3), avg (16^2), sheen dir (16^2,
+ * bsdf/albedo_tables.h:281-300). Writes at most
  * `capacity` floats and returns the total count through *count. */
 int prt_cuda_albedo_tables(prt_context* ctx, float* out, int64_t capacity, int64_t* count);
 

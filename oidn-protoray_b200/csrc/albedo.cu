@@ -103,6 +103,37 @@ __global__ void kDielTable(float* dir, float minEta, float maxEta, int kind)
 }
 
 // integrateAvg: one thread per row of `size` directional values.
+// MicrofacetSheenAlbedo::integrate (bsdf/albedo.h:287-330): 32 x 32 midpoint samples of the
+// uniformly sampled sheen lobe per (cos, roughness) entry.
+__global__ void kSheenTable(float* dir)
+{
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= kTableSize * kTableSize) return;
+  const int i = idx % kTableSize, j = idx / kTableSize;
+  const float cosThetaO = fmaxf((float)i / (float)(kTableSize - 1), 1e-6f);
+  const float roughness = (float)j / (float)(kTableSize - 1);
+  SheenDist mf;
+  mf.r = roughnessToAlpha(roughness);
+  const f3 wo = mk(sqrtf(fmaxf(1.f - cosThetaO * cosThetaO, 0.f)), 0.f, cosThetaO);
+  const int n = 32;
+  float sum = 0.f;
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b < n; ++b)
+    {
+      const float sx = sampleCoord(a, n), sy = sampleCoord(b, n);
+      const float cosThetaI = sy;
+      const float sinThetaI = sqrtf(fmaxf(1.f - sy * sy, 0.f));
+      float sinPhi, cosPhi;
+      sincospif(2.f * sx, &sinPhi, &cosPhi);
+      const f3 wi = mk(cosPhi * sinThetaI, sinPhi * sinThetaI, cosThetaI);
+      const f3 wh = normalize(wo + wi);
+      const float D = mf.eval(wh.z);
+      const float G = mf.G2(cosThetaO, cosThetaI);
+      sum += D * G * (2.f * kPi) / (4.f * cosThetaO);
+    }
+  dir[idx] = fminf(sum / (float)(n * n), 1.f);
+}
+
 __global__ void kAvg(const float* dir, float* avg, int rows, int size)
 {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -158,6 +189,7 @@ cudaError_t buildAlbedoTables(DevTables& t, float** storage)
   kAvg<<<(t2 + 127) / 128, 128>>>(dielRcpDir, dielRcpAvg, t2, kTableSize);
   kDielTable<<<(t3 + 127) / 128, 128>>>(reflDir, 1.f / maxIor, 1.f / minIor, 1);
   kAvg<<<(t2 + 127) / 128, 128>>>(reflDir, reflAvg, t2, kTableSize);
+  kSheenTable<<<(t2 + 127) / 128, 128>>>(sheenDir);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   e = cudaDeviceSynchronize();

@@ -129,6 +129,13 @@ PRT_D float reflAlbedo(const DevTables& t, float cosThetaO, float eta, float rou
   return interp3D(t.reflDir, kTableSize, cosThetaO * k, e * k, roughness * k);
 }
 
+// MicrofacetSheenAlbedoTable (bsdf/albedo_tables.h:281-300): 16 x 16 over (cos, roughness).
+PRT_D float sheenAlbedo(const DevTables& t, float cosThetaO, float roughness)
+{
+  const float k = (float)(kTableSize - 1);
+  return interp2D(t.sheenDir, kTableSize, cosThetaO * k, roughness * k);
+}
+
 PRT_D float reflAlbedoAvg(const DevTables& t, float eta, float roughness)
 {
   const float k = (float)(kTableSize - 1);
@@ -268,9 +275,13 @@ PRT_D f3 lerp3(f3 a, f3 b, float s) { return a + s * (b - a); }
 // ---- lobes ---------------------------------------------------------------------------------------
 
 // DiffuseBrdf (bsdf/diffuse.h:45-82).
-struct DiffuseLobe
+// R: the instance may be rough (kFeatRoughDiffuse); R = false compiles the rough branch out.
+template <bool R>
+struct DiffuseLobeT
 {
   f3 color;
+  float roughness;  // Oren-Nayar roughness (rough lobe only)
+  bool rough;       // RoughDiffuseBrdf (bsdf/rough_diffuse.h:53-108) instead of DiffuseBrdf
 
   PRT_D int flags() const { return kDiffuseReflection; }
   PRT_D float importance() const { return reduceMax(color); }
@@ -278,6 +289,18 @@ struct DiffuseLobe
 
   PRT_D f3 eval(const Frame& fr, f3 Ng, f3 wo, f3 wi, float& pdf) const
   {
+    if (R && rough)
+    {
+      // Oren-Nayar with Fujii's simplification ("A tiny improvement of Oren-Nayar reflectance
+      // model", 2012): f = color (1 + r s / t) / (pi + (pi/2 - 2/3) r), s = wo.wi - cos_o cos_i,
+      // t = max(cos_o, cos_i) where s > 0, else 1.
+      const float cosThetaO = fmaxf(dot(wo, fr.N), 0.f);
+      const float cosThetaI = fmaxf(dot(wi, fr.N), 0.f);
+      pdf = cosThetaI * kInvPi;
+      const float s = dot(wo, wi) - cosThetaO * cosThetaI;
+      const float sInvt = s > 0.f ? s * rcpSafe(fmaxf(cosThetaO, cosThetaI)) : s;
+      return color * (cosThetaI * (1.f + roughness * sInvt) * (1.f / (kPi + (0.5f * kPi - 2.f / 3.f) * roughness)));
+    }
     const float cosThetaI = fmaxf(dot(wi, fr.N), 0.f);
     pdf = cosThetaI * kInvPi;
     return color * kInvPi * cosThetaI;
@@ -287,7 +310,59 @@ struct DiffuseLobe
   {
     wi = toWorld(fr, cosineSampleHemisphere(pdf, sx, sy));
     type = kDiffuseReflection;
-    return dot(wi, Ng) > 0.f ? color : mk(0.f);
+    if (!(dot(wi, Ng) > 0.f)) return mk(0.f);
+    if (R && rough)
+    {
+      const f3 v = eval(fr, Ng, wo, wi, pdf);
+      return v * (1.f / pdf);
+    }
+    return color;
+  }
+};
+
+// Microfiber sheen distribution (Conty and Kulla 2017, "Production Friendly Microfacet Sheen
+// BRDF"; Kulla and Conty 2017, "Revisiting Physically Based Shading at Imageworks"):
+// D = (2 + 1/r) sin^(1/r)(theta) / (2 pi); Lambda from the papers' fitted curve; the incoming
+// Lambda is softened near the terminator as bsdf/sheen_distribution.h:60-67 does.
+struct SheenDist
+{
+  float r;  // alpha in (0, 1]
+
+  PRT_D float eval(float cosTheta) const
+  {
+    const float sinTheta = sqrtf(fmaxf(1.f - cosTheta * cosTheta, 0.f));
+    const float invr = 1.f / r;
+    return (2.f + invr) * powf(sinTheta, invr) * (1.f / (2.f * kPi));
+  }
+
+  // The published fit of log Lambda, interpolated in (1 - r)^2 between its two end points.
+  PRT_D float fitL(float x) const
+  {
+    const float w0 = (1.f - r) * (1.f - r), w1 = 1.f - w0;
+    const float a = w0 * 25.3245f + w1 * 21.5473f;
+    const float b = w0 * 3.32435f + w1 * 3.82987f;
+    const float c = w0 * 0.16801f + w1 * 0.19823f;
+    const float d = w0 * -1.27393f + w1 * -1.97760f;
+    const float e = w0 * -4.85967f + w1 * -4.32054f;
+    return a / (1.f + b * powf(x, c)) + d * x + e;
+  }
+
+  PRT_D float lambda(float cosTheta) const
+  {
+    return cosTheta < 0.5f ? expf(fitL(cosTheta)) : expf(2.f * fitL(0.5f) - fitL(1.f - cosTheta));
+  }
+
+  PRT_D float lambdaI(float cosTheta) const
+  {
+    const float u = 1.f - cosTheta;
+    const float u2 = u * u, u4 = u2 * u2;
+    return powf(lambda(cosTheta), 1.f + 2.f * u4 * u4);
+  }
+
+  // Height-correlated masking-shadowing.
+  PRT_D float G2(float cosThetaO, float cosThetaI) const
+  {
+    return 1.f / (1.f + lambda(cosThetaO) + lambdaI(cosThetaI));
   }
 };
 
@@ -760,6 +835,120 @@ struct CoatLayer
   }
 };
 
+// SheenBsdf (bsdf/sheen.h:199-451): a sheen layer over a substrate. The sheen lobe is
+// sampled uniformly over the hemisphere and picked against the substrate by Ro * max(color)
+// versus (1 - Ro) * importance(substrate); the substrate is scaled by min(1 - Ro, 1 - Ri), where
+// R is the sheen's directional albedo.
+struct SheenLayer
+{
+  f3 color;
+  SheenDist mf;
+  float roughness;
+  float scale;
+
+  PRT_D void init(f3 col, float rgh, float s)
+  {
+    color = col;
+    roughness = rgh;
+    mf.r = roughnessToAlpha(rgh);
+    scale = s;
+  }
+
+  PRT_D int flags(int baseFlags) const { return baseFlags | kDiffuseReflection; }
+
+  PRT_D f3 sheenValue(const Frame& fr, f3 wo, f3 wi, float cosThetaO, float cosThetaI) const
+  {
+    const f3 wh = normalize(wo + wi);
+    const float D = mf.eval(dot(wh, fr.N));
+    const float G = mf.G2(cosThetaO, cosThetaI);
+    return color * (D * G * (1.f / (4.f * cosThetaO)) * scale);
+  }
+
+  template <class Sub>
+  PRT_D f3 eval(const DevTables& t, const Sub& base, const Frame& fr, f3 Ng, f3 wo, f3 wi, float& pdf) const
+  {
+    pdf = 0.f;
+    const float cosThetaO = dot(wo, fr.N);
+    if (!(cosThetaO > 0.f)) return mk(0.f);
+    const float cosThetaI = dot(wi, fr.N);
+    if (!(cosThetaI * dot(wi, Ng) > 0.f)) return mk(0.f);
+    float basePdf;
+    f3 baseValue = base.eval(t, wo, wi, basePdf);
+    const float Ro = sheenAlbedo(t, cosThetaO, roughness) * scale;
+    const float Ri = sheenAlbedo(t, fabsf(cosThetaI), roughness) * scale;
+    baseValue *= fminf(1.f - Ro, 1.f - Ri);
+    const float coatImp = Ro * reduceMax(color);
+    const float baseImp = (1.f - Ro) * base.importance();
+    const float coatPick = coatImp * (1.f / (coatImp + baseImp));
+    const float basePick = 1.f - coatPick;
+    if (cosThetaI > 0.f)
+    {
+      pdf = coatPick * (1.f / (2.f * kPi)) + basePick * basePdf;
+      return sheenValue(fr, wo, wi, cosThetaO, cosThetaI) + baseValue;
+    }
+    pdf = basePdf * basePick;
+    return baseValue;
+  }
+
+  template <class Sub>
+  PRT_D f3 sample(const DevTables& t, const Sub& base, const Frame& fr, f3 Ng, f3 wo, float sx, float sy, float sc,
+                  f3& wi, float& pdf, int& type) const
+  {
+    pdf = 0.f;
+    type = 0;
+    wi = mk(0.f);
+    const float cosThetaO = dot(wo, fr.N);
+    if (!(cosThetaO > 0.f)) return mk(0.f);
+    const float Ro = sheenAlbedo(t, cosThetaO, roughness) * scale;
+    const float coatImp = Ro * reduceMax(color);
+    const float baseImp = (1.f - Ro) * base.importance();
+    const float coatPick = coatImp * (1.f / (coatImp + baseImp));
+    const float basePick = 1.f - coatPick;
+    float basePdf = 0.f;
+    f3 baseValue = mk(0.f);
+    if (sc <= coatPick)
+    {
+      type = kDiffuseReflection;
+      // uniformSampleHemisphere: phi = 2 pi sx, cos(theta) = sy
+      const float cosTheta = sy;
+      const float sinTheta = sqrtf(fmaxf(1.f - sy * sy, 0.f));
+      float sinPhi, cosPhi;
+      sincospif(2.f * sx, &sinPhi, &cosPhi);
+      wi = toWorld(fr, mk(cosPhi * sinTheta, sinPhi * sinTheta, cosTheta));
+      baseValue = base.eval(t, wo, wi, basePdf);
+    }
+    else
+    {
+      const float s1 = (sc - coatPick) * (1.f / basePick);
+      f3 baseWi;
+      float basePdf2;
+      int baseType;
+      const f3 bw = base.sample(t, wo, sx, sy, s1, baseWi, basePdf2, baseType);
+      if (!(reduceMax(bw) > 0.f)) return mk(0.f);
+      wi = baseWi;
+      basePdf = basePdf2;
+      type = baseType;
+      baseValue = bw * ((type & kBsdfDelta) != 0 ? 1.f : basePdf);
+    }
+    const float cosThetaI = dot(wi, fr.N);
+    if (!(cosThetaI * dot(wi, Ng) > 0.f)) return mk(0.f);
+    const float Ri = sheenAlbedo(t, fabsf(cosThetaI), roughness) * scale;
+    baseValue *= fminf(1.f - Ro, 1.f - Ri);
+    if (type & kBsdfDelta)
+    {
+      pdf = basePdf;
+      return baseValue * (1.f / basePick);
+    }
+    if (cosThetaI <= 0.f)
+    {
+      pdf = basePick * basePdf;
+      return baseValue * (1.f / pdf);
+    }
+    pdf = coatPick * (1.f / (2.f * kPi)) + basePick * basePdf;
+    return (sheenValue(fr, wo, wi, cosThetaO, cosThetaI) + baseValue) * (1.f / pdf);
+  }
+};
+
 // ---- Standard material composition -----------------------------------------------------------
 
 enum : int
@@ -772,17 +961,19 @@ enum : int
 
 // The opaque base: a Lambertian lobe, optionally under the specular dielectric layer
 // (material/standard.cpp:441-502).
+template <bool R>
 struct OpaqueBase
 {
-  DiffuseLobe diff;
+  DiffuseLobeT<R> diff;
   CoatLayer spec;
   bool hasSpec;
 };
 
 // Substrate adaptor for the specular layer: the diffuse lobe.
+template <bool R>
 struct DiffuseSub
 {
-  DiffuseLobe d;
+  DiffuseLobeT<R> d;
   Frame fr;
   f3 Ng;
   PRT_D int flags() const { return kDiffuseReflection; }
@@ -807,14 +998,17 @@ struct StdBsdfT
   float imp[3];
   float impSum;
   int baseFlags;
-  OpaqueBase opaque;
+  OpaqueBase<(F & kFeatRoughDiffuse) != 0> opaque;
   DielectricLobe diel;
   ConductorLobe cond;
   CoatLayer coat;
   bool hasCoat;
+  SheenLayer sheen;
+  bool hasSheen;
   f3 albedoV;
 
-  PRT_D int flags() const { return ((F & kFeatCoat) && hasCoat) ? coat.flags(baseFlags) : baseFlags; }
+  PRT_D int coatedFlags() const { return ((F & kFeatCoat) && hasCoat) ? coat.flags(baseFlags) : baseFlags; }
+  PRT_D int flags() const { return ((F & kFeatSheen) && hasSheen) ? sheen.flags(coatedFlags()) : coatedFlags(); }
 
   PRT_D f3 evalSlot(const DevTables& t, int k, f3 wo, f3 wi, float& pdf) const
   {
@@ -822,7 +1016,7 @@ struct StdBsdfT
     {
       if ((F & kFeatSpecular) && opaque.hasSpec)
       {
-        const DiffuseSub sub{opaque.diff, fr, Ng};
+        const DiffuseSub<(F & kFeatRoughDiffuse) != 0> sub{opaque.diff, fr, Ng};
         return opaque.spec.eval(t, sub, fr, Ng, wo, wi, pdf);
       }
       return opaque.diff.eval(fr, Ng, wo, wi, pdf);
@@ -840,7 +1034,7 @@ struct StdBsdfT
     {
       if ((F & kFeatSpecular) && opaque.hasSpec)
       {
-        const DiffuseSub sub{opaque.diff, fr, Ng};
+        const DiffuseSub<(F & kFeatRoughDiffuse) != 0> sub{opaque.diff, fr, Ng};
         return opaque.spec.sample(t, sub, fr, Ng, wo, sx, sy, sc, wi, pdf, type);
       }
       return opaque.diff.sample(fr, Ng, wo, sx, sy, sc, wi, pdf, type);
@@ -927,16 +1121,44 @@ struct StdBsdfT
     }
   };
 
-  PRT_D f3 eval(const DevTables& t, f3 wo, f3 wi, float& pdf) const
+  // The base with its coat (when present): the substrate of the sheen layer.
+  PRT_D f3 evalCoated(const DevTables& t, f3 wo, f3 wi, float& pdf) const
   {
     if ((F & kFeatCoat) && hasCoat) return coat.eval(t, BaseSub{this}, fr, Ng, wo, wi, pdf);
     return evalBase(t, wo, wi, pdf);
   }
 
-  PRT_D f3 sample(const DevTables& t, f3 wo, float sx, float sy, float sz, f3& wi, float& pdf, int& type) const
+  PRT_D f3 sampleCoated(const DevTables& t, f3 wo, float sx, float sy, float sz, f3& wi, float& pdf, int& type) const
   {
     if ((F & kFeatCoat) && hasCoat) return coat.sample(t, BaseSub{this}, fr, Ng, wo, sx, sy, sz, wi, pdf, type);
     return sampleBase(t, wo, sx, sy, sz, wi, pdf, type);
+  }
+
+  struct CoatedSub
+  {
+    const StdBsdfT* b;
+    PRT_D int flags() const { return b->coatedFlags(); }
+    PRT_D float importance() const
+    {
+      return ((F & kFeatCoat) && b->hasCoat) ? b->coat.importance(b->impSum) : b->impSum;
+    }
+    PRT_D f3 eval(const DevTables& t, f3 wo, f3 wi, float& pdf) const { return b->evalCoated(t, wo, wi, pdf); }
+    PRT_D f3 sample(const DevTables& t, f3 wo, float sx, float sy, float sc, f3& wi, float& pdf, int& type) const
+    {
+      return b->sampleCoated(t, wo, sx, sy, sc, wi, pdf, type);
+    }
+  };
+
+  PRT_D f3 eval(const DevTables& t, f3 wo, f3 wi, float& pdf) const
+  {
+    if ((F & kFeatSheen) && hasSheen) return sheen.eval(t, CoatedSub{this}, fr, Ng, wo, wi, pdf);
+    return evalCoated(t, wo, wi, pdf);
+  }
+
+  PRT_D f3 sample(const DevTables& t, f3 wo, float sx, float sy, float sz, f3& wi, float& pdf, int& type) const
+  {
+    if ((F & kFeatSheen) && hasSheen) return sheen.sample(t, CoatedSub{this}, fr, Ng, wo, sx, sy, sz, wi, pdf, type);
+    return sampleCoated(t, wo, sx, sy, sz, wi, pdf, type);
   }
 
   PRT_D f3 albedo() const { return albedoV; }
@@ -976,6 +1198,7 @@ PRT_D void resolveStandard(const DevScene& sc, const DevTables& t, const DevMate
   b.impSum = 0.f;
   b.baseFlags = 0;
   b.hasCoat = false;
+  b.hasSheen = false;
   b.opaque.hasSpec = false;
   const float base = clamp01(m.baseWeight);
   f3 baseColor = mk(m.baseColor[0], m.baseColor[1], m.baseColor[2]);
@@ -996,6 +1219,8 @@ PRT_D void resolveStandard(const DevScene& sc, const DevTables& t, const DevMate
     if ((F & kFeatOpaque) && opaque > kMatEps)
     {
       b.opaque.diff.color = baseColor * base;
+      b.opaque.diff.rough = m.hasDiffuseRoughness != 0;
+      b.opaque.diff.roughness = clamp01(m.diffuseRoughness);
       f3 a = b.opaque.diff.color;
       int fl = kDiffuseReflection;
       if ((F & kFeatSpecular) && fabsf(m.specularIor - m.ambientIor) > kMatEps && specular > kMatEps)
@@ -1034,6 +1259,14 @@ PRT_D void resolveStandard(const DevScene& sc, const DevTables& t, const DevMate
     b.coat.init(t, coatEta, coatColor, 0.5f, clamp01(m.coatRoughness), m.hasCoatRoughness != 0, coat);
     b.hasCoat = true;
     albedo = b.coat.albedo(albedo);
+  }
+  const float sheen = clamp01(m.sheenWeight);
+  if ((F & kFeatSheen) && sheen > kMatEps)
+  {
+    const f3 sheenColor = clamp01(mk(m.sheenColor[0], m.sheenColor[1], m.sheenColor[2]));
+    const float tint = clamp01(m.sheenTint);
+    b.sheen.init(sheenColor + tint * (baseColor - sheenColor), clamp01(m.sheenRoughness), sheen);
+    b.hasSheen = true;
   }
   b.albedoV = albedo;
 }

@@ -180,6 +180,7 @@ DevMaterial resolveMaterial(const prt_material& m, std::vector<float>& media, in
   d.sheenWeight = m.sheen_weight;
   for (int k = 0; k < 3; ++k) d.sheenColor[k] = m.sheen_color[k];
   d.sheenRoughness = m.sheen_roughness;
+  d.sheenTint = 0.f;
   for (int k = 0; k < 3; ++k) d.emission[k] = m.emission_color[k] * m.emission_luminance;
   d.thinWalled = m.thin_walled;
   d.opacity = m.opacity;
@@ -213,8 +214,8 @@ DevMaterial resolveMaterial(const prt_material& m, std::vector<float>& media, in
     }
   }
   // Lobes the device implements: see resolveStandard (bsdf.cuh).
-  const bool unsupported = d.subsurfaceWeight != 0.f || d.sheenWeight != 0.f || d.opacity != 1.f ||
-                           d.hasDiffuseRoughness || (d.thinWalled && d.transmissionWeight != 0.f) ||
+  const bool unsupported = d.subsurfaceWeight != 0.f || d.opacity != 1.f ||
+                           (d.thinWalled && d.transmissionWeight != 0.f) ||
                            (d.transmissionWeight != 0.f && std::fabs(d.specularIor - d.ambientIor) <= 1e-4f);
   if (unsupported && !(d.type & kMatEmissive))
     throw std::invalid_argument("material uses lobes not yet supported by the CUDA device");
@@ -228,11 +229,13 @@ DevMaterial resolveMaterial(const prt_material& m, std::vector<float>& media, in
   if (diel > eps && diel * (1.f - trans) > eps)
   {
     d.features |= kFeatOpaque;
+    if (d.hasDiffuseRoughness) d.features |= kFeatRoughDiffuse;
     if (std::fabs(d.specularIor - d.ambientIor) > eps && spec > eps) d.features |= kFeatSpecular;
   }
   if (diel > eps && diel * trans * spec > eps) d.features |= kFeatDielectric;
   if (metal * spec > eps) d.features |= kFeatConductor;
   if (c01(d.coatWeight) > eps && std::fabs(d.coatIor - d.ambientIor) > eps) d.features |= kFeatCoat;
+  if (c01(d.sheenWeight) > eps) d.features |= kFeatSheen;
   d.shadeClass = kShadeClasses - 1;
   for (int k = 1; k < kShadeClasses; ++k)
     if (kShadeClassFeatures[k] == d.features)
@@ -985,12 +988,17 @@ int prt_cuda_albedo_tables(prt_context* ctx, float* out, int64_t capacity, int64
 {
   return guarded(ctx, [&](Context& c) {
     if (!count || capacity < 0 || (capacity > 0 && !out)) throw std::invalid_argument("invalid table query");
-    const int64_t total = 32 * 32 + 32 + 3 * (16 * 16 * 16 + 16 * 16);
+    const int64_t head = 32 * 32 + 32 + 3 * (16 * 16 * 16 + 16 * 16);
+    const int64_t total = head + 16 * 16;
     *count = total;
     if (capacity == 0) return;
-    // The tables were allocated back to back from one buffer in this order (albedo.cu).
-    cuCheck(cudaMemcpy(out, c.tableStorage, sizeof(float) * std::min(capacity, total), cudaMemcpyDeviceToHost),
+    // GGX, dielectric and reflection tables were allocated back to back in this order
+    // (albedo.cu); the sheen table follows them.
+    cuCheck(cudaMemcpy(out, c.tableStorage, sizeof(float) * std::min(capacity, head), cudaMemcpyDeviceToHost),
             "table copy");
+    if (capacity > head)
+      cuCheck(cudaMemcpy(out + head, c.tables.sheenDir, sizeof(float) * std::min<int64_t>(capacity - head, 16 * 16),
+                         cudaMemcpyDeviceToHost), "table copy");
   });
 }
 

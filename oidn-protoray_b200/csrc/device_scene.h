@@ -24,7 +24,9 @@ enum : int
   kFeatDielectric = 1 << 2, // transmissive dielectric base
   kFeatConductor = 1 << 3,  // metal base
   kFeatCoat = 1 << 4,       // outer coat layer
-  kFeatAll = 31,
+  kFeatSheen = 1 << 5,      // outermost sheen layer
+  kFeatRoughDiffuse = 1 << 6, // Oren-Nayar base instead of Lambert
+  kFeatAll = 127,
 };
 
 // Shading classes: 0 ends the path (miss, area-light hit, maxDepth); 1.. shade a surface with
@@ -77,6 +79,7 @@ struct DevMaterial
   float sheenWeight;
   float sheenColor[3];
   float sheenRoughness;
+  float sheenTint;       // sheen colour = lerp(sheenColor, baseColor, sheenTint) (Principled)
   float emission[3];     // emissionColor * emissionLuminance
   int thinWalled;
   float opacity;

@@ -141,6 +141,7 @@ int64_t ref_albedo_tables(float* out)
   put(MicrofacetDielectricAlbedoTable::rcpEtaAvg, 16 * 16);
   put(MicrofacetDielectricReflectionAlbedoTable::etaDir, 16 * 16 * 16);
   put(MicrofacetDielectricReflectionAlbedoTable::etaAvg, 16 * 16);
+  put(MicrofacetSheenAlbedoTable::dir, 16 * 16);
   return (int64_t)(o - out);
 }
 

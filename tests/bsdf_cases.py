@@ -30,6 +30,15 @@ def cases():
                                            coat_roughness=0.0), 0),
         ("coat_tinted_plastic", T.material(base_color=(0.8, 0.2, 0.2), coat_weight=0.7, coat_roughness=0.35,
                                            coat_color=(0.9, 0.8, 0.6)), 0),
+        ("rough_diffuse", T.material(base_color=(0.6, 0.5, 0.4), specular_weight=0.0, diffuse_roughness=0.7), 0),
+        ("rough_diffuse_plastic", T.material(base_color=(0.2, 0.5, 0.7), diffuse_roughness=0.4,
+                                             specular_roughness=0.25), 0),
+        ("sheen_lambert", T.material(base_color=(0.4, 0.3, 0.6), specular_weight=0.0, sheen_weight=0.8,
+                                     sheen_color=(1.0, 0.9, 0.8), sheen_roughness=0.4), 0),
+        ("sheen_coat_plastic", T.material(base_color=(0.7, 0.6, 0.2), specular_roughness=0.3, coat_weight=0.6,
+                                          coat_roughness=0.2, sheen_weight=0.5, sheen_roughness=0.2), 0),
+        ("sheen_gold", T.material(metalness=1.0, base_color=GOLD_R, specular_color=GOLD_G, specular_roughness=0.3,
+                                  sheen_weight=1.0, sheen_roughness=0.6), 0),
     ]
 
 

