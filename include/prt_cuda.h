@@ -85,8 +85,24 @@ typedef struct prt_material
   float opacity;
   int32_t thin_walled;
   int32_t base_color_texture;
+  int32_t model;          /* PRT_MATERIAL_STANDARD or PRT_MATERIAL_PRINCIPLED */
+  float   ambient_ior;    /* Standard "ambientIOR" / Principled "outsideIor" (default 1) */
+  float   coat_thickness; /* Principled "coatThickness" (Standard uses its fixed 0.5) */
+  float   sheen_tint;     /* Principled "sheenTint" */
+  float   backlight;      /* Principled "backlight" (thin only) */
+  float   thickness;      /* "thickness" of thin-walled transmission */
   int32_t reserved[2];
 } prt_material;
+
+/* Material models. PRT_MATERIAL_PRINCIPLED is the reference's deprecated PrincipledMaterial
+ * (material/principled.cpp:21-575), read from the same record: base_color = "baseColor",
+ * specular_color = "edgeColor", metalness = "metallic", base_weight = "diffuse",
+ * specular_weight = "specular", specular_ior = "ior", specular_roughness = "roughness" (which
+ * also makes the diffuse lobe Oren-Nayar), transmission_* = "transmission*", coat_* = "coat*",
+ * sheen_* = "sheen*", thin_walled = "thin", opacity = "opacity"; it has no emission.
+ * prt_cuda_principled_defaults() fills its defaults. */
+#define PRT_MATERIAL_STANDARD   0
+#define PRT_MATERIAL_PRINCIPLED 1
 
 /* An RGB FP32 image (row 0 at the top, as stored by the reference's ImageIo). */
 typedef struct prt_texture
@@ -191,6 +207,8 @@ const char* prt_cuda_last_error(const prt_context* ctx);
 
 /* Fills a material with the reference's Standard defaults. */
 void prt_cuda_material_defaults(prt_material* m);
+/* Defaults of PrincipledMaterial's parameters (material/principled.cpp:21-60), model set. */
+void prt_cuda_principled_defaults(prt_material* m);
 
 /* ---- scene, renderer, camera, frame ----------------------------------------------------- */
 

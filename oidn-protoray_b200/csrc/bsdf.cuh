@@ -1246,7 +1246,8 @@ PRT_D void resolveStandard(const DevScene& sc, const DevTables& t, const DevMate
   if ((F & kFeatConductor) && metal > kMatEps)
   {
     const f3 specColor = clamp01(mk(m.specularColor[0], m.specularColor[1], m.specularColor[2]));
-    b.cond.init(t, baseColor * base, specColor, specularRoughness, m.hasSpecularRoughness != 0);
+    b.cond.init(t, m.principled ? baseColor : baseColor * base, specColor, specularRoughness,
+                m.hasSpecularRoughness != 0);
     addSlot(b, kSlotConductor, metal, 1.f, b.cond.flags());
     albedo += b.cond.albedo() * metal;
   }
@@ -1256,7 +1257,7 @@ PRT_D void resolveStandard(const DevScene& sc, const DevTables& t, const DevMate
     float coatEta = fromOutside ? m.ambientIor * (1.f / m.coatIor) : m.coatIor * (1.f / m.ambientIor);
     coatEta = fminf(fmaxf(coatEta, 1.f / 3.f), 3.f);
     const f3 coatColor = clamp01(mk(m.coatColor[0], m.coatColor[1], m.coatColor[2]));
-    b.coat.init(t, coatEta, coatColor, 0.5f, clamp01(m.coatRoughness), m.hasCoatRoughness != 0, coat);
+    b.coat.init(t, coatEta, coatColor, m.coatThickness, clamp01(m.coatRoughness), m.hasCoatRoughness != 0, coat);
     b.hasCoat = true;
     albedo = b.coat.albedo(albedo);
   }

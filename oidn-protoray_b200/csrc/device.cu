@@ -153,7 +153,10 @@ DevMaterial resolveMaterial(const prt_material& m, std::vector<float>& media, in
     x = std::max(x, 0.f);
     return x < 1.f ? 1.f / x : x;
   };
-  d.ambientIor = 1.f;
+  d.ambientIor = ior(m.ambient_ior > 0.f ? m.ambient_ior : 1.f);
+  d.principled = m.model == PRT_MATERIAL_PRINCIPLED ? 1 : 0;
+  if (m.model != PRT_MATERIAL_STANDARD && m.model != PRT_MATERIAL_PRINCIPLED)
+    throw std::invalid_argument("unknown material model");
   d.baseWeight = m.base_weight;
   for (int k = 0; k < 3; ++k) d.baseColor[k] = m.base_color[k];
   d.baseColorTex = m.base_color_texture;
@@ -180,12 +183,21 @@ DevMaterial resolveMaterial(const prt_material& m, std::vector<float>& media, in
   d.sheenWeight = m.sheen_weight;
   for (int k = 0; k < 3; ++k) d.sheenColor[k] = m.sheen_color[k];
   d.sheenRoughness = m.sheen_roughness;
-  d.sheenTint = 0.f;
+  d.sheenTint = d.principled ? m.sheen_tint : 0.f;
   for (int k = 0; k < 3; ++k) d.emission[k] = m.emission_color[k] * m.emission_luminance;
+  d.coatThickness = d.principled ? std::max(m.coat_thickness, 0.f) : 0.5f;
+  if (d.principled)
+  {
+    // PrincipledMaterial: "roughness" also turns the diffuse lobe into Oren-Nayar, and the
+    // material has no emission.
+    d.diffuseRoughness = d.specularRoughness;
+    d.hasDiffuseRoughness = d.hasSpecularRoughness;
+    for (int k = 0; k < 3; ++k) d.emission[k] = 0.f;
+  }
   d.thinWalled = m.thin_walled;
   d.opacity = m.opacity;
   d.type = 0;
-  if (m.emission_luminance > 0.f) d.type |= kMatEmissive;
+  if (m.emission_luminance > 0.f && m.model == PRT_MATERIAL_STANDARD) d.type |= kMatEmissive;
   d.mediumInt = d.mediumExt = 0;
   if (m.opacity != 1.f) d.type |= kMatTransparent;
   if (m.transmission_weight != 0.f)
@@ -214,7 +226,7 @@ DevMaterial resolveMaterial(const prt_material& m, std::vector<float>& media, in
     }
   }
   // Lobes the device implements: see resolveStandard (bsdf.cuh).
-  const bool unsupported = d.subsurfaceWeight != 0.f || d.opacity != 1.f ||
+  const bool unsupported = d.subsurfaceWeight != 0.f || d.opacity != 1.f || (d.principled && m.thin_walled && m.backlight > 0.f) ||
                            (d.thinWalled && d.transmissionWeight != 0.f) ||
                            (d.transmissionWeight != 0.f && std::fabs(d.specularIor - d.ambientIor) <= 1e-4f);
   if (unsupported && !(d.type & kMatEmissive))
@@ -719,6 +731,23 @@ void prt_cuda_material_defaults(prt_material* m)
   m->emission_color[0] = m->emission_color[1] = m->emission_color[2] = 1.f;
   m->opacity = 1.f;
   m->base_color_texture = -1;
+  m->model = PRT_MATERIAL_STANDARD;
+  m->ambient_ior = 1.f;
+  m->coat_thickness = 1.f;
+  m->thickness = 1.f;
+}
+
+void prt_cuda_principled_defaults(prt_material* m)
+{
+  if (!m) return;
+  prt_cuda_material_defaults(m);
+  m->model = PRT_MATERIAL_PRINCIPLED;
+  m->specular_color[0] = m->specular_color[1] = m->specular_color[2] = 1.f;  // edgeColor
+  m->specular_roughness = 0.f;                                               // roughness
+  m->specular_ior = 1.f;                                                     // ior = outsideIor
+  m->coat_ior = 1.5f;
+  m->sheen_roughness = 0.2f;
+  m->emission_luminance = 0.f;
 }
 
 int prt_cuda_scene_upload(prt_context* ctx, const prt_scene_desc* scene)

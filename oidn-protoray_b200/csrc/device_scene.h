@@ -80,6 +80,8 @@ struct DevMaterial
   float sheenColor[3];
   float sheenRoughness;
   float sheenTint;       // sheen colour = lerp(sheenColor, baseColor, sheenTint) (Principled)
+  float coatThickness;   // 0.5 for Standard, "coatThickness" for Principled
+  int principled;        // PrincipledMaterial: the conductor uses the unweighted base colour
   float emission[3];     // emissionColor * emissionLuminance
   int thinWalled;
   float opacity;

@@ -68,6 +68,12 @@ class Material(C.Structure):
         ("opacity", C.c_float),
         ("thin_walled", C.c_int32),
         ("base_color_texture", C.c_int32),
+        ("model", C.c_int32),
+        ("ambient_ior", C.c_float),
+        ("coat_thickness", C.c_float),
+        ("sheen_tint", C.c_float),
+        ("backlight", C.c_float),
+        ("thickness", C.c_float),
         ("reserved", C.c_int32 * 2),
     ]
 
@@ -101,6 +107,30 @@ def material(**kw):
     m.opacity = 1.0
     m.thin_walled = 0
     m.base_color_texture = -1
+    m.model = PRT_MATERIAL_STANDARD
+    m.ambient_ior = 1.0
+    m.coat_thickness = 1.0
+    m.thickness = 1.0
+    for k, v in kw.items():
+        if isinstance(v, (tuple, list, np.ndarray)):
+            getattr(m, k)[:] = tuple(float(x) for x in v)
+        else:
+            setattr(m, k, v)
+    return m
+
+
+PRT_MATERIAL_STANDARD = 0
+PRT_MATERIAL_PRINCIPLED = 1
+
+
+def principled(**kw):
+    """A Material of the Principled model with PrincipledMaterial's defaults
+    (material/principled.cpp:21-60), overridden by kw (field names of the shared record:
+    base_color = baseColor, specular_color = edgeColor, metalness = metallic, base_weight =
+    diffuse, specular_weight = specular, specular_ior = ior, specular_roughness = roughness, ...)."""
+    m = material(specular_color=(1.0, 1.0, 1.0), specular_roughness=0.0, specular_ior=1.0, coat_ior=1.5,
+                 sheen_roughness=0.2)
+    m.model = PRT_MATERIAL_PRINCIPLED
     for k, v in kw.items():
         if isinstance(v, (tuple, list, np.ndarray)):
             getattr(m, k)[:] = tuple(float(x) for x in v)

@@ -35,6 +35,7 @@ Props standardProps(const prt_material& m)
   Props p;
   auto v3 = [](const float* a) { return Vec3f(a[0], a[1], a[2]); };
   p.set("type", "Standard");
+  p.set("ambientIOR", m.ambient_ior);
   p.set("baseWeight", m.base_weight);
   p.set("baseColor", v3(m.base_color));
   p.set("metalness", m.metalness);
@@ -63,6 +64,39 @@ Props standardProps(const prt_material& m)
   return p;
 }
 
+// The keys PrincipledMaterial reads (material/principled.cpp:21-60), from the same record.
+Props principledProps(const prt_material& m)
+{
+  Props p;
+  auto v3 = [](const float* a) { return Vec3f(a[0], a[1], a[2]); };
+  p.set("type", "Principled");
+  p.set("baseColor", v3(m.base_color));
+  p.set("edgeColor", v3(m.specular_color));
+  p.set("metallic", m.metalness);
+  p.set("diffuse", m.base_weight);
+  p.set("specular", m.specular_weight);
+  p.set("outsideIor", m.ambient_ior);
+  p.set("ior", m.specular_ior);
+  p.set("transmission", m.transmission_weight);
+  p.set("transmissionColor", v3(m.transmission_color));
+  p.set("transmissionDepth", m.transmission_depth);
+  p.set("roughness", m.specular_roughness);
+  p.set("coat", m.coat_weight);
+  p.set("coatIor", m.coat_ior);
+  p.set("coatColor", v3(m.coat_color));
+  p.set("coatThickness", m.coat_thickness);
+  p.set("coatRoughness", m.coat_roughness);
+  p.set("sheen", m.sheen_weight);
+  p.set("sheenColor", v3(m.sheen_color));
+  p.set("sheenTint", m.sheen_tint);
+  p.set("sheenRoughness", m.sheen_roughness);
+  p.set("thin", m.thin_walled);
+  p.set("backlight", m.backlight);
+  p.set("thickness", m.thickness);
+  p.set("opacity", m.opacity);
+  return p;
+}
+
 } // namespace
 
 extern "C" {
@@ -73,7 +107,8 @@ int ref_bsdf_query(const prt_material* mat, int mediumId, int64_t n, const float
   {
     precomputeAlbedoTables();
     MaterialFactory factory("", Props());
-    std::shared_ptr<Material> material = factory.make(standardProps(*mat));
+    std::shared_ptr<Material> material =
+      factory.make(mat->model == PRT_MATERIAL_PRINCIPLED ? principledProps(*mat) : standardProps(*mat));
     for (int64_t base = 0; base < n; base += simdSize)
     {
       const int lanes = (int)std::min<int64_t>(simdSize, n - base);

@@ -39,6 +39,15 @@ def cases():
                                           coat_roughness=0.2, sheen_weight=0.5, sheen_roughness=0.2), 0),
         ("sheen_gold", T.material(metalness=1.0, base_color=GOLD_R, specular_color=GOLD_G, specular_roughness=0.3,
                                   sheen_weight=1.0, sheen_roughness=0.6), 0),
+        ("principled_plastic", T.principled(base_color=(0.6, 0.3, 0.2), specular_ior=1.5, specular_roughness=0.35), 0),
+        ("principled_smooth_plastic", T.principled(base_color=(0.2, 0.4, 0.6), specular_ior=1.45, base_weight=0.8), 0),
+        ("principled_metal", T.principled(base_color=GOLD_R, specular_color=GOLD_G, metalness=1.0,
+                                          specular_roughness=0.3, base_weight=0.5), 0),
+        ("principled_glass", T.principled(transmission_weight=1.0, specular_ior=1.5, specular_roughness=0.2), 0),
+        ("principled_coat_sheen", T.principled(base_color=(0.3, 0.6, 0.4), specular_ior=1.5, specular_roughness=0.4,
+                                               coat_weight=0.8, coat_roughness=0.1, coat_thickness=2.0,
+                                               coat_color=(0.9, 0.7, 0.5), sheen_weight=0.7, sheen_tint=0.5,
+                                               sheen_roughness=0.3), 0),
     ]
 
 
