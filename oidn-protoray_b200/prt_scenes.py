@@ -197,6 +197,29 @@ def cornell(seed=0, width=256, height=256, spp=16, max_depth=5, n_spheres=32, sp
     return s
 
 
+def cornell_lobes(seed=0, width=128, height=128, spp=16, max_depth=5):
+    """The small scene with its spheres cycling through the Oren-Nayar, sheen and layered
+    lobes (rough diffuse, rough-diffuse plastic, sheen over Lambert, sheen over coated plastic)."""
+    s = cornell(seed=seed, width=width, height=height, spp=spp, max_depth=max_depth)
+    rng = np.random.default_rng(seed + 77)
+    first = 4  # the room's white, red, green and light materials come first
+    for k in range(first, len(s.materials)):
+        c = tuple(float(x) for x in s.materials[k].base_color)
+        kind = (k - first) % 4
+        if kind == 0:
+            m = T.material(base_color=c, specular_weight=0.0, diffuse_roughness=float(rng.uniform(0.3, 1.0)))
+        elif kind == 1:
+            m = T.material(base_color=c, diffuse_roughness=0.6, specular_roughness=float(rng.uniform(0.1, 0.5)))
+        elif kind == 2:
+            m = T.material(base_color=c, specular_weight=0.0, sheen_weight=1.0, sheen_color=(1.0, 0.9, 0.8),
+                           sheen_roughness=float(rng.uniform(0.2, 0.6)))
+        else:
+            m = T.material(base_color=c, specular_roughness=0.3, coat_weight=0.5, coat_roughness=0.1,
+                           sheen_weight=0.6, sheen_roughness=0.3)
+        s.materials[k] = m
+    return s
+
+
 def smooth_noise_texture(size, seed, lo=0.1, hi=0.9):
     """(size, size, 3) smooth value noise in [lo, hi], one seeded noise per channel."""
     u = (np.arange(size) + 0.5) / size

@@ -16,6 +16,7 @@ Fixtures (small, seeded, committed):
                    seeds 0 and 1
   terrain_img.npz  small terrain renders (96^2 heightfield, 24 spheres of all four material
                    kinds, sun-sky) at 128x64: 16 spp and 256 spp, seeds 0 and 1
+  lobes_img.npz    the small scene with Oren-Nayar, sheen and layered spheres, 16 spp, seeds 0, 1
   bsdf.npz         the reference's Standard-material BSDF (eval, sample) on 512 seeded tuples
                    for each case of tests/bsdf_cases.py
   sunsky_t3_e30.npz the reference's sun-sky products (sun radiance and angle, 512x256 sky) for
@@ -99,6 +100,19 @@ def make_images():
     np.savez_compressed(OUT / "cornell_img.npz", **out)
 
 
+def make_lobe_images():
+    """The small scene with Oren-Nayar, sheen and layered spheres at 16 spp, seeds 0 and 1."""
+    out = {}
+    for seed in (0, 1):
+        s = prt_scenes.cornell_lobes(seed=0)
+        dev = ref.RefDevice(s, seed=seed)
+        st = dev.render(16)
+        out[f"spp16_seed{seed}"] = dev.blit()
+        out[f"spp16_seed{seed}_rays"] = np.float64(st["rays"])
+        dev.close()
+    np.savez_compressed(OUT / "lobes_img.npz", **out)
+
+
 def make_bsdf():
     sys.path.insert(0, str(ROOT / "tests"))
     import bsdf_cases
@@ -133,11 +147,13 @@ def make_sunsky():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["sobol", "rays", "images", "sunsky", "bsdf", "terrain"]
+    which = sys.argv[1:] or ["sobol", "rays", "images", "sunsky", "bsdf", "terrain", "lobes"]
     if "terrain" in which:
         make_terrain_images()
     if "bsdf" in which:
         make_bsdf()
+    if "lobes" in which:
+        make_lobe_images()
     if "sunsky" in which:
         make_sunsky()
     if "sobol" in which:

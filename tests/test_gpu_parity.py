@@ -133,3 +133,15 @@ def test_terrain_converged_relmse_bound(device, golden):
     assert rel_mse(img0, z["spp256_seed0"]) < 0.05 * seeds
     img1, _ = render(device, small_terrain(256), seed=1, spp=256)
     assert rel_mse(img1, z["spp256_seed0"]) <= 1.5 * seeds
+
+
+def test_lobes_same_seed_tracks_oracle(device, golden):
+    """Oren-Nayar, sheen and sheen-over-coat spheres: the same-seed render follows the
+    reference's far closer than two seeds do, with the same ray count within 1%."""
+    z = golden("lobes_img.npz")
+    img, st = render(device, prt_scenes.cornell_lobes(seed=0), seed=0, spp=16)
+    assert np.isfinite(img).all()
+    same = rel_mse(img, z["spp16_seed0"])
+    other = rel_mse(z["spp16_seed1"], z["spp16_seed0"])
+    assert same < 0.2 * other, (same, other)
+    assert abs(st["rays"] / float(z["spp16_seed0_rays"]) - 1.0) < 0.01
