@@ -308,6 +308,22 @@ int prt_cuda_batch_render(prt_batch* batch, prt_render_stats* stats);
 int prt_cuda_batch_blit(prt_batch* batch, int32_t item, int32_t aov, float* dst);
 int prt_cuda_batch_destroy(prt_batch* batch);
 
+/* ---- batched differentiation -----------------------------------------------------------
+ * No counterpart in the reference. The path-replay adjoint for a whole batch, many inverse-
+ * rendering problems per launch: prt_cuda_batch_enable_adjoint makes every later
+ * prt_cuda_batch_render also store each pixel-sample's radiance (16 bytes per pixel-sample);
+ * prt_cuda_batch_adjoint then replays all paths of all items in one persistent wavefront and
+ * writes, per item k, dLoss/d(texel) into grad_textures[k] and dLoss/d(specular roughness) into
+ * grad_roughness[k] for the image gradient d_loss_d_images[k] (layouts as prt_cuda_adjoint;
+ * device or managed memory). The updates change one item's parameters between steps. */
+int prt_cuda_batch_enable_adjoint(prt_batch* batch);
+int prt_cuda_batch_adjoint(prt_batch* batch, const float* const* d_loss_d_images, float* const* grad_textures,
+                           float* const* grad_roughness, prt_render_stats* stats);
+int prt_cuda_batch_update_texture(prt_batch* batch, int32_t item, int32_t texture, const float* rgb);
+int prt_cuda_batch_update_material(prt_batch* batch, int32_t item, int32_t material, const prt_material* m);
+int prt_cuda_batch_update_materials(prt_batch* batch, int32_t item, int32_t first, int32_t count,
+                                    const prt_material* ms);
+
 /* ---- differentiation -------------------------------------------------------------------
  * No counterpart in the reference. Path-replay adjoint of the image prt_cuda_render produces:
  * given dLoss/dImage (width*height RGB floats, row-major, row 0 at the top; host or device
@@ -332,6 +348,8 @@ int prt_cuda_adjoint(prt_context* ctx, uint32_t first_sample, int32_t spp, const
  * reloads the scene. */
 int prt_cuda_update_texture(prt_context* ctx, int32_t texture, const float* rgb);
 int prt_cuda_update_material(prt_context* ctx, int32_t material, const prt_material* m);
+/* The same for materials [first, first + count) in one call (one copy to the device). */
+int prt_cuda_update_materials(prt_context* ctx, int32_t first, int32_t count, const prt_material* ms);
 
 /* Enables PRT_PROFILE_* instrumentation for subsequent render calls (0 = off). */
 int prt_cuda_set_profiling(prt_context* ctx, int32_t flags);

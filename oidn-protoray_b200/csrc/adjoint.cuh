@@ -24,24 +24,15 @@
 namespace prt {
 
 constexpr int kAdjointFeatures = kFeatOpaque | kFeatSpecular;
-constexpr int kAdjointMaxTextures = 32;
 
-// What the replay wave needs besides the frame-form launch.
-struct AdjointView
-{
-  const float* dLdI;     // width * height * 3, row-major, row 0 at the top
-  float* gradTex;        // concatenated textures, each width * height * 3, row 0 at the top
-  float* gradRough;      // one per material
-  long long texOffset[kAdjointMaxTextures];
-  float step;            // roughness step of the central difference
-  float invSpp;          // 1 / samples per pixel of the differentiated image
-};
-
-// Adds v (3 channels) to dst[3 * key ..] once per group of active lanes with equal keys.
+// Adds v (3 channels) to dst[3 * key ..] once per group of active lanes with the same target
+// address (lanes of one warp may belong to different frames of a batch, so the address, not
+// the key alone, identifies the target).
 PRT_D void groupAdd3(bool has, uint32_t key, f3 v, float* dst)
 {
+  float* d = dst + 3 * (size_t)key;
   const unsigned active = __activemask();
-  const unsigned grp = __match_any_sync(active, has ? key : 0xffffffffu);
+  const unsigned grp = __match_any_sync(active, has ? (unsigned long long)d : 0ull);
   if (!has) return;
   f3 s = mk(0.f);
   for (unsigned m = grp; m; m &= m - 1u)
@@ -53,7 +44,6 @@ PRT_D void groupAdd3(bool has, uint32_t key, f3 v, float* dst)
   }
   if (laneId() == __ffs(grp) - 1)
   {
-    float* d = dst + 3 * (size_t)key;
     if (s.x != 0.f) atomicAdd(d + 0, s.x);
     if (s.y != 0.f) atomicAdd(d + 1, s.y);
     if (s.z != 0.f) atomicAdd(d + 2, s.z);
@@ -62,12 +52,13 @@ PRT_D void groupAdd3(bool has, uint32_t key, f3 v, float* dst)
 
 PRT_D void groupAdd1(bool has, uint32_t key, float v, float* dst)
 {
+  float* d = dst + key;
   const unsigned active = __activemask();
-  const unsigned grp = __match_any_sync(active, has ? key : 0xffffffffu);
+  const unsigned grp = __match_any_sync(active, has ? (unsigned long long)d : 0ull);
   if (!has) return;
   float s = 0.f;
   for (unsigned m = grp; m; m &= m - 1u) s += __shfl_sync(grp, v, __ffs(m) - 1);
-  if (laneId() == __ffs(grp) - 1 && s != 0.f) atomicAdd(dst + key, s);
+  if (laneId() == __ffs(grp) - 1 && s != 0.f) atomicAdd(d, s);
 }
 
 // Bilinear footprint of texLookup (repeat in u and v): the four texels and the fractions.

@@ -1279,6 +1279,8 @@ void freeBatch(BatchState& b)
 {
   if (b.exec) cudaGraphExecDestroy(b.exec);
   b.exec = nullptr;
+  if (b.execReplay) cudaGraphExecDestroy(b.execReplay);
+  b.execReplay = nullptr;
   for (auto& x : b.bufs) cudaFree(x.ptr);
   b.bufs.clear();
 }
@@ -1315,6 +1317,8 @@ int prt_cuda_batch_create(prt_context* ctx, const prt_batch_item* items, int32_t
         uploadScene(tmp, it.scene);
         B.bufs.insert(B.bufs.end(), tmp.sceneBufs.begin(), tmp.sceneBufs.end());
         tmp.sceneBufs.clear();
+        B.itemMaterials.push_back(tmp.materialsHost);
+        B.itemTextures.push_back(tmp.texturesHost);
         BatchItem bi;
         std::memset(&bi, 0, sizeof(bi));
         bi.sc = tmp.scene;
@@ -1436,6 +1440,72 @@ int prt_cuda_batch_destroy(prt_batch* batch)
 
 // ---- differentiation ----------------------------------------------------------------------------
 
+namespace {
+
+// New contents of one texture (caller order, row 0 at the top; host or device memory).
+void updateTexture(Context& c, const std::vector<DevTexture>& textures, int texture, const float* rgb)
+{
+  if (texture < 0 || texture >= (int)textures.size() || !rgb) throw std::invalid_argument("invalid texture update");
+  cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+  const DevTexture& t = textures[texture];
+  Staged src(c, rgb, 3ull * t.width * t.height * sizeof(float), true);
+  cuCheck(launchTextureUpdate(c, t, (const float*)src.dev), "texture update");
+  cuCheck(cudaStreamSynchronize(c.stream), "texture update sync");
+}
+
+// New parameters of materials [first, first + count); each keeps its lobe set, emission and
+// medium. One copy to the device for the whole range.
+void updateMaterials(Context& c, DevMaterial* devMaterials, std::vector<DevMaterial>& host, int textureCount, int first,
+                     int count, const prt_material* ms)
+{
+  if (first < 0 || count < 0 || first + count > (int)host.size() || (count > 0 && !ms))
+    throw std::invalid_argument("invalid material update");
+  if (count == 0) return;
+  std::vector<DevMaterial> ds(count);
+  for (int i = 0; i < count; ++i)
+  {
+    std::vector<float> media = {1.f, 1.f, 1.f, 1.f};
+    DevMaterial d = resolveMaterial(ms[i], media, textureCount);
+    const DevMaterial& old = host[first + i];
+    if (d.type != old.type || d.features != old.features || d.shadeClass != old.shadeClass)
+      throw std::invalid_argument("a material update must keep the material's lobes (re-upload the scene instead)");
+    if ((d.type & kMatMediaInterface) && (d.specularIor != old.specularIor || d.transmissionDepth != old.transmissionDepth ||
+                                          std::memcmp(d.transmissionColor, old.transmissionColor, sizeof(float) * 3) != 0))
+      throw std::invalid_argument("a material update must keep the medium of a transmissive material");
+    if (std::memcmp(d.emission, old.emission, sizeof(float) * 3) != 0)
+      throw std::invalid_argument("a material update must keep the emission (re-upload the scene instead)");
+    d.mediumInt = old.mediumInt;
+    d.mediumExt = old.mediumExt;
+    ds[i] = d;
+  }
+  cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+  cuCheck(cudaMemcpyAsync(devMaterials + first, ds.data(), sizeof(DevMaterial) * count, cudaMemcpyHostToDevice, c.stream),
+          "material update");
+  cuCheck(cudaStreamSynchronize(c.stream), "material update sync");
+  for (int i = 0; i < count; ++i) host[first + i] = ds[i];
+}
+
+void requireAdjointMaterials(const std::vector<DevMaterial>& materials)
+{
+  for (const DevMaterial& m : materials)
+    if (!(m.type & kMatEmissive) && (m.features & ~(kFeatOpaque | kFeatSpecular)))
+      throw std::invalid_argument("the adjoint supports Lambertian materials with an optional specular layer");
+}
+
+bool isDeviceMemory(const void* p)
+{
+  cudaPointerAttributes attr;
+  if (!p || cudaPointerGetAttributes(&attr, p) != cudaSuccess)
+  {
+    cudaGetLastError();
+    return false;
+  }
+  return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+} // namespace
+
+
 extern "C" {
 
 int prt_cuda_adjoint(prt_context* ctx, uint32_t first_sample, int32_t spp, const float* d_loss_d_image,
@@ -1446,9 +1516,7 @@ int prt_cuda_adjoint(prt_context* ctx, uint32_t first_sample, int32_t spp, const
     requireScene(c);
     if (!c.hasRenderer || !c.hasCamera || !c.accum) throw ApiError{PRT_ERR_STATE, "renderer, camera and frame are required"};
     if (spp <= 0 || !d_loss_d_image) throw std::invalid_argument("invalid adjoint request");
-    for (const DevMaterial& m : c.materialsHost)
-      if (!(m.type & kMatEmissive) && (m.features & ~(kFeatOpaque | kFeatSpecular)))
-        throw std::invalid_argument("the adjoint supports Lambertian materials with an optional specular layer");
+    requireAdjointMaterials(c.materialsHost);
     if (c.texturesHost.size() > 32) throw std::invalid_argument("the adjoint supports at most 32 textures");
     int64_t texFloats = 0;
     for (const DevTexture& t : c.texturesHost) texFloats += 3ll * t.width * t.height;
@@ -1493,12 +1561,7 @@ int prt_cuda_update_texture(prt_context* ctx, int32_t texture, const float* rgb)
 {
   return guarded(ctx, [&](Context& c) {
     requireScene(c);
-    if (texture < 0 || texture >= (int)c.texturesHost.size() || !rgb) throw std::invalid_argument("invalid texture update");
-    cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
-    const DevTexture& t = c.texturesHost[texture];
-    Staged src(c, rgb, 3ull * t.width * t.height * sizeof(float), true);
-    cuCheck(launchTextureUpdate(c, t, (const float*)src.dev), "texture update");
-    cuCheck(cudaStreamSynchronize(c.stream), "texture update sync");
+    updateTexture(c, c.texturesHost, texture, rgb);
   });
 }
 
@@ -1506,24 +1569,140 @@ int prt_cuda_update_material(prt_context* ctx, int32_t material, const prt_mater
 {
   return guarded(ctx, [&](Context& c) {
     requireScene(c);
-    if (material < 0 || material >= (int)c.materialsHost.size() || !m) throw std::invalid_argument("invalid material update");
-    std::vector<float> media = {1.f, 1.f, 1.f, 1.f};
-    DevMaterial d = resolveMaterial(*m, media, (int)c.texturesHost.size());
-    const DevMaterial& old = c.materialsHost[material];
-    if (d.type != old.type || d.features != old.features || d.shadeClass != old.shadeClass)
-      throw std::invalid_argument("a material update must keep the material's lobes (re-upload the scene instead)");
-    if ((d.type & kMatMediaInterface) && (d.specularIor != old.specularIor || d.transmissionDepth != old.transmissionDepth ||
-                                          std::memcmp(d.transmissionColor, old.transmissionColor, sizeof(float) * 3) != 0))
-      throw std::invalid_argument("a material update must keep the medium of a transmissive material");
-    if (std::memcmp(d.emission, old.emission, sizeof(float) * 3) != 0)
-      throw std::invalid_argument("a material update must keep the emission (re-upload the scene instead)");
-    d.mediumInt = old.mediumInt;
-    d.mediumExt = old.mediumExt;
+    updateMaterials(c, const_cast<DevMaterial*>(c.scene.materials), c.materialsHost, (int)c.texturesHost.size(),
+                    material, 1, m);
+  });
+}
+
+int prt_cuda_update_materials(prt_context* ctx, int32_t first, int32_t count, const prt_material* ms)
+{
+  return guarded(ctx, [&](Context& c) {
+    requireScene(c);
+    updateMaterials(c, const_cast<DevMaterial*>(c.scene.materials), c.materialsHost, (int)c.texturesHost.size(),
+                    first, count, ms);
+  });
+}
+
+} // extern "C"
+
+// ---- batched differentiation --------------------------------------------------------------------
+
+extern "C" {
+
+int prt_cuda_batch_enable_adjoint(prt_batch* batch)
+{
+  if (!batch) return PRT_ERR_INVALID_ARG;
+  return guarded(batch->ctx, [&](Context& c) {
+    BatchState& B = batch->b;
+    for (const auto& mats : B.itemMaterials) requireAdjointMaterials(mats);
+    for (const auto& texs : B.itemTextures)
+      if (texs.size() > (size_t)kAdjointMaxTextures) throw std::invalid_argument("the adjoint supports at most 32 textures");
+    if (B.pathL) return;
     cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
-    cuCheck(cudaMemcpyAsync(const_cast<DevMaterial*>(c.scene.materials) + material, &d, sizeof(d), cudaMemcpyHostToDevice,
-                            c.stream), "material update");
-    cuCheck(cudaStreamSynchronize(c.stream), "material update sync");
-    c.materialsHost[material] = d;
+    cuCheck(cudaStreamSynchronize(c.stream), "sync");
+    B.pathL = (float4*)devAlloc(c, (size_t)B.workTotal * sizeof(float4), &B.bufs);
+    // The replay keeps each path's radiance still to come in ps.out, which the forward batch
+    // does not use (it accumulates finished paths directly).
+    B.ps.out = (float4*)devAlloc(c, (size_t)B.ps.capacity * sizeof(float4), &B.bufs);
+    // Graphs capture the launch parameters: capture both again with the new buffers.
+    if (B.exec) cudaGraphExecDestroy(B.exec);
+    B.exec = nullptr;
+    if (B.execReplay) cudaGraphExecDestroy(B.execReplay);
+    B.execReplay = nullptr;
+  });
+}
+
+int prt_cuda_batch_adjoint(prt_batch* batch, const float* const* d_loss_d_images, float* const* grad_textures,
+                           float* const* grad_roughness, prt_render_stats* stats)
+{
+  if (!batch) return PRT_ERR_INVALID_ARG;
+  return guarded(batch->ctx, [&](Context& c) {
+    BatchState& B = batch->b;
+    if (!B.pathL) throw ApiError{PRT_ERR_STATE, "call prt_cuda_batch_enable_adjoint and render the batch first"};
+    if (!d_loss_d_images || !grad_textures || !grad_roughness) throw std::invalid_argument("null gradient arrays");
+    cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+    std::vector<BatchItem> items = B.items;
+    for (size_t k = 0; k < items.size(); ++k)
+    {
+      const float* dl = d_loss_d_images[k];
+      float* gt = grad_textures[k];
+      float* gr = grad_roughness[k];
+      int64_t texFloats = 0;
+      for (const DevTexture& t : B.itemTextures[k]) texFloats += 3ll * t.width * t.height;
+      const int64_t mats = (int64_t)B.itemMaterials[k].size();
+      if (!isDeviceMemory(dl) || !isDeviceMemory(gr) || (texFloats > 0 && !isDeviceMemory(gt)))
+        throw std::invalid_argument("batch adjoint buffers must be device or managed memory");
+      AdjointView& A = items[k].adj;
+      std::memset(&A, 0, sizeof(A));
+      A.dLdI = dl;
+      A.gradTex = gt;
+      A.gradRough = gr;
+      long long off = 0;
+      for (size_t i = 0; i < B.itemTextures[k].size(); ++i)
+      {
+        A.texOffset[i] = off;
+        off += 3ll * B.itemTextures[k][i].width * B.itemTextures[k][i].height;
+      }
+      A.step = 1e-3f;
+      A.invSpp = (float)((double)items[k].pixelCount / (double)items[k].workCount);
+      if (texFloats > 0) cuCheck(cudaMemsetAsync(gt, 0, (size_t)texFloats * sizeof(float), c.stream), "clear");
+      cuCheck(cudaMemsetAsync(gr, 0, (size_t)mats * sizeof(float), c.stream), "clear");
+    }
+    cuCheck(cudaMemcpyAsync(B.dItems, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice, c.stream),
+            "batch items");
+    RenderCounters rc;
+    cuCheck(cudaEventRecord(c.ev0, c.stream), "event");
+    const cudaError_t e = replayBatch(c, B, rc);
+    if (e == cudaErrorLaunchTimeout)
+      throw ApiError{PRT_ERR_DEVICE_ABORT, "batch replay did not finish within its iteration bound"};
+    cuCheck(e, "batch adjoint");
+    cuCheck(cudaEventRecord(c.ev1, c.stream), "event");
+    cuCheck(cudaEventSynchronize(c.ev1), "batch adjoint sync");
+    checkDeviceErrors(c);
+    float ms = 0.f;
+    cuCheck(cudaEventElapsedTime(&ms, c.ev0, c.ev1), "event time");
+    if (stats)
+    {
+      std::memset(stats, 0, sizeof(*stats));
+      stats->render_ms = ms;
+      stats->closest_rays = rc.closestRays;
+      stats->rays = rc.closestRays;
+      stats->kernel_launches = rc.launches;
+      stats->trace_launches = rc.traceLaunches;
+    }
+  });
+}
+
+int prt_cuda_batch_update_texture(prt_batch* batch, int32_t item, int32_t texture, const float* rgb)
+{
+  if (!batch) return PRT_ERR_INVALID_ARG;
+  return guarded(batch->ctx, [&](Context& c) {
+    BatchState& B = batch->b;
+    if (item < 0 || item >= (int)B.items.size()) throw std::invalid_argument("invalid batch item");
+    updateTexture(c, B.itemTextures[item], texture, rgb);
+  });
+}
+
+int prt_cuda_batch_update_material(prt_batch* batch, int32_t item, int32_t material, const prt_material* m)
+{
+  if (!batch) return PRT_ERR_INVALID_ARG;
+  return guarded(batch->ctx, [&](Context& c) {
+    BatchState& B = batch->b;
+    if (item < 0 || item >= (int)B.items.size()) throw std::invalid_argument("invalid batch item");
+    updateMaterials(c, const_cast<DevMaterial*>(B.items[item].sc.materials), B.itemMaterials[item],
+                    (int)B.itemTextures[item].size(), material, 1, m);
+  });
+}
+
+int prt_cuda_batch_update_materials(prt_batch* batch, int32_t item, int32_t first, int32_t count,
+                                    const prt_material* ms)
+{
+  if (!batch) return PRT_ERR_INVALID_ARG;
+  return guarded(batch->ctx, [&](Context& c) {
+    BatchState& B = batch->b;
+    if (item < 0 || item >= (int)B.items.size()) throw std::invalid_argument("invalid batch item");
+    updateMaterials(c, const_cast<DevMaterial*>(B.items[item].sc.materials), B.itemMaterials[item],
+                    (int)B.itemTextures[item].size(), first, count, ms);
   });
 }
 

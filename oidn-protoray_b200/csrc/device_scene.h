@@ -196,4 +196,16 @@ struct DevRenderer
   uint32_t seed;
 };
 
+// What the adjoint's replay needs per frame besides the frame itself (csrc/adjoint.cuh).
+constexpr int kAdjointMaxTextures = 32;
+struct AdjointView
+{
+  const float* dLdI;     // width * height * 3, row-major, row 0 at the top
+  float* gradTex;        // concatenated textures, each width * height * 3, row 0 at the top
+  float* gradRough;      // one per material
+  long long texOffset[kAdjointMaxTextures];
+  float step;            // roughness step of the central difference
+  float invSpp;          // 1 / samples per pixel of the differentiated image
+};
+
 } // namespace prt

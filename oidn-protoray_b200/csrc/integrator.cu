@@ -37,8 +37,10 @@ struct Launch
   int itemCount;
   BatchCtl* ctl;
   int* freeList[2];
-  // Replay form of the adjoint only.
+  // Replay form of the adjoint only (frame form; the batch form keeps one per item).
   AdjointView adj;
+  // Batch form: radiance of every work item (pixel-sample) when the batch is differentiable.
+  float4* pathL;
 };
 
 template <int... Fs>
@@ -175,8 +177,9 @@ struct PathEnv<false>
 {
   const DevScene& sc;
   const DevRenderer& rd;
-  int aovMask;
-  PRT_D PathEnv(const Launch& L, uint32_t) : sc(L.sc), rd(L.rd), aovMask(L.aovMask) {}
+  const AdjointView& adj;
+  int aovMask, width;
+  PRT_D PathEnv(const Launch& L, uint32_t) : sc(L.sc), rd(L.rd), adj(L.adj), aovMask(L.aovMask), width(L.width) {}
 };
 
 template <>
@@ -185,8 +188,12 @@ struct PathEnv<true>
   const BatchItem& it;
   const DevScene& sc;
   const DevRenderer& rd;
-  int aovMask;
-  PRT_D PathEnv(const Launch& L, uint32_t item) : it(L.items[item]), sc(it.sc), rd(it.rd), aovMask(it.aovMask) {}
+  const AdjointView& adj;
+  int aovMask, width;
+  PRT_D PathEnv(const Launch& L, uint32_t item)
+      : it(L.items[item]), sc(it.sc), rd(it.rd), adj(it.adj), aovMask(it.aovMask), width(it.width)
+  {
+  }
 };
 
 constexpr uint32_t kDepthShift = 16;
@@ -256,6 +263,7 @@ __global__ void kBatchStep(BatchCtl* ctl, int a)
 
 // Batch form: fills the slots on free list `a` with new camera paths (path regeneration) and
 // appends them to queue[a] after the paths extended by the previous iteration.
+template <bool Adj>
 __global__ void kBatchRegen(Launch L, int a, int* __restrict__ queue)
 {
   const BatchCtl* ctl = L.ctl;
@@ -279,7 +287,8 @@ __global__ void kBatchRegen(Launch L, int a, int* __restrict__ queue)
     const int s = (int)(local / it.pixelCount);
     const int idx = (int)(local - (long long)s * it.pixelCount);
     const int slot = freeList[i];
-    initPath(L.ps, slot, it.cam, it.rd, it.width, it.height, idx, (uint32_t)s, (uint32_t)lo, it.aovMask != 0);
+    initPath(L.ps, slot, it.cam, it.rd, it.width, it.height, idx, (uint32_t)s, (uint32_t)lo, it.aovMask != 0 && !Adj);
+    if (Adj) L.ps.out[slot] = L.pathL[w];  // replay: the radiance still to come is the whole path's
     queue[offset + i] = slot;
   }
 }
@@ -375,8 +384,11 @@ PRT_D void finishPath(const Launch& L, int p, f3 rad, const uint4& info)
   const BatchItem& it = L.items[info.w];
   const f3 c = clampL(rad, it.rd.maxRadiance);
   const uint32_t pid = info.x;
-  const int q = (int)((pid >> 16) & 0x0fffu) * it.width + (int)(pid & 0x0fffu);
+  const int px = (int)(pid & 0x0fffu), py = (int)((pid >> 16) & 0x0fffu);
+  const int q = py * it.width + px;
   atomicAdd(it.accum + q, make_float4(c.x, c.y, c.z, 1.f));
+  if (L.pathL)
+    L.pathL[it.workBase + (long long)info.y * it.pixelCount + slotOfPixel(px, py, it.width)] = make_float4(c.x, c.y, c.z, 0.f);
   if (it.aovMask)
   {
     const float4 va = L.ps.aovA[p], vn = L.ps.aovN[p];
@@ -450,7 +462,7 @@ __global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__
 // Paths that end at this bounce without shading a surface (render/path_renderer_stream.h:287-582
 // and the depth cut-off at :612): misses (environment lights), area-light hits, and surface
 // hits at maxDepth.
-template <bool Batch>
+template <bool Batch, bool Adj = false>
 __global__ void __launch_bounds__(256) kShadeEnd(Launch L, const int* __restrict__ queue, const int* __restrict__ count,
                                                  int depth, int parity)
 {
@@ -460,7 +472,7 @@ __global__ void __launch_bounds__(256) kShadeEnd(Launch L, const int* __restrict
     const int i = base + threadIdx.x;
     const bool active = i < n;
     const int p = active ? __ldg(queue + i) : 0;
-    if (active)
+    if (active && !Adj)
     {
       const float4 rd = L.ps.rayD[p], hh = L.ps.hit[p];
       const float4 tp = L.ps.thr[p];
@@ -645,9 +657,9 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
         const float4 o = L.ps.out[p];
         const f3 rest = mk(o.x, o.y, o.z) - neeL;
         const uint32_t px = pixelId & kPixelIdMask;
-        const float* g = L.adj.dLdI + 3 * ((size_t)(px >> 16) * L.width + (px & 0xffffu));
-        const f3 delta = mk(g[0], g[1], g[2]) * L.adj.invSpp;
-        adjointVertex<F>(L.adj, E.sc, L.tab, mat, ctx, bsdf, wo, wi, neeWi, extend, neeVisible, neeL,
+        const float* g = E.adj.dLdI + 3 * ((size_t)(px >> 16) * E.width + (px & 0xffffu));
+        const f3 delta = mk(g[0], g[1], g[2]) * E.adj.invSpp;
+        adjointVertex<F>(E.adj, E.sc, L.tab, mat, ctx, bsdf, wo, wi, neeWi, extend, neeVisible, neeL,
                          extend ? rest : mk(0.f), delta);
         if (extend) L.ps.out[p] = make_float4(rest.x, rest.y, rest.z, o.w);
       }
@@ -666,9 +678,9 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
       }
       info.x = pixelId;
       L.ps.info[p] = info;
-      if (!Adj && !extend && !shadow)
+      if (!extend && (Adj || !shadow))
       {
-        finishPath<Batch>(L, p, Lr, info);
+        if (!Adj) finishPath<Batch>(L, p, Lr, info);
         freed = true;
       }
       if (shadow) shL.w = __uint_as_float((uint32_t)p | (extend ? 0u : kShadowFinish));
@@ -1073,16 +1085,30 @@ int* batchCounts(BatchCtl* ctl, int parity)
 // One bounce iteration of the batch: control step, regeneration, closest hit, shading by
 // class, shadow rays. Every count is read on the device, so the sequence can be captured once
 // and replayed.
-int batchIteration(const Context& ctx, const Launch& L, int a, int persistent, int shadeGrid, int regenGrid)
+int batchIteration(const Context& ctx, const Launch& L, int a, int persistent, int shadeGrid, int regenGrid, bool replay)
 {
   const int b = a ^ 1;
   int* ca = batchCounts(L.ctl, a);
   int* cb = batchCounts(L.ctl, b);
   cudaStream_t st = ctx.stream;
   kBatchStep<<<1, 1, 0, st>>>(L.ctl, a);
-  kBatchRegen<<<regenGrid, 256, 0, st>>>(L, a, L.ps.queue[a]);
+  if (replay)
+    kBatchRegen<true><<<regenGrid, 256, 0, st>>>(L, a, L.ps.queue[a]);
+  else
+    kBatchRegen<false><<<regenGrid, 256, 0, st>>>(L, a, L.ps.queue[a]);
   kTrace<false, true><<<persistent, 256, 0, st>>>(L, L.ps.queue[a], ca, ca + kBatchCntShadow + 1, 0,
                                                   L.ps.classQueues, ca + 1);
+  if (replay)
+  {
+    // Adjoint replay: class-0 paths only return their slots; classes 1 and 2 (the adjoint's
+    // material set) shade with inline shadow rays and scatter gradients.
+    kShadeEnd<true, true><<<shadeGrid, 256, 0, st>>>(L, L.ps.classQueues, ca + 1, 0, a);
+    kShadeSurface<kShadeClassFeatures[1], true, true><<<shadeGrid, 256, 0, st>>>(
+      L, L.ps.classQueues + (int64_t)1 * L.ps.capacity, ca + 2, 0, L.ps.queue[b], cb, ca + kBatchCntShadow, a);
+    kShadeSurface<kShadeClassFeatures[2], true, true><<<shadeGrid, 256, 0, st>>>(
+      L, L.ps.classQueues + (int64_t)2 * L.ps.capacity, ca + 3, 0, L.ps.queue[b], cb, ca + kBatchCntShadow, a);
+    return 6;
+  }
   kShadeEnd<true><<<shadeGrid, 256, 0, st>>>(L, L.ps.classQueues, ca + 1, 0, a);
   ShadeClassList::run<true>(1, L, st, shadeGrid, L.ps.classQueues, ca, 0, L.ps.queue[b], cb, ca + kBatchCntShadow, a);
   kShadow<false, true><<<persistent, 256, 0, st>>>(L, ca + kBatchCntShadow, ca + kBatchCntShadow + 2, a);
@@ -1091,13 +1117,14 @@ int batchIteration(const Context& ctx, const Launch& L, int a, int persistent, i
 
 } // namespace
 
-cudaError_t renderBatch(Context& ctx, BatchState& B, RenderCounters& rc)
+static cudaError_t runBatch(Context& ctx, BatchState& B, RenderCounters& rc, bool replay)
 {
   rc = RenderCounters();
   cudaError_t e = cudaSuccess;
   const int64_t C = B.ps.capacity;
   for (const BatchItem& it : B.items)
   {
+    if (replay) break;  // the replay only scatters gradients
     const size_t bytes = (size_t)it.pixelCount * sizeof(float4);
     e = cudaMemsetAsync(it.accum, 0, bytes, ctx.stream);
     if (e == cudaSuccess && it.accA) e = cudaMemsetAsync(it.accA, 0, bytes, ctx.stream);
@@ -1115,7 +1142,9 @@ cudaError_t renderBatch(Context& ctx, BatchState& B, RenderCounters& rc)
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
 
-  if (!B.exec)
+  cudaGraphExec_t& exec = replay ? B.execReplay : B.exec;
+  int& graphKernels = replay ? B.graphKernelsReplay : B.graphKernels;
+  if (!exec)
   {
     Launch L;
     std::memset(&L, 0, sizeof(L));
@@ -1126,6 +1155,7 @@ cudaError_t renderBatch(Context& ctx, BatchState& B, RenderCounters& rc)
     L.ctl = B.ctl;
     L.freeList[0] = B.freeList[0];
     L.freeList[1] = B.freeList[1];
+    L.pathL = B.pathL;
     const int persistent = ctx.smCount * ctx.traceBlocks;
     const int shadeGrid = ctx.smCount * ctx.shadeBlocks;
     const int regenGrid = gridFor(ctx, C);
@@ -1133,14 +1163,15 @@ cudaError_t renderBatch(Context& ctx, BatchState& B, RenderCounters& rc)
     e = cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
     int kernels = 0;
-    for (int k = 0; k < kGraphIterations; ++k) kernels += batchIteration(ctx, L, k & 1, persistent, shadeGrid, regenGrid);
+    for (int k = 0; k < kGraphIterations; ++k)
+      kernels += batchIteration(ctx, L, k & 1, persistent, shadeGrid, regenGrid, replay);
     cudaError_t launchErr = cudaGetLastError();
     e = cudaStreamEndCapture(ctx.stream, &graph);
     if (e == cudaSuccess) e = launchErr;
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&B.exec, graph, 0);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
     if (graph) cudaGraphDestroy(graph);
     if (e != cudaSuccess) return e;
-    B.graphKernels = kernels;
+    graphKernels = kernels;
   }
 
   // Each slot finishes a path at least every maxDepth + 1 iterations while work remains.
@@ -1158,14 +1189,14 @@ cudaError_t renderBatch(Context& ctx, BatchState& B, RenderCounters& rc)
       cudaFreeHost(done);
       return cudaErrorLaunchTimeout;
     }
-    e = cudaGraphLaunch(B.exec, ctx.stream);
+    e = cudaGraphLaunch(exec, ctx.stream);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(done, reinterpret_cast<char*>(B.ctl) + offsetof(BatchCtl, done), sizeof(int),
                           cudaMemcpyDeviceToHost, ctx.stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx.stream);
     if (e != cudaSuccess) break;
     iterations += kGraphIterations;
-    rc.launches += B.graphKernels;
+    rc.launches += graphKernels;
   }
   cudaFreeHost(done);
   if (e != cudaSuccess) return e;
@@ -1176,5 +1207,9 @@ cudaError_t renderBatch(Context& ctx, BatchState& B, RenderCounters& rc)
   rc.traceLaunches = iterations;
   return cudaSuccess;
 }
+
+cudaError_t renderBatch(Context& ctx, BatchState& B, RenderCounters& rc) { return runBatch(ctx, B, rc, false); }
+
+cudaError_t replayBatch(Context& ctx, BatchState& B, RenderCounters& rc) { return runBatch(ctx, B, rc, true); }
 
 } // namespace prt

@@ -56,6 +56,7 @@ struct BatchItem
   float4* accum;        // sum rgb + weight per pixel
   float4* accA;         // first-hit albedo sums (aovMask != 0)
   float4* accN;         // first-hit normal sums
+  AdjointView adj;      // gradient targets of the batch adjoint (prt_cuda_batch_adjoint)
 };
 
 // Counter block of one batch iteration (ints): [0] paths to trace, [1..kShadeClasses] paths
@@ -91,6 +92,12 @@ struct BatchState
   int* freeList[2] = {nullptr, nullptr};
   cudaGraphExec_t exec = nullptr;  // kGraphIterations bounce iterations
   int graphKernels = 0;
+  // Differentiable batches: radiance per work item (float4) and the replay graph.
+  float4* pathL = nullptr;
+  cudaGraphExec_t execReplay = nullptr;
+  int graphKernelsReplay = 0;
+  std::vector<std::vector<DevMaterial>> itemMaterials;  // host copies per item
+  std::vector<std::vector<DevTexture>> itemTextures;
 };
 
 struct Context
@@ -149,6 +156,9 @@ cudaError_t launchBlit(Context& ctx, int aov, float* dst);
 // Renders every item of a batch to completion (path regeneration over one shared path pool,
 // bounce loop replayed as a CUDA graph) into the items' accumulation planes.
 cudaError_t renderBatch(Context& ctx, BatchState& b, RenderCounters& rc);
+// Path-replay adjoint of the last renderBatch of a differentiable batch: scatters each item's
+// gradients into the targets of its BatchItem::adj (set on the device before the call).
+cudaError_t replayBatch(Context& ctx, BatchState& b, RenderCounters& rc);
 cudaError_t launchBlitPlane(Context& ctx, const float4* plane, int n, float* dst);
 // Path-replay adjoint (adjoint.cu): dLoss/d(texel) of every scene texture and dLoss/d(specular
 // roughness) of every material for the image gradient dLdI (W*H*3, device memory).

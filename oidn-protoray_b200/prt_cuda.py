@@ -10,6 +10,7 @@ loading fails loudly when the library or a CUDA device is missing.
 """
 import ctypes as C
 import os
+import weakref
 import pathlib
 
 import numpy as np
@@ -62,6 +63,12 @@ def load_library():
     lib.prt_cuda_batch_render.argtypes = [vp, P(T.RenderStats)]
     lib.prt_cuda_batch_blit.argtypes = [vp, C.c_int32, C.c_int32, P(C.c_float)]
     lib.prt_cuda_batch_destroy.argtypes = [vp]
+    lib.prt_cuda_batch_enable_adjoint.argtypes = [vp]
+    lib.prt_cuda_batch_adjoint.argtypes = [vp, P(vp), P(vp), P(vp), P(T.RenderStats)]
+    lib.prt_cuda_batch_update_texture.argtypes = [vp, C.c_int32, C.c_int32, vp]
+    lib.prt_cuda_batch_update_material.argtypes = [vp, C.c_int32, C.c_int32, P(T.Material)]
+    lib.prt_cuda_batch_update_materials.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, P(T.Material)]
+    lib.prt_cuda_update_materials.argtypes = [vp, C.c_int32, C.c_int32, P(T.Material)]
     lib.prt_cuda_get_tuning.argtypes = [vp, P(T.Tuning)]
     lib.prt_cuda_autotune.argtypes = [vp, C.c_int32, P(T.Tuning), P(C.c_double)]
     lib.prt_cuda_blit.argtypes = [vp, C.c_int32, P(C.c_float)]
@@ -110,6 +117,8 @@ class DeviceCuda:
         self._keep = None
 
     def close(self):
+        for b in list(getattr(self, "_batches", [])):
+            b.close()
         if getattr(self, "h", None):
             self.lib.prt_cuda_destroy(self.h)
             self.h = None
@@ -215,6 +224,10 @@ class DeviceCuda:
     def update_material(self, index, material):
         self._check(self.lib.prt_cuda_update_material(self.h, index, C.byref(material)))
 
+    def update_materials(self, first, materials):
+        arr = (T.Material * len(materials))(*materials)
+        self._check(self.lib.prt_cuda_update_materials(self.h, first, len(materials), arr))
+
     def set_profiling(self, flags):
         self._check(self.lib.prt_cuda_set_profiling(self.h, flags))
 
@@ -310,6 +323,9 @@ class Batch:
         h = C.c_void_p()
         device._check(device.lib.prt_cuda_batch_create(device.h, items, len(descs), C.byref(h)))
         self.h = h
+        if not hasattr(device, "_batches"):
+            device._batches = weakref.WeakSet()
+        device._batches.add(self)
         self.samples = sum(sc.width * sc.height * sc.spp for sc, _, _ in self.frames)
 
     def render(self):
@@ -323,10 +339,41 @@ class Batch:
         self.dev._check(self.dev.lib.prt_cuda_batch_blit(self.h, item, aov, T.fptr(img)))
         return img
 
+    # -- differentiation ---------------------------------------------------------------------
+    def enable_adjoint(self):
+        """Later renders also keep each pixel-sample's radiance for adjoint()."""
+        self.dev._check(self.dev.lib.prt_cuda_batch_enable_adjoint(self.h))
+
+    def adjoint(self, d_loss_d_images, grad_textures, grad_roughness):
+        """Path-replay adjoint of the last render for every item at once. Arguments are lists
+        (one entry per item) of CUDA torch tensors: dLoss/dImage (h, w, 3), the concatenated
+        texture gradients, the per-material roughness gradients (written)."""
+        n = len(self.frames)
+        ptr = DeviceCuda._ptr
+        dl = (C.c_void_p * n)(*[ptr(x.contiguous()) for x in d_loss_d_images])
+        gt = (C.c_void_p * n)(*[ptr(x) for x in grad_textures])
+        gr = (C.c_void_p * n)(*[ptr(x) for x in grad_roughness])
+        st = T.RenderStats()
+        self.dev._check(self.dev.lib.prt_cuda_batch_adjoint(self.h, dl, gt, gr, C.byref(st)))
+        return {name: getattr(st, name) for name, _ in T.RenderStats._fields_}
+
+    def update_texture(self, item, texture, rgb):
+        if not hasattr(rgb, "data_ptr"):
+            rgb = np.ascontiguousarray(rgb, np.float32)
+        self.dev._check(self.dev.lib.prt_cuda_batch_update_texture(self.h, item, texture, DeviceCuda._ptr(rgb)))
+
+    def update_material(self, item, material, m):
+        self.dev._check(self.dev.lib.prt_cuda_batch_update_material(self.h, item, material, C.byref(m)))
+
+    def update_materials(self, item, first, materials):
+        arr = (T.Material * len(materials))(*materials)
+        self.dev._check(self.dev.lib.prt_cuda_batch_update_materials(self.h, item, first, len(materials), arr))
+
     def close(self):
-        if getattr(self, "h", None):
+        # A batch lives inside its device's context: destroy it first (DeviceCuda.close does).
+        if getattr(self, "h", None) and getattr(self.dev, "h", None):
             self.dev.lib.prt_cuda_batch_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:

@@ -440,3 +440,46 @@ def batch_frames(count=64, seed=0, tri_range=(1e3, 5e5), sizes=BATCH_SIZES, spps
                     max_depth=depth, rr_depth=3)
         frames.append((s, int(rng.integers(0, 2**31 - 1)), aov_mask))
     return frames
+
+
+def terrain_inverse(seed=0, target=False, tris=2e5, size=512, spp=16, max_depth=6, tex_size=512,
+                    albedo_init=0.5, roughness_init=0.3):
+    """One inverse-rendering problem of the batched differentiable workload: a terrain from the
+    large-scene generator with `tris` triangles (about 80% heightfield, 20% icospheres), its
+    ground textured by a tex_size^2 RGB albedo texture and every sphere a Lambertian base under
+    a specular layer whose roughness is a parameter; sun-sky light. target=False: texture at
+    albedo_init, roughness roughness_init; target=True: texture from seeded smooth noise in
+    [0.1, 0.9], roughness uniform in [0.05, 0.6]. Returns (scene, params)."""
+    n_spheres = int(0.2 * tris / 1280)
+    grid = max(8, int(math.sqrt(max(tris - 1280 * n_spheres, 128) / 2.0)) + 1)
+    s = terrain(seed=seed, grid=grid, n_spheres=n_spheres, width=size, height=size, spp=spp, max_depth=max_depth,
+                rr_depth=3)
+    rng = np.random.default_rng(seed + 4242)
+    tex = smooth_noise_texture(tex_size, seed + 7) if target else np.full((tex_size, tex_size, 3), albedo_init,
+                                                                           np.float32)
+    t = s.add_texture(tex)
+    s.materials[0] = T.material(base_color=(1.0, 1.0, 1.0), base_color_texture=t, specular_weight=0.0)
+    rough_ids = []
+    for k in range(1, len(s.materials)):
+        c = tuple(float(x) for x in rng.uniform(0.1, 0.9, 3))
+        r = float(rng.uniform(0.05, 0.6)) if target else roughness_init
+        s.materials[k] = T.material(base_color=c, specular_weight=1.0, specular_roughness=r, specular_ior=1.5)
+        rough_ids.append(k)
+    return s, {"textures": [t], "roughness": rough_ids}
+
+
+def batch_inverse_frames(count=16, seed=0, tri_range=(1e5, 1e6), size=512, spp=16, max_depth=6, tex_size=512,
+                         target=False):
+    """The batched differentiable workload: `count` inverse problems with triangle counts
+    log-uniform in tri_range. Returns a list of (scene, params, sampler seed)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        tris = float(np.exp(rng.uniform(np.log(tri_range[0]), np.log(tri_range[1]))))
+        scene_seed = int(rng.integers(0, 2**31 - 1))
+        sampler_seed = int(rng.integers(0, 2**31 - 1))
+        s, params = terrain_inverse(seed=scene_seed, target=target, tris=tris, size=size, spp=spp,
+                                    max_depth=max_depth, tex_size=tex_size)
+        out.append((s, params, sampler_seed))
+    return out
+
