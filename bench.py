@@ -345,6 +345,13 @@ def small_scene_bench(dev, repeats=5):
     triangles), 256x256, 16 spp, max depth 5, seed 0. Best of `repeats` device-timed frames."""
     scene = prt_scenes.cornell(seed=0)
     dev.setup(scene, seed=0)
+    dev.set_profiling(T.PRT_PROFILE_COUNTS)
+    c = dev.render(1)
+    dev.set_profiling(0)
+    per_ray = {"closest_nodes": c["closest_nodes"] / max(c["closest_rays"], 1),
+               "closest_tris": c["closest_tris"] / max(c["closest_rays"], 1),
+               "shadow_nodes": c["shadow_nodes"] / max(c["shadow_rays"], 1),
+               "shadow_tris": c["shadow_tris"] / max(c["shadow_rays"], 1)}
     dev.render(scene.spp)
     best = None
     for _ in range(repeats):
@@ -355,7 +362,9 @@ def small_scene_bench(dev, repeats=5):
             best = st
     return {"workload": "room + 32 icospheres, 10,252 tris, 256x256, 16 spp, depth 5", "mrays_per_s": best["mray"],
             "samples_per_s": scene.width * scene.height * scene.spp / (best["render_ms"] * 1e-3),
-            "ms_per_frame": best["render_ms"], "rays": best["rays"]}
+            "ms_per_frame": best["render_ms"], "rays": best["rays"], "per_ray": per_ray,
+            "bytes_per_ray": {"closest": 48 + 80 * per_ray["closest_nodes"] + 48 * per_ray["closest_tris"],
+                              "shadow": 36 + 80 * per_ray["shadow_nodes"] + 48 * per_ray["shadow_tris"]}}
 
 
 def batched_bench(dev, count=64, repeats=3):
