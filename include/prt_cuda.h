@@ -160,7 +160,25 @@ typedef struct prt_renderer_desc
   int32_t rr_depth;       /* "rrDepth", reference default 8 */
   float   min_weight;     /* "minWeight", reference default 1e-4 */
   float   max_radiance;   /* "maxRadiance", reference default FLT_MAX (no clamping) */
+  int32_t type;           /* renderer "type": PRT_RENDERER_* (0 = pathStream) */
+  int32_t samples;        /* aoStream "samples" (AO rays per pixel sample; 0 = the default 16) */
 } prt_renderer_desc;
+
+/* Renderer types (render/renderer_factory_stream.cpp:54-67): the path tracer and its sibling
+ * stream renderers, which reuse its camera rays and traversal:
+ * PRIMARY  "primaryStream": shading normal (N + 1) / 2 of the first hit, 0.05 on a miss
+ *          (render/primary_renderer_stream.h);
+ * AO       "aoStream": fraction of `samples` cosine-distributed rays that escape
+ *          (render/ao_renderer_stream.h);
+ * DIFFUSE  "diffuseStream": white diffuse paths lit by a white sky, throughput x 0.8 per bounce
+ *          (render/diffuse_renderer_stream.h);
+ * DIFFUSE2 "diffuse2Stream": the same with a cosine-sampled sky ray per bounce, half-weighted
+ *          (render/diffuse2_renderer_stream.h). */
+#define PRT_RENDERER_PATH     0
+#define PRT_RENDERER_PRIMARY  1
+#define PRT_RENDERER_AO       2
+#define PRT_RENDERER_DIFFUSE  3
+#define PRT_RENDERER_DIFFUSE2 4
 
 /* AOV selection bits for prt_cuda_frame (render/device_cpu.cpp:178-232). */
 #define PRT_AOV_ALBEDO1  (1 << 0)   /* "aovAlbedo1": first-hit albedo */

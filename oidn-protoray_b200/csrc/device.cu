@@ -762,6 +762,10 @@ int prt_cuda_renderer(prt_context* ctx, const prt_renderer_desc* r)
 {
   return guarded(ctx, [&](Context& c) {
     if (!r || r->max_depth < 0 || r->max_depth > 1000) throw std::invalid_argument("invalid renderer settings");
+    if (r->type < PRT_RENDERER_PATH || r->type > PRT_RENDERER_DIFFUSE2) throw std::invalid_argument("invalid renderer type");
+    if (r->samples < 0 || r->samples > 4096) throw std::invalid_argument("invalid renderer samples");
+    c.renderer.type = r->type;
+    c.renderer.aoSamples = r->samples ? r->samples : 16;
     c.renderer.maxDepth = r->max_depth;
     c.renderer.rrDepth = r->rr_depth;
     c.renderer.minWeight = r->min_weight;
@@ -1308,6 +1312,7 @@ int prt_cuda_batch_create(prt_context* ctx, const prt_batch_item* items, int32_t
           throw std::logic_error("image size is not divisible by the tile size");
         if (it.width > 4096 || it.height > 4096) throw std::logic_error("image size is too large");
         if (it.renderer.max_depth < 0 || it.renderer.max_depth > 1000) throw std::invalid_argument("invalid renderer settings");
+        if (it.renderer.type != PRT_RENDERER_PATH) throw std::invalid_argument("batches render with the path tracer");
         if (it.aov_mask & ~(PRT_AOV_ALBEDO1 | PRT_AOV_NORMAL1)) throw std::invalid_argument("unknown AOV bits");
         // Scene upload through the frame form's path, into buffers the batch owns.
         Context tmp;
@@ -1324,7 +1329,7 @@ int prt_cuda_batch_create(prt_context* ctx, const prt_batch_item* items, int32_t
         bi.sc = tmp.scene;
         bi.cam = makeCamera(it.camera, it.width, it.height);
         bi.rd = DevRenderer{it.renderer.max_depth, it.renderer.rr_depth, it.renderer.min_weight, it.renderer.max_radiance,
-                            it.seed};
+                            it.seed, PRT_RENDERER_PATH, 16};
         bi.width = it.width;
         bi.height = it.height;
         bi.pixelCount = it.width * it.height;
@@ -1516,6 +1521,7 @@ int prt_cuda_adjoint(prt_context* ctx, uint32_t first_sample, int32_t spp, const
     requireScene(c);
     if (!c.hasRenderer || !c.hasCamera || !c.accum) throw ApiError{PRT_ERR_STATE, "renderer, camera and frame are required"};
     if (spp <= 0 || !d_loss_d_image) throw std::invalid_argument("invalid adjoint request");
+    if (c.renderer.type != PRT_RENDERER_PATH) throw std::invalid_argument("the adjoint differentiates the path tracer");
     requireAdjointMaterials(c.materialsHost);
     if (c.texturesHost.size() > 32) throw std::invalid_argument("the adjoint supports at most 32 textures");
     int64_t texFloats = 0;

@@ -194,6 +194,8 @@ struct DevRenderer
   float minWeight;
   float maxRadiance;
   uint32_t seed;
+  int type;        // PRT_RENDERER_*
+  int aoSamples;
 };
 
 // What the adjoint's replay needs per frame besides the frame itself (csrc/adjoint.cuh).

@@ -14,6 +14,7 @@
 // without atomics, so the image does not depend on scheduling.
 #include "wavefront.cuh"
 #include "adjoint.cuh"
+#include "../../include/prt_cuda.h"
 
 #include <algorithm>
 #include <cstddef>
@@ -698,6 +699,115 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
   }
 }
 
+// ---- sibling stream renderers ---------------------------------------------------------------
+//
+// The path tracer's simpler siblings (render/renderer_factory_stream.cpp:54-67), one thread per
+// pixel-sample: the camera ray of the path tracer, then
+//   Type 1 (primaryStream, render/primary_renderer_stream.h:140-176): (N + 1) / 2 of the first
+//          hit's shading normal, 0.05 on a miss;
+//   Type 2 (aoStream, render/ao_renderer_stream.h:150-238): the fraction of aoSamples
+//          cosine-distributed rays from the first hit that escape, 0 on a miss;
+//   Type 3 (diffuseStream, render/diffuse_renderer_stream.h:146-213): a white diffuse walk under
+//          a white sky, throughput x 0.8 per bounce, 0 at maxDepth;
+//   Type 4 (diffuse2Stream, render/diffuse2_renderer_stream.h:150-255): the same with a
+//          cosine-sampled sky ray per bounce; sky seen by either ray counts half, except from
+//          the camera.
+// Bounce k draws its directions from dimensions 4 + 2k (4 + 4k and 4 + 4k + 2 for type 4, AO ray
+// k from 4 + 2k). Writes ps.out, which kAccumulate adds in sample order.
+template <int Type>
+__global__ void __launch_bounds__(256) kSimpleRender(Launch L)
+{
+  const int64_t P = (int64_t)L.pixelCount * L.samples;
+  unsigned long long traced = 0, occl = 0;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P; p += (int64_t)gridDim.x * blockDim.x)
+  {
+    const int s = (int)(p / L.pixelCount);
+    const int idx = (int)(p - (int64_t)s * L.pixelCount);
+    int x, y;
+    pixelOf(idx, L.width, x, y);
+    const uint32_t pixelId = (uint32_t)x | ((uint32_t)y << 16);
+    const uint32_t sampleIndex = L.firstSample + (uint32_t)s;
+    const SobolState st = sobolSetSample(L.rd.seed, sampleIndex, pixelId);
+    float sx, sy;
+    sobolGet2D(st, kDimPixel, sx, sy);
+    f3 org, dir;
+    float tnear;
+    cameraRay(L.cam, ((float)x + sx) * (1.f / (float)L.width), ((float)y + sy) * (1.f / (float)L.height), org, dir,
+              tnear);
+    f3 color = mk(0.f);
+    float throughput = 1.f, Lsum = 0.f;
+    for (int depth = 0;; ++depth)
+    {
+      const TraceHit h = traverse<false>(L.sc.nodes, L.sc.tris, org, dir, tnear, kPosMax, L.ps.err);
+      ++traced;
+      if (h.triId < 0)
+      {
+        if (Type == 1) color = mk(0.05f);
+        if (Type == 3) color = mk(throughput);
+        if (Type == 4) color = mk(Lsum + throughput * (depth > 0 ? 0.5f : 1.f));
+        break;
+      }
+      ShadeCtx ctx;
+      postIntersect(L.sc, org, dir, h.t, h.triId, h.u, h.v, ctx);
+      if (Type == 1)
+      {
+        color = (ctx.f.N + mk(1.f)) * 0.5f;
+        break;
+      }
+      if (Type == 2)
+      {
+        int open = 0;
+        for (int k = 0; k < L.rd.aoSamples; ++k)
+        {
+          float ax, ay, pdf;
+          sobolGet2D(st, kDimBase + 2u * (uint32_t)k, ax, ay);
+          const f3 d = toWorld(ctx.f, cosineSampleHemisphere(pdf, ax, ay));
+          open += traverse<true>(L.sc.nodes, L.sc.tris, ctx.p, d, ctx.eps, kPosMax, L.ps.err).triId < 0 ? 1 : 0;
+          ++occl;
+        }
+        color = mk((float)open * (1.f / (float)L.rd.aoSamples));
+        break;
+      }
+      if (depth == L.rd.maxDepth)
+      {
+        if (Type == 4) color = mk(Lsum);
+        break;
+      }
+      float bx, by, pdf;
+      if (Type == 4)
+      {
+        sobolGet2D(st, kDimBase + 4u * (uint32_t)depth, bx, by);
+        const f3 ds = toWorld(ctx.f, cosineSampleHemisphere(pdf, bx, by));
+        sobolGet2D(st, kDimBase + 4u * (uint32_t)depth + 2u, bx, by);
+        throughput *= 0.8f;
+        const bool open = traverse<true>(L.sc.nodes, L.sc.tris, ctx.p, ds, ctx.eps, kPosMax, L.ps.err).triId < 0;
+        ++occl;
+        if (open) Lsum += throughput * 0.5f;
+      }
+      else
+      {
+        sobolGet2D(st, kDimBase + 2u * (uint32_t)depth, bx, by);
+        throughput *= 0.8f;
+      }
+      dir = toWorld(ctx.f, cosineSampleHemisphere(pdf, bx, by));
+      org = ctx.p;
+      tnear = ctx.eps;
+    }
+    L.ps.out[p] = make_float4(color.x, color.y, color.z, 1.f);
+  }
+  // Ray counts: one atomic per warp.
+  for (int o = 16; o > 0; o >>= 1)
+  {
+    traced += __shfl_down_sync(0xffffffffu, traced, o);
+    occl += __shfl_down_sync(0xffffffffu, occl, o);
+  }
+  if (laneId() == 0)
+  {
+    atomicAdd(L.ps.travCounts, traced);
+    atomicAdd(L.ps.travCounts + 1, occl);
+  }
+}
+
 // Adds the wave's samples of each pixel, in sample order, to the accumulation planes.
 __global__ void kAccumulate(Launch L, float4* __restrict__ accum, float4* __restrict__ accA, float4* __restrict__ accN)
 {
@@ -986,11 +1096,31 @@ cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
   cudaError_t e = cudaSuccess;
   if (counting) e = cudaMemsetAsync(ctx.ps.travCounts, 0, 4 * sizeof(unsigned long long), ctx.stream);
   if (e != cudaSuccess) return e;
+  const int type = ctx.renderer.type;
+  unsigned long long simpleRays[2] = {0, 0};
+  if (type != PRT_RENDERER_PATH)
+  {
+    e = cudaMemsetAsync(ctx.ps.travCounts, 0, 4 * sizeof(unsigned long long), ctx.stream);
+    if (e != cudaSuccess) return e;
+  }
   for (int done = 0; done < spp;)
   {
     const int S = std::min(ctx.waveSamples, spp - done);
     const Launch L = frameLaunch(ctx, ctx.sampleIndex + (uint32_t)done, S);
-    e = bounceLoop(ctx, L, pixelCount * S, false, counting, begin, end, rc);
+    if (type == PRT_RENDERER_PATH)
+      e = bounceLoop(ctx, L, pixelCount * S, false, counting, begin, end, rc);
+    else
+    {
+      const int P = pixelCount * S;
+      begin(0);
+      if (type == PRT_RENDERER_PRIMARY) kSimpleRender<1><<<gridFor(ctx, P), 256, 0, ctx.stream>>>(L);
+      else if (type == PRT_RENDERER_AO) kSimpleRender<2><<<gridFor(ctx, P), 256, 0, ctx.stream>>>(L);
+      else if (type == PRT_RENDERER_DIFFUSE) kSimpleRender<3><<<gridFor(ctx, P), 256, 0, ctx.stream>>>(L);
+      else kSimpleRender<4><<<gridFor(ctx, P), 256, 0, ctx.stream>>>(L);
+      end();
+      rc.launches++;
+      e = cudaGetLastError();
+    }
     if (e != cudaSuccess) return e;
     kAccumulate<<<gridFor(ctx, pixelCount), 256, 0, ctx.stream>>>(L, reinterpret_cast<float4*>(ctx.accum),
                                                                    reinterpret_cast<float4*>(ctx.accumA),
@@ -1001,6 +1131,14 @@ cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
     done += S;
   }
   ctx.sampleIndex += (uint32_t)spp;
+  if (type != PRT_RENDERER_PATH)
+  {
+    e = cudaMemcpyAsync(simpleRays, ctx.ps.travCounts, sizeof(simpleRays), cudaMemcpyDeviceToHost, ctx.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx.stream);
+    if (e != cudaSuccess) return e;
+    rc.closestRays = (int64_t)simpleRays[0];
+    rc.shadowRays = (int64_t)simpleRays[1];
+  }
   if (timing || counting)
   {
     e = cudaStreamSynchronize(ctx.stream);

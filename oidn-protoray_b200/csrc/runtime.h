@@ -113,7 +113,7 @@ struct Context
   std::vector<int> meshTriOffsetHost;
   std::vector<DevMaterial> materialsHost;  // host copies of the uploaded material records
   std::vector<DevTexture> texturesHost;    // device pointers and sizes of the scene's textures
-  DevRenderer renderer{100, 8, 1e-4f, 3.402823466e38f, 0u};
+  DevRenderer renderer{100, 8, 1e-4f, 3.402823466e38f, 0u, 0, 16};
   bool hasRenderer = false;
   DevCamera camera{};
   bool hasCamera = false;

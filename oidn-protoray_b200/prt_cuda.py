@@ -150,8 +150,9 @@ class DeviceCuda:
         self._check(self.lib.prt_cuda_scene_upload(self.h, C.byref(desc)))
         self.scene = scene
 
-    def init_renderer(self, max_depth=100, rr_depth=8, min_weight=1e-4, max_radiance=3.4028234663852886e38):
-        r = T.RendererDesc(max_depth, rr_depth, min_weight, max_radiance)
+    def init_renderer(self, max_depth=100, rr_depth=8, min_weight=1e-4, max_radiance=3.4028234663852886e38,
+                      type=T.PRT_RENDERER_PATH, samples=16):
+        r = T.RendererDesc(max_depth, rr_depth, min_weight, max_radiance, type, samples)
         self._check(self.lib.prt_cuda_renderer(self.h, C.byref(r)))
 
     def init_sampler(self, seed):
@@ -245,7 +246,7 @@ class DeviceCuda:
         self.init_scene(scene)
         self.init_frame(scene.width, scene.height, aov_mask)
         self.init_camera(scene.camera)
-        self.init_renderer(scene.max_depth, scene.rr_depth)
+        self.init_renderer(scene.max_depth, scene.rr_depth, type=scene.renderer_type, samples=scene.ao_samples)
         self.init_sampler(seed)
 
     # -- queries --------------------------------------------------------------------------------
@@ -318,7 +319,7 @@ class Batch:
             it = items[k]
             it.scene = C.pointer(d)
             it.camera = sc.camera
-            it.renderer = T.RendererDesc(sc.max_depth, sc.rr_depth, 1e-4, 3.4028234663852886e38)
+            it.renderer = T.RendererDesc(sc.max_depth, sc.rr_depth, 1e-4, 3.4028234663852886e38, T.PRT_RENDERER_PATH, 16)
             it.width, it.height, it.spp, it.aov_mask, it.seed = sc.width, sc.height, sc.spp, aov, seed
         h = C.c_void_p()
         device._check(device.lib.prt_cuda_batch_create(device.h, items, len(descs), C.byref(h)))

@@ -38,6 +38,8 @@ class Scene:
         self.spp = 1
         self.max_depth = 5
         self.rr_depth = 8
+        self.renderer_type = T.PRT_RENDERER_PATH
+        self.ao_samples = 16
         self._keep = []
 
     # -- construction ---------------------------------------------------------------------
@@ -105,6 +107,8 @@ class Scene:
         r.max_depth = self.max_depth
         r.rr_depth = self.rr_depth
         r.min_weight = min_weight
+        r.type = self.renderer_type
+        r.samples = self.ao_samples
         r.max_radiance = max_radiance
         return r
 

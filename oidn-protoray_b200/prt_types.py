@@ -187,7 +187,16 @@ class RendererDesc(C.Structure):
         ("rr_depth", C.c_int32),
         ("min_weight", C.c_float),
         ("max_radiance", C.c_float),
+        ("type", C.c_int32),
+        ("samples", C.c_int32),
     ]
+
+
+PRT_RENDERER_PATH = 0
+PRT_RENDERER_PRIMARY = 1
+PRT_RENDERER_AO = 2
+PRT_RENDERER_DIFFUSE = 3
+PRT_RENDERER_DIFFUSE2 = 4
 
 
 class RenderStats(C.Structure):

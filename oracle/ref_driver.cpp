@@ -227,7 +227,9 @@ int ref_create(const prt_scene_desc* scene, const prt_camera_desc* cam, const pr
     h->size = Vec2i(width, height);
     h->device.initFrame(h->size, frameProps);
     Props rprops;
-    rprops.set("type", "pathStream");
+    static const char* kTypes[] = {"pathStream", "primaryStream", "aoStream", "diffuseStream", "diffuse2Stream"};
+    rprops.set("type", kTypes[(rd->type >= 0 && rd->type <= 4) ? rd->type : 0]);
+    rprops.set("samples", rd->samples > 0 ? rd->samples : 16);
     rprops.set("sampler", "sobolBurley");
     rprops.set("maxDepth", rd->max_depth);
     rprops.set("rrDepth", rd->rr_depth);

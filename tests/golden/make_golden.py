@@ -17,6 +17,7 @@ Fixtures (small, seeded, committed):
   terrain_img.npz  small terrain renders (96^2 heightfield, 24 spheres of all four material
                    kinds, sun-sky) at 128x64: 16 spp and 256 spp, seeds 0 and 1
   lobes_img.npz    the small scene with Oren-Nayar, sheen and layered spheres, 16 spp, seeds 0, 1
+  siblings_img.npz primaryStream, aoStream, diffuseStream, diffuse2Stream renders of the small scene
   bsdf.npz         the reference's Standard-material BSDF (eval, sample) on 512 seeded tuples
                    for each case of tests/bsdf_cases.py
   sunsky_t3_e30.npz the reference's sun-sky products (sun radiance and angle, 512x256 sky) for
@@ -113,6 +114,26 @@ def make_lobe_images():
     np.savez_compressed(OUT / "lobes_img.npz", **out)
 
 
+def sibling_scene(kind):
+    s = prt_scenes.cornell(seed=0, width=64, height=64, spp=4)
+    s.renderer_type = kind
+    s.ao_samples = 8
+    return s
+
+
+def make_sibling_images():
+    """primaryStream, aoStream (8 rays), diffuseStream, diffuse2Stream on the small scene,
+    64x64, 4 spp, seed 0."""
+    out = {}
+    for kind in (1, 2, 3, 4):
+        dev = ref.RefDevice(sibling_scene(kind), seed=0)
+        st = dev.render(4)
+        out[f"type{kind}"] = dev.blit()
+        out[f"type{kind}_rays"] = np.float64(st["rays"])
+        dev.close()
+    np.savez_compressed(OUT / "siblings_img.npz", **out)
+
+
 def make_bsdf():
     sys.path.insert(0, str(ROOT / "tests"))
     import bsdf_cases
@@ -147,13 +168,15 @@ def make_sunsky():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["sobol", "rays", "images", "sunsky", "bsdf", "terrain", "lobes"]
+    which = sys.argv[1:] or ["sobol", "rays", "images", "sunsky", "bsdf", "terrain", "lobes", "siblings"]
     if "terrain" in which:
         make_terrain_images()
     if "bsdf" in which:
         make_bsdf()
     if "lobes" in which:
         make_lobe_images()
+    if "siblings" in which:
+        make_sibling_images()
     if "sunsky" in which:
         make_sunsky()
     if "sobol" in which:

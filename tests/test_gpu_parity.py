@@ -145,3 +145,19 @@ def test_lobes_same_seed_tracks_oracle(device, golden):
     other = rel_mse(z["spp16_seed1"], z["spp16_seed0"])
     assert same < 0.2 * other, (same, other)
     assert abs(st["rays"] / float(z["spp16_seed0_rays"]) - 1.0) < 0.01
+
+
+@pytest.mark.parametrize("kind", [1, 2, 3, 4], ids=["primary", "ao", "diffuse", "diffuse2"])
+def test_sibling_renderers_match_oracle(device, golden, kind):
+    """primaryStream / aoStream / diffuseStream / diffuse2Stream: the same samples, hits and
+    directions as the reference, so the images agree to rounding (rare near-tie hits aside)."""
+    z = golden("siblings_img.npz")
+    s = prt_scenes.cornell(seed=0, width=64, height=64, spp=4)
+    s.renderer_type = kind
+    s.ao_samples = 8
+    img, st = render(device, s, seed=0, spp=4)
+    ref = z[f"type{kind}"]
+    diff = np.abs(img.astype(np.float64) - ref)
+    assert diff.mean() < 2e-3, diff.mean()
+    assert np.mean(diff > 1e-3) < 0.01, np.mean(diff > 1e-3)
+    assert abs(st["rays"] / float(z[f"type{kind}_rays"]) - 1.0) < 1e-3
