@@ -43,9 +43,9 @@ public:
 
   // Device::initRenderer for type "pathStream" / sampler "sobolBurley" (render/device_cpu.cpp:32-46).
   void initRenderer(int maxDepth = 100, int rrDepth = 8, float minWeight = 1e-4f,
-                    float maxRadiance = 3.402823466e38f)
+                    float maxRadiance = 3.402823466e38f, int type = PRT_RENDERER_PATH, int samples = 16)
   {
-    const prt_renderer_desc r{maxDepth, rrDepth, minWeight, maxRadiance};
+    const prt_renderer_desc r{maxDepth, rrDepth, minWeight, maxRadiance, type, samples};
     check(prt_cuda_renderer(ctx_, &r));
   }
 
