@@ -184,10 +184,25 @@ typedef struct prt_renderer_desc
 #define PRT_AOV_ALBEDO1  (1 << 0)   /* "aovAlbedo1": first-hit albedo */
 #define PRT_AOV_NORMAL1  (1 << 1)   /* "aovNormal1": first-hit normal */
 
+#define PRT_AOV_HDR_VAR  (1 << 2)   /* "aovHdrVar": per-pixel sample variance of the colour */
+
 /* AOV identifiers for prt_cuda_blit. */
 #define PRT_BLIT_HDR      0
 #define PRT_BLIT_ALBEDO1  1
 #define PRT_BLIT_NORMAL1  2
+#define PRT_BLIT_HDR_VAR  3   /* FrameAovs::hdrVar: sample variance (needs PRT_AOV_HDR_VAR) */
+#define PRT_BLIT_LDR      4   /* Device::blitFrame(Surface&): tone-mapped 8-bit colour, one uint32
+                                 per pixel (blue in bits 0-7, green 8-15, red 16-23; gamma 2.2,
+                                 image/pixel.h:36-40); dst is then width * height uint32 */
+#define PRT_BLIT_LDR_RGB  5   /* FrameAovs::ldr: tone-mapped colour clamped to [0, 1], RGB floats */
+
+/* Tone mappers for PRT_BLIT_LDR and the frame error (render/device_cpu.cpp:286-303). */
+#define PRT_TONE_NONE     0
+#define PRT_TONE_LINEAR   1
+#define PRT_TONE_REINHARD 2
+#define PRT_TONE_ACES     3
+#define PRT_TONE_FILMIC   4
+#define PRT_TONE_LOG      5
 
 /* Per-call statistics, the reference's Props stats of one render() (render/path_renderer_stream.h:175-178). */
 typedef struct prt_render_stats
@@ -368,6 +383,16 @@ int prt_cuda_update_texture(prt_context* ctx, int32_t texture, const float* rgb)
 int prt_cuda_update_material(prt_context* ctx, int32_t material, const prt_material* m);
 /* The same for materials [first, first + count) in one call (one copy to the device). */
 int prt_cuda_update_materials(prt_context* ctx, int32_t first, int32_t count, const prt_material* ms);
+
+/* ---- film post-step ----------------------------------------------------------------------
+ * Device::initToneMapper (render/device_cpu.cpp:286-303): `type` PRT_TONE_*, "exposure" and
+ * Reinhard's "burn" (0..1). */
+int prt_cuda_tone_mapper(prt_context* ctx, int32_t type, float exposure, float burn);
+
+/* Device::getFrameError (render/device_cpu.cpp:436-439, image/accum_buffer.h:752-795): the mean
+ * relative L1 difference between the current image and the image at the last power-of-two sample
+ * count (the checkpoint copy every frame keeps), scaled by the tone mapper's exposure. */
+int prt_cuda_frame_error(prt_context* ctx, float* error);
 
 /* Enables PRT_PROFILE_* instrumentation for subsequent render calls (0 = off). */
 int prt_cuda_set_profiling(prt_context* ctx, int32_t flags);

@@ -108,6 +108,9 @@ void freeFrame(Context& c)
   f(c.accum);
   f(c.accumA);
   f(c.accumN);
+  f(c.accumC);
+  f(c.accum2);
+  f(c.errPartials);
   PathState& s = c.ps;
   f(s.rayO); f(s.rayD); f(s.hit); f(s.thr); f(s.rad); f(s.info);
   f(s.shO); f(s.shD); f(s.shL); f(s.out); f(s.aovA); f(s.aovN);
@@ -518,13 +521,17 @@ void allocFrame(Context& c, int width, int height, int aovMask)
   if (width % 32 != 0 || height % 8 != 0)
     throw std::logic_error("image size is not divisible by the tile size");
   if (width > 4096 || height > 4096) throw std::logic_error("image size is too large");
+  if (aovMask & ~(PRT_AOV_ALBEDO1 | PRT_AOV_NORMAL1 | PRT_AOV_HDR_VAR)) throw std::invalid_argument("unknown AOV bits");
   freeFrame(c);
   c.width = width;
   c.height = height;
-  c.aovMask = aovMask;
+  c.aovMask = aovMask & (PRT_AOV_ALBEDO1 | PRT_AOV_NORMAL1);  // per-path first-hit AOVs
   const size_t px = (size_t)width * height;
   c.accum = (float*)devAlloc(c, px * sizeof(float4), nullptr);
-  if (aovMask)
+  c.accumC = (float*)devAlloc(c, px * sizeof(float4), nullptr);
+  c.errPartials = (double*)devAlloc(c, sizeof(double) * (size_t)c.smCount * 16, nullptr);
+  if (aovMask & PRT_AOV_HDR_VAR) c.accum2 = (float*)devAlloc(c, px * sizeof(float4), nullptr);
+  if (c.aovMask)
   {
     c.accumA = (float*)devAlloc(c, px * sizeof(float4), nullptr);
     c.accumN = (float*)devAlloc(c, px * sizeof(float4), nullptr);
@@ -860,11 +867,41 @@ int prt_cuda_blit(prt_context* ctx, int32_t aov, float* dst)
 {
   return guarded(ctx, [&](Context& c) {
     if (!c.accum || !dst) throw std::invalid_argument("no frame or null destination");
-    if (aov < 0 || aov > 2 || (aov > 0 && !c.accumA)) throw std::invalid_argument("AOV not enabled");
-    Staged out(c, dst, (size_t)c.width * c.height * 3 * sizeof(float), false);
-    cuCheck(launchBlit(c, aov, (float*)out.dev), "blit");
+    if (aov < 0 || aov > PRT_BLIT_LDR_RGB || ((aov == PRT_BLIT_ALBEDO1 || aov == PRT_BLIT_NORMAL1) && !c.accumA) ||
+        (aov == PRT_BLIT_HDR_VAR && !c.accum2))
+      throw std::invalid_argument("AOV not enabled");
+    const size_t px = (size_t)c.width * c.height;
+    Staged out(c, dst, aov == PRT_BLIT_LDR ? px * sizeof(uint32_t) : px * 3 * sizeof(float), false);
+    if (aov == PRT_BLIT_HDR_VAR) cuCheck(launchBlitVariance(c, (float*)out.dev), "blit");
+    else if (aov == PRT_BLIT_LDR) cuCheck(launchBlitLdr(c, (uint32_t*)out.dev), "blit");
+    else if (aov == PRT_BLIT_LDR_RGB) cuCheck(launchBlitLdrRgb(c, (float*)out.dev), "blit");
+    else cuCheck(launchBlit(c, aov, (float*)out.dev), "blit");
     out.copyOut();
     cuCheck(cudaStreamSynchronize(c.stream), "blit sync");
+  });
+}
+
+int prt_cuda_tone_mapper(prt_context* ctx, int32_t type, float exposure, float burn)
+{
+  return guarded(ctx, [&](Context& c) {
+    if (type < PRT_TONE_NONE || type > PRT_TONE_LOG) throw std::invalid_argument("invalid tone mapper type");
+    if (type == PRT_TONE_REINHARD && (burn < 0.f || burn > 1.f)) throw std::invalid_argument("burn must be between 0 and 1");
+    c.toneType = type;
+    // FilmicToneMapper folds its 18% middle-grey bias into the exposure (image/filmic_tone_mapper.h).
+    c.toneExposure = type == PRT_TONE_FILMIC ? exposure * 1.758141f : exposure;
+    c.toneInvWhite2 = burn * burn;
+  });
+}
+
+int prt_cuda_frame_error(prt_context* ctx, float* error)
+{
+  return guarded(ctx, [&](Context& c) {
+    if (!error) throw std::invalid_argument("null output");
+    if (!c.accum) throw ApiError{PRT_ERR_STATE, "no frame"};
+    cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+    double e = 0.0;
+    cuCheck(frameError(c, e), "frame error");
+    *error = (float)e;
   });
 }
 
@@ -1188,17 +1225,22 @@ struct StaticSwap
 {
   Context& c;
   PathState ps;
-  float *accum, *accumA, *accumN;
+  float *accum, *accumA, *accumN, *accumC, *accum2;
+  int64_t accumCount;
   int waveSamples, profileFlags;
   uint32_t sampleIndex;
   explicit StaticSwap(Context& ctx)
-      : c(ctx), ps(ctx.ps), accum(ctx.accum), accumA(ctx.accumA), accumN(ctx.accumN), waveSamples(ctx.waveSamples),
-        profileFlags(ctx.profileFlags), sampleIndex(ctx.sampleIndex)
+      : c(ctx), ps(ctx.ps), accum(ctx.accum), accumA(ctx.accumA), accumN(ctx.accumN), accumC(ctx.accumC),
+        accum2(ctx.accum2), accumCount(ctx.accumCount), waveSamples(ctx.waveSamples), profileFlags(ctx.profileFlags),
+        sampleIndex(ctx.sampleIndex)
   {
   }
   ~StaticSwap()
   {
     c.ps = ps;
+    c.accumC = accumC;
+    c.accum2 = accum2;
+    c.accumCount = accumCount;
     c.accum = accum;
     c.accumA = accumA;
     c.accumN = accumN;
@@ -1236,6 +1278,9 @@ int prt_cuda_render_static(prt_context* ctx, uint32_t first_sample, int32_t spp,
     unsigned char* base = staticScratchOf(c.device);
 
     StaticSwap keep(c);
+  c.accumC = nullptr;   // the static render keeps no checkpoint or variance of its own
+  c.accum2 = nullptr;
+  c.accumCount = 0;
     PathState s;
     s.capacity = kStaticPaths;
     float4* planes[kStaticPathPlanes];

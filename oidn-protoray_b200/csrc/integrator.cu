@@ -809,7 +809,11 @@ __global__ void __launch_bounds__(256) kSimpleRender(Launch L)
 }
 
 // Adds the wave's samples of each pixel, in sample order, to the accumulation planes.
-__global__ void kAccumulate(Launch L, float4* __restrict__ accum, float4* __restrict__ accA, float4* __restrict__ accN)
+// Also keeps, per pixel, the checkpoint copy of the sums taken before every power-of-two-th
+// sample (AccumBuffer::begin, image/accum_buffer.h:252-260; `count` = samples since the clear)
+// and, when enabled, the sums of squared samples (addSerial, :439-486).
+__global__ void kAccumulate(Launch L, float4* __restrict__ accum, float4* __restrict__ accA, float4* __restrict__ accN,
+                            float4* __restrict__ accC, float4* __restrict__ acc2, long long countBase)
 {
   const int n = L.pixelCount;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
@@ -819,14 +823,23 @@ __global__ void kAccumulate(Launch L, float4* __restrict__ accum, float4* __rest
     float4 acc = accum[q];
     float4 a = accA ? accA[q] : make_float4(0.f, 0.f, 0.f, 0.f);
     float4 nn = accN ? accN[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 sq = acc2 ? acc2[q] : make_float4(0.f, 0.f, 0.f, 0.f);
     for (int s = 0; s < L.samples; ++s)
     {
+      const long long count = countBase + s;
+      if (accC && (count & (count - 1)) == 0) accC[q] = acc;
       const int64_t p = (int64_t)s * L.pixelCount + idx;
       const float4 o = L.ps.out[p];
       acc.x += o.x;
       acc.y += o.y;
       acc.z += o.z;
       acc.w += 1.f;
+      if (acc2)
+      {
+        sq.x += o.x * o.x;
+        sq.y += o.y * o.y;
+        sq.z += o.z * o.z;
+      }
       if (accA)
       {
         const float4 va = L.ps.aovA[p];
@@ -842,12 +855,137 @@ __global__ void kAccumulate(Launch L, float4* __restrict__ accum, float4* __rest
       }
     }
     accum[q] = acc;
+    if (acc2) acc2[q] = sq;
     if (accA)
     {
       accA[q] = a;
       accN[q] = nn;
     }
   }
+}
+
+// Tone mappers (image/*_tone_mapper.h): linear, Reinhard with burn, the ACES fit used by the
+// reference (RRT + ODT approximation between its input and output matrices), Hable's filmic
+// curve (white point 11.2, exposure bias 1.758141), log.
+struct ToneMap
+{
+  int type;
+  float exposure, invWhite2;
+
+  PRT_D float filmic(float x) const
+  {
+    const float A = 0.22f, B = 0.30f, C = 0.10f, D = 0.20f, E = 0.01f, F = 0.30f;
+    return ((x * (A * x + C * B) + D * E) / (x * (A * x + B) + D * F)) - E / F;
+  }
+
+  PRT_D f3 apply(f3 c) const
+  {
+    if (type == PRT_TONE_NONE) return c;
+    const f3 v = c * exposure;
+    if (type == PRT_TONE_LINEAR) return v;
+    if (type == PRT_TONE_REINHARD)
+    {
+      const f3 mapped = mk(v.x * (1.f + v.x * invWhite2) * (1.f / (1.f + v.x)),
+                           v.y * (1.f + v.y * invWhite2) * (1.f / (1.f + v.y)),
+                           v.z * (1.f + v.z * invWhite2) * (1.f / (1.f + v.z)));
+      return mk(v.x * (mapped.x * rcpSafe(v.x)), v.y * (mapped.y * rcpSafe(v.y)), v.z * (mapped.z * rcpSafe(v.z)));
+    }
+    if (type == PRT_TONE_ACES)
+    {
+      const f3 x0 = mk(0.5972782409f, 0.0760130499f, 0.0284085382f) * v.x +
+                    mk(0.3545713181f, 0.9083220973f, 0.1338243154f) * v.y +
+                    mk(0.0482176639f, 0.0156579968f, 0.8375684636f) * v.z;
+      const float a = 1.6773f, d = 0.9714f, b = 1.1174f, cc = 0.2447f;
+      const f3 x1 = mk(powf(x0.x, a) / (powf(x0.x, a * d) * b + cc), powf(x0.y, a) / (powf(x0.y, a * d) * b + cc),
+                       powf(x0.z, a) / (powf(x0.z, a * d) * b + cc));
+      const f3 y = mk(1.6047539945f, -0.1020831870f, -0.0032670420f) * x1.x +
+                   mk(-0.5310794927f, 1.1081322801f, -0.0727552477f) * x1.y +
+                   mk(-0.0736720338f, -0.0060518756f, 1.0760219533f) * x1.z;
+      return clamp01(y);
+    }
+    if (type == PRT_TONE_FILMIC)
+    {
+      const float ws = 1.f / filmic(11.2f);
+      return mk(filmic(v.x), filmic(v.y), filmic(v.z)) * ws;
+    }
+    return mk(logf(v.x + 1.f), logf(v.y + 1.f), logf(v.z + 1.f)) * (1.f / 16.f);
+  }
+};
+
+// encodeBgr8 (image/pixel.h:36-40): gamma 2.2, truncation to 0..255, blue in the low byte.
+PRT_D uint32_t encodeBgr8(f3 c)
+{
+  const float g = 1.f / 2.2f;
+  const int r = min(max(__float2int_rz(powf(c.x, g) * 255.f), 0), 255);
+  const int gr = min(max(__float2int_rz(powf(c.y, g) * 255.f), 0), 255);
+  const int b = min(max(__float2int_rz(powf(c.z, g) * 255.f), 0), 255);
+  return (uint32_t)b | ((uint32_t)gr << 8) | ((uint32_t)r << 16);
+}
+
+__global__ void kBlitLdr(const float4* __restrict__ acc, int n, ToneMap tm, uint32_t* __restrict__ dst)
+{
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+  {
+    const float4 a = acc[q];
+    const float r = rcpSafe(a.w);
+    dst[q] = encodeBgr8(tm.apply(mk(a.x * r, a.y * r, a.z * r)));
+  }
+}
+
+// AccumBuffer::blitLdr(Vec3f*) (image/accum_buffer.h:681-733): tone-mapped, clamped to [0, 1].
+__global__ void kBlitLdrRgb(const float4* __restrict__ acc, int n, ToneMap tm, float* __restrict__ dst)
+{
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+  {
+    const float4 a = acc[q];
+    const float r = rcpSafe(a.w);
+    const f3 c = clamp01(tm.apply(mk(a.x * r, a.y * r, a.z * r)));
+    dst[3 * q + 0] = c.x;
+    dst[3 * q + 1] = c.y;
+    dst[3 * q + 2] = c.z;
+  }
+}
+
+// Sample variance max(sum2 - sum^2 / w, 0) / max(w - 1, 1) (image/accum_buffer.h:627-634).
+__global__ void kBlitVariance(const float4* __restrict__ acc, const float4* __restrict__ acc2, int n,
+                              float* __restrict__ dst)
+{
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+  {
+    const float4 a = acc[q], b = acc2[q];
+    const float r = rcpSafe(a.w);
+    const float k = rcpSafe(fmaxf(a.w - 1.f, 1.f));
+    dst[3 * q + 0] = fmaxf(b.x - a.x * a.x * r, 0.f) * k;
+    dst[3 * q + 1] = fmaxf(b.y - a.y * a.y * r, 0.f) * k;
+    dst[3 * q + 2] = fmaxf(b.z - a.z * a.z * r, 0.f) * k;
+  }
+}
+
+// Per-block sums of the relative L1 error against the checkpoint (AccumBuffer::getError,
+// image/accum_buffer.h:752-795), in a fixed tree order.
+__global__ void __launch_bounds__(256) kFrameError(const float4* __restrict__ acc, const float4* __restrict__ accC,
+                                                   int n, float scale, double* __restrict__ partials)
+{
+  __shared__ double s[256];
+  double e = 0.0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+  {
+    const float4 a = acc[q], c = accC[q];
+    const float ra = rcpSafe(a.w), rc = rcpSafe(c.w);
+    const f3 I = mk(a.x * ra, a.y * ra, a.z * ra) * scale;
+    const f3 B = mk(c.x * rc, c.y * rc, c.z * rc) * scale;
+    float norm = I.x + I.y + I.z;
+    if (norm < 1.f) norm = sqrtf(norm);
+    e += (double)((fabsf(I.x - B.x) + fabsf(I.y - B.y) + fabsf(I.z - B.z)) / (norm + 1e-4f));
+  }
+  s[threadIdx.x] = e;
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1)
+  {
+    if ((int)threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partials[blockIdx.x] = s[0];
 }
 
 // sum * rcpSafe(weight) (image/accum_buffer.h:607-650).
@@ -922,7 +1060,62 @@ cudaError_t launchClear(Context& ctx)
   cudaError_t e = cudaMemsetAsync(ctx.accum, 0, bytes, ctx.stream);
   if (e == cudaSuccess && ctx.accumA) e = cudaMemsetAsync(ctx.accumA, 0, bytes, ctx.stream);
   if (e == cudaSuccess && ctx.accumN) e = cudaMemsetAsync(ctx.accumN, 0, bytes, ctx.stream);
+  if (e == cudaSuccess && ctx.accumC) e = cudaMemsetAsync(ctx.accumC, 0, bytes, ctx.stream);
+  if (e == cudaSuccess && ctx.accum2) e = cudaMemsetAsync(ctx.accum2, 0, bytes, ctx.stream);
+  ctx.accumCount = 0;
   return e;
+}
+
+cudaError_t launchBlitVariance(Context& ctx, float* dst)
+{
+  const int n = ctx.width * ctx.height;
+  kBlitVariance<<<gridFor(ctx, n), 256, 0, ctx.stream>>>(reinterpret_cast<const float4*>(ctx.accum),
+                                                          reinterpret_cast<const float4*>(ctx.accum2), n, dst);
+  return cudaGetLastError();
+}
+
+static ToneMap toneMapOf(const Context& ctx)
+{
+  ToneMap tm;
+  tm.type = ctx.toneType;
+  tm.exposure = ctx.toneExposure;
+  tm.invWhite2 = ctx.toneInvWhite2;
+  return tm;
+}
+
+cudaError_t launchBlitLdr(Context& ctx, uint32_t* dst)
+{
+  const int n = ctx.width * ctx.height;
+  kBlitLdr<<<gridFor(ctx, n), 256, 0, ctx.stream>>>(reinterpret_cast<const float4*>(ctx.accum), n, toneMapOf(ctx), dst);
+  return cudaGetLastError();
+}
+
+cudaError_t launchBlitLdrRgb(Context& ctx, float* dst)
+{
+  const int n = ctx.width * ctx.height;
+  kBlitLdrRgb<<<gridFor(ctx, n), 256, 0, ctx.stream>>>(reinterpret_cast<const float4*>(ctx.accum), n, toneMapOf(ctx),
+                                                        dst);
+  return cudaGetLastError();
+}
+
+cudaError_t frameError(Context& ctx, double& error)
+{
+  const int n = ctx.width * ctx.height;
+  const int blocks = gridFor(ctx, n);
+  // The reference scales by the tone mapper's exposure (Filmic's includes its bias).
+  const float scale = ctx.toneType == PRT_TONE_NONE ? 1.f : ctx.toneExposure;
+  kFrameError<<<blocks, 256, 0, ctx.stream>>>(reinterpret_cast<const float4*>(ctx.accum),
+                                              reinterpret_cast<const float4*>(ctx.accumC), n, scale, ctx.errPartials);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  std::vector<double> part(blocks);
+  e = cudaMemcpyAsync(part.data(), ctx.errPartials, sizeof(double) * blocks, cudaMemcpyDeviceToHost, ctx.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx.stream);
+  if (e != cudaSuccess) return e;
+  double sum = 0.0;
+  for (double v : part) sum += v;
+  error = sum / (double)n;
+  return cudaSuccess;
 }
 
 using ShadeClassList = ShadeLaunch<PRT_SHADE_CLASS_LIST>;
@@ -1122,9 +1315,11 @@ cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
       e = cudaGetLastError();
     }
     if (e != cudaSuccess) return e;
-    kAccumulate<<<gridFor(ctx, pixelCount), 256, 0, ctx.stream>>>(L, reinterpret_cast<float4*>(ctx.accum),
-                                                                   reinterpret_cast<float4*>(ctx.accumA),
-                                                                   reinterpret_cast<float4*>(ctx.accumN));
+    kAccumulate<<<gridFor(ctx, pixelCount), 256, 0, ctx.stream>>>(
+      L, reinterpret_cast<float4*>(ctx.accum), reinterpret_cast<float4*>(ctx.accumA),
+      reinterpret_cast<float4*>(ctx.accumN), reinterpret_cast<float4*>(ctx.accumC),
+      reinterpret_cast<float4*>(ctx.accum2), (long long)ctx.accumCount);
+    ctx.accumCount += S;
     rc.launches++;
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;

@@ -121,6 +121,12 @@ struct Context
   float* accum = nullptr;         // sum rgb + weight per pixel (float4)
   float* accumA = nullptr;        // first-hit albedo sums
   float* accumN = nullptr;        // first-hit normal sums
+  float* accumC = nullptr;        // checkpoint: the sums at the last power-of-two sample count
+  float* accum2 = nullptr;        // squared samples (PRT_AOV_HDR_VAR)
+  double* errPartials = nullptr;  // per-block partial sums of the frame error
+  int64_t accumCount = 0;         // samples accumulated since the last clear
+  int toneType = 0;               // PRT_TONE_*
+  float toneExposure = 1.f, toneInvWhite2 = 0.f;
   uint32_t sampleIndex = 0;
   PathState ps;
   int waveSamples = 0;            // samples per pixel per wave
@@ -160,6 +166,12 @@ cudaError_t renderBatch(Context& ctx, BatchState& b, RenderCounters& rc);
 // gradients into the targets of its BatchItem::adj (set on the device before the call).
 cudaError_t replayBatch(Context& ctx, BatchState& b, RenderCounters& rc);
 cudaError_t launchBlitPlane(Context& ctx, const float4* plane, int n, float* dst);
+// PRT_BLIT_HDR_VAR and PRT_BLIT_LDR (film post-step).
+cudaError_t launchBlitVariance(Context& ctx, float* dst);
+cudaError_t launchBlitLdr(Context& ctx, uint32_t* dst);
+cudaError_t launchBlitLdrRgb(Context& ctx, float* dst);
+// Frame error against the checkpoint (Device::getFrameError).
+cudaError_t frameError(Context& ctx, double& error);
 // Path-replay adjoint (adjoint.cu): dLoss/d(texel) of every scene texture and dLoss/d(specular
 // roughness) of every material for the image gradient dLdI (W*H*3, device memory).
 cudaError_t launchAdjoint(Context& ctx, uint32_t firstSample, int spp, const float* dLdI, float* gradTex,

@@ -55,6 +55,8 @@ def load_library():
     lib.prt_cuda_clear.argtypes = [vp]
     lib.prt_cuda_render.argtypes = [vp, C.c_int32, P(T.RenderStats)]
     lib.prt_cuda_set_profiling.argtypes = [vp, C.c_int32]
+    lib.prt_cuda_tone_mapper.argtypes = [vp, C.c_int32, C.c_float, C.c_float]
+    lib.prt_cuda_frame_error.argtypes = [vp, P(C.c_float)]
     lib.prt_cuda_set_tuning.argtypes = [vp, P(T.Tuning)]
     lib.prt_cuda_adjoint.argtypes = [vp, C.c_uint32, C.c_int32, vp, vp, C.c_int64, vp, C.c_int32, P(T.RenderStats)]
     lib.prt_cuda_update_texture.argtypes = [vp, C.c_int32, vp]
@@ -232,8 +234,21 @@ class DeviceCuda:
     def set_profiling(self, flags):
         self._check(self.lib.prt_cuda_set_profiling(self.h, flags))
 
+    def tone_mapper(self, kind, exposure=1.0, burn=0.0):
+        self._check(self.lib.prt_cuda_tone_mapper(self.h, kind, exposure, burn))
+
+    def frame_error(self):
+        e = C.c_float()
+        self._check(self.lib.prt_cuda_frame_error(self.h, C.byref(e)))
+        return e.value
+
     def blit_frame(self, aov=T.PRT_BLIT_HDR, out=None):
-        """Returns (height, width, 3) float32; `out` may be a CUDA torch tensor (zero copy)."""
+        """Returns (height, width, 3) float32 ((height, width) uint32 for PRT_BLIT_LDR); `out` may
+        be a CUDA torch tensor (zero copy)."""
+        if aov == T.PRT_BLIT_LDR and out is None:
+            ldr = np.zeros((self.height, self.width), np.uint32)
+            self._check(self.lib.prt_cuda_blit(self.h, aov, ldr.ctypes.data_as(C.POINTER(C.c_float))))
+            return ldr
         if out is not None and hasattr(out, "data_ptr"):
             self._check(self.lib.prt_cuda_blit(self.h, aov, C.cast(C.c_void_p(out.data_ptr()), C.POINTER(C.c_float))))
             return out

@@ -18,10 +18,20 @@ PRT_ERR_STATE = -6
 
 PRT_AOV_ALBEDO1 = 1 << 0
 PRT_AOV_NORMAL1 = 1 << 1
+PRT_AOV_HDR_VAR = 1 << 2
 
 PRT_BLIT_HDR = 0
 PRT_BLIT_ALBEDO1 = 1
 PRT_BLIT_NORMAL1 = 2
+PRT_BLIT_HDR_VAR = 3
+PRT_BLIT_LDR = 4
+PRT_BLIT_LDR_RGB = 5
+PRT_TONE_NONE = 0
+PRT_TONE_LINEAR = 1
+PRT_TONE_REINHARD = 2
+PRT_TONE_ACES = 3
+PRT_TONE_FILMIC = 4
+PRT_TONE_LOG = 5
 
 F3 = C.c_float * 3
 

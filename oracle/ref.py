@@ -163,9 +163,23 @@ class RefDevice:
         return dict(rays=st[0], seconds=st[1])
 
     def blit(self, aov=T.PRT_BLIT_HDR):
+        if aov == T.PRT_BLIT_LDR:
+            out = np.zeros((self.scene.height, self.scene.width), np.uint32)
+            _check(_lib().ref_blit(self.h, aov, out.ctypes.data_as(C.POINTER(C.c_float))))
+            return out
         out = np.zeros((self.scene.height, self.scene.width, 3), np.float32)
         _check(_lib().ref_blit(self.h, aov, T.fptr(out)))
         return out
+
+    def tone_mapper(self, kind, exposure=1.0, burn=0.0):
+        _lib().ref_tone_mapper.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_float]
+        _check(_lib().ref_tone_mapper(self.h, kind, exposure, burn))
+
+    def frame_error(self):
+        e = C.c_float()
+        _lib().ref_frame_error.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
+        _check(_lib().ref_frame_error(self.h, C.byref(e)))
+        return e.value
 
     def trace(self, rays):
         rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)

@@ -16,6 +16,7 @@
 
 #include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <filesystem>
 #include <memory>
@@ -33,6 +34,7 @@
 #include "sampling/sobol_burley_sampler_simd.h"
 #include "image/image_io.h"
 #include "image/morton.h"
+#include "image/surface.h"
 #include "bsdf/albedo_tables.h"
 #include "accel/embree_intersector_stream.h"
 #include "render/integrator.h"
@@ -224,6 +226,7 @@ int ref_create(const prt_scene_desc* scene, const prt_camera_desc* cam, const pr
     Props frameProps;
     if (aov_mask & PRT_AOV_ALBEDO1) frameProps.set("aovAlbedo1");
     if (aov_mask & PRT_AOV_NORMAL1) frameProps.set("aovNormal1");
+    if (aov_mask & PRT_AOV_HDR_VAR) frameProps.set("aovHdrVar");
     h->size = Vec2i(width, height);
     h->device.initFrame(h->size, frameProps);
     Props rprops;
@@ -307,9 +310,27 @@ int ref_blit(void* handle, int aov, float* dst)
   {
     auto h = (RefHandle*)handle;
     FrameAovs aovs;
+    std::vector<Vec3f> hdr((size_t)h->size.x * h->size.y);
+    if (aov == PRT_BLIT_LDR)
+    {
+      // blitLdr stores whole SIMD vectors: give it a 64-byte aligned surface.
+      const size_t bytes = (size_t)h->size.x * h->size.y * sizeof(int);
+      void* aligned = std::aligned_alloc(64, (bytes + 63) / 64 * 64);
+      Surface surface{aligned, h->size.x, h->size.y, (int)(h->size.x * sizeof(int))};
+      h->device.blitFrame(surface);
+      std::memcpy(dst, aligned, bytes);
+      std::free(aligned);
+      return 0;
+    }
     if (aov == PRT_BLIT_HDR) aovs.hdr = (Vec3f*)dst;
     else if (aov == PRT_BLIT_ALBEDO1) aovs.albedo1 = (Vec3f*)dst;
     else if (aov == PRT_BLIT_NORMAL1) aovs.normal1 = (Vec3f*)dst;
+    else if (aov == PRT_BLIT_HDR_VAR)
+    {
+      aovs.hdr = hdr.data();
+      aovs.hdrVar = (Vec3f*)dst;
+    }
+    else if (aov == PRT_BLIT_LDR_RGB) aovs.ldr = (Vec3f*)dst;
     else return fail("invalid aov");
     h->device.blitFrame(aovs);
     return 0;
@@ -479,6 +500,39 @@ int ref_query_primary(void* handle, uint32_t sampleIndex, float* raysOut, int32_
       }
     }
     return ref_trace(handle, (int64_t)W * H, raysOut, geomId, primId, t, nullptr, nullptr);
+  }
+  catch (const std::exception& e)
+  {
+    return fail(e.what());
+  }
+}
+
+int ref_tone_mapper(void* handle, int type, float exposure, float burn)
+{
+  auto* h = static_cast<RefHandle*>(handle);
+  try
+  {
+    static const char* kTypes[] = {"none", "linear", "reinhard", "aces", "filmic", "log"};
+    Props p;
+    p.set("type", std::string(kTypes[(type >= 0 && type <= 5) ? type : 0]));
+    p.set("exposure", exposure);
+    p.set("burn", burn);
+    h->device.initToneMapper(p);
+    return 0;
+  }
+  catch (const std::exception& e)
+  {
+    return fail(e.what());
+  }
+}
+
+int ref_frame_error(void* handle, float* error)
+{
+  auto* h = static_cast<RefHandle*>(handle);
+  try
+  {
+    *error = h->device.getFrameError();
+    return 0;
   }
   catch (const std::exception& e)
   {

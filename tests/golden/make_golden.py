@@ -18,6 +18,7 @@ Fixtures (small, seeded, committed):
                    kinds, sun-sky) at 128x64: 16 spp and 256 spp, seeds 0 and 1
   lobes_img.npz    the small scene with Oren-Nayar, sheen and layered spheres, 16 spp, seeds 0, 1
   siblings_img.npz primaryStream, aoStream, diffuseStream, diffuse2Stream renders of the small scene
+  film.npz         sample variance, tone-mapped LDR images and frame errors of the small scene
   bsdf.npz         the reference's Standard-material BSDF (eval, sample) on 512 seeded tuples
                    for each case of tests/bsdf_cases.py
   sunsky_t3_e30.npz the reference's sun-sky products (sun radiance and angle, 512x256 sky) for
@@ -33,6 +34,7 @@ ROOT = pathlib.Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT / "oidn-protoray_b200"))
 sys.path.insert(0, str(ROOT / "oracle"))
 import prt_scenes  # noqa: E402
+import prt_types as T  # noqa: E402
 import ref  # noqa: E402
 
 OUT = pathlib.Path(__file__).resolve().parent
@@ -134,6 +136,27 @@ def make_sibling_images():
     np.savez_compressed(OUT / "siblings_img.npz", **out)
 
 
+TONES = [(0, 1.0, 0.0), (1, 1.5, 0.0), (2, 1.0, 0.3), (3, 1.2, 0.0), (4, 0.8, 0.0), (5, 2.0, 0.0)]
+
+
+def make_film():
+    """Film post-step of the small scene (64x64, 5 one-sample renders, variance on): the HDR
+    image and its sample variance, and per tone mapper the 8-bit and float LDR images and the
+    frame error against the checkpoint."""
+    s = prt_scenes.cornell(seed=0, width=64, height=64, spp=1)
+    dev = ref.RefDevice(s, seed=0, aov_mask=T.PRT_AOV_HDR_VAR)
+    for _ in range(5):
+        dev.render(1)
+    out = {"hdr": dev.blit(T.PRT_BLIT_HDR), "var": dev.blit(T.PRT_BLIT_HDR_VAR)}
+    for kind, exposure, burn in TONES:
+        dev.tone_mapper(kind, exposure, burn)
+        out[f"ldr{kind}"] = dev.blit(T.PRT_BLIT_LDR)
+        out[f"ldrrgb{kind}"] = dev.blit(T.PRT_BLIT_LDR_RGB)
+        out[f"error{kind}"] = np.float64(dev.frame_error())
+    dev.close()
+    np.savez_compressed(OUT / "film.npz", **out)
+
+
 def make_bsdf():
     sys.path.insert(0, str(ROOT / "tests"))
     import bsdf_cases
@@ -168,7 +191,7 @@ def make_sunsky():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["sobol", "rays", "images", "sunsky", "bsdf", "terrain", "lobes", "siblings"]
+    which = sys.argv[1:] or ["sobol", "rays", "images", "sunsky", "bsdf", "terrain", "lobes", "siblings", "film"]
     if "terrain" in which:
         make_terrain_images()
     if "bsdf" in which:
@@ -177,6 +200,8 @@ if __name__ == "__main__":
         make_lobe_images()
     if "siblings" in which:
         make_sibling_images()
+    if "film" in which:
+        make_film()
     if "sunsky" in which:
         make_sunsky()
     if "sobol" in which:
