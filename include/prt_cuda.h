@@ -136,9 +136,19 @@ typedef struct prt_scene_desc
   const prt_material* materials;
   const prt_texture*  textures;
   int32_t             texture_count;
-  int32_t             reserved;
+  int32_t             bvh_build;   /* PRT_BVH_HOST (0) or PRT_BVH_DEVICE (1) */
   prt_env_desc        env;
 } prt_scene_desc;
+
+/* BVH8 builders. The reference builds with Embree (accel/embree_intersector.cpp:68-90). Both
+ * builders emit the same compressed 8-wide format, so every ray finds the same closest hit and
+ * every image is the same whichever built the tree; they differ in build time and tree quality.
+ *   PRT_BVH_HOST:   binned-SAH binary build on the host threads, collapsed to 8-wide nodes;
+ *   PRT_BVH_DEVICE: on the GPU from the triangles in HBM: Morton sort, PLOC clustering
+ *                   (nearest neighbours within 16 positions of the Morton order), the same
+ *                   8-wide collapse. Deterministic: the same scene gives the same bytes. */
+#define PRT_BVH_HOST   0
+#define PRT_BVH_DEVICE 1
 
 /* Pinhole camera (camera/pinhole_camera.h:20-59). The basis is (U right, V up, N back):
  * the view direction is -N. fov is the vertical field of view in radians. */
@@ -246,8 +256,30 @@ void prt_cuda_principled_defaults(prt_material* m);
 /* ---- scene, renderer, camera, frame ----------------------------------------------------- */
 
 /* Device::initScene + initLights (render/device_cpu.cpp:96-107): copies the scene to HBM,
- * builds the BVH8 on the host and derives area lights and the light-pick distribution. */
+ * builds the BVH8 (on the host or the device, as scene->bvh_build says) and derives area
+ * lights and the light-pick distribution. */
 int prt_cuda_scene_upload(prt_context* ctx, const prt_scene_desc* scene);
+
+/* The uploaded scene's acceleration structure; the reference reports the build as
+ * buildMs / buildMprim (accel/embree_intersector.cpp:88-90). */
+typedef struct prt_scene_stats
+{
+  double  build_ms;     /* BVH build wall time (the device build includes its launches and waits) */
+  int64_t node_count;   /* 80-byte wide nodes */
+  int64_t tri_count;    /* 48-byte triangle records */
+  int32_t builder;      /* PRT_BVH_HOST or PRT_BVH_DEVICE */
+  int32_t depth;        /* wide levels */
+  int32_t top_count;    /* nodes of the first three levels, stored first */
+  int32_t iterations;   /* device build: clustering iterations; host build: 0 */
+} prt_scene_stats;
+
+int prt_cuda_scene_stats(prt_context* ctx, prt_scene_stats* out);
+
+/* Copies the uploaded scene's BVH8 to host memory: min(node_capacity, node_count) 80-byte
+ * nodes and min(tri_capacity, tri_count) 48-byte triangle records (bvh8.h layout; either
+ * pointer may be NULL with capacity 0 to query the counts, written to *node_count / *tri_count). */
+int prt_cuda_scene_bvh(prt_context* ctx, void* nodes, int64_t node_capacity, void* tris, int64_t tri_capacity,
+                       int64_t* node_count, int64_t* tri_count);
 
 /* Device::initRenderer (render/device_cpu.cpp:32-46) for type "pathStream", sampler "sobolBurley". */
 int prt_cuda_renderer(prt_context* ctx, const prt_renderer_desc* renderer);
@@ -448,6 +480,28 @@ int prt_cuda_albedo_tables(prt_context* ctx, float* out, int64_t capacity, int64
  * nodes/prims per-ray statistic (render/path_renderer_stream.h:180-184). */
 int prt_bvh8_count(const float* tri_verts, int64_t tri_count, int64_t n, const float* rays, int32_t* tri_out,
                    float* t_out, int64_t* node_visits, int64_t* tri_tests, int64_t* node_count);
+
+/* Host-only (no GPU needed): checks a BVH8 given as arrays (bvh8.h layout) over tri_count
+ * triangles (tri_verts: 9 floats each, v0 v1 v2): every node reached once from the root, child
+ * and triangle indices in range, every triangle stored once with v0 and the single-precision
+ * edges v1 - v0 and v2 - v0, every 8-bit child box containing its subtree's triangles (as
+ * dequantised in single precision), the first top_count nodes exactly the first three levels,
+ * and the depth within the traversal stack. Writes the depth (wide levels) to *depth when not
+ * NULL. Returns PRT_OK, or PRT_ERR_INVALID_ARG with the first violation in msg. */
+int prt_bvh8_check(const void* nodes, int64_t node_count, const void* tris, int64_t tri_count,
+                   const float* tri_verts, int32_t top_count, int32_t* depth, char* msg, int32_t msg_capacity);
+
+/* Host-only: the PRT_BVH_HOST build (binned SAH, 8-wide collapse) into caller arrays of at
+ * least max(tri_count, 1) nodes and tri_count triangle records; writes the node count and the
+ * top-level node count. */
+int prt_bvh8_build_host(const float* tri_verts, int64_t tri_count, void* nodes, int64_t node_capacity, void* tris,
+                        int64_t tri_capacity, int64_t* node_count, int32_t* top_count);
+
+/* Host-only: the counting traversal of prt_bvh8_count over a BVH8 given as arrays that pass
+ * prt_bvh8_check (for instance one built on the device and copied back with
+ * prt_cuda_scene_bvh). */
+int prt_bvh8_trace(const void* nodes, int64_t node_count, const void* tris, int64_t tri_count, int64_t n,
+                   const float* rays, int32_t* tri_out, float* t_out, int64_t* node_visits, int64_t* tri_tests);
 
 #ifdef __cplusplus
 }

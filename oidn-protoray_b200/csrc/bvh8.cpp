@@ -492,6 +492,12 @@ inline float expScale(uint8_t e)
 int bvh8TraceCount(const Bvh8& bvh, const float org[3], const float dir[3], float tnear, float& tfar,
                    int64_t& nodeVisits, int64_t& triTests)
 {
+  return bvh8TraceCount(bvh.nodes.data(), bvh.tris.data(), org, dir, tnear, tfar, nodeVisits, triTests);
+}
+
+int bvh8TraceCount(const Bvh8Node* nodes, const Bvh8Tri* tris, const float org[3], const float dir[3], float tnear,
+                   float& tfar, int64_t& nodeVisits, int64_t& triTests)
+{
   float inv[3];
   for (int k = 0; k < 3; ++k)
   {
@@ -507,7 +513,7 @@ int bvh8TraceCount(const Bvh8& bvh, const float org[3], const float dir[3], floa
   float bestT = tfar;
   while (!stack.empty())
   {
-    const Bvh8Node& n = bvh.nodes[stack.back()];
+    const Bvh8Node& n = nodes[stack.back()];
     stack.pop_back();
     nodeVisits++;
     const float sx = expScale(n.ex), sy = expScale(n.ey), sz = expScale(n.ez);
@@ -544,7 +550,7 @@ int bvh8TraceCount(const Bvh8& bvh, const float org[3], const float dir[3], floa
       const int cnt = n.meta[s] >> 5, off = n.meta[s] & 31;
       for (int j = 0; j < cnt; ++j)
       {
-        const Bvh8Tri& t = bvh.tris[n.triBase + off + j];
+        const Bvh8Tri& t = tris[n.triBase + off + j];
         triTests++;
         float tt, uu, vv;
         if (triTest(t, org, dir, tnear, bestT, tt, uu, vv))
@@ -560,6 +566,126 @@ int bvh8TraceCount(const Bvh8& bvh, const float org[3], const float dir[3], floa
   }
   if (best >= 0) tfar = bestT;
   return best;
+}
+
+// ---- structural check -----------------------------------------------------------------------
+
+std::string bvh8Check(const Bvh8Node* nodes, int64_t nodeCount, const Bvh8Tri* tris, int64_t triCount,
+                      const float* triVerts, int topCount, int& depth)
+{
+  depth = 0;
+  if (nodeCount < 1 || !nodes) return "no nodes";
+  if (triCount < 0 || (triCount > 0 && (!tris || !triVerts))) return "invalid triangle arrays";
+  auto at = [](const char* what, int64_t i) { return std::string(what) + " (node " + std::to_string(i) + ")"; };
+  // Breadth-first walk from the root: every node reached once, indices in range.
+  std::vector<int> level(nodeCount, 0);
+  std::vector<uint8_t> recSeen(triCount, 0);
+  std::vector<int64_t> order;
+  order.reserve(nodeCount);
+  order.push_back(0);
+  level[0] = 1;
+  for (size_t q = 0; q < order.size(); ++q)
+  {
+    const int64_t i = order[q];
+    const Bvh8Node& n = nodes[i];
+    depth = std::max(depth, level[i]);
+    int inner = 0;
+    for (int s = 0; s < 8; ++s)
+    {
+      if (n.imask & (1u << s))
+      {
+        if (n.meta[s] != 0) return at("inner slot with leaf metadata", i);
+        const int64_t c = (int64_t)n.childBase + inner++;
+        if (c >= nodeCount || c <= 0) return at("child index out of range", i);
+        if (level[c] != 0) return at("node reached twice", c);
+        level[c] = level[i] + 1;
+        order.push_back(c);
+      }
+      else if (n.meta[s] != 0)
+      {
+        const int cnt = n.meta[s] >> 5, off = n.meta[s] & 31;
+        if (cnt < 1 || cnt > 3 || off + cnt > 24) return at("bad leaf metadata", i);
+        for (int j = 0; j < cnt; ++j)
+        {
+          const int64_t r = (int64_t)n.triBase + off + j;
+          if (r >= triCount) return at("triangle index out of range", i);
+          if (recSeen[r]) return at("triangle record referenced twice", i);
+          recSeen[r] = 1;
+        }
+      }
+    }
+  }
+  if (depth > kBvh8TraceStack) return "tree deeper than the traversal stack (" + std::to_string(depth) + " levels)";
+  if ((int64_t)order.size() != nodeCount) return "unreachable nodes";
+  // Triangle records: every record referenced, every triangle stored once, exact vertex data.
+  std::vector<uint8_t> idSeen(triCount, 0);
+  auto same = [](float a, float b) { return std::memcmp(&a, &b, 4) == 0; };
+  for (int64_t r = 0; r < triCount; ++r)
+  {
+    if (!recSeen[r]) return "triangle record " + std::to_string(r) + " never referenced";
+    const Bvh8Tri& t = tris[r];
+    if (t.triId < 0 || t.triId >= triCount) return "triangle id out of range (record " + std::to_string(r) + ")";
+    if (idSeen[t.triId]) return "triangle " + std::to_string(t.triId) + " stored twice";
+    idSeen[t.triId] = 1;
+    const float* v = triVerts + 9 * (size_t)t.triId;
+    const float e1[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]}, e2[3] = {v[6] - v[0], v[7] - v[1], v[8] - v[2]};
+    if (!same(t.v0x, v[0]) || !same(t.v0y, v[1]) || !same(t.v0z, v[2]) || !same(t.e1x, e1[0]) ||
+        !same(t.e1y, e1[1]) || !same(t.e1z, e1[2]) || !same(t.e2x, e2[0]) || !same(t.e2y, e2[1]) ||
+        !same(t.e2z, e2[2]))
+      return "triangle " + std::to_string(t.triId) + " has wrong vertex data";
+  }
+  // Containment, children before parents: each slot's 8-bit box, dequantised in single
+  // precision, holds the boxes of the triangles below it (reconstructed vertices).
+  std::vector<Box> content(nodeCount);
+  for (size_t q = order.size(); q-- > 0;)
+  {
+    const int64_t i = order[q];
+    const Bvh8Node& n = nodes[i];
+    const float p[3] = {n.px, n.py, n.pz};
+    const uint8_t e[3] = {n.ex, n.ey, n.ez};
+    const uint8_t* qlo[3] = {n.qlox, n.qloy, n.qloz};
+    const uint8_t* qhi[3] = {n.qhix, n.qhiy, n.qhiz};
+    Box all;
+    all.reset();
+    int inner = 0;
+    for (int s = 0; s < 8; ++s)
+    {
+      Box b;
+      b.reset();
+      if (n.imask & (1u << s))
+        b = content[n.childBase + inner++];
+      else if (n.meta[s] != 0)
+        for (int j = 0; j < (n.meta[s] >> 5); ++j)
+        {
+          const Bvh8Tri& t = tris[n.triBase + (n.meta[s] & 31) + j];
+          const float v0[3] = {t.v0x, t.v0y, t.v0z}, a[3] = {t.e1x, t.e1y, t.e1z}, c[3] = {t.e2x, t.e2y, t.e2z};
+          for (int k = 0; k < 3; ++k)
+          {
+            const float x1 = v0[k] + a[k], x2 = v0[k] + c[k];
+            const float* v = triVerts + 9 * (size_t)t.triId;
+            b.lo[k] = std::min(b.lo[k], std::min(std::min(v0[k], x1), std::min(x2, std::min(v[3 + k], v[6 + k]))));
+            b.hi[k] = std::max(b.hi[k], std::max(std::max(v0[k], x1), std::max(x2, std::max(v[3 + k], v[6 + k]))));
+          }
+        }
+      else
+        continue;
+      for (int k = 0; k < 3; ++k)
+      {
+        const float fs = (float)std::ldexp(1.0, (int)e[k] - 127);
+        const float lo = p[k] + (float)qlo[k][s] * fs, hi = p[k] + (float)qhi[k][s] * fs;
+        if (qlo[k][s] > qhi[k][s] || lo > b.lo[k] || hi < b.hi[k])
+          return at("child box does not contain its subtree", i) + " slot " + std::to_string(s) + " axis " +
+                 std::to_string(k);
+      }
+      all.grow(b);
+    }
+    content[i] = all;
+  }
+  // The first topCount nodes are exactly the first kBvh8TopLevels levels.
+  if (topCount < 1 || topCount > kBvh8TopNodes || topCount > nodeCount) return "top count out of range";
+  for (int64_t i = 0; i < nodeCount; ++i)
+    if ((level[i] <= kBvh8TopLevels) != (i < topCount)) return at("top levels not stored first", i);
+  return std::string();
 }
 
 } // namespace prt

@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 #include <vector>
 
 namespace prt {
@@ -44,6 +45,10 @@ static_assert(sizeof(Bvh8Tri) == 48, "Bvh8Tri must be 48 bytes");
 constexpr int kBvh8TopLevels = 3;
 constexpr int kBvh8TopNodes = 73;
 
+// Node-group stack entries of the traversal kernels. A ray holds at most one group per level
+// above the node it visits, so a tree of at most kBvh8TraceStack wide levels never overflows.
+constexpr int kBvh8TraceStack = 48;
+
 struct Bvh8
 {
   std::vector<Bvh8Node> nodes;
@@ -64,5 +69,13 @@ void buildBvh8(const float* triVerts, int64_t triCount, Bvh8& out, int threads =
 // triangles tested. Used to state the algorithmic bytes per ray.
 int bvh8TraceCount(const Bvh8& bvh, const float org[3], const float dir[3], float tnear, float& tfar,
                    int64_t& nodeVisits, int64_t& triTests);
+int bvh8TraceCount(const Bvh8Node* nodes, const Bvh8Tri* tris, const float org[3], const float dir[3], float tnear,
+                   float& tfar, int64_t& nodeVisits, int64_t& triTests);
+
+// Structural check of a BVH8 given as arrays over triCount triangles (9 floats each): see
+// prt_bvh8_check. Returns an empty string when the tree is valid, else the first violation;
+// depth receives the number of wide levels.
+std::string bvh8Check(const Bvh8Node* nodes, int64_t nodeCount, const Bvh8Tri* tris, int64_t triCount,
+                      const float* triVerts, int topCount, int& depth);
 
 } // namespace prt

@@ -3,6 +3,7 @@
 // This is the CUDA sibling of the reference's DeviceCpu (render/device_cpu.cpp).
 #include "../../include/prt_cuda.h"
 #include "runtime.h"
+#include "bvh_build.h"
 
 #include <algorithm>
 #include <cfloat>
@@ -266,6 +267,9 @@ void uploadScene(Context& c, const prt_scene_desc* s)
 {
   if (!s || s->mesh_count < 0 || s->material_count <= 0 || !s->materials)
     throw std::invalid_argument("invalid scene description");
+  if (s->bvh_build != PRT_BVH_HOST && s->bvh_build != PRT_BVH_DEVICE)
+    throw std::invalid_argument("unknown BVH builder");
+  const bool hostBuild = s->bvh_build == PRT_BVH_HOST;
   freeScene(c);
   DevScene sc;
   std::memset(&sc, 0, sizeof(sc));
@@ -313,7 +317,7 @@ void uploadScene(Context& c, const prt_scene_desc* s)
   if (anyN) nrm.assign(totalVerts, make_float4(0.f, 0.f, 1.f, 0.f));
   if (anyUV) uv.assign(totalVerts, make_float2(0.f, 0.f));
   std::vector<int4> triVerts(totalTris);
-  std::vector<float> triPos((size_t)totalTris * 9);
+  std::vector<float> triPos(hostBuild ? (size_t)totalTris * 9 : 0);
   std::vector<int> meshFlags(s->mesh_count), meshMat(s->mesh_count), meshOff(s->mesh_count), meshLight(s->mesh_count, -1);
   float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
   int64_t vbase = 0, tbase = 0;
@@ -338,13 +342,14 @@ void uploadScene(Context& c, const prt_scene_desc* s)
         if (idx[k] < 0 || idx[k] >= m.vertex_count) throw std::invalid_argument("triangle index out of range");
       }
       triVerts[tbase + t] = make_int4((int)(vbase + idx[0]), (int)(vbase + idx[1]), (int)(vbase + idx[2]), g);
-      float* tp = &triPos[(size_t)(tbase + t) * 9];
+      float* tp = hostBuild ? &triPos[(size_t)(tbase + t) * 9] : nullptr;
       for (int k = 0; k < 3; ++k)
         for (int a = 0; a < 3; ++a)
         {
-          tp[3 * k + a] = m.positions[3 * idx[k] + a];
-          lo[a] = std::min(lo[a], tp[3 * k + a]);
-          hi[a] = std::max(hi[a], tp[3 * k + a]);
+          const float x = m.positions[3 * idx[k] + a];
+          if (tp) tp[3 * k + a] = x;
+          lo[a] = std::min(lo[a], x);
+          hi[a] = std::max(hi[a], x);
         }
     }
     vbase += m.vertex_count;
@@ -352,14 +357,41 @@ void uploadScene(Context& c, const prt_scene_desc* s)
   }
   if (totalTris == 0)
     for (int a = 0; a < 3; ++a) lo[a] = hi[a] = 0.f;
-  // BVH8
-  buildBvh8(triPos.data(), totalTris, c.bvh);
-  sc.nodes = reinterpret_cast<const uint4*>(upload(c, c.bvh.nodes));
-  sc.tris = reinterpret_cast<const float4*>(upload(c, c.bvh.tris));
-  sc.topNodes = std::min(c.bvh.topCount, kBvh8TopNodes);
   sc.triCount = totalTris;
   sc.triVerts = upload(c, triVerts);
   sc.pos = upload(c, pos);
+  // BVH8, on the host or on the device from the vertex and index arrays just uploaded.
+  c.bvh = Bvh8();
+  c.bvhBuilder = s->bvh_build;
+  if (hostBuild)
+  {
+    buildBvh8(triPos.data(), totalTris, c.bvh);
+    sc.nodes = reinterpret_cast<const uint4*>(upload(c, c.bvh.nodes));
+    sc.tris = reinterpret_cast<const float4*>(upload(c, c.bvh.tris));
+    c.bvhBuildMs = c.bvh.buildMs;
+    c.bvhNodes = (int64_t)c.bvh.nodes.size();
+    c.bvhTris = (int64_t)c.bvh.tris.size();
+    c.bvhDepth = c.bvh.maxDepth;
+    c.bvhTop = std::min(c.bvh.topCount, kBvh8TopNodes);
+    c.bvhIterations = 0;
+  }
+  else
+  {
+    DeviceBvh8 db;
+    buildBvh8Device(sc.pos, sc.triVerts, totalTris, c.stream, db);
+    c.sceneBufs.push_back(DevBuf{db.nodes, sizeof(Bvh8Node) * (size_t)db.nodeCount});
+    c.sceneBufs.push_back(DevBuf{db.tris, sizeof(Bvh8Tri) * (size_t)std::max<int64_t>(db.triCount, 1)});
+    sc.nodes = reinterpret_cast<const uint4*>(db.nodes);
+    sc.tris = reinterpret_cast<const float4*>(db.tris);
+    c.bvhBuildMs = db.buildMs;
+    c.bvhNodes = db.nodeCount;
+    c.bvhTris = db.triCount;
+    c.bvhDepth = db.maxDepth;
+    c.bvhTop = db.topCount;
+    c.bvhIterations = db.plocIterations;
+  }
+  if (c.bvhDepth > kBvh8TraceStack) throw std::runtime_error("BVH8 deeper than the traversal stack");
+  sc.topNodes = c.bvhTop;
   sc.nrm = anyN ? upload(c, nrm) : nullptr;
   sc.uv = anyUV ? upload(c, uv) : nullptr;
   sc.meshFlags = upload(c, meshFlags);
@@ -389,7 +421,9 @@ void uploadScene(Context& c, const prt_scene_desc* s)
     float sumL = 0.f;
     for (int t = 0; t < m.tri_count; ++t)
     {
-      const float* tp = &triPos[(size_t)(meshOff[g] + t) * 9];
+      float tp[9];
+      for (int k = 0; k < 3; ++k)
+        for (int a = 0; a < 3; ++a) tp[3 * k + a] = m.positions[3 * m.indices[3 * t + k] + a];
       const float e1[3] = {tp[3] - tp[0], tp[4] - tp[1], tp[5] - tp[2]};
       const float e2[3] = {tp[6] - tp[0], tp[7] - tp[1], tp[8] - tp[2]};
       const float n[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
@@ -905,6 +939,42 @@ int prt_cuda_frame_error(prt_context* ctx, float* error)
   });
 }
 
+int prt_cuda_scene_stats(prt_context* ctx, prt_scene_stats* out)
+{
+  return guarded(ctx, [&](Context& c) {
+    if (!out) throw std::invalid_argument("null output");
+    if (!c.hasScene) throw ApiError{PRT_ERR_STATE, "no scene"};
+    out->build_ms = c.bvhBuildMs;
+    out->node_count = c.bvhNodes;
+    out->tri_count = c.bvhTris;
+    out->builder = c.bvhBuilder;
+    out->depth = c.bvhDepth;
+    out->top_count = c.bvhTop;
+    out->iterations = c.bvhIterations;
+  });
+}
+
+int prt_cuda_scene_bvh(prt_context* ctx, void* nodes, int64_t node_capacity, void* tris, int64_t tri_capacity,
+                       int64_t* node_count, int64_t* tri_count)
+{
+  return guarded(ctx, [&](Context& c) {
+    if (node_capacity < 0 || tri_capacity < 0 || (node_capacity > 0 && !nodes) || (tri_capacity > 0 && !tris))
+      throw std::invalid_argument("invalid output arrays");
+    if (!c.hasScene) throw ApiError{PRT_ERR_STATE, "no scene"};
+    cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+    const int64_t nn = std::min(node_capacity, c.bvhNodes), nt = std::min(tri_capacity, c.bvhTris);
+    if (nn > 0)
+      cuCheck(cudaMemcpyAsync(nodes, c.scene.nodes, sizeof(Bvh8Node) * (size_t)nn, cudaMemcpyDeviceToHost, c.stream),
+              "copy nodes");
+    if (nt > 0)
+      cuCheck(cudaMemcpyAsync(tris, c.scene.tris, sizeof(Bvh8Tri) * (size_t)nt, cudaMemcpyDeviceToHost, c.stream),
+              "copy triangles");
+    cuCheck(cudaStreamSynchronize(c.stream), "copy BVH");
+    if (node_count) *node_count = c.bvhNodes;
+    if (tri_count) *tri_count = c.bvhTris;
+  });
+}
+
 int prt_cuda_sobol(prt_context* ctx, int64_t n, const uint32_t* sample_index, const uint32_t* pixel_id,
                    const uint32_t* dim_set, int32_t dims, float* out)
 {
@@ -1035,6 +1105,79 @@ int prt_bvh8_count(const float* tri_verts, int64_t tri_count, int64_t n, const f
   {
     return PRT_ERR_LOGIC;
   }
+}
+
+int prt_bvh8_check(const void* nodes, int64_t node_count, const void* tris, int64_t tri_count,
+                   const float* tri_verts, int32_t top_count, int32_t* depth, char* msg, int32_t msg_capacity)
+{
+  if (node_count < 1 || !nodes || tri_count < 0 || (tri_count > 0 && (!tris || !tri_verts)) || msg_capacity < 0 ||
+      (msg_capacity > 0 && !msg))
+    return PRT_ERR_INVALID_ARG;
+  try
+  {
+    int d = 0;
+    const std::string err = bvh8Check(static_cast<const Bvh8Node*>(nodes), node_count,
+                                      static_cast<const Bvh8Tri*>(tris), tri_count, tri_verts, top_count, d);
+    if (depth) *depth = d;
+    if (msg_capacity > 0)
+    {
+      const size_t k = std::min(err.size(), (size_t)msg_capacity - 1);
+      std::memcpy(msg, err.data(), k);
+      msg[k] = 0;
+    }
+    return err.empty() ? PRT_OK : PRT_ERR_INVALID_ARG;
+  }
+  catch (...)
+  {
+    return PRT_ERR_LOGIC;
+  }
+}
+
+int prt_bvh8_build_host(const float* tri_verts, int64_t tri_count, void* nodes, int64_t node_capacity, void* tris,
+                        int64_t tri_capacity, int64_t* node_count, int32_t* top_count)
+{
+  if (tri_count < 0 || (tri_count > 0 && !tri_verts) || !nodes || node_capacity < std::max<int64_t>(tri_count, 1) ||
+      (tri_count > 0 && (!tris || tri_capacity < tri_count)) || !node_count || !top_count)
+    return PRT_ERR_INVALID_ARG;
+  try
+  {
+    Bvh8 bvh;
+    buildBvh8(tri_verts, tri_count, bvh);
+    if ((int64_t)bvh.nodes.size() > node_capacity) return PRT_ERR_LOGIC;
+    std::memcpy(nodes, bvh.nodes.data(), sizeof(Bvh8Node) * bvh.nodes.size());
+    if (!bvh.tris.empty()) std::memcpy(tris, bvh.tris.data(), sizeof(Bvh8Tri) * bvh.tris.size());
+    *node_count = (int64_t)bvh.nodes.size();
+    *top_count = std::min(bvh.topCount, kBvh8TopNodes);
+    return PRT_OK;
+  }
+  catch (const std::invalid_argument&)
+  {
+    return PRT_ERR_INVALID_ARG;
+  }
+  catch (...)
+  {
+    return PRT_ERR_LOGIC;
+  }
+}
+
+int prt_bvh8_trace(const void* nodes, int64_t node_count, const void* tris, int64_t tri_count, int64_t n,
+                   const float* rays, int32_t* tri_out, float* t_out, int64_t* node_visits, int64_t* tri_tests)
+{
+  if (node_count < 1 || !nodes || tri_count < 0 || (tri_count > 0 && !tris) || n < 0 ||
+      (n > 0 && (!rays || !tri_out || !t_out)) || !node_visits || !tri_tests)
+    return PRT_ERR_INVALID_ARG;
+  int64_t nv = 0, tt = 0;
+  for (int64_t i = 0; i < n; ++i)
+  {
+    const float* r = rays + 8 * i;
+    float tfar = r[7];
+    tri_out[i] = bvh8TraceCount(static_cast<const Bvh8Node*>(nodes), static_cast<const Bvh8Tri*>(tris), r, r + 4,
+                                r[3], tfar, nv, tt);
+    t_out[i] = tfar;
+  }
+  *node_visits += nv;
+  *tri_tests += tt;
+  return PRT_OK;
 }
 
 int prt_cuda_bsdf_query(prt_context* ctx, const prt_material* material, int32_t medium_id, int64_t n,

@@ -109,7 +109,11 @@ struct Context
   std::vector<DevBuf> sceneBufs;  // freed on re-upload
   DevScene scene{};
   bool hasScene = false;
-  Bvh8 bvh;                       // host copy (for counting and re-upload)
+  Bvh8 bvh;                       // host copy of a host-built tree
+  int bvhBuilder = 0;             // PRT_BVH_HOST / PRT_BVH_DEVICE of the uploaded scene
+  double bvhBuildMs = 0.0;
+  int64_t bvhNodes = 0, bvhTris = 0;
+  int bvhDepth = 0, bvhTop = 1, bvhIterations = 0;
   std::vector<int> meshTriOffsetHost;
   std::vector<DevMaterial> materialsHost;  // host copies of the uploaded material records
   std::vector<DevTexture> texturesHost;    // device pointers and sizes of the scene's textures

@@ -18,7 +18,7 @@
 
 namespace prt {
 
-constexpr int kTraceStack = 48;           // node-group stack entries per ray
+constexpr int kTraceStack = kBvh8TraceStack;  // node-group stack entries per ray
 constexpr int kTraceMaxIter = 1 << 20;    // loop cap: a corrupt tree ends the ray, not the kernel
 constexpr uint32_t kErrStackOverflow = 1u;
 constexpr uint32_t kErrIterCap = 2u;

@@ -84,6 +84,14 @@ def load_library():
     lib.prt_cuda_albedo_tables.argtypes = [vp, P(C.c_float), C.c_int64, P(C.c_int64)]
     lib.prt_bvh8_count.argtypes = [P(C.c_float), C.c_int64, C.c_int64, P(C.c_float), P(C.c_int32), P(C.c_float),
                                    P(C.c_int64), P(C.c_int64), P(C.c_int64)]
+    lib.prt_cuda_scene_stats.argtypes = [vp, P(T.SceneStats)]
+    lib.prt_cuda_scene_bvh.argtypes = [vp, vp, C.c_int64, vp, C.c_int64, P(C.c_int64), P(C.c_int64)]
+    lib.prt_bvh8_check.argtypes = [vp, C.c_int64, vp, C.c_int64, P(C.c_float), C.c_int32, P(C.c_int32),
+                                   C.c_char_p, C.c_int32]
+    lib.prt_bvh8_trace.argtypes = [vp, C.c_int64, vp, C.c_int64, C.c_int64, P(C.c_float), P(C.c_int32),
+                                   P(C.c_float), P(C.c_int64), P(C.c_int64)]
+    lib.prt_bvh8_build_host.argtypes = [P(C.c_float), C.c_int64, vp, C.c_int64, vp, C.c_int64, P(C.c_int64),
+                                        P(C.c_int32)]
     _lib = lib
     return lib
 
@@ -102,6 +110,58 @@ def bvh8_count(tri_verts, rays):
         raise ValueError(f"prt_bvh8_count failed ({rc})")
     n = max(r.shape[0], 1)
     return tri, t, nv.value / n, tt.value / n, nc.value
+
+
+BVH8_NODE_BYTES = 80
+BVH8_TRI_BYTES = 48
+
+
+def bvh8_build_host(tri_verts):
+    """Host-only PRT_BVH_HOST build into arrays: (nodes uint8[N, 80], tris uint8[M, 48], top count)."""
+    lib = load_library()
+    tv = np.ascontiguousarray(tri_verts, np.float32).reshape(-1, 9)
+    n = tv.shape[0]
+    nodes = np.zeros((max(n, 1), BVH8_NODE_BYTES), np.uint8)
+    tris = np.zeros((n, BVH8_TRI_BYTES), np.uint8)
+    nc, top = C.c_int64(0), C.c_int32(0)
+    rc = lib.prt_bvh8_build_host(T.fptr(tv), n, nodes.ctypes.data, nodes.shape[0], tris.ctypes.data if n else None,
+                                 n, C.byref(nc), C.byref(top))
+    if rc != T.PRT_OK:
+        raise ValueError(f"prt_bvh8_build_host failed ({rc})")
+    return nodes[: nc.value].copy(), tris, top.value
+
+
+def bvh8_check(nodes, tris, tri_verts, top_count):
+    """Host-only structural check of a BVH8 given as byte arrays (prt_bvh8_check): returns
+    (depth, "") for a valid tree, (depth, first violation) otherwise."""
+    lib = load_library()
+    nb = np.ascontiguousarray(nodes, np.uint8).reshape(-1, BVH8_NODE_BYTES)
+    tb = np.ascontiguousarray(tris, np.uint8).reshape(-1, BVH8_TRI_BYTES)
+    tv = np.ascontiguousarray(tri_verts, np.float32).reshape(-1, 9)
+    depth = C.c_int32(0)
+    msg = C.create_string_buffer(256)
+    rc = lib.prt_bvh8_check(nb.ctypes.data, nb.shape[0], tb.ctypes.data if tb.size else None, tb.shape[0],
+                            T.fptr(tv), int(top_count), C.byref(depth), msg, 256)
+    if rc not in (T.PRT_OK, T.PRT_ERR_INVALID_ARG):
+        raise RuntimeError(f"prt_bvh8_check failed ({rc})")
+    return depth.value, msg.value.decode()
+
+
+def bvh8_trace(nodes, tris, rays):
+    """Host-only counting traversal over a BVH8 given as byte arrays: (tri ids, t, nodes/ray, tris/ray)."""
+    lib = load_library()
+    nb = np.ascontiguousarray(nodes, np.uint8).reshape(-1, BVH8_NODE_BYTES)
+    tb = np.ascontiguousarray(tris, np.uint8).reshape(-1, BVH8_TRI_BYTES)
+    r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    tri = np.zeros(r.shape[0], np.int32)
+    t = np.zeros(r.shape[0], np.float32)
+    nv, tt = C.c_int64(0), C.c_int64(0)
+    rc = lib.prt_bvh8_trace(nb.ctypes.data, nb.shape[0], tb.ctypes.data if tb.size else None, tb.shape[0],
+                            r.shape[0], T.fptr(r), T.iptr(tri), T.fptr(t), C.byref(nv), C.byref(tt))
+    if rc != T.PRT_OK:
+        raise ValueError(f"prt_bvh8_trace failed ({rc})")
+    n = max(r.shape[0], 1)
+    return tri, t, nv.value / n, tt.value / n
 
 
 class DeviceCuda:
@@ -151,6 +211,22 @@ class DeviceCuda:
         self._keep = desc
         self._check(self.lib.prt_cuda_scene_upload(self.h, C.byref(desc)))
         self.scene = scene
+
+    def scene_stats(self):
+        """BVH statistics of the uploaded scene (prt_scene_stats) as a dict."""
+        st = T.SceneStats()
+        self._check(self.lib.prt_cuda_scene_stats(self.h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in T.SceneStats._fields_}
+
+    def scene_bvh(self):
+        """The uploaded scene's BVH8 copied back: (nodes uint8[N, 80], tris uint8[M, 48])."""
+        nc, tc = C.c_int64(0), C.c_int64(0)
+        self._check(self.lib.prt_cuda_scene_bvh(self.h, None, 0, None, 0, C.byref(nc), C.byref(tc)))
+        nodes = np.zeros((nc.value, BVH8_NODE_BYTES), np.uint8)
+        tris = np.zeros((tc.value, BVH8_TRI_BYTES), np.uint8)
+        self._check(self.lib.prt_cuda_scene_bvh(self.h, nodes.ctypes.data, nc.value, tris.ctypes.data if tc.value else None,
+                                            tc.value, C.byref(nc), C.byref(tc)))
+        return nodes, tris
 
     def init_renderer(self, max_depth=100, rr_depth=8, min_weight=1e-4, max_radiance=3.4028234663852886e38,
                       type=T.PRT_RENDERER_PATH, samples=16):

@@ -94,6 +94,7 @@ class Scene:
         d.material_count = len(self.materials)
         d.textures = texs
         d.texture_count = len(self.textures)
+        d.bvh_build = getattr(self, "bvh_build", T.PRT_BVH_HOST)
         d.env = self.env
         d.env.image_rgb = T.fptr(self.env_image)
         if oracle and self.sunsky is not None:
@@ -198,6 +199,38 @@ def cornell(seed=0, width=256, height=256, spp=16, max_depth=5, n_spheres=32, sp
         s.add_mesh(sv * r + c, sf, m, normals=sv)
     s.camera = look_at((0.0, 1.0, 3.4), (0.0, 1.0, 0.0), fov_deg=40.0)
     s.width, s.height, s.spp, s.max_depth, s.rr_depth = width, height, spp, max_depth, 8
+    return s
+
+
+def tri_verts(scene):
+    """The scene's triangles as (N, 9) float32 (v0, v1, v2), meshes concatenated in scene order:
+    row i is global triangle i, the index the BVH8 stores."""
+    rows = [m["positions"][m["indices"]].reshape(-1, 9) for m in scene.meshes]
+    return np.concatenate(rows).astype(np.float32) if rows else np.zeros((0, 9), np.float32)
+
+
+def triangle_soup(seed=0, n=5000, dup_frac=0.1, degenerate_frac=0.05, width=64, height=64, spp=1):
+    """Random triangles in [-1, 1]^3 with exact duplicates and degenerate (zero-area or
+    collapsed) triangles mixed in, for BVH builds: a worst case for both builders."""
+    rng = np.random.default_rng(seed)
+    s = Scene()
+    m = s.add_material(T.material(base_color=(0.7, 0.7, 0.7), specular_weight=0.0))
+    c = rng.uniform(-1.0, 1.0, (n, 1, 3))
+    v = (c + rng.normal(0.0, 0.05, (n, 3, 3))).astype(np.float32)
+    if n >= 4:
+        k = int(n * dup_frac)
+        src = rng.integers(0, n, k)
+        dst = rng.integers(0, n, k)
+        v[dst] = v[src]
+        k = int(n * degenerate_frac)
+        d = rng.integers(0, n, k)
+        v[d[: k // 2], 1] = v[d[: k // 2], 0]                     # two equal vertices
+        v[d[k // 2:], :] = v[d[k // 2:], :1]                       # a point
+    s.add_mesh(v.reshape(-1, 3), np.arange(3 * n, dtype=np.int32).reshape(-1, 3), m)
+    s.env.distant_color[:] = (0.0, 0.0, 0.0)
+    s.env.ambient_color[:] = (1.0, 1.0, 1.0)
+    s.camera = look_at((0.0, 0.0, 4.0), (0.0, 0.0, 0.0), fov_deg=40.0)
+    s.width, s.height, s.spp, s.max_depth, s.rr_depth = width, height, spp, 3, 8
     return s
 
 

@@ -175,8 +175,24 @@ class SceneDesc(C.Structure):
         ("materials", C.POINTER(Material)),
         ("textures", C.POINTER(Texture)),
         ("texture_count", C.c_int32),
-        ("reserved", C.c_int32),
+        ("bvh_build", C.c_int32),
         ("env", EnvDesc),
+    ]
+
+
+PRT_BVH_HOST = 0
+PRT_BVH_DEVICE = 1
+
+
+class SceneStats(C.Structure):
+    _fields_ = [
+        ("build_ms", C.c_double),
+        ("node_count", C.c_int64),
+        ("tri_count", C.c_int64),
+        ("builder", C.c_int32),
+        ("depth", C.c_int32),
+        ("top_count", C.c_int32),
+        ("iterations", C.c_int32),
     ]
 
 
