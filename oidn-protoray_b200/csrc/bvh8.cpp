@@ -1,5 +1,6 @@
-// Host BVH8 builder: binned-SAH binary BVH, greedy collapse to 8-wide nodes, octant slot
-// assignment and 8-bit child-box quantisation. See bvh8.h for the node format.
+// Host BVH8 builder: binned-SAH binary BVH down to single primitives, SAH-optimal collapse to
+// 8-wide nodes and leaves of at most three triangles, octant slot assignment and 8-bit child-box
+// quantisation. See bvh8.h for the node format.
 #include "bvh8.h"
 
 #include <deque>
@@ -36,17 +37,67 @@ struct Box
   }
 };
 
+// Binary node. The binary tree is split down to single primitives; which subtrees become leaves
+// of at most kMaxLeaf triangles, and which binary nodes become wide nodes, is decided by the
+// SAH-optimal wide collapse of Ylitie, Karras and Laine 2017 (section 3): cost[i - 1] is the
+// least SAH cost of representing the subtree by at most i children of a wide node,
+//   C(n, 1) = min(Cleaf(n), Cinner(n)),   C(n, i) = min(C(n, i - 1), Cdist(n, i)),
+//   Cdist(n, j) = min over k = 1..j-1 of C(left, k) + C(right, j - k),
+//   Cleaf(n) = area * primitives * kTriCost (at most kMaxLeaf primitives),
+//   Cinner(n) = area * kNodeCost + Cdist(n, 8),
+// and dec[i - 1] its decision: for i = 1 kLeafDecision, or kInnerDecision | (slots of the left
+// child in Cdist(n, 8)); for i > 1 0 = take C(n, i - 1), k = split the slots k : i - k.
 struct BinNode
 {
   Box box;
-  int left;   // -1 for leaves
+  int left;   // -1 for single-primitive leaves
   int right;
-  int first;  // leaves: first index into the primitive order
-  int count;  // leaves: number of primitives (1..3)
+  int first;  // leaves: index into the primitive order
+  int count;  // primitives in the subtree
+  float cost[8];
+  uint8_t dec[8];
 };
 
 constexpr int kMaxLeaf = 3;
 constexpr int kBins = 32;
+constexpr float kNodeCost = 1.0f;
+constexpr float kTriCost = 0.6f;
+constexpr uint8_t kLeafDecision = 0x40;
+constexpr uint8_t kInnerDecision = 0x80;
+
+// Fills the collapse table of an inner node from its children's tables.
+void collapseTable(BinNode& n, const BinNode& l, const BinNode& r)
+{
+  float dist[9];
+  uint8_t split[9];
+  for (int j = 2; j <= 8; ++j)
+  {
+    float best = l.cost[0] + r.cost[j - 2];
+    int kb = 1;
+    for (int k = 2; k < j; ++k)
+    {
+      const float c = l.cost[k - 1] + r.cost[j - k - 1];
+      if (c < best)
+      {
+        best = c;
+        kb = k;
+      }
+    }
+    dist[j] = best;
+    split[j] = (uint8_t)kb;
+  }
+  const float a = n.box.area();
+  const float cInner = a * kNodeCost + dist[8];
+  const bool leaf = n.count <= kMaxLeaf && a * (float)n.count * kTriCost <= cInner;
+  n.cost[0] = leaf ? a * (float)n.count * kTriCost : cInner;
+  n.dec[0] = leaf ? kLeafDecision : (uint8_t)(kInnerDecision | split[8]);
+  for (int i = 1; i < 8; ++i)
+  {
+    const bool take = dist[i + 1] < n.cost[i - 1];
+    n.cost[i] = take ? dist[i + 1] : n.cost[i - 1];
+    n.dec[i] = take ? split[i + 1] : 0;
+  }
+}
 
 struct BinaryBuilder
 {
@@ -93,9 +144,10 @@ struct BinaryBuilder
     }
     node.box = bb;
     const int count = end - begin;
+    node.count = count;
     if (count == 1)
     {
-      makeLeaf(node, begin, count);
+      makeLeaf(node, begin);
       return;
     }
     // Binned SAH over all three axes.
@@ -140,13 +192,6 @@ struct BinaryBuilder
         if (cost < bestCost) { bestCost = cost; bestAxis = axis; bestSplit = b; }
       }
     }
-    // Leaf if small enough and splitting does not pay (traversal cost 1, triangle cost 1).
-    const float leafCost = bb.area() * count;
-    if (count <= kMaxLeaf && (bestAxis < 0 || leafCost <= bb.area() + bestCost))
-    {
-      makeLeaf(node, begin, count);
-      return;
-    }
     int mid;
     if (bestAxis >= 0)
     {
@@ -171,7 +216,6 @@ struct BinaryBuilder
     node.left = left;
     node.right = left + 1;
     node.first = 0;
-    node.count = 0;
     const bool spawn = (end - begin) > 65536 && activeTasks.load() < maxTasks;
     if (spawn)
     {
@@ -186,13 +230,21 @@ struct BinaryBuilder
       build(left, begin, mid);
       build(left + 1, mid, end);
     }
+    collapseTable(nodes[nodeIndex], nodes[left], nodes[left + 1]);
   }
 
-  void makeLeaf(BinNode& node, int begin, int count)
+  void makeLeaf(BinNode& node, int begin)
   {
     node.left = node.right = -1;
     node.first = begin;
-    node.count = count;
+    node.count = 1;
+    const float c = node.box.area() * kTriCost;
+    for (int i = 0; i < 8; ++i)
+    {
+      node.cost[i] = c;
+      node.dec[i] = 0;
+    }
+    node.dec[0] = kLeafDecision;
   }
 };
 
@@ -239,34 +291,44 @@ struct WideBuilder
     qhi = (uint8_t)b;
   }
 
-  // Emits the wide node `wideIndex` for binary node `binIndex`.
+  // Emits the wide node `wideIndex` for binary node `binIndex`. Its children follow the collapse
+  // table: a binary node whose C(n, 1) is a leaf is one leaf child; otherwise its eight slots are
+  // split between its children as recorded, and each (node, slots) pair is resolved by its own
+  // decisions until it is one child (a leaf, or the root of a wide subtree).
   void emit(int wideIndex, int binIndex, int depth)
   {
     maxDepth = std::max(maxDepth, depth + 1);
     int children[8];
+    bool childInner[8];
     int n = 0;
     const BinNode& root = bin.nodes[binIndex];
-    if (root.left < 0)
+    if (root.dec[0] & kLeafDecision)
     {
-      children[n++] = binIndex;
+      children[n] = binIndex;
+      childInner[n++] = false;
     }
     else
     {
-      children[n++] = root.left;
-      children[n++] = root.right;
-      while (n < 8)
+      int pn[8], pi[8];
+      int sp = 0;
+      const int k0 = root.dec[0] & 15;
+      pn[sp] = root.right; pi[sp++] = 8 - k0;
+      pn[sp] = root.left; pi[sp++] = k0;
+      while (sp > 0 && n < 8)
       {
-        int best = -1;
-        float bestArea = -1.f;
-        for (int i = 0; i < n; ++i)
+        const int x = pn[--sp];
+        int i = pi[sp];
+        const BinNode& c = bin.nodes[x];
+        while (i > 1 && c.dec[i - 1] == 0) --i;
+        if (i <= 1)
         {
-          const BinNode& c = bin.nodes[children[i]];
-          if (c.left >= 0 && c.box.area() > bestArea) { bestArea = c.box.area(); best = i; }
+          children[n] = x;
+          childInner[n++] = (c.dec[0] & kInnerDecision) != 0;
+          continue;
         }
-        if (best < 0) break;
-        const BinNode& c = bin.nodes[children[best]];
-        children[best] = c.left;
-        children[n++] = c.right;
+        const int k = c.dec[i - 1];
+        pn[sp] = c.right; pi[sp++] = i - k;
+        pn[sp] = c.left; pi[sp++] = k;
       }
     }
     // Node box.
@@ -320,12 +382,6 @@ struct WideBuilder
     quantAxis(nb.lo[2], nb.hi[2], node.pz, node.ez);
 
     // Leaf triangles first (contiguous per node), then inner children as one block.
-    int innerCount = 0;
-    for (int s = 0; s < 8; ++s)
-    {
-      if (childOfSlot[s] < 0) continue;
-      if (bin.nodes[children[childOfSlot[s]]].left >= 0) innerCount++;
-    }
     node.triBase = (uint32_t)out.tris.size();
     int triOffset = 0;
     int innerSlots[8];
@@ -338,17 +394,37 @@ struct WideBuilder
       quantChild(node.px, node.ex, c.box.lo[0], c.box.hi[0], node.qlox[s], node.qhix[s]);
       quantChild(node.py, node.ey, c.box.lo[1], c.box.hi[1], node.qloy[s], node.qhiy[s]);
       quantChild(node.pz, node.ez, c.box.lo[2], c.box.hi[2], node.qloz[s], node.qhiz[s]);
-      if (c.left >= 0)
+      if (childInner[ci])
       {
         node.imask |= (uint8_t)(1u << s);
         innerSlots[innerN++] = children[ci];
       }
       else
       {
-        node.meta[s] = (uint8_t)((c.count << 5) | triOffset);
-        for (int j = 0; j < c.count; ++j)
+        // The leaf's primitives, left to right (at most kMaxLeaf, so at most two inner nodes).
+        int prims[kMaxLeaf];
+        int np = 0;
+        int stack[kMaxLeaf + 1];
+        int sp = 0;
+        stack[sp++] = children[ci];
+        while (sp > 0)
         {
-          const int prim = bin.order[c.first + j];
+          const BinNode& x = bin.nodes[stack[--sp]];
+          if (x.left < 0)
+          {
+            if (np < kMaxLeaf) prims[np++] = bin.order[x.first];
+          }
+          else if (sp + 2 <= kMaxLeaf + 1)
+          {
+            stack[sp++] = x.right;
+            stack[sp++] = x.left;
+          }
+        }
+        if (np != c.count) throw std::logic_error("BVH8: leaf larger than the leaf limit");
+        node.meta[s] = (uint8_t)((np << 5) | triOffset);
+        for (int j = 0; j < np; ++j)
+        {
+          const int prim = prims[j];
           const float* v = verts + 9 * (size_t)prim;
           Bvh8Tri t;
           t.v0x = v[0]; t.v0y = v[1]; t.v0z = v[2];
@@ -358,7 +434,7 @@ struct WideBuilder
           t.pad1 = t.pad2 = 0.f;
           out.tris.push_back(t);
         }
-        triOffset += c.count;
+        triOffset += np;
       }
     }
     node.childBase = (uint32_t)out.nodes.size();

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 namespace prt {
@@ -223,6 +224,17 @@ __global__ void kTriBoxes(const float4* __restrict__ pos, const int4* __restrict
     }
 }
 
+// Morton codes: 21 bits per axis in a 63-bit key (PRT_MORTON_BITS 63, the default) or 10 bits
+// per axis in a 30-bit key. Dense clusters of small triangles (a finely tessellated sphere
+// inside one coarse cell) need the longer code: with equal keys the sort falls back to the
+// triangle index, which loses their spatial order.
+#ifndef PRT_MORTON_BITS
+#define PRT_MORTON_BITS 63
+#endif
+constexpr int kMortonBits = PRT_MORTON_BITS;
+static_assert(kMortonBits == 63 || kMortonBits == 30, "Morton code length");
+using MortonKey = std::conditional_t<kMortonBits == 63, u64, uint32_t>;
+
 __device__ __forceinline__ uint32_t spreadBits10(uint32_t x)
 {
   x &= 1023u;
@@ -233,10 +245,21 @@ __device__ __forceinline__ uint32_t spreadBits10(uint32_t x)
   return x;
 }
 
-// 30-bit Morton code of the box centre in the centroid bounds, scaled uniformly by the largest
-// extent so that a flat or long scene keeps its spatial neighbourhoods.
+__device__ __forceinline__ u64 spreadBits21(u64 x)
+{
+  x &= 0x1fffffull;
+  x = (x | (x << 32)) & 0x001f00000000ffffull;
+  x = (x | (x << 16)) & 0x001f0000ff0000ffull;
+  x = (x | (x << 8)) & 0x100f00f00f00f00full;
+  x = (x | (x << 4)) & 0x10c30c30c30c30c3ull;
+  x = (x | (x << 2)) & 0x1249249249249249ull;
+  return x;
+}
+
+// Morton code of the box centre in the centroid bounds, scaled uniformly by the largest extent
+// so that a flat or long scene keeps its spatial neighbourhoods.
 __global__ void kMorton(const float4* __restrict__ boxLo, const float4* __restrict__ boxHi, int64_t n,
-                        const uint32_t* __restrict__ cb, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals)
+                        const uint32_t* __restrict__ cb, MortonKey* __restrict__ keys, uint32_t* __restrict__ vals)
 {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
@@ -248,14 +271,19 @@ __global__ void kMorton(const float4* __restrict__ boxLo, const float4* __restri
     mn[k] = fromOrdered(cb[k]);
     ext = fmaxf(ext, fromOrdered(cb[3 + k]) - mn[k]);
   }
-  const float scale = ext > 0.f ? 1024.f / ext : 0.f;
+  constexpr int kAxisBits = kMortonBits / 3;
+  constexpr uint32_t kCells = 1u << kAxisBits;
+  const float scale = ext > 0.f ? (float)kCells / ext : 0.f;
   uint32_t q[3];
   for (int k = 0; k < 3; ++k)
   {
     const float f = (c[k] - mn[k]) * scale;
-    q[k] = (uint32_t)min(max((int)f, 0), 1023);
+    q[k] = f > 0.f ? min((uint32_t)f, kCells - 1u) : 0u;
   }
-  keys[t] = (spreadBits10(q[0]) << 2) | (spreadBits10(q[1]) << 1) | spreadBits10(q[2]);
+  if constexpr (kMortonBits == 63)
+    keys[t] = (spreadBits21(q[0]) << 2) | (spreadBits21(q[1]) << 1) | spreadBits21(q[2]);
+  else
+    keys[t] = (spreadBits10(q[0]) << 2) | (spreadBits10(q[1]) << 1) | spreadBits10(q[2]);
   vals[t] = (uint32_t)t;
 }
 
@@ -267,7 +295,8 @@ constexpr int kSortWarps = kSortThreads / 32;
 
 // Per-tile digit counts, stored digit-major (hist[digit * tiles + tile]) so that one exclusive
 // scan gives every (digit, tile) its first output position.
-__global__ void __launch_bounds__(kSortThreads) kRadixHist(const uint32_t* __restrict__ keys, int64_t n, int shift,
+template <class K>
+__global__ void __launch_bounds__(kSortThreads) kRadixHist(const K* __restrict__ keys, int64_t n, int shift,
                                                            uint32_t* __restrict__ hist, int tiles)
 {
   __shared__ uint32_t cnt[256];
@@ -275,7 +304,7 @@ __global__ void __launch_bounds__(kSortThreads) kRadixHist(const uint32_t* __res
   __syncthreads();
   const int64_t base = (int64_t)blockIdx.x * kSortTile;
   for (int k = threadIdx.x; k < kSortTile; k += kSortThreads)
-    if (base + k < n) atomicAdd(&cnt[(keys[base + k] >> shift) & 255u], 1u);
+    if (base + k < n) atomicAdd(&cnt[(uint32_t)(keys[base + k] >> shift) & 255u], 1u);
   __syncthreads();
   hist[(int64_t)threadIdx.x * tiles + blockIdx.x] = cnt[threadIdx.x];
 }
@@ -283,9 +312,10 @@ __global__ void __launch_bounds__(kSortThreads) kRadixHist(const uint32_t* __res
 // Stable scatter: warp w of a tile ranks its 256 keys in input order (8 rounds of 32, lanes
 // with equal digits found with __match_any_sync), the warps' counts are prefixed in warp order,
 // and the tile's base for each digit comes from the scanned histogram.
-__global__ void __launch_bounds__(kSortThreads) kRadixScatter(const uint32_t* __restrict__ keysIn,
+template <class K>
+__global__ void __launch_bounds__(kSortThreads) kRadixScatter(const K* __restrict__ keysIn,
                                                               const uint32_t* __restrict__ valsIn,
-                                                              uint32_t* __restrict__ keysOut,
+                                                              K* __restrict__ keysOut,
                                                               uint32_t* __restrict__ valsOut, int64_t n, int shift,
                                                               const uint32_t* __restrict__ offsets, int tiles)
 {
@@ -297,14 +327,15 @@ __global__ void __launch_bounds__(kSortThreads) kRadixScatter(const uint32_t* __
   __syncthreads();
   const int64_t base = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * 32 * kSortItems;
   const unsigned below = (1u << lane) - 1u;
-  uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+  K key[kSortItems];
+  uint32_t val[kSortItems], rank[kSortItems];
   for (int k = 0; k < kSortItems; ++k)
   {
     const int64_t i = base + k * 32 + lane;
     const bool ok = i < n;
-    key[k] = ok ? keysIn[i] : 0u;
+    key[k] = ok ? keysIn[i] : K(0);
     val[k] = ok ? valsIn[i] : 0u;
-    const uint32_t digit = ok ? (key[k] >> shift) & 255u : 256u;
+    const uint32_t digit = ok ? (uint32_t)(key[k] >> shift) & 255u : 256u;
     const unsigned peers = __match_any_sync(0xffffffffu, digit);
     const int leader = __ffs(peers) - 1;
     uint32_t prior = 0u;
@@ -332,7 +363,7 @@ __global__ void __launch_bounds__(kSortThreads) kRadixScatter(const uint32_t* __
   {
     const int64_t i = base + k * 32 + lane;
     if (i >= n) continue;
-    const uint32_t digit = (key[k] >> shift) & 255u;
+    const uint32_t digit = (uint32_t)(key[k] >> shift) & 255u;
     const uint32_t dst = tileBase[digit] + warpCnt[warp][digit] + rank[k];
     keysOut[dst] = key[k];
     valsOut[dst] = val[k];
@@ -341,53 +372,123 @@ __global__ void __launch_bounds__(kSortThreads) kRadixScatter(const uint32_t* __
 
 // ---- PLOC clustering ---------------------------------------------------------------------------
 // Binary nodes: leaves 0..n-1 (one triangle each, in Morton order), inner nodes after them in
-// creation order, so a node's children always have smaller indices. lo.w holds the subtree's SAH
-// cost, hi.w the bits of (triangle count | kLeafFlag), child = (left, right) or (-1, triangle).
-// kLeafFlag marks a subtree that the collapse stores as one leaf: a single triangle, or at most
-// kMaxLeafTris triangles whose SAH cost as a leaf (area * count) does not exceed the cost as an
-// inner node (area + children's costs).
+// creation order, so a node's children always have smaller indices and are complete when the
+// node is made. Per node: box (lo, hi), hi.w = bits of (triangle count | kLeafFlag), child =
+// (left, right) or (-1, triangle), and the table of the wide collapse below.
+//
+// Wide collapse (Ylitie, Karras and Laine 2017, "Efficient Incoherent Ray Traversal on GPUs
+// Through Compressed Wide BVHs", section 3): C(n, i) is the least SAH cost of representing the
+// subtree n by at most i children of a wide node,
+//   C(n, 1) = min(Cleaf(n), Cinner(n)),   C(n, i) = min(C(n, i - 1), Cdist(n, i)),
+//   Cdist(n, j) = min over k = 1..j-1 of C(left, k) + C(right, j - k),
+//   Cleaf(n) = area * triangles * kTriCost for at most kMaxLeafTris triangles (else none),
+//   Cinner(n) = area * kNodeCost + Cdist(n, 8),
+// with the decision of each entry kept in one byte: for i = 1 kLeafDecision or kInnerDecision |
+// (slots of the left child in Cdist(n, 8)); for i > 1 0 = take C(n, i - 1), k = split the i
+// slots k : i - k between the children. The table is filled when a node is merged (its
+// children's tables are final then), and the top-down collapse follows the decisions.
+// kLeafFlag marks the nodes whose C(n, 1) is a leaf: a single triangle or a subtree stored as
+// one leaf of at most kMaxLeafTris triangles.
 constexpr uint32_t kLeafFlag = 0x80000000u;
 constexpr uint32_t kMaxLeafTris = 3;
-constexpr int kPlocRadius = 16;        // neighbour window on each side in the Morton order
+#ifndef PRT_TRI_COST
+#define PRT_TRI_COST 0.6f
+#endif
+constexpr float kNodeCost = 1.0f;
+constexpr float kTriCost = PRT_TRI_COST;
+constexpr uint32_t kLeafDecision = 0x40u;
+constexpr uint32_t kInnerDecision = 0x80u;
+#ifndef PRT_PLOC_RADIUS
+#define PRT_PLOC_RADIUS 16
+#endif
+constexpr int kPlocRadius = PRT_PLOC_RADIUS;  // neighbour window on each side in the Morton order
 constexpr int kNearestThreads = 256;
 constexpr int kTailThreads = 1024;     // the in-block tail: one CTA clusters the last kTailMax
 constexpr int kTailItems = 4;
 constexpr int kTailMax = kTailThreads * kTailItems;
 constexpr size_t kTailSmem = (size_t)kTailMax * (6 * sizeof(float) + 2 * sizeof(int));
 
+struct BinNodes
+{
+  float4* lo;      // xyz box minimum, w = C(n, 1)
+  float4* hi;      // xyz box maximum, w = bits of (triangles | kLeafFlag)
+  int2* child;     // (left, right), or (-1, triangle index) for a triangle
+  float4* costA;   // C(n, 1..4)
+  float4* costB;   // C(n, 5..8)
+  uint2* dec;      // decision bytes of C(n, 1..8)
+};
+
 __device__ __forceinline__ bool isLeafNode(float4 hi) { return (__float_as_uint(hi.w) & kLeafFlag) != 0u; }
 __device__ __forceinline__ uint32_t nodeTris(float4 hi) { return __float_as_uint(hi.w) & ~kLeafFlag; }
+__device__ __forceinline__ uint32_t decisionByte(uint2 d, int i)  // i = 0..7 for C(n, i + 1)
+{
+  return ((i < 4 ? d.x : d.y) >> (8 * (i & 3))) & 0xffu;
+}
 
 __global__ void kInitLeaves(const uint32_t* __restrict__ sortedTri, const float4* __restrict__ boxLo,
-                            const float4* __restrict__ boxHi, int64_t n, float4* __restrict__ nLo,
-                            float4* __restrict__ nHi, int2* __restrict__ nChild, int* __restrict__ cid,
+                            const float4* __restrict__ boxHi, int64_t n, BinNodes N, int* __restrict__ cid,
                             float4* __restrict__ cLo, float4* __restrict__ cHi)
 {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t tri = sortedTri[i];
   const float4 lo = boxLo[tri], hi = boxHi[tri];
-  nLo[i] = make_float4(lo.x, lo.y, lo.z, boxArea(xyz(lo), xyz(hi)));
-  nHi[i] = make_float4(hi.x, hi.y, hi.z, __uint_as_float(1u | kLeafFlag));
-  nChild[i] = make_int2(-1, (int)tri);
+  const float c = boxArea(xyz(lo), xyz(hi)) * kTriCost;
+  N.lo[i] = make_float4(lo.x, lo.y, lo.z, c);
+  N.hi[i] = make_float4(hi.x, hi.y, hi.z, __uint_as_float(1u | kLeafFlag));
+  N.child[i] = make_int2(-1, (int)tri);
+  N.costA[i] = make_float4(c, c, c, c);
+  N.costB[i] = make_float4(c, c, c, c);
+  N.dec[i] = make_uint2(kLeafDecision, 0u);
   cid[i] = (int)i;
   cLo[i] = make_float4(lo.x, lo.y, lo.z, 0.f);
   cHi[i] = make_float4(hi.x, hi.y, hi.z, 0.f);
 }
 
-// Writes the inner node `id` over children l and r and returns nothing; the merged box is lo/hi.
-__device__ __forceinline__ void makeInner(int id, int l, int r, float3 lo, float3 hi, float4* nLo, float4* nHi,
-                                          int2* nChild)
+// Writes the inner node `id` over children l and r (merged box lo/hi) with its collapse table.
+__device__ __forceinline__ void makeInner(int id, int l, int r, float3 lo, float3 hi, const BinNodes& N)
 {
-  const float4 ll = nLo[l], lh = nHi[l], rl = nLo[r], rh = nHi[r];
-  const uint32_t cnt = nodeTris(lh) + nodeTris(rh);
+  const float4 la = N.costA[l], lb = N.costB[l], ra = N.costA[r], rb = N.costB[r];
+  const float cl[8] = {la.x, la.y, la.z, la.w, lb.x, lb.y, lb.z, lb.w};
+  const float cr[8] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y, rb.z, rb.w};
+  const uint32_t cnt = nodeTris(N.hi[l]) + nodeTris(N.hi[r]);
   const float a = boxArea(lo, hi);
-  const float inner = a + ll.w + rl.w;
-  const float asLeaf = a * (float)cnt;
-  const bool leaf = cnt <= kMaxLeafTris && asLeaf <= inner;
-  nLo[id] = make_float4(lo.x, lo.y, lo.z, leaf ? asLeaf : inner);
-  nHi[id] = make_float4(hi.x, hi.y, hi.z, __uint_as_float(cnt | (leaf ? kLeafFlag : 0u)));
-  nChild[id] = make_int2(l, r);
+  float dist[9];
+  uint32_t split[9];
+  for (int j = 2; j <= 8; ++j)
+  {
+    float best = cl[0] + cr[j - 2];
+    uint32_t kb = 1u;
+    for (int k = 2; k < j; ++k)
+    {
+      const float c = cl[k - 1] + cr[j - k - 1];
+      if (c < best)
+      {
+        best = c;
+        kb = (uint32_t)k;
+      }
+    }
+    dist[j] = best;
+    split[j] = kb;
+  }
+  const float cInner = a * kNodeCost + dist[8];
+  const bool leaf = cnt <= kMaxLeafTris && a * (float)cnt * kTriCost <= cInner;
+  float c[8];
+  uint32_t d[8];
+  c[0] = leaf ? a * (float)cnt * kTriCost : cInner;
+  d[0] = leaf ? kLeafDecision : (kInnerDecision | split[8]);
+  for (int i = 1; i < 8; ++i)
+  {
+    const bool take = dist[i + 1] < c[i - 1];
+    c[i] = take ? dist[i + 1] : c[i - 1];
+    d[i] = take ? split[i + 1] : 0u;
+  }
+  N.lo[id] = make_float4(lo.x, lo.y, lo.z, c[0]);
+  N.hi[id] = make_float4(hi.x, hi.y, hi.z, __uint_as_float(cnt | (leaf ? kLeafFlag : 0u)));
+  N.child[id] = make_int2(l, r);
+  N.costA[id] = make_float4(c[0], c[1], c[2], c[3]);
+  N.costB[id] = make_float4(c[4], c[5], c[6], c[7]);
+  N.dec[id] = make_uint2(d[0] | (d[1] << 8) | (d[2] << 16) | (d[3] << 24), d[4] | (d[5] << 8) | (d[6] << 16) | (d[7] << 24));
 }
 
 __device__ __forceinline__ float mergedArea(float3 alo, float3 ahi, float3 blo, float3 bhi)
@@ -457,7 +558,7 @@ __global__ void kMergeFlags(const int* __restrict__ nn, int count, u64* __restri
 __global__ void kCompact(const int* __restrict__ nn, int count, const u64* __restrict__ scan,
                          const int* __restrict__ cidIn, const float4* __restrict__ cLoIn,
                          const float4* __restrict__ cHiIn, int* __restrict__ cidOut, float4* __restrict__ cLoOut,
-                         float4* __restrict__ cHiOut, float4* nLo, float4* nHi, int2* nChild, int nodeBase)
+                         float4* __restrict__ cHiOut, BinNodes N, int nodeBase)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
@@ -472,7 +573,7 @@ __global__ void kCompact(const int* __restrict__ nn, int count, const u64* __res
     const float4 al = cLoIn[i], ah = cHiIn[i], bl = cLoIn[j], bh = cHiIn[j];
     const float3 lo = make_float3(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z));
     const float3 hi = make_float3(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z));
-    makeInner(id, cidIn[i], cidIn[j], lo, hi, nLo, nHi, nChild);
+    makeInner(id, cidIn[i], cidIn[j], lo, hi, N);
     cidOut[pos] = id;
     cLoOut[pos] = make_float4(lo.x, lo.y, lo.z, 0.f);
     cHiOut[pos] = make_float4(hi.x, hi.y, hi.z, 0.f);
@@ -492,8 +593,8 @@ __global__ void kCompact(const int* __restrict__ nn, int count, const u64* __res
 // result: [0] root node, [1] iterations, [2] next free node index.
 __global__ void __launch_bounds__(kTailThreads, 1) kPlocTail(int count, int force, const int* __restrict__ cid,
                                                              const float4* __restrict__ cLo,
-                                                             const float4* __restrict__ cHi, float4* nLo,
-                                                             float4* nHi, int2* nChild, int nodeBase, int* result)
+                                                             const float4* __restrict__ cHi, BinNodes N,
+                                                             int nodeBase, int* result)
 {
   extern __shared__ float tailSmem[];
   float* lx = tailSmem;
@@ -569,7 +670,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) kPlocTail(int count, int forc
           outLo[k] = make_float3(fminf(lo.x, blo.x), fminf(lo.y, blo.y), fminf(lo.z, blo.z));
           outHi[k] = make_float3(fmaxf(hi.x, bhi.x), fmaxf(hi.y, bhi.y), fmaxf(hi.z, bhi.z));
           outId[k] = nodeBase + (int)(run >> 16);
-          makeInner(outId[k], ids[i], ids[j], outLo[k], outHi[k], nLo, nHi, nChild);
+          makeInner(outId[k], ids[i], ids[j], outLo[k], outHi[k], N);
         }
         else
         {
@@ -607,63 +708,62 @@ __global__ void __launch_bounds__(kTailThreads, 1) kPlocTail(int count, int forc
 // ---- collapse to 8-wide nodes ------------------------------------------------------------------
 constexpr int kCollapseThreads = 128;
 
-// Children of the wide node over binary node b, the host builder's rule: a leaf-flagged b is one
-// leaf child; otherwise start from b's two children and open the inner (not leaf-flagged) child
-// of largest surface area until there are eight. Children go to octant slots greedily by
-// dot(child centre - node centre, slot direction), largest first (bvh8.cpp's assignment).
-// slotNode[8w + s] = binary node in slot s or -1; counts[w] = (inner children << 32) | triangles.
-__global__ void __launch_bounds__(kCollapseThreads) kCollapsePlan(const int* __restrict__ work, int m,
-                                                                  const float4* __restrict__ nLo,
-                                                                  const float4* __restrict__ nHi,
-                                                                  const int2* __restrict__ nChild,
+// Children of the wide node over binary node b, from the collapse table: a leaf-flagged b (a
+// tree of at most kMaxLeafTris triangles) is one leaf child; otherwise b's eight slots are split
+// between its children as C(b, 1) recorded, and each (node, slots) pair is resolved by its own
+// decisions until it is one child -- a leaf or the root of a wide subtree. Children go to octant
+// slots greedily by dot(child centre - node centre, slot direction), largest first (bvh8.cpp's
+// assignment). slotNode[8w + s] = binary node in slot s or -1; counts[w] = (inner children << 32)
+// | triangles.
+__global__ void __launch_bounds__(kCollapseThreads) kCollapsePlan(const int* __restrict__ work, int m, BinNodes N,
                                                                   int* __restrict__ slotNode, u64* __restrict__ counts)
 {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= m) return;
   const int b = work[w];
-  const float4 blo = nLo[b], bhi = nHi[b];
+  const float4 blo = N.lo[b], bhi = N.hi[b];
   int ch[8];
-  float area[8];
   bool inner[8];
   int n = 0;
-  auto set = [&](int i, int node) {
-    const float4 lo = nLo[node], hi = nHi[node];
-    ch[i] = node;
-    area[i] = boxArea(xyz(lo), xyz(hi));
-    inner[i] = !isLeafNode(hi);
-  };
   if (isLeafNode(bhi))
   {
-    set(0, b);
+    ch[0] = b;
+    inner[0] = false;
     n = 1;
   }
   else
   {
-    const int2 c = nChild[b];
-    set(0, c.x);
-    set(1, c.y);
-    n = 2;
-    while (n < 8)
+    // Pending (node, slots) pairs; their slots sum to at most 8, so at most 8 are pending.
+    int sn[8], si[8];
+    int sp = 0;
+    const uint32_t k0 = decisionByte(N.dec[b], 0) & 15u;
+    const int2 c = N.child[b];
+    sn[sp] = c.y; si[sp++] = 8 - (int)k0;
+    sn[sp] = c.x; si[sp++] = (int)k0;
+    while (sp > 0 && n < 8)
     {
-      int best = -1;
-      float bestArea = -1.f;
-      for (int i = 0; i < n; ++i)
-        if (inner[i] && area[i] > bestArea)
-        {
-          bestArea = area[i];
-          best = i;
-        }
-      if (best < 0) break;
-      const int2 c2 = nChild[ch[best]];
-      set(best, c2.x);
-      set(n, c2.y);
-      ++n;
+      const int x = sn[--sp];
+      int i = si[sp];
+      const uint2 d = N.dec[x];
+      while (i > 1 && decisionByte(d, i - 1) == 0u) --i;
+      if (i <= 1)
+      {
+        ch[n] = x;
+        inner[n] = (decisionByte(d, 0) & kInnerDecision) != 0u;
+        ++n;
+        continue;
+      }
+      const int k = (int)decisionByte(d, i - 1);
+      const int2 cx = N.child[x];
+      if (sp + 2 > 8) break;  // cannot happen: pending slots never exceed 8
+      sn[sp] = cx.y; si[sp++] = i - k;
+      sn[sp] = cx.x; si[sp++] = k;
     }
   }
   float cost[8][8];
   for (int i = 0; i < n; ++i)
   {
-    const float4 lo = nLo[ch[i]], hi = nHi[ch[i]];
+    const float4 lo = N.lo[ch[i]], hi = N.hi[ch[i]];
     const float d[3] = {0.5f * (lo.x + hi.x) - 0.5f * (blo.x + bhi.x), 0.5f * (lo.y + hi.y) - 0.5f * (blo.y + bhi.y),
                         0.5f * (lo.z + hi.z) - 0.5f * (blo.z + bhi.z)};
     for (int s = 0; s < 8; ++s)
@@ -703,7 +803,7 @@ __global__ void __launch_bounds__(kCollapseThreads) kCollapsePlan(const int* __r
     slotNode[8 * w + s] = ci >= 0 ? ch[ci] : -1;
     if (ci < 0) continue;
     if (inner[ci]) ++innerN;
-    else triN += nodeTris(nHi[ch[ci]]);
+    else triN += nodeTris(N.hi[ch[ci]]);
   }
   counts[w] = ((u64)innerN << 32) | triN;
 }
@@ -763,8 +863,7 @@ __device__ __forceinline__ void writeTri(float4* __restrict__ out, uint32_t slot
 // slot order, which also become the next level's work items.
 __global__ void __launch_bounds__(kCollapseThreads) kCollapseEmit(
   const int* __restrict__ work, int m, const int* __restrict__ slotNode, const u64* __restrict__ offs, int levelBase,
-  int nextBase, int64_t triBase0, const float4* __restrict__ nLo, const float4* __restrict__ nHi,
-  const int2* __restrict__ nChild, const float4* __restrict__ pos, const int4* __restrict__ tv,
+  int nextBase, int64_t triBase0, BinNodes N, const float4* __restrict__ pos, const int4* __restrict__ tv,
   uint4* __restrict__ outNodes, float4* __restrict__ outTris, int* __restrict__ nextWork, int* err)
 {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
@@ -772,7 +871,7 @@ __global__ void __launch_bounds__(kCollapseThreads) kCollapseEmit(
   const int b = work[w];
   const u64 o = offs[w];
   const uint32_t innerOff = (uint32_t)(o >> 32), triOff = (uint32_t)o;
-  const float4 blo = nLo[b], bhi = nHi[b];
+  const float4 blo = N.lo[b], bhi = N.hi[b];
   Bvh8Node node;
   memset(&node, 0, sizeof(node));
   if (!quantAxisD(blo.x, bhi.x, node.px, node.ex) || !quantAxisD(blo.y, bhi.y, node.py, node.ey) ||
@@ -785,7 +884,7 @@ __global__ void __launch_bounds__(kCollapseThreads) kCollapseEmit(
   {
     const int c = slotNode[8 * w + s];
     if (c < 0) continue;
-    const float4 clo = nLo[c], chi = nHi[c];
+    const float4 clo = N.lo[c], chi = N.hi[c];
     quantChildD(node.px, node.ex, clo.x, chi.x, node.qlox[s], node.qhix[s]);
     quantChildD(node.py, node.ey, clo.y, chi.y, node.qloy[s], node.qhiy[s]);
     quantChildD(node.pz, node.ez, clo.z, chi.z, node.qloz[s], node.qhiz[s]);
@@ -803,7 +902,7 @@ __global__ void __launch_bounds__(kCollapseThreads) kCollapseEmit(
     while (sp > 0)
     {
       const int x = stack[--sp];
-      const int2 k = nChild[x];
+      const int2 k = N.child[x];
       if (k.x < 0)
       {
         writeTri(outTris, node.triBase + triK, k.y, pos, tv);
@@ -869,19 +968,18 @@ void buildBvh8Device(const float4* pos, const int4* triVerts, int64_t triCount, 
   uint32_t* cb = s.alloc<uint32_t>(6);
   kFillU32<<<1, 32, 0, st>>>(cb, 6, 0xffffffffu, 0u, 3);
   kTriBoxes<<<blocksFor(n, 256), 256, 0, st>>>(pos, triVerts, n, triLo, triHi, cb);
-  uint32_t* keysA = s.alloc<uint32_t>(n);
+  MortonKey* keysA = s.alloc<MortonKey>(n);
   uint32_t* valsA = s.alloc<uint32_t>(n);
-  uint32_t* keysB = s.alloc<uint32_t>(n);
+  MortonKey* keysB = s.alloc<MortonKey>(n);
   uint32_t* valsB = s.alloc<uint32_t>(n);
   kMorton<<<blocksFor(n, 256), 256, 0, st>>>(triLo, triHi, n, cb, keysA, valsA);
-  // 2. Stable radix sort, four 8-bit passes (the codes have 30 bits).
+  // 2. Stable radix sort, 8 bits per pass over the code's bits.
   const int tiles = (int)blocksFor(n, kSortTile);
   uint32_t* hist = s.alloc<uint32_t>((size_t)256 * tiles);
   Scanner<uint32_t> scan32;
   scan32.init(s, (int64_t)256 * tiles);
-  for (int pass = 0; pass < 4; ++pass)
+  for (int shift = 0; shift < kMortonBits; shift += 8)
   {
-    const int shift = 8 * pass;
     kRadixHist<<<tiles, kSortThreads, 0, st>>>(keysA, n, shift, hist, tiles);
     scan32.run(hist, hist, (int64_t)256 * tiles, st);
     kRadixScatter<<<tiles, kSortThreads, 0, st>>>(keysA, valsA, keysB, valsB, n, shift, hist, tiles);
@@ -890,16 +988,20 @@ void buildBvh8Device(const float4* pos, const int4* triVerts, int64_t triCount, 
   }
   // 3. PLOC: large iterations over the whole device, then the in-block tail.
   const size_t nodeCap = 2 * (size_t)n;
-  float4* nLo = s.alloc<float4>(nodeCap);
-  float4* nHi = s.alloc<float4>(nodeCap);
-  int2* nChild = s.alloc<int2>(nodeCap);
+  BinNodes N;
+  N.lo = s.alloc<float4>(nodeCap);
+  N.hi = s.alloc<float4>(nodeCap);
+  N.child = s.alloc<int2>(nodeCap);
+  N.costA = s.alloc<float4>(nodeCap);
+  N.costB = s.alloc<float4>(nodeCap);
+  N.dec = s.alloc<uint2>(nodeCap);
   int* cidA = s.alloc<int>(n);
   int* cidB = s.alloc<int>(n);
   float4* cLoA = s.alloc<float4>(n);
   float4* cHiA = s.alloc<float4>(n);
   float4* cLoB = s.alloc<float4>(n);
   float4* cHiB = s.alloc<float4>(n);
-  kInitLeaves<<<blocksFor(n, 256), 256, 0, st>>>(valsA, triLo, triHi, n, nLo, nHi, nChild, cidA, cLoA, cHiA);
+  kInitLeaves<<<blocksFor(n, 256), 256, 0, st>>>(valsA, triLo, triHi, n, N, cidA, cLoA, cHiA);
   int* nn = s.alloc<int>(n);
   u64* flags = s.alloc<u64>(n);
   Scanner<u64> scan64;
@@ -910,8 +1012,8 @@ void buildBvh8Device(const float4* pos, const int4* triVerts, int64_t triCount, 
     kNearest<<<blocksFor(count, kNearestThreads), kNearestThreads, 0, st>>>(cLoA, cHiA, count, nn, force);
     kMergeFlags<<<blocksFor(count, 256), 256, 0, st>>>(nn, count, flags);
     scan64.run(flags, flags, count, st);
-    kCompact<<<blocksFor(count, 256), 256, 0, st>>>(nn, count, flags, cidA, cLoA, cHiA, cidB, cLoB, cHiB, nLo, nHi,
-                                                    nChild, nodeBase);
+    kCompact<<<blocksFor(count, 256), 256, 0, st>>>(nn, count, flags, cidA, cLoA, cHiA, cidB, cLoB, cHiB, N,
+                                                    nodeBase);
     const u64 tot = readScalar(scan64.total, st);
     const int merges = (int)(tot >> 32);
     force = (int64_t)merges * 64 < count;
@@ -924,7 +1026,7 @@ void buildBvh8Device(const float4* pos, const int4* triVerts, int64_t triCount, 
   }
   int* result = s.alloc<int>(3);
   check(cudaFuncSetAttribute(kPlocTail, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTailSmem), "build");
-  kPlocTail<<<1, kTailThreads, kTailSmem, st>>>(count, force, cidA, cLoA, cHiA, nLo, nHi, nChild, nodeBase, result);
+  kPlocTail<<<1, kTailThreads, kTailSmem, st>>>(count, force, cidA, cLoA, cHiA, N, nodeBase, result);
   check(cudaGetLastError(), "clustering");
   int res[3];
   check(cudaMemcpyAsync(res, result, sizeof(res), cudaMemcpyDeviceToHost, st), "read back");
@@ -946,11 +1048,10 @@ void buildBvh8Device(const float4* pos, const int4* triVerts, int64_t triCount, 
   while (m > 0)
   {
     if ((int64_t)levelBase + m > n) throw std::runtime_error("BVH8 device build: node count exceeds the bound");
-    kCollapsePlan<<<blocksFor(m, kCollapseThreads), kCollapseThreads, 0, st>>>(workA, m, nLo, nHi, nChild, slotNode,
-                                                                                flags);
+    kCollapsePlan<<<blocksFor(m, kCollapseThreads), kCollapseThreads, 0, st>>>(workA, m, N, slotNode, flags);
     scan64.run(flags, flags, m, st);
     kCollapseEmit<<<blocksFor(m, kCollapseThreads), kCollapseThreads, 0, st>>>(
-      workA, m, slotNode, flags, levelBase, levelBase + m, triBase, nLo, nHi, nChild, pos, triVerts,
+      workA, m, slotNode, flags, levelBase, levelBase + m, triBase, N, pos, triVerts,
       reinterpret_cast<uint4*>(nodesTmp), reinterpret_cast<float4*>(tris), workB, err);
     const u64 tot = readScalar(scan64.total, st);
     if (depth < kBvh8TopLevels) top += m;

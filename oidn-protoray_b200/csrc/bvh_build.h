@@ -3,17 +3,18 @@
 // Replaces the reference's Embree build (accel/embree_intersector.cpp:68-90, rtcCommitScene,
 // reported as buildMs / buildMprim) with a build that runs on the GPU from the scene arrays
 // already in HBM:
-//   1. triangle boxes and centroid bounds, 30-bit Morton codes of the centroids;
+//   1. triangle boxes and centroid bounds, 63-bit Morton codes of the centroids;
 //   2. a stable LSD radix sort of (code, triangle) pairs;
 //   3. PLOC clustering (Meister and Bittner 2018, "Parallel Locally-Ordered Clustering for
 //      Bounding Volume Hierarchy Construction"): every cluster finds its nearest neighbour by
 //      merged-box surface area within a window of the Morton order, mutual neighbours merge,
-//      the survivors are compacted; repeated until one cluster is left. Each merge records the
-//      subtree's triangle count and SAH cost, and marks subtrees of at most three triangles
-//      whose cost as a leaf is lower than as an inner node;
-//   4. a top-down collapse, one wide level per step: a wide node takes a binary node and
-//      opens its largest inner descendants until it has eight children, assigns children to
-//      ray-octant slots and quantises their boxes to 8 bits, exactly as the host builder does.
+//      the survivors are compacted; repeated until one cluster is left. Each merge also fills
+//      the node's table of the SAH-optimal wide collapse (Ylitie, Karras and Laine 2017), whose
+//      inputs, the children's tables, are final by then;
+//   4. a top-down collapse, one wide level per step, that follows the tables: which subtrees
+//      become leaves of at most three triangles and which become wide nodes; children are
+//      assigned to ray-octant slots and their boxes quantised to 8 bits exactly as the host
+//      builder does.
 // Wide nodes are stored breadth-first over the whole tree, so the first three levels come
 // first (the shared-memory staged top levels). Every step is a scan-based, order-independent
 // computation, so a build is deterministic: the same scene gives the same bytes.
