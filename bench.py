@@ -296,7 +296,7 @@ def run_ours(args):
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded terrain scene, reference sun-sky model output)",
         "config": {"workload": f"terrain 2.6M tris, 1920x1080, {args.spp} spp per step, depth 8, rr 3, sun-sky",
-                   "triangles": scene.tri_count, "flush": "inputs larger than L2 (BVH 149 MB, path state GBs)",
+                   "triangles": scene.tri_count, "flush": "inputs larger than L2 (BVH 148 MB, path state GBs)",
                    "parallelism": f"replicas x{world}"},
         "samples_per_s": samples_per_s,
         "wall_ms_per_step": wall * 1e3 / args.steps,
@@ -320,6 +320,7 @@ def run_ours(args):
     }
     if not args.headline_only:
         barrier()
+        out["bvh_build"] = bvh_build_bench(dev, scene)
         out["small_scene"] = small_scene_bench(dev)
         out["batched"] = batched_bench(dev)
         out["adjoint"] = adjoint_bench(dev)
@@ -338,7 +339,32 @@ def run_ours(args):
 
 # DRAM bytes (read + write) of the 9 kTrace launches of one 1920x1080 x 1-spp terrain frame,
 # from ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum (profiles/kTrace_terrain_1spp.md).
-NCU_TRACE_DRAM_BYTES = 781_850_368
+NCU_TRACE_DRAM_BYTES = 738_353_920
+
+def bvh_build_bench(dev, scene, builds=3, spp=8):
+    """BVH8 build of the terrain workload on the host (binned SAH) and on the device (PLOC), the
+    reference's buildMs / buildMprim (accel/embree_intersector.cpp:88-90): best of `builds`
+    uploads each, wall time of the build alone; then the render speed over each tree (one
+    `spp`-sample frame, device-timed) -- the images are identical, the trees differ in quality."""
+    out = {"triangles": scene.tri_count}
+    for name, builder in (("host", T.PRT_BVH_HOST), ("device", T.PRT_BVH_DEVICE)):
+        scene.bvh_build = builder
+        best = None
+        for _ in range(builds if builder == T.PRT_BVH_DEVICE else 1):
+            dev.init_scene(scene)
+            st = dev.scene_stats()
+            best = st if best is None or st["build_ms"] < best["build_ms"] else best
+        dev.setup(scene, seed=0)
+        dev.render(1)
+        r = dev.render(spp)
+        out[name] = {"ms": best["build_ms"], "mprim_s": scene.tri_count / 1e3 / best["build_ms"],
+                     "nodes": best["node_count"], "depth": best["depth"], "iterations": best["iterations"],
+                     "render_mrays_s": r["mray"]}
+    scene.bvh_build = T.PRT_BVH_HOST
+    out["note"] = (f"build = wall time of the BVH build inside the scene upload; render = one 1920x1080 x {spp}-spp "
+                   "frame over that tree")
+    return out
+
 
 def small_scene_bench(dev, repeats=5):
     """The small plain-render workload: the Cornell-style room with 32 icospheres (10.3k
@@ -432,7 +458,7 @@ def inverse_batched_bench(dev, count=16, steps=5, lr=1e-2):
     """Batched differentiable workload: 16 terrain inverse-rendering problems (100k-1M
     triangles, 512x512, 16 spp, depth 6), each optimising a 512^2 RGB albedo texture on its
     terrain and the roughness of every sphere against a target render (L2 loss). One step =
-    push parameters, batched forward of all 16 (one persistent wavefront), image read-back,
+    push parameters, batched forward of all 16 (one persistent wavefront), images blitted into torch tensors,
     batched path-replay adjoint of all 16 (one persistent wavefront), Adam update (torch,
     lr 1e-2). Compared with the same step done as 16 sequential frame-form renders and
     adjoints. Wall time per step; scene upload outside both."""
@@ -477,7 +503,7 @@ def inverse_batched_bench(dev, count=16, steps=5, lr=1e-2):
         for k in range(count):
             push(k, tex[k].detach(), rough[k].detach().cpu().numpy())
         batch.render()
-        imgs = [torch.from_numpy(batch.blit(k)).cuda() for k in range(count)]
+        imgs = [batch.blit(k, out=torch.empty_like(target_imgs[k])) for k in range(count)]
         dls = [2.0 * (imgs[k] - target_imgs[k]) for k in range(count)]
         batch.adjoint(dls, gts, grs)
         loss = sum(float(((imgs[k] - target_imgs[k]) ** 2).sum()) for k in range(count))
@@ -515,7 +541,7 @@ def inverse_batched_bench(dev, count=16, steps=5, lr=1e-2):
         dev.init_sampler(seed)
         dev.clear_frame()
         dev.render(s.spp)
-        img = torch.from_numpy(dev.blit_frame()).cuda()
+        img = dev.blit_frame(out=torch.empty_like(target_imgs[k]))
         dl = 2.0 * (img - target_imgs[k])
         gt = torch.zeros(tex[k].numel(), device="cuda")
         gr = torch.zeros(len(s.materials), device="cuda")

@@ -425,7 +425,12 @@ class Batch:
         self.dev._check(self.dev.lib.prt_cuda_batch_render(self.h, C.byref(st)))
         return {name: getattr(st, name) for name, _ in T.RenderStats._fields_}
 
-    def blit(self, item, aov=T.PRT_BLIT_HDR):
+    def blit(self, item, aov=T.PRT_BLIT_HDR, out=None):
+        """(height, width, 3) float32 of one item; `out` may be a CUDA torch tensor (zero copy)."""
+        if out is not None and hasattr(out, "data_ptr"):
+            self.dev._check(self.dev.lib.prt_cuda_batch_blit(self.h, item, aov,
+                                                             C.cast(C.c_void_p(out.data_ptr()), C.POINTER(C.c_float))))
+            return out
         sc = self.frames[item][0]
         img = np.zeros((sc.height, sc.width, 3), np.float32)
         self.dev._check(self.dev.lib.prt_cuda_batch_blit(self.h, item, aov, T.fptr(img)))
