@@ -281,6 +281,33 @@ int prt_cuda_scene_stats(prt_context* ctx, prt_scene_stats* out);
 int prt_cuda_scene_bvh(prt_context* ctx, void* nodes, int64_t node_capacity, void* tris, int64_t tri_capacity,
                        int64_t* node_count, int64_t* tri_count);
 
+/* ---- scene files -------------------------------------------------------------------------
+ * The reference's rkscene format: a JSON document (.rkscene) with one binary buffer (.rkbin) of
+ * typed arrays (rkscene/rkscene.h:264-905). A loaded scene is the flat description above:
+ * every file material a Standard material (texture maps for baseColor only, read from
+ * little-endian colour PFM images, UV set 0, no transform), geometries without a valid
+ * material bound to the default (Principled) material appended after the file's, and each
+ * object's geometries added once, or once per instance transform with positions and normals
+ * transformed (instances are always flattened), in file order (render/scene.cpp:174-362). The
+ * file's lights list is checked but, as in Scene::loadScene, not used: the environment comes
+ * from the caller. Host-only: no GPU is needed to load or describe a file. */
+typedef struct prt_rkscene prt_rkscene;
+
+/* Loads `path`. On failure returns PRT_ERR_INVALID_ARG (malformed or unsupported content) or
+ * PRT_ERR_LOGIC (a file that cannot be opened or read) and writes the reason to msg
+ * (msg_capacity bytes, may be 0). */
+int prt_rkscene_load(const char* path, prt_rkscene** out, char* msg, int32_t msg_capacity);
+/* Points desc at the loaded scene's arrays (valid until prt_rkscene_free); env is zeroed and
+ * bvh_build is PRT_BVH_HOST: set them before prt_cuda_scene_upload. */
+int prt_rkscene_desc(const prt_rkscene* scene, prt_scene_desc* desc);
+int prt_rkscene_free(prt_rkscene* scene);
+
+/* Device::initScene(path, props) + initLights(props) (render/device_cpu.cpp:96-110) for an
+ * rkscene file: loads it, applies the environment lights (env may be NULL: none) and the BVH
+ * builder, and uploads it as prt_cuda_scene_upload does. A file that cannot be read or parsed
+ * gives PRT_ERR_INVALID_ARG with the reason in prt_cuda_last_error. */
+int prt_cuda_scene_load(prt_context* ctx, const char* path, const prt_env_desc* env, int32_t bvh_build);
+
 /* Device::initRenderer (render/device_cpu.cpp:32-46) for type "pathStream", sampler "sobolBurley". */
 int prt_cuda_renderer(prt_context* ctx, const prt_renderer_desc* renderer);
 

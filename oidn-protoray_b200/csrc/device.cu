@@ -4,6 +4,7 @@
 #include "../../include/prt_cuda.h"
 #include "runtime.h"
 #include "bvh_build.h"
+#include "rkscene_load.h"
 
 #include <algorithm>
 #include <cfloat>
@@ -21,6 +22,11 @@ using namespace prt;
 struct prt_context
 {
   Context c;
+};
+
+struct prt_rkscene
+{
+  RkScene scene;
 };
 
 namespace {
@@ -939,6 +945,28 @@ int prt_cuda_frame_error(prt_context* ctx, float* error)
   });
 }
 
+int prt_cuda_scene_load(prt_context* ctx, const char* path, const prt_env_desc* env, int32_t bvh_build)
+{
+  return guarded(ctx, [&](Context& c) {
+    if (!path) throw std::invalid_argument("null path");
+    RkScene scene;
+    try
+    {
+      loadRkScene(path, scene);
+    }
+    catch (const std::runtime_error& e)
+    {
+      throw std::invalid_argument(e.what());  // a path that cannot be read is a bad argument here
+    }
+    prt_scene_desc desc;
+    scene.describe(desc);
+    if (env) desc.env = *env;
+    desc.bvh_build = bvh_build;
+    cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+    uploadScene(c, &desc);
+  });
+}
+
 int prt_cuda_scene_stats(prt_context* ctx, prt_scene_stats* out)
 {
   return guarded(ctx, [&](Context& c) {
@@ -1131,6 +1159,51 @@ int prt_bvh8_check(const void* nodes, int64_t node_count, const void* tris, int6
   {
     return PRT_ERR_LOGIC;
   }
+}
+
+int prt_rkscene_load(const char* path, prt_rkscene** out, char* msg, int32_t msg_capacity)
+{
+  auto report = [&](const char* what) {
+    if (msg && msg_capacity > 0)
+    {
+      const size_t k = std::min(std::strlen(what), (size_t)msg_capacity - 1);
+      std::memcpy(msg, what, k);
+      msg[k] = 0;
+    }
+  };
+  if (!path || !out || msg_capacity < 0 || (msg_capacity > 0 && !msg)) return PRT_ERR_INVALID_ARG;
+  report("");
+  *out = nullptr;
+  try
+  {
+    std::unique_ptr<prt_rkscene> r(new prt_rkscene);
+    loadRkScene(path, r->scene);
+    *out = r.release();
+    return PRT_OK;
+  }
+  catch (const std::invalid_argument& e)
+  {
+    report(e.what());
+    return PRT_ERR_INVALID_ARG;
+  }
+  catch (const std::exception& e)
+  {
+    report(e.what());
+    return PRT_ERR_LOGIC;
+  }
+}
+
+int prt_rkscene_desc(const prt_rkscene* scene, prt_scene_desc* desc)
+{
+  if (!scene || !desc) return PRT_ERR_INVALID_ARG;
+  scene->scene.describe(*desc);
+  return PRT_OK;
+}
+
+int prt_rkscene_free(prt_rkscene* scene)
+{
+  delete scene;
+  return PRT_OK;
 }
 
 int prt_bvh8_build_host(const float* tri_verts, int64_t tri_count, void* nodes, int64_t node_capacity, void* tris,

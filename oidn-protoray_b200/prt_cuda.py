@@ -92,6 +92,10 @@ def load_library():
                                    P(C.c_float), P(C.c_int64), P(C.c_int64)]
     lib.prt_bvh8_build_host.argtypes = [P(C.c_float), C.c_int64, vp, C.c_int64, vp, C.c_int64, P(C.c_int64),
                                         P(C.c_int32)]
+    lib.prt_rkscene_load.argtypes = [C.c_char_p, P(vp), C.c_char_p, C.c_int32]
+    lib.prt_rkscene_desc.argtypes = [vp, P(T.SceneDesc)]
+    lib.prt_rkscene_free.argtypes = [vp]
+    lib.prt_cuda_scene_load.argtypes = [vp, C.c_char_p, P(T.EnvDesc), C.c_int32]
     _lib = lib
     return lib
 
@@ -114,6 +118,57 @@ def bvh8_count(tri_verts, rays):
 
 BVH8_NODE_BYTES = 80
 BVH8_TRI_BYTES = 48
+
+
+class RkScene:
+    """An rkscene file loaded on the host (prt_rkscene_load): the flat scene description the
+    device uploads, readable as numpy arrays. Raises ValueError for malformed or unsupported
+    content and OSError for files that cannot be read."""
+
+    def __init__(self, path):
+        self.lib = load_library()
+        self.h = None
+        h = C.c_void_p()
+        msg = C.create_string_buffer(512)
+        rc = self.lib.prt_rkscene_load(str(path).encode(), C.byref(h), msg, 512)
+        if rc == T.PRT_ERR_INVALID_ARG:
+            raise ValueError(msg.value.decode())
+        if rc != T.PRT_OK:
+            raise OSError(msg.value.decode())
+        self.h = h
+        self.d = T.SceneDesc()
+        self.lib.prt_rkscene_desc(self.h, C.byref(self.d))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.prt_rkscene_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def meshes(self):
+        out = []
+        for i in range(self.d.mesh_count):
+            m = self.d.meshes[i]
+            nv, nt = m.vertex_count, m.tri_count
+            arr = lambda p, n: np.ctypeslib.as_array(p, (n,)).copy()
+            out.append(dict(positions=arr(m.positions, 3 * nv).reshape(-1, 3) if nv else np.zeros((0, 3), np.float32),
+                            normals=arr(m.normals, 3 * nv).reshape(-1, 3) if m.normals else None,
+                            texcoords=arr(m.texcoords, 2 * nv).reshape(-1, 2) if m.texcoords else None,
+                            indices=arr(m.indices, 3 * nt).reshape(-1, 3) if nt else np.zeros((0, 3), np.int32),
+                            material=m.material))
+        return out
+
+    def materials(self):
+        return [T.Material.from_buffer_copy(self.d.materials[i]) for i in range(self.d.material_count)]
+
+    def textures(self):
+        out = []
+        for i in range(self.d.texture_count):
+            t = self.d.textures[i]
+            out.append(np.ctypeslib.as_array(t.rgb, (t.height * t.width * 3,)).reshape(t.height, t.width, 3).copy())
+        return out
 
 
 def bvh8_build_host(tri_verts):
@@ -211,6 +266,12 @@ class DeviceCuda:
         self._keep = desc
         self._check(self.lib.prt_cuda_scene_upload(self.h, C.byref(desc)))
         self.scene = scene
+
+    def load_scene(self, path, env=None, bvh_build=T.PRT_BVH_HOST):
+        """Device::initScene(path) + initLights: uploads an rkscene file (prt_cuda_scene_load);
+        `env` is a prt_types.EnvDesc or None (no environment light)."""
+        self._check(self.lib.prt_cuda_scene_load(self.h, str(path).encode(), C.byref(env) if env is not None else None,
+                                                 int(bvh_build)))
 
     def scene_stats(self):
         """BVH statistics of the uploaded scene (prt_scene_stats) as a dict."""

@@ -520,3 +520,88 @@ def batch_inverse_frames(count=16, seed=0, tri_range=(1e5, 1e6), size=512, spp=1
         out.append((s, params, sampler_seed))
     return out
 
+
+
+# -- rkscene files ---------------------------------------------------------------------------------
+_RK_SCALARS = [("baseWeight", "base_weight"), ("metalness", "metalness"), ("diffuseRoughness", "diffuse_roughness"),
+               ("specularWeight", "specular_weight"), ("specularRoughness", "specular_roughness"),
+               ("specularIOR", "specular_ior"), ("transmissionWeight", "transmission_weight"),
+               ("transmissionDepth", "transmission_depth"), ("subsurfaceWeight", "subsurface_weight"),
+               ("subsurfaceAnisotropy", "subsurface_anisotropy"), ("coatWeight", "coat_weight"),
+               ("coatRoughness", "coat_roughness"), ("coatIOR", "coat_ior"), ("sheenWeight", "sheen_weight"),
+               ("sheenRoughness", "sheen_roughness"), ("emissionLuminance", "emission_luminance"),
+               ("opacity", "opacity")]
+_RK_COLORS = [("specularColor", "specular_color"), ("transmissionColor", "transmission_color"),
+              ("subsurfaceColor", "subsurface_color"), ("coatColor", "coat_color"), ("sheenColor", "sheen_color"),
+              ("emissionColor", "emission_color")]
+
+
+def write_pfm(path, rgb):
+    """Little-endian colour PFM of an (h, w, 3) image given top row first."""
+    rgb = np.ascontiguousarray(rgb, np.float32)
+    with open(path, "wb") as f:
+        f.write(f"PF\n{rgb.shape[1]} {rgb.shape[0]}\n-1.0\n".encode())
+        f.write(rgb[::-1].astype("<f4").tobytes())
+
+
+def write_rkscene(scene, path, objects=None):
+    """Writes `scene` as an rkscene file (JSON + .rkbin buffer + PFM textures), the layout of
+    rkscene::save (rkscene/rkscene.h:907-941). One geometry per mesh; `objects` is a list of
+    (geometry indices, transforms or None) with transforms (k, 3, 4) arrays whose columns are
+    U V N P -- by default one object per geometry, without instances. Only Standard materials
+    are representable."""
+    import json
+
+    path = pathlib.Path(path)
+    bin_path = path.with_suffix(".rkbin")
+    blob = bytearray()
+
+    def buf(arr, kind):
+        nonlocal blob
+        a = np.ascontiguousarray(arr)
+        view = {"type": kind, "count": int(a.shape[0]), "byteOffset": len(blob)}
+        blob += a.tobytes()
+        return view
+
+    mats = []
+    for i, m in enumerate(scene.materials):
+        if m.model != T.PRT_MATERIAL_STANDARD:
+            raise ValueError("rkscene materials are Standard materials")
+        j = {"name": f"mat{i}"}
+        for key, field in _RK_SCALARS:
+            j[key] = float(getattr(m, field))
+        base = [float(x) for x in m.base_color]
+        if m.base_color_texture >= 0:
+            j["baseColor"] = {"image": f"{path.stem}_tex{m.base_color_texture}.pfm", "factor": base}
+        else:
+            j["baseColor"] = base
+        for key, field in _RK_COLORS:
+            j[key] = [float(x) for x in getattr(m, field)]
+        j["thinWalled"] = bool(m.thin_walled)
+        mats.append(j)
+    for k, t in enumerate(scene.textures):
+        write_pfm(path.parent / f"{path.stem}_tex{k}.pfm", t)
+    geoms = []
+    for g, mesh in enumerate(scene.meshes):
+        j = {"name": f"mesh{g}", "type": "triangle", "positions": buf(mesh["positions"].astype("<f4"), "float3")}
+        if mesh["normals"] is not None:
+            j["normals"] = buf(mesh["normals"].astype("<f4"), "float3")
+        if mesh["texcoords"] is not None:
+            j["texcoords"] = buf(mesh["texcoords"].astype("<f4"), "float2")
+        j["indices"] = buf(mesh["indices"].astype("<u4").reshape(-1), "uint")
+        j["material"] = int(mesh["material"])
+        geoms.append(j)
+    if objects is None:
+        objects = [([g], None) for g in range(len(scene.meshes))]
+    objs = []
+    for k, (ids, xfs) in enumerate(objects):
+        j = {"name": f"object{k}", "geometries": [int(i) for i in ids]}
+        if xfs is not None:
+            xf = np.asarray(xfs, np.float32).reshape(-1, 3, 4)
+            j["instances"] = buf(np.ascontiguousarray(xf.transpose(0, 2, 1)).astype("<f4").reshape(-1, 12), "float3x4")
+        objs.append(j)
+    doc = {"name": path.stem, "materials": mats, "geometries": geoms, "objects": objs, "lights": [],
+           "buffers": [{"uri": bin_path.name, "byteLength": len(blob)}]}
+    bin_path.write_bytes(bytes(blob))
+    path.write_text(json.dumps(doc, indent=2))
+    return path

@@ -120,6 +120,17 @@ def sobol(seed, sample_index, pixel_id, dim_set, dims):
     return out_simd.reshape(n, dims), out_scalar.reshape(n, dims)
 
 
+def write_rkscene(scene, directory):
+    """Writes `scene` with the reference's own rkscene::save (textures as PFM beside it) and
+    returns the .rkscene path."""
+    lib = _lib()
+    lib.ref_write_rkscene.argtypes = [C.POINTER(T.SceneDesc), C.c_char_p, C.c_char_p, C.c_int]
+    desc = scene.desc(oracle=True)
+    out = C.create_string_buffer(4096)
+    _check(lib.ref_write_rkscene(C.byref(desc), str(directory).encode(), out, 4096))
+    return out.value.decode()
+
+
 class RefDevice:
     """The reference's DeviceCpu running pathStream/sobolBurley on a Scene."""
 

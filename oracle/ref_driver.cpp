@@ -253,6 +253,23 @@ int ref_create(const prt_scene_desc* scene, const prt_camera_desc* cam, const pr
   }
 }
 
+// The scene written by the reference's own rkscene::save (rkscene/rkscene.h:907-941) into
+// `dir`; the path of the .rkscene file goes to path_out (capacity bytes).
+int ref_write_rkscene(const prt_scene_desc* scene, const char* dir, char* path_out, int capacity)
+{
+  try
+  {
+    const std::string path = writeScene(scene, dir);
+    if (!path_out || capacity <= (int)path.size()) return -1;
+    std::memcpy(path_out, path.c_str(), path.size() + 1);
+    return 0;
+  }
+  catch (const std::exception&)
+  {
+    return -1;
+  }
+}
+
 int ref_destroy(void* handle)
 {
   delete (RefHandle*)handle;
