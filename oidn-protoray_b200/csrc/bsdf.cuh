@@ -685,6 +685,29 @@ struct CoatLayer
     return baseValue * T;
   }
 
+  // Straight-through transmittance of the layer over a substrate transmittance (CoatingBsdf /
+  // RoughCoatingBsdf::getTransparency): absorption along the refracted path, times 1 - F
+  // (Fresnel, or the directional reflection albedo when rough).
+  PRT_D f3 transparency(const DevTables& t, const Frame& fr, f3 wo, f3 baseT) const
+  {
+    const float cosThetaO = dot(wo, fr.N);
+    if (!(cosThetaO > 0.f)) return mk(0.f);
+    float F, length;
+    if (rough)
+    {
+      length = 1.f / refractCos(cosThetaO, eta);
+      F = reflAlbedo(t, cosThetaO, eta, roughness) * scale;
+    }
+    else
+    {
+      float cosThetaO1;
+      F = fresnelDielectricEx(cosThetaO, cosThetaO1, eta) * scale;
+      length = 1.f / cosThetaO1;
+    }
+    baseT = lerp3(baseT, baseT * powf3(color, thickness * length), scale);
+    return baseT * (1.f - F);
+  }
+
   PRT_D f3 coatValue(const Frame& fr, f3 wo, f3 wi, float cosThetaO, float& coatPdf) const
   {
     const f3 wh = normalize(wo + wi);
@@ -956,40 +979,369 @@ enum : int
   kSlotOpaque = 0,
   kSlotDielectric = 1,
   kSlotConductor = 2,
+  kSlotThin = 3,         // thin-walled dielectric (translucent base of a thin-walled material)
+  kSlotTransparent = 4,  // TransparentBtdf (translucent base whose IOR equals the ambient IOR)
 };
 
 
-// The opaque base: a Lambertian lobe, optionally under the specular dielectric layer
-// (material/standard.cpp:441-502).
-template <bool R>
+// DiffuseBtdf (bsdf/diffuse.h:126-166): Lambertian transmission to the far side of the shading
+// normal.
+struct DiffuseBtdfLobe
+{
+  f3 color;
+
+  PRT_D int flags() const { return kDiffuseTransmission; }
+  PRT_D float importance() const { return reduceMax(color); }
+  PRT_D f3 albedo() const { return color; }
+
+  PRT_D f3 eval(const Frame& fr, f3 Ng, f3 wo, f3 wi, float& pdf) const
+  {
+    const float cosThetaI = fmaxf(-dot(wi, fr.N), 0.f);
+    pdf = cosThetaI * kInvPi;
+    return color * kInvPi * cosThetaI;
+  }
+
+  PRT_D f3 sample(const Frame& fr, f3 Ng, f3 wo, float sx, float sy, float sc, f3& wi, float& pdf, int& type) const
+  {
+    wi = -toWorld(fr, cosineSampleHemisphere(pdf, sx, sy));
+    type = kDiffuseTransmission;
+    if (!(dot(wi, Ng) <= 0.f)) return mk(0.f);
+    return color;
+  }
+};
+
+// Thin-walled dielectric: ThinDielectricBsdf (bsdf/thin_dielectric.h:74-160) when smooth,
+// ThinRoughDielectricBsdf (bsdf/thin_rough_dielectric.h:166-340) when rough. Light is reflected
+// (specular, or GGX with Kulla-Conty energy compensation) or passes straight through
+// (unbent) attenuated by color^(thickness / cos(refracted angle)).
+struct ThinDielectricLobe
+{
+  float eta;
+  f3 color;
+  float thickness;
+  GGX mf;
+  float roughness;
+  float Eavg, fmsScale;
+  bool rough;
+
+  PRT_D void init(const DevTables& t, float e, f3 col, float thick, float rgh, bool isRough)
+  {
+    eta = e;
+    color = col;
+    thickness = thick;
+    rough = isRough;
+    roughness = rgh;
+    mf.ax = mf.ay = roughnessToAlpha(rgh);
+    if (rough)
+    {
+      Eavg = ggxAlbedoAvg(t, rgh);
+      const float Favg = fresnelDielectricAvg(eta);
+      fmsScale = Favg * (1.f - Eavg) * (1.f / (1.f - Favg * Eavg));
+    }
+  }
+
+  PRT_D int flags() const { return (rough ? kGlossyReflection : kSpecularReflection) | kUnbentTransmission; }
+  PRT_D float importance() const { return 1.f; }
+  PRT_D f3 albedo() const { return powf3(color, thickness); }
+
+  // Probability of reflection: Fresnel (smooth) or the directional reflection albedo plus the
+  // compensated multiple scattering (rough).
+  PRT_D float reflectance(const DevTables& t, float cosThetaO, float& cosThetaT) const
+  {
+    if (!rough) return fresnelDielectricEx(cosThetaO, cosThetaT, eta);
+    cosThetaT = refractCos(cosThetaO, eta);
+    const float Eo = ggxAlbedo(t, cosThetaO, roughness);
+    return reflAlbedo(t, cosThetaO, eta, roughness) + fmsScale * (1.f - Eo);
+  }
+
+  PRT_D f3 transparency(const DevTables& t, const Frame& fr, f3 wo) const
+  {
+    const float cosThetaO = dot(wo, fr.N);
+    if (!(cosThetaO > 0.f)) return mk(0.f);
+    float cosThetaT;
+    const float R = reflectance(t, cosThetaO, cosThetaT);
+    return (1.f - R) * powf3(color, (1.f / cosThetaT) * thickness);
+  }
+
+  PRT_D f3 eval(const DevTables& t, const Frame& fr, f3 Ng, f3 wo, f3 wi, float& pdf) const
+  {
+    pdf = 0.f;
+    if (!rough) return mk(0.f);
+    const float cosThetaO = dot(wo, fr.N);
+    if (!(cosThetaO > 0.f)) return mk(0.f);
+    const float cosThetaI = dot(wi, fr.N);
+    if (!(cosThetaI * dot(wi, Ng) > 0.f) || !(cosThetaI > 0.f)) return mk(0.f);
+    const f3 wh = normalize(wi + wo);
+    const float cosThetaOH = dot(wo, wh);
+    const f3 wo0 = toLocal(fr, wo), wi0 = toLocal(fr, wi), wh0 = toLocal(fr, wh);
+    const float F = fresnelDielectric(cosThetaOH, eta);
+    float whPdf;
+    const float D = mf.evalVisible(wh0, wo0, cosThetaOH, whPdf);
+    const float G = mf.G2(wo0, wi0);
+    const float Eo = ggxAlbedo(t, cosThetaO, roughness);
+    const float Ei = ggxAlbedo(t, cosThetaI, roughness);
+    const float fms = fmsScale * ((1.f - Eo) * (1.f - Ei) * (1.f / (kPi * (1.f - Eavg))) * cosThetaI);
+    const float R = reflAlbedo(t, cosThetaO, eta, roughness) + fmsScale * (1.f - Eo);
+    pdf = whPdf * (1.f / (4.f * fabsf(cosThetaOH))) * R;
+    return mk(F * D * G * (1.f / (4.f * cosThetaO)) + fms);
+  }
+
+  PRT_D f3 sample(const DevTables& t, const Frame& fr, f3 Ng, f3 wo, float sx, float sy, float sc, f3& wi,
+                  float& pdf, int& type) const
+  {
+    pdf = 0.f;
+    wi = mk(0.f);
+    const float cosThetaO = dot(wo, fr.N);
+    if (!(cosThetaO > 0.f)) return mk(0.f);
+    if (!rough)
+    {
+      float cosThetaT;
+      const float F = fresnelDielectricEx(cosThetaO, cosThetaT, eta);
+      if (sc <= F)
+      {
+        wi = 2.f * cosThetaO * fr.N - wo;
+        type = kSpecularReflection;
+        pdf = F;
+        return dot(wi, Ng) > 0.f ? mk(1.f) : mk(0.f);
+      }
+      wi = -wo;
+      type = kUnbentTransmission;
+      pdf = 1.f - F;
+      return dot(wi, Ng) < 0.f ? powf3(color, (1.f / cosThetaT) * thickness) : mk(0.f);
+    }
+    const float Eo = ggxAlbedo(t, cosThetaO, roughness);
+    const float R = reflAlbedo(t, cosThetaO, eta, roughness) + fmsScale * (1.f - Eo);
+    if (sc <= R)
+    {
+      const f3 wo0 = toLocal(fr, wo);
+      float whPdf;
+      const f3 wh = toWorld(fr, mf.sampleVisible(wo0, whPdf, sx, sy));
+      const float cosThetaOH = dot(wo, wh);
+      wi = 2.f * cosThetaOH * wh - wo;
+      const float cosThetaI = dot(wi, fr.N);
+      type = kGlossyReflection;
+      if (!(cosThetaI > 0.f) || !(dot(wi, Ng) > 0.f)) return mk(0.f);
+      const f3 wi0 = toLocal(fr, wi);
+      const float F = fresnelDielectric(cosThetaOH, eta);
+      const float G = mf.G2(wo0, wi0);
+      const float Ei = ggxAlbedo(t, cosThetaI, roughness);
+      const float fms = fmsScale * ((1.f - Eo) * (1.f - Ei) * (1.f / (kPi * (1.f - Eavg))) * cosThetaI);
+      pdf = whPdf * (1.f / (4.f * fabsf(cosThetaOH))) * R;
+      return mk(F * G * rcpSafe(mf.G1(wo0)) * (1.f / R) + fms * (1.f / pdf));
+    }
+    wi = -wo;
+    type = kUnbentTransmission;
+    pdf = 1.f - R;
+    return dot(wi, Ng) < 0.f ? powf3(color, (1.f / refractCos(cosThetaO, eta)) * thickness) : mk(0.f);
+  }
+};
+
+// MultiBsdf (bsdf/multi_bsdf.h:151-270) over two children given by callables: eval(pdf) and
+// sample(sc, wi, pdf, type) for child 0 and 1, with scales s and importances i (the child's
+// importance times its scale; a child with importance 0 takes no part).
+template <class E0, class E1>
+PRT_D f3 multi2Eval(float s0, float i0, float s1, float i1, const E0& e0, const E1& e1, float& pdf)
+{
+  f3 v = mk(0.f);
+  pdf = 0.f;
+  if (i0 > 0.f)
+  {
+    float p;
+    v += e0(p) * s0;
+    pdf += p * i0;
+  }
+  if (i1 > 0.f)
+  {
+    float p;
+    v += e1(p) * s1;
+    pdf += p * i1;
+  }
+  pdf *= 1.f / (i0 + i1);
+  return v;
+}
+
+template <class S0, class S1, class E0, class E1>
+PRT_D f3 multi2Sample(float s0, float i0, float s1, float i1, const S0& smp0, const S1& smp1, const E0& e0,
+                      const E1& e1, float sc, f3& wi, float& pdf, int& type)
+{
+  pdf = 0.f;
+  type = 0;
+  wi = mk(0.f);
+  const float isum = i0 + i1;
+  if (!(isum > 0.f)) return mk(0.f);
+  const float x = sc * isum;
+  const int choice = x > i0 ? 1 : 0;
+  const float importance = choice ? i1 : i0, prefix = choice ? i0 + i1 : i0, scale = choice ? s1 : s0;
+  const float s1c = (x + importance - prefix) * (1.f / importance);
+  f3 weight = choice ? smp1(s1c, wi, pdf, type) : smp0(s1c, wi, pdf, type);
+  if (!(reduceMax(weight) > 0.f))
+  {
+    weight = mk(0.f);
+    pdf = 0.f;
+    type = 0;
+    wi = mk(0.f);
+  }
+  weight *= scale;
+  if (!(reduceMax(weight) > 0.f) || !(pdf > 0.f)) return mk(0.f);
+  if (type & kBsdfDelta) return weight * isum * (1.f / importance);
+  f3 value = weight * pdf;
+  pdf *= importance;
+  const float io = choice ? i0 : i1;
+  if (io > 0.f)
+  {
+    float p;
+    value += (choice ? e0(p) * s0 : e1(p) * s1);
+    pdf += p * io;
+  }
+  pdf *= 1.f / isum;
+  return value * (1.f / pdf);
+}
+
+// MultiBsdf::getAlbedo accumulated child by child (no arrays, so nothing goes to local memory).
+struct AlbedoSum
+{
+  f3 v = mk(0.f);
+  float scaleSum = 0.f, total = 0.f;
+  PRT_D void add(f3 a, float s, float imp)
+  {
+    if (!(imp > 0.f)) return;
+    total += s;
+    if (!(a.x >= 0.f)) return;
+    v += a * s;
+    scaleSum += s;
+  }
+  PRT_D f3 value() const { return v * (total * rcpSafe(scaleSum)); }
+  // Without transparent children the scale sums are equal and the renormalisation is 1.
+  PRT_D f3 valueOpaque() const { return v; }
+};
+
+// The opaque base of the Standard material (material/standard.cpp:441-502): a Lambertian (or
+// Oren-Nayar) lobe, blended with the thin-walled subsurface approximation when the material has
+// one -- Multi{diffuse x (1 - subsurface), subsurface x subsurface} with subsurface =
+// Multi{diffuse BRDF x (1 - t), diffuse BTDF x t} in the subsurface colour, t = (1 +
+// anisotropy) / 2, each Multi collapsing to its only child when the other weight is below eps --
+// optionally under the specular dielectric layer. S = false compiles the subsurface out.
+template <bool R, bool S>
 struct OpaqueBase
 {
   DiffuseLobeT<R> diff;
   CoatLayer spec;
   bool hasSpec;
+  DiffuseLobeT<R> ssRefl;
+  DiffuseBtdfLobe ssTrans;
+  bool hasDiff, hasSS, ssHasR, ssHasT;
+  float wDiff, wSS, wR, wT;
 };
 
-// Substrate adaptor for the specular layer: the diffuse lobe.
-template <bool R>
-struct DiffuseSub
+// The subsurface blend alone: Multi{BRDF x wR, BTDF x wT}, or its only child.
+template <bool R, bool S>
+struct SubsurfaceTree
 {
-  DiffuseLobeT<R> d;
+  const OpaqueBase<R, S>* o;
   Frame fr;
   f3 Ng;
-  PRT_D int flags() const { return kDiffuseReflection; }
-  PRT_D float importance() const { return d.importance(); }
-  PRT_D f3 eval(const DevTables& t, f3 wo, f3 wi, float& pdf) const { return d.eval(fr, Ng, wo, wi, pdf); }
-  PRT_D f3 sample(const DevTables& t, f3 wo, float sx, float sy, float sc, f3& wi, float& pdf, int& type) const
+  PRT_D float i0() const { return o->ssHasR ? o->ssRefl.importance() * o->wR : 0.f; }
+  PRT_D float i1() const { return o->ssHasT ? o->ssTrans.importance() * o->wT : 0.f; }
+  PRT_D int flags() const { return (o->ssHasR ? kDiffuseReflection : 0) | (o->ssHasT ? kDiffuseTransmission : 0); }
+  PRT_D float importance() const
   {
-    return d.sample(fr, Ng, wo, sx, sy, sc, wi, pdf, type);
+    if (o->ssHasR && o->ssHasT) return i0() + i1();
+    return o->ssHasR ? o->ssRefl.importance() : o->ssTrans.importance();
+  }
+  PRT_D f3 albedo() const
+  {
+    if (o->ssHasR && o->ssHasT)
+    {
+      AlbedoSum sum;
+      sum.add(o->ssRefl.albedo(), o->wR, i0());
+      sum.add(o->ssTrans.albedo(), o->wT, i1());
+      return sum.value();
+    }
+    return o->ssHasR ? o->ssRefl.albedo() : o->ssTrans.albedo();
+  }
+  PRT_D f3 eval(f3 wo, f3 wi, float& pdf) const
+  {
+    if (!o->ssHasT) return o->ssRefl.eval(fr, Ng, wo, wi, pdf);
+    if (!o->ssHasR) return o->ssTrans.eval(fr, Ng, wo, wi, pdf);
+    return multi2Eval(
+      o->wR, i0(), o->wT, i1(), [&](float& p) { return o->ssRefl.eval(fr, Ng, wo, wi, p); },
+      [&](float& p) { return o->ssTrans.eval(fr, Ng, wo, wi, p); }, pdf);
+  }
+  PRT_D f3 sample(f3 wo, float sx, float sy, float sc, f3& wi, float& pdf, int& type) const
+  {
+    if (!o->ssHasT) return o->ssRefl.sample(fr, Ng, wo, sx, sy, sc, wi, pdf, type);
+    if (!o->ssHasR) return o->ssTrans.sample(fr, Ng, wo, sx, sy, sc, wi, pdf, type);
+    return multi2Sample(
+      o->wR, i0(), o->wT, i1(),
+      [&](float c, f3& w, float& p, int& ty) { return o->ssRefl.sample(fr, Ng, wo, sx, sy, c, w, p, ty); },
+      [&](float c, f3& w, float& p, int& ty) { return o->ssTrans.sample(fr, Ng, wo, sx, sy, c, w, p, ty); },
+      [&](float& p) { return o->ssRefl.eval(fr, Ng, wo, wi, p); },
+      [&](float& p) { return o->ssTrans.eval(fr, Ng, wo, wi, p); }, sc, wi, pdf, type);
   }
 };
 
-// MultiBsdf over the base lobes (bsdf/multi_bsdf.h:151-270) and the outer coat. F is the
+// The whole opaque base below the specular layer: Multi{diffuse x wDiff, subsurface x wSS}, or
+// its only child; with S = false just the diffuse lobe.
+template <bool R, bool S>
+struct OpaqueSub
+{
+  const OpaqueBase<R, S>* o;
+  Frame fr;
+  f3 Ng;
+  PRT_D SubsurfaceTree<R, S> ss() const { return SubsurfaceTree<R, S>{o, fr, Ng}; }
+  PRT_D bool blend() const { return S && o->hasSS; }
+  PRT_D float i0() const { return o->hasDiff ? o->diff.importance() * o->wDiff : 0.f; }
+  PRT_D float i1() const { return o->hasSS ? ss().importance() * o->wSS : 0.f; }
+  PRT_D int flags() const
+  {
+    if (!blend()) return kDiffuseReflection;
+    return (o->hasDiff ? kDiffuseReflection : 0) | ss().flags();
+  }
+  PRT_D float importance() const
+  {
+    if (!blend()) return o->diff.importance();
+    if (!o->hasDiff) return ss().importance();
+    return i0() + i1();
+  }
+  PRT_D f3 albedo() const
+  {
+    if (!blend()) return o->diff.albedo();
+    if (!o->hasDiff) return ss().albedo();
+    AlbedoSum sum;
+    sum.add(o->diff.albedo(), o->wDiff, i0());
+    sum.add(ss().albedo(), o->wSS, i1());
+    return sum.value();
+  }
+  PRT_D f3 eval(const DevTables& t, f3 wo, f3 wi, float& pdf) const
+  {
+    if (!blend()) return o->diff.eval(fr, Ng, wo, wi, pdf);
+    if (!o->hasDiff) return ss().eval(wo, wi, pdf);
+    return multi2Eval(
+      o->wDiff, i0(), o->wSS, i1(), [&](float& p) { return o->diff.eval(fr, Ng, wo, wi, p); },
+      [&](float& p) { return ss().eval(wo, wi, p); }, pdf);
+  }
+  PRT_D f3 sample(const DevTables& t, f3 wo, float sx, float sy, float sc, f3& wi, float& pdf, int& type) const
+  {
+    if (!blend()) return o->diff.sample(fr, Ng, wo, sx, sy, sc, wi, pdf, type);
+    if (!o->hasDiff) return ss().sample(wo, sx, sy, sc, wi, pdf, type);
+    return multi2Sample(
+      o->wDiff, i0(), o->wSS, i1(),
+      [&](float c, f3& w, float& p, int& ty) { return o->diff.sample(fr, Ng, wo, sx, sy, c, w, p, ty); },
+      [&](float c, f3& w, float& p, int& ty) { return ss().sample(wo, sx, sy, c, w, p, ty); },
+      [&](float& p) { return o->diff.eval(fr, Ng, wo, wi, p); }, [&](float& p) { return ss().eval(wo, wi, p); },
+      sc, wi, pdf, type);
+  }
+};
+
+// The Standard material's BSDF tree (material/standard.cpp:410-620): MultiBsdf over the base
+// lobes (opaque, translucent, metal; bsdf/multi_bsdf.h:151-270), the outer coat, the sheen,
+// and -- for opacity below 1 -- Multi{that x opacity, TransparentBtdf x (1 - opacity)}. F is the
 // feature set the instance may contain (branches outside F are compiled out).
 template <int F>
 struct StdBsdfT
 {
+  static constexpr bool kR = (F & kFeatRoughDiffuse) != 0;
+  static constexpr bool kS = (F & kFeatSubsurface) != 0;
   Frame fr;
   f3 Ng;
   int nLobes;
@@ -998,31 +1350,39 @@ struct StdBsdfT
   float imp[3];
   float impSum;
   int baseFlags;
-  OpaqueBase<(F & kFeatRoughDiffuse) != 0> opaque;
+  OpaqueBase<kR, kS> opaque;
   DielectricLobe diel;
+  ThinDielectricLobe thin;
   ConductorLobe cond;
   CoatLayer coat;
   bool hasCoat;
   SheenLayer sheen;
   bool hasSheen;
+  bool hasTransp;    // top-level opacity blend
+  bool hasInner;     // opacity > eps: the tree above takes part
+  float opacityW, transpW;
   f3 albedoV;
 
+  PRT_D OpaqueSub<kR, kS> opaqueSub() const { return OpaqueSub<kR, kS>{&opaque, fr, Ng}; }
+
   PRT_D int coatedFlags() const { return ((F & kFeatCoat) && hasCoat) ? coat.flags(baseFlags) : baseFlags; }
-  PRT_D int flags() const { return ((F & kFeatSheen) && hasSheen) ? sheen.flags(coatedFlags()) : coatedFlags(); }
+  PRT_D int innerFlags() const { return ((F & kFeatSheen) && hasSheen) ? sheen.flags(coatedFlags()) : coatedFlags(); }
+  PRT_D int flags() const
+  {
+    if ((F & kFeatTransparent) && hasTransp) return (hasInner ? innerFlags() : 0) | kTransparency;
+    return innerFlags();
+  }
 
   PRT_D f3 evalSlot(const DevTables& t, int k, f3 wo, f3 wi, float& pdf) const
   {
     if ((F & kFeatOpaque) && k == kSlotOpaque)
     {
-      if ((F & kFeatSpecular) && opaque.hasSpec)
-      {
-        const DiffuseSub<(F & kFeatRoughDiffuse) != 0> sub{opaque.diff, fr, Ng};
-        return opaque.spec.eval(t, sub, fr, Ng, wo, wi, pdf);
-      }
-      return opaque.diff.eval(fr, Ng, wo, wi, pdf);
+      if ((F & kFeatSpecular) && opaque.hasSpec) return opaque.spec.eval(t, opaqueSub(), fr, Ng, wo, wi, pdf);
+      return opaqueSub().eval(t, wo, wi, pdf);
     }
     if ((F & kFeatDielectric) && k == kSlotDielectric) return diel.eval(t, fr, Ng, wo, wi, pdf);
-    if (F & kFeatConductor) return cond.eval(t, fr, Ng, wo, wi, pdf);
+    if ((F & kFeatThin) && k == kSlotThin) return thin.eval(t, fr, Ng, wo, wi, pdf);
+    if ((F & kFeatConductor) && k == kSlotConductor) return cond.eval(t, fr, Ng, wo, wi, pdf);
     pdf = 0.f;
     return mk(0.f);
   }
@@ -1033,14 +1393,20 @@ struct StdBsdfT
     if ((F & kFeatOpaque) && k == kSlotOpaque)
     {
       if ((F & kFeatSpecular) && opaque.hasSpec)
-      {
-        const DiffuseSub<(F & kFeatRoughDiffuse) != 0> sub{opaque.diff, fr, Ng};
-        return opaque.spec.sample(t, sub, fr, Ng, wo, sx, sy, sc, wi, pdf, type);
-      }
-      return opaque.diff.sample(fr, Ng, wo, sx, sy, sc, wi, pdf, type);
+        return opaque.spec.sample(t, opaqueSub(), fr, Ng, wo, sx, sy, sc, wi, pdf, type);
+      return opaqueSub().sample(t, wo, sx, sy, sc, wi, pdf, type);
     }
     if ((F & kFeatDielectric) && k == kSlotDielectric) return diel.sample(t, fr, Ng, wo, sx, sy, sc, wi, pdf, type);
-    if (F & kFeatConductor) return cond.sample(t, fr, Ng, wo, sx, sy, sc, wi, pdf, type);
+    if ((F & kFeatThin) && k == kSlotThin) return thin.sample(t, fr, Ng, wo, sx, sy, sc, wi, pdf, type);
+    if ((F & kFeatConductor) && k == kSlotConductor) return cond.sample(t, fr, Ng, wo, sx, sy, sc, wi, pdf, type);
+    if ((F & kFeatTransparent) && k == kSlotTransparent)
+    {
+      // TransparentBtdf::sample (bsdf/transparent.h:32-45): straight through, weight 1.
+      wi = -wo;
+      type = kTransparency;
+      pdf = 1.f;
+      return mk(1.f);
+    }
     pdf = 0.f;
     return mk(0.f);
   }
@@ -1134,14 +1500,13 @@ struct StdBsdfT
     return sampleBase(t, wo, sx, sy, sz, wi, pdf, type);
   }
 
+  PRT_D float coatedImportance() const { return ((F & kFeatCoat) && hasCoat) ? coat.importance(impSum) : impSum; }
+
   struct CoatedSub
   {
     const StdBsdfT* b;
     PRT_D int flags() const { return b->coatedFlags(); }
-    PRT_D float importance() const
-    {
-      return ((F & kFeatCoat) && b->hasCoat) ? b->coat.importance(b->impSum) : b->impSum;
-    }
+    PRT_D float importance() const { return b->coatedImportance(); }
     PRT_D f3 eval(const DevTables& t, f3 wo, f3 wi, float& pdf) const { return b->evalCoated(t, wo, wi, pdf); }
     PRT_D f3 sample(const DevTables& t, f3 wo, float sx, float sy, float sc, f3& wi, float& pdf, int& type) const
     {
@@ -1149,20 +1514,73 @@ struct StdBsdfT
     }
   };
 
-  PRT_D f3 eval(const DevTables& t, f3 wo, f3 wi, float& pdf) const
+  // The tree below the opacity blend.
+  PRT_D f3 evalInner(const DevTables& t, f3 wo, f3 wi, float& pdf) const
   {
     if ((F & kFeatSheen) && hasSheen) return sheen.eval(t, CoatedSub{this}, fr, Ng, wo, wi, pdf);
     return evalCoated(t, wo, wi, pdf);
   }
 
-  PRT_D f3 sample(const DevTables& t, f3 wo, float sx, float sy, float sz, f3& wi, float& pdf, int& type) const
+  PRT_D f3 sampleInner(const DevTables& t, f3 wo, float sx, float sy, float sz, f3& wi, float& pdf, int& type) const
   {
     if ((F & kFeatSheen) && hasSheen) return sheen.sample(t, CoatedSub{this}, fr, Ng, wo, sx, sy, sz, wi, pdf, type);
     return sampleCoated(t, wo, sx, sy, sz, wi, pdf, type);
   }
 
+  // SheenBsdf::getImportance is max(max(sheen colour), substrate importance).
+  PRT_D float innerImportance() const
+  {
+    if ((F & kFeatSheen) && hasSheen) return fmaxf(reduceMax(sheen.color), coatedImportance());
+    return coatedImportance();
+  }
+
+  PRT_D f3 eval(const DevTables& t, f3 wo, f3 wi, float& pdf) const
+  {
+    if ((F & kFeatTransparent) && hasTransp)
+    {
+      if (!hasInner)
+      {
+        pdf = 0.f;
+        return mk(0.f);
+      }
+      return multi2Eval(
+        opacityW, innerImportance() * opacityW, transpW, transpW,
+        [&](float& p) { return evalInner(t, wo, wi, p); },
+        [&](float& p) {
+          p = 0.f;
+          return mk(0.f);
+        },
+        pdf);
+    }
+    return evalInner(t, wo, wi, pdf);
+  }
+
+  PRT_D f3 sample(const DevTables& t, f3 wo, float sx, float sy, float sz, f3& wi, float& pdf, int& type) const
+  {
+    if ((F & kFeatTransparent) && hasTransp)
+    {
+      auto transparent = [&](float c, f3& w, float& p, int& ty) {
+        w = -wo;
+        ty = kTransparency;
+        p = 1.f;
+        return mk(1.f);
+      };
+      if (!hasInner) return transparent(sz, wi, pdf, type);
+      return multi2Sample(
+        opacityW, innerImportance() * opacityW, transpW, transpW,
+        [&](float c, f3& w, float& p, int& ty) { return sampleInner(t, wo, sx, sy, c, w, p, ty); }, transparent,
+        [&](float& p) { return evalInner(t, wo, wi, p); },
+        [&](float& p) {
+          p = 0.f;
+          return mk(0.f);
+        },
+        sz, wi, pdf, type);
+    }
+    return sampleInner(t, wo, sx, sy, sz, wi, pdf, type);
+  }
+
   PRT_D f3 albedo() const { return albedoV; }
-  PRT_D f3 normal() const { return fr.N; }
+  PRT_D f3 normal() const { return ((F & kFeatTransparent) && hasTransp && !hasInner) ? mk(0.f) : fr.N; }
 };
 
 // Material texture lookup: repeat in both directions (image/image_texture.h:197-226).
@@ -1184,10 +1602,19 @@ PRT_D void addSlot(StdBsdfT<F>& b, int kind, float scale, float importance, int 
   b.baseFlags |= flags;
 }
 
-// StandardMaterial::getBsdfLobes (material/standard.cpp:410-620) for the lobes the device
-// implements: Lambertian base with an optional specular layer, rough or smooth dielectric
-// transmission, rough or smooth artistic conductor, rough or smooth coat. `backfacing` is the
-// medium-interface orientation (material/material.h:66-76).
+// The material's (textured) base colour.
+PRT_D f3 standardBaseColor(const DevScene& sc, const DevMaterial& m, const ShadeCtx& ctx)
+{
+  f3 baseColor = mk(m.baseColor[0], m.baseColor[1], m.baseColor[2]);
+  if (m.baseColorTex >= 0) baseColor = textureRgb(sc.textures[m.baseColorTex], ctx.uvx, ctx.uvy) * baseColor;
+  return clamp01(baseColor);
+}
+
+// StandardMaterial::getBsdfLobes (material/standard.cpp:410-620): Lambertian or Oren-Nayar base
+// with the thin-walled subsurface blend and an optional specular layer, rough or smooth
+// dielectric transmission (thin-walled: unbent; IOR equal to the ambient IOR: transparent),
+// rough or smooth artistic conductor, rough or smooth coat, sheen, and the opacity blend.
+// `backfacing` is the medium-interface orientation (material/material.h:66-76).
 template <int F>
 PRT_D void resolveStandard(const DevScene& sc, const DevTables& t, const DevMaterial& m, const ShadeCtx& ctx, f3 wo,
                            bool backfacing, StdBsdfT<F>& b)
@@ -1199,18 +1626,35 @@ PRT_D void resolveStandard(const DevScene& sc, const DevTables& t, const DevMate
   b.baseFlags = 0;
   b.hasCoat = false;
   b.hasSheen = false;
+  b.hasTransp = false;
+  b.hasInner = true;
   b.opaque.hasSpec = false;
+  b.opaque.hasSS = false;
+  b.opaque.hasDiff = true;
+  b.opacityW = 1.f;
+  b.transpW = 0.f;
+  const float opacity = (F & kFeatTransparent) ? clamp01(m.opacity) : 1.f;
+  if ((F & kFeatTransparent) && 1.f - opacity > kMatEps)
+  {
+    b.hasTransp = true;
+    b.opacityW = opacity;
+    b.transpW = 1.f - opacity;
+    b.hasInner = opacity > kMatEps;
+    if (!b.hasInner)
+    {
+      b.albedoV = mk(-1.f);  // TransparentBtdf::getAlbedo
+      return;
+    }
+  }
   const float base = clamp01(m.baseWeight);
-  f3 baseColor = mk(m.baseColor[0], m.baseColor[1], m.baseColor[2]);
-  if (m.baseColorTex >= 0) baseColor = textureRgb(sc.textures[m.baseColorTex], ctx.uvx, ctx.uvy) * baseColor;
-  baseColor = clamp01(baseColor);
+  const f3 baseColor = standardBaseColor(sc, m, ctx);
   const float metalness = clamp01(m.metalness);
   const float specular = clamp01(m.specularWeight);
   const float specularRoughness = clamp01(m.specularRoughness);
   const bool fromOutside = m.thinWalled ? true : !backfacing;
-  f3 albedo = mk(0.f);
+  AlbedoSum albedoSum;
   const float dielectric = 1.f - metalness;
-  if ((F & (kFeatOpaque | kFeatDielectric)) && dielectric > kMatEps)
+  if ((F & (kFeatOpaque | kFeatDielectric | kFeatThin | kFeatTransparent)) && dielectric > kMatEps)
   {
     const float transmission = clamp01(m.transmissionWeight);
     float eta = fromOutside ? m.ambientIor * (1.f / m.specularIor) : m.specularIor * (1.f / m.ambientIor);
@@ -1218,28 +1662,73 @@ PRT_D void resolveStandard(const DevScene& sc, const DevTables& t, const DevMate
     const float opaque = dielectric * (1.f - transmission);
     if ((F & kFeatOpaque) && opaque > kMatEps)
     {
-      b.opaque.diff.color = baseColor * base;
-      b.opaque.diff.rough = m.hasDiffuseRoughness != 0;
-      b.opaque.diff.roughness = clamp01(m.diffuseRoughness);
-      f3 a = b.opaque.diff.color;
-      int fl = kDiffuseReflection;
+      auto& o = b.opaque;
+      o.diff.color = baseColor * base;
+      o.diff.rough = m.hasDiffuseRoughness != 0;
+      o.diff.roughness = clamp01(m.diffuseRoughness);
+      if (F & kFeatSubsurface)
+      {
+        const float subsurface = clamp01(m.subsurfaceWeight);
+        const float diffuse = 1.f - subsurface;
+        o.hasDiff = diffuse > kMatEps;
+        o.hasSS = subsurface > kMatEps;
+        o.wDiff = diffuse;
+        o.wSS = subsurface;
+        if (o.hasSS)
+        {
+          const f3 ssColor = m.subsurfaceFromBase
+                               ? baseColor * base
+                               : clamp01(mk(m.subsurfaceColor[0], m.subsurfaceColor[1], m.subsurfaceColor[2]));
+          const float aniso = fminf(fmaxf(m.subsurfaceAnisotropy, -1.f), 1.f);
+          o.wT = (1.f + aniso) * 0.5f;
+          o.wR = 1.f - o.wT;
+          o.ssHasR = o.wR > kMatEps;
+          o.ssHasT = o.wT > kMatEps;
+          o.ssRefl.color = ssColor;
+          o.ssRefl.rough = o.diff.rough;
+          o.ssRefl.roughness = o.diff.roughness;
+          o.ssTrans.color = ssColor;
+        }
+      }
+      const auto sub = b.opaqueSub();
+      f3 a = sub.albedo();
+      int fl = sub.flags();
+      float impo = sub.importance();
       if ((F & kFeatSpecular) && fabsf(m.specularIor - m.ambientIor) > kMatEps && specular > kMatEps)
       {
-        b.opaque.hasSpec = true;
-        b.opaque.spec.init(t, eta, mk(1.f), 1.f, specularRoughness, m.hasSpecularRoughness != 0, specular);
-        fl = b.opaque.spec.flags(fl);
-        a = b.opaque.spec.albedo(a);
+        o.hasSpec = true;
+        o.spec.init(t, eta, mk(1.f), 1.f, specularRoughness, m.hasSpecularRoughness != 0, specular);
+        fl = o.spec.flags(fl);
+        a = o.spec.albedo(a);
+        impo = o.spec.importance(impo);
       }
-      const float impo = b.opaque.hasSpec ? b.opaque.spec.importance(b.opaque.diff.importance()) : b.opaque.diff.importance();
       addSlot(b, kSlotOpaque, opaque, impo, fl);
-      albedo += a * opaque;
+      albedoSum.add(a, opaque, impo * opaque);
     }
     const float translucent = dielectric * transmission * specular;
-    if ((F & kFeatDielectric) && translucent > kMatEps)
+    if ((F & (kFeatDielectric | kFeatThin | kFeatTransparent)) && translucent > kMatEps)
     {
-      b.diel.init(t, eta, specularRoughness, m.hasSpecularRoughness != 0);
-      addSlot(b, kSlotDielectric, translucent, 1.f, b.diel.flags());
-      albedo += mk(translucent);
+      if (fabsf(m.specularIor - m.ambientIor) > kMatEps)
+      {
+        if ((F & kFeatThin) && m.thinWalled)
+        {
+          const f3 tc = mk(m.transmissionColor[0], m.transmissionColor[1], m.transmissionColor[2]);
+          b.thin.init(t, eta, tc, m.thinThickness, specularRoughness, m.hasSpecularRoughness != 0);
+          addSlot(b, kSlotThin, translucent, 1.f, b.thin.flags());
+          albedoSum.add(b.thin.albedo(), translucent, translucent);
+        }
+        else if ((F & kFeatDielectric) && !m.thinWalled)
+        {
+          b.diel.init(t, eta, specularRoughness, m.hasSpecularRoughness != 0);
+          addSlot(b, kSlotDielectric, translucent, 1.f, b.diel.flags());
+          albedoSum.add(mk(1.f), translucent, translucent);
+        }
+      }
+      else if (F & kFeatTransparent)
+      {
+        addSlot(b, kSlotTransparent, translucent, 1.f, kTransparency);
+        albedoSum.add(mk(-1.f), translucent, translucent);
+      }
     }
   }
   const float metal = metalness * specular;
@@ -1249,8 +1738,9 @@ PRT_D void resolveStandard(const DevScene& sc, const DevTables& t, const DevMate
     b.cond.init(t, m.principled ? baseColor : baseColor * base, specColor, specularRoughness,
                 m.hasSpecularRoughness != 0);
     addSlot(b, kSlotConductor, metal, 1.f, b.cond.flags());
-    albedo += b.cond.albedo() * metal;
+    albedoSum.add(b.cond.albedo(), metal, metal);
   }
+  f3 albedo = (F & kFeatTransparent) ? albedoSum.value() : albedoSum.valueOpaque();
   const float coat = clamp01(m.coatWeight);
   if ((F & kFeatCoat) && coat > kMatEps && fabsf(m.coatIor - m.ambientIor) > kMatEps)
   {
@@ -1269,7 +1759,69 @@ PRT_D void resolveStandard(const DevScene& sc, const DevTables& t, const DevMate
     b.sheen.init(sheenColor + tint * (baseColor - sheenColor), clamp01(m.sheenRoughness), sheen);
     b.hasSheen = true;
   }
+  if ((F & kFeatTransparent) && b.hasTransp)
+  {
+    AlbedoSum top;
+    top.add(albedo, b.opacityW, b.innerImportance() * b.opacityW);
+    top.add(mk(-1.f), b.transpW, b.transpW);
+    albedo = top.value();
+  }
   b.albedoV = albedo;
+}
+
+// Material::getTransparency for a shadow ray crossing the surface (StandardMaterial,
+// material/standard.cpp:626-645): 1 - opacity for materials without transmission; otherwise the
+// transmittance of the BSDF tree built without its opaque and metal lobes -- thin-walled
+// dielectric (1 - R) color^(thickness / cos), transparent lobe 1, solid dielectric 0, scaled by
+// the translucent weight, through the coat (CoatLayer::transparency); a sheen layer passes
+// nothing (SheenBsdf has no transparency) -- blended with the opacity as the BSDF is.
+PRT_D f3 standardTransparency(const DevScene& sc, const DevTables& t, const DevMaterial& m, const ShadeCtx& ctx, f3 wo)
+{
+  const float opacity = clamp01(m.opacity);
+  if (!(m.type & kMatTransmissive)) return mk(1.f - opacity);
+  const bool hasTransp = 1.f - opacity > kMatEps;
+  if (hasTransp && !(opacity > kMatEps)) return mk(1.f);
+  const Frame fr = makeShadingFrame(ctx, wo);
+  f3 T = mk(0.f);
+  const float metalness = clamp01(m.metalness);
+  const float specular = clamp01(m.specularWeight);
+  const float dielectric = 1.f - metalness;
+  if (dielectric > kMatEps)
+  {
+    const float transmission = clamp01(m.transmissionWeight);
+    const float translucent = dielectric * transmission * specular;
+    if (translucent > kMatEps)
+    {
+      if (fabsf(m.specularIor - m.ambientIor) > kMatEps)
+      {
+        if (m.thinWalled)
+        {
+          float eta = m.ambientIor * (1.f / m.specularIor);
+          eta = fminf(fmaxf(eta, 1.f / 3.f), 3.f);
+          ThinDielectricLobe thin;
+          thin.init(t, eta, mk(m.transmissionColor[0], m.transmissionColor[1], m.transmissionColor[2]),
+                    m.thinThickness, clamp01(m.specularRoughness), m.hasSpecularRoughness != 0);
+          T = thin.transparency(t, fr, wo) * translucent;
+        }
+      }
+      else
+        T = mk(translucent);
+    }
+  }
+  const float coat = clamp01(m.coatWeight);
+  if (coat > kMatEps && fabsf(m.coatIor - m.ambientIor) > kMatEps)
+  {
+    const bool fromOutside = m.thinWalled ? true : !ctx.backfacing;
+    float coatEta = fromOutside ? m.ambientIor * (1.f / m.coatIor) : m.coatIor * (1.f / m.ambientIor);
+    coatEta = fminf(fmaxf(coatEta, 1.f / 3.f), 3.f);
+    CoatLayer c;
+    c.init(t, coatEta, clamp01(mk(m.coatColor[0], m.coatColor[1], m.coatColor[2])), m.coatThickness,
+           clamp01(m.coatRoughness), m.hasCoatRoughness != 0, coat);
+    T = c.transparency(t, fr, wo, T);
+  }
+  if (clamp01(m.sheenWeight) > kMatEps) T = mk(0.f);
+  if (hasTransp) T = T * opacity + mk(1.f - opacity);
+  return T;
 }
 
 } // namespace prt

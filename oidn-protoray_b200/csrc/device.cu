@@ -206,6 +206,25 @@ DevMaterial resolveMaterial(const prt_material& m, std::vector<float>& media, in
   }
   d.thinWalled = m.thin_walled;
   d.opacity = m.opacity;
+  // Thin-walled transmission: thickness / transmissionDepth, the thickness being 1 for Standard
+  // (its "thickness" parameter has scale 1 and no prop) and "thickness" for Principled.
+  d.thinThickness = (d.principled ? std::max(m.thickness, 0.f) : 1.f) / d.transmissionDepth;
+  d.subsurfaceFromBase = 0;
+  if (d.principled)
+  {
+    // PrincipledMaterial has no subsurface; a thin one has "backlight" (material/principled.cpp:
+    // 334-360): Multi{diffuse BRDF x (1 - b/2), diffuse BTDF x b/2} in the diffuse colour, b in
+    // [0, 2] -- the Standard subsurface blend with weight 1, anisotropy b - 1 and the diffuse
+    // colour.
+    d.subsurfaceWeight = 0.f;
+    const float backlight = m.thin_walled ? std::min(std::max(m.backlight, 0.f), 2.f) : 0.f;
+    if (backlight > 0.f)
+    {
+      d.subsurfaceWeight = 1.f;
+      d.subsurfaceAnisotropy = backlight - 1.f;
+      d.subsurfaceFromBase = 1;
+    }
+  }
   d.type = 0;
   if (m.emission_luminance > 0.f && m.model == PRT_MATERIAL_STANDARD) d.type |= kMatEmissive;
   d.mediumInt = d.mediumExt = 0;
@@ -235,12 +254,6 @@ DevMaterial resolveMaterial(const prt_material& m, std::vector<float>& media, in
       d.mediumExt = medium(one, d.ambientIor);
     }
   }
-  // Lobes the device implements: see resolveStandard (bsdf.cuh).
-  const bool unsupported = d.subsurfaceWeight != 0.f || d.opacity != 1.f || (d.principled && m.thin_walled && m.backlight > 0.f) ||
-                           (d.thinWalled && d.transmissionWeight != 0.f) ||
-                           (d.transmissionWeight != 0.f && std::fabs(d.specularIor - d.ambientIor) <= 1e-4f);
-  if (unsupported && !(d.type & kMatEmissive))
-    throw std::invalid_argument("material uses lobes not yet supported by the CUDA device");
   // Static lobe features (StandardMaterial::getBsdfLobes branch conditions with the
   // material's constant parameters; only the base colour can be textured).
   auto c01 = [](float x) { return std::min(std::max(x, 0.f), 1.f); };
@@ -253,8 +266,14 @@ DevMaterial resolveMaterial(const prt_material& m, std::vector<float>& media, in
     d.features |= kFeatOpaque;
     if (d.hasDiffuseRoughness) d.features |= kFeatRoughDiffuse;
     if (std::fabs(d.specularIor - d.ambientIor) > eps && spec > eps) d.features |= kFeatSpecular;
+    if (c01(d.subsurfaceWeight) > eps) d.features |= kFeatSubsurface;
   }
-  if (diel > eps && diel * trans * spec > eps) d.features |= kFeatDielectric;
+  if (diel > eps && diel * trans * spec > eps)
+  {
+    if (std::fabs(d.specularIor - d.ambientIor) <= eps) d.features |= kFeatTransparent;
+    else d.features |= d.thinWalled ? kFeatThin : kFeatDielectric;
+  }
+  if (1.f - c01(d.opacity) > eps) d.features |= kFeatTransparent;
   if (metal * spec > eps) d.features |= kFeatConductor;
   if (c01(d.coatWeight) > eps && std::fabs(d.coatIor - d.ambientIor) > eps) d.features |= kFeatCoat;
   if (c01(d.sheenWeight) > eps) d.features |= kFeatSheen;
@@ -398,6 +417,8 @@ void uploadScene(Context& c, const prt_scene_desc* s)
   }
   if (c.bvhDepth > kBvh8TraceStack) throw std::runtime_error("BVH8 deeper than the traversal stack");
   sc.topNodes = c.bvhTop;
+  sc.hasTransparent = 0;
+  for (const DevMaterial& m : mats) sc.hasTransparent |= (m.type & kMatTransparent) ? 1 : 0;
   sc.nrm = anyN ? upload(c, nrm) : nullptr;
   sc.uv = anyUV ? upload(c, uv) : nullptr;
   sc.meshFlags = upload(c, meshFlags);
@@ -1754,8 +1775,8 @@ void updateMaterials(Context& c, DevMaterial* devMaterials, std::vector<DevMater
 void requireAdjointMaterials(const std::vector<DevMaterial>& materials)
 {
   for (const DevMaterial& m : materials)
-    if (!(m.type & kMatEmissive) && (m.features & ~(kFeatOpaque | kFeatSpecular)))
-      throw std::invalid_argument("the adjoint supports Lambertian materials with an optional specular layer");
+    if ((m.type & kMatTransparent) || (!(m.type & kMatEmissive) && (m.features & ~(kFeatOpaque | kFeatSpecular))))
+      throw std::invalid_argument("the adjoint supports opaque Lambertian materials with an optional specular layer");
 }
 
 bool isDeviceMemory(const void* p)

@@ -26,7 +26,10 @@ enum : int
   kFeatCoat = 1 << 4,       // outer coat layer
   kFeatSheen = 1 << 5,      // outermost sheen layer
   kFeatRoughDiffuse = 1 << 6, // Oren-Nayar base instead of Lambert
-  kFeatAll = 127,
+  kFeatSubsurface = 1 << 7, // thin-walled subsurface / backlight: diffuse BRDF + BTDF in the opaque base
+  kFeatThin = 1 << 8,       // thin-walled dielectric transmission (unbent)
+  kFeatTransparent = 1 << 9, // transparent (continuation) lobe: opacity < 1, or transmission with ior == ambient
+  kFeatAll = 1023,
 };
 
 // Shading classes: 0 ends the path (miss, area-light hit, maxDepth); 1.. shade a surface with
@@ -85,6 +88,8 @@ struct DevMaterial
   float emission[3];     // emissionColor * emissionLuminance
   int thinWalled;
   float opacity;
+  float thinThickness;   // thin-walled transmission: thickness / transmissionDepth
+  int subsurfaceFromBase; // Principled backlight: the subsurface colour is the (textured) diffuse colour
 };
 
 struct DevTexture
@@ -158,6 +163,7 @@ struct DevScene
   int mediaCount;
   float sceneRadius;
   int topNodes;          // BVH nodes stored breadth-first at the start (shared-memory staging)
+  int hasTransparent;    // some material is transparent: shadow rays use the transparency filter
 };
 
 // BSDF energy-compensation tables (bsdf/albedo_tables.h), computed on the device at context

@@ -42,6 +42,9 @@ struct Launch
   AdjointView adj;
   // Batch form: radiance of every work item (pixel-sample) when the batch is differentiable.
   float4* pathL;
+  // Some scene of the launch has transparent materials: shadow rays take the transparency
+  // filter (host-side choice of the kShadow instantiation).
+  int anyTransparent;
 };
 
 template <int... Fs>
@@ -408,9 +411,36 @@ PRT_D void freeSlots(const Launch& L, int b, bool freed, int p)
   if (freed) L.freeList[b][f] = p;
 }
 
+// TransparentShadowFilterSimd (render/transparent_filter.h:42-94): a shadow ray that hits a
+// transparent material continues through it with its transmittance multiplied by the
+// material's transparency; any other hit, or a transmittance below 1e-5, occludes it.
+struct ShadowFilter
+{
+  const DevScene* sc;
+  const DevTables* tab;
+  f3 o, d;
+  f3* T;
+
+  PRT_D bool operator()(int triId, float t, float u, float v) const
+  {
+    const int mesh = __ldg(&sc->triVerts[triId].w);
+    const DevMaterial& m = sc->materials[__ldg(sc->meshMaterial + mesh)];
+    if (!(m.type & kMatTransparent))
+    {
+      *T = mk(0.f);
+      return true;
+    }
+    ShadeCtx ctx;
+    postIntersect(*sc, o, d, t, triId, u, v, ctx);
+    *T *= standardTransparency(*sc, *tab, m, ctx, -d);
+    return reduceMax(*T) < 1e-5f;
+  }
+};
+
 // Any-hit test of the queued shadow rays; adds the unoccluded NEE contribution and
-// finishes paths that ended at this bounce (render/path_renderer_stream.h:953-1010).
-template <bool Count, bool Batch, bool Top = false>
+// finishes paths that ended at this bounce (render/path_renderer_stream.h:953-1010). Transp:
+// scenes with transparent materials filter the hits (ShadowFilter).
+template <bool Count, bool Batch, bool Top = false, bool Transp = false>
 __global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__ count, int* __restrict__ work,
                                                int parity)
 {
@@ -435,18 +465,27 @@ __global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__
       if (Batch) info = L.ps.info[p];
       const PathEnv<Batch> E(L, info.w);
       bool unoccluded = b.w > 0.f;
+      f3 T = mk(1.f);
       if (unoccluded)
       {
-        const TraceHit h = traverse<true, Count, Top && !Batch>(E.sc.nodes, E.sc.tris, mk(a.x, a.y, a.z),
-                                                                mk(b.x, b.y, b.z), a.w, b.w, L.ps.err, &tc, top);
-        unoccluded = h.triId < 0;
+        const f3 o = mk(a.x, a.y, a.z), d = mk(b.x, b.y, b.z);
+        if (Transp && E.sc.hasTransparent)
+        {
+          const ShadowFilter flt{&E.sc, &L.tab, o, d, &T};
+          unoccluded =
+            traverse<true, Count, Top && !Batch>(E.sc.nodes, E.sc.tris, o, d, a.w, b.w, L.ps.err, &tc, top, flt)
+              .triId < 0;
+        }
+        else
+          unoccluded = traverse<true, Count, Top && !Batch>(E.sc.nodes, E.sc.tris, o, d, a.w, b.w, L.ps.err, &tc, top)
+                         .triId < 0;
       }
       float4 r = L.ps.rad[p];
       if (unoccluded)
       {
-        r.x += c.x;
-        r.y += c.y;
-        r.z += c.z;
+        r.x += c.x * T.x;
+        r.y += c.y * T.y;
+        r.z += c.z * T.z;
         L.ps.rad[p] = r;
       }
       if (tag & kShadowFinish)
@@ -1223,7 +1262,14 @@ static cudaError_t bounceLoop(Context& ctx, const Launch& L, int P, bool replay,
     if (!replay)
     {
       begin(1);
-      if (counting)
+      if (L.anyTransparent)
+      {
+        if (counting)
+          kShadow<true, false, false, true><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0);
+        else
+          kShadow<false, false, false, true><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0);
+      }
+      else if (counting)
         kShadow<true, false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0);
       else if (ctx.topStage)
         kShadow<false, false, true><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0);
@@ -1264,6 +1310,7 @@ static Launch frameLaunch(const Context& ctx, uint32_t firstSample, int samples)
   L.firstSample = firstSample;
   L.samples = samples;
   L.aovMask = ctx.aovMask;
+  L.anyTransparent = ctx.scene.hasTransparent;
   return L;
 }
 
@@ -1444,7 +1491,10 @@ int batchIteration(const Context& ctx, const Launch& L, int a, int persistent, i
   }
   kShadeEnd<true><<<shadeGrid, 256, 0, st>>>(L, L.ps.classQueues, ca + 1, 0, a);
   ShadeClassList::run<true>(1, L, st, shadeGrid, L.ps.classQueues, ca, 0, L.ps.queue[b], cb, ca + kBatchCntShadow, a);
-  kShadow<false, true><<<persistent, 256, 0, st>>>(L, ca + kBatchCntShadow, ca + kBatchCntShadow + 2, a);
+  if (L.anyTransparent)
+    kShadow<false, true, false, true><<<persistent, 256, 0, st>>>(L, ca + kBatchCntShadow, ca + kBatchCntShadow + 2, a);
+  else
+    kShadow<false, true><<<persistent, 256, 0, st>>>(L, ca + kBatchCntShadow, ca + kBatchCntShadow + 2, a);
   return 5 + (kShadeClasses - 1);
 }
 
@@ -1489,6 +1539,7 @@ static cudaError_t runBatch(Context& ctx, BatchState& B, RenderCounters& rc, boo
     L.freeList[0] = B.freeList[0];
     L.freeList[1] = B.freeList[1];
     L.pathL = B.pathL;
+    for (const BatchItem& it : B.items) L.anyTransparent |= it.sc.hasTransparent;
     const int persistent = ctx.smCount * ctx.traceBlocks;
     const int shadeGrid = ctx.smCount * ctx.shadeBlocks;
     const int regenGrid = gridFor(ctx, C);

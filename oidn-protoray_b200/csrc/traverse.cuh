@@ -157,10 +157,18 @@ struct TraceCount
   int tris = 0;
 };
 
-template <bool AnyHit, bool Count = false, bool Top = false>
+// Any-hit filter that accepts every hit (plain occlusion).
+struct AcceptAll
+{
+  PRT_D bool operator()(int triId, float t, float u, float v) const { return true; }
+};
+
+// AnyHit: stop at the first hit the filter accepts (filter(triangle, t, u, v) == true); hits it
+// rejects are skipped without shortening the ray. Closest hit ignores the filter.
+template <bool AnyHit, bool Count = false, bool Top = false, class Filter = AcceptAll>
 PRT_D TraceHit traverse(const uint4* __restrict__ nodes, const float4* __restrict__ tris, f3 o, f3 d,
                         float tnear, float tfar, uint32_t* errFlag, TraceCount* count = nullptr,
-                        int topCount = 0)
+                        int topCount = 0, const Filter& filter = Filter())
 {
   TraceHit h;
   h.triId = -1;
@@ -185,6 +193,7 @@ PRT_D TraceHit traverse(const uint4* __restrict__ nodes, const float4* __restric
       {
         if (AnyHit)
         {
+          if (!filter(id, t, u, v)) continue;
           h.triId = id;
           h.t = t;
           return h;

@@ -257,6 +257,46 @@ def cornell_lobes(seed=0, width=128, height=128, spp=16, max_depth=5):
     return s
 
 
+def cornell_translucent(seed=0, width=128, height=128, spp=16, max_depth=6):
+    """The small scene with the see-through lobes: spheres cycling through thin smooth glass,
+    thin rough tinted glass, half-opaque Lambert, Standard subsurface, half transmission at the
+    ambient IOR and a thin-walled Oren-Nayar subsurface that transmits most of its light (the
+    structure of a Principled backlight); plus a thin glass pane under the ceiling light and a
+    half-opaque panel, so that shadow rays cross transparent surfaces. Standard materials only:
+    the reference renders scenes from rkscene files, which hold Standard materials."""
+    s = cornell(seed=seed, width=width, height=height, spp=spp, max_depth=max_depth)
+    rng = np.random.default_rng(seed + 91)
+    first = 4
+    for k in range(first, len(s.materials)):
+        c = tuple(float(x) for x in s.materials[k].base_color)
+        kind = (k - first) % 6
+        if kind == 0:
+            m = T.material(transmission_weight=1.0, thin_walled=1, specular_roughness=0.0,
+                           transmission_color=(0.9, 0.95, 0.8))
+        elif kind == 1:
+            m = T.material(transmission_weight=1.0, thin_walled=1, specular_roughness=float(rng.uniform(0.1, 0.3)),
+                           transmission_color=c, transmission_depth=0.5)
+        elif kind == 2:
+            m = T.material(base_color=c, specular_weight=0.0, opacity=0.5)
+        elif kind == 3:
+            m = T.material(base_color=c, specular_roughness=0.3, subsurface_weight=0.6,
+                           subsurface_color=(0.9, 0.6, 0.4), subsurface_anisotropy=float(rng.uniform(-0.5, 0.5)))
+        elif kind == 4:
+            m = T.material(base_color=c, transmission_weight=0.5, specular_ior=1.0)
+        else:
+            m = T.material(base_color=c, specular_roughness=0.4, diffuse_roughness=0.4, thin_walled=1,
+                           subsurface_weight=1.0, subsurface_color=c, subsurface_anisotropy=0.5)
+        s.materials[k] = m
+    pane = s.add_material(T.material(transmission_weight=1.0, thin_walled=1, specular_roughness=0.05,
+                                     transmission_color=(0.8, 0.9, 1.0)))
+    p, i = _quad((-0.6, 1.6, -0.6), (0.3, 1.6, -0.6), (0.3, 1.6, 0.4), (-0.6, 1.6, 0.4))
+    s.add_mesh(p, i, pane)
+    panel = s.add_material(T.material(base_color=(0.9, 0.8, 0.3), specular_weight=0.0, opacity=0.4))
+    p, i = _quad((0.2, 0.0, -0.8), (0.9, 0.0, -0.2), (0.9, 1.2, -0.2), (0.2, 1.2, -0.8))
+    s.add_mesh(p, i, panel)
+    return s
+
+
 def smooth_noise_texture(size, seed, lo=0.1, hi=0.9):
     """(size, size, 3) smooth value noise in [lo, hi], one seeded noise per channel."""
     u = (np.arange(size) + 0.5) / size

@@ -220,6 +220,41 @@ public:
     return false;
   }
 
+  // Any-hit with an intersection filter: f(triangle, t, u, v) is called for every triangle the
+  // ray hits within [tnear, tfar] (each once, in traversal order) until it returns true, which
+  // makes the ray occluded; hits it rejects do not shorten the ray (Embree's occluded-filter
+  // semantics).
+  template <class F>
+  bool occludedFiltered(const float o[3], const float d[3], float tnear, float tfar, F&& f) const
+  {
+    float inv[3];
+    for (int k = 0; k < 3; ++k) inv[k] = 1.0f / d[k];
+    int stack[128];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0)
+    {
+      const Node& node = nodes[stack[--sp]];
+      if (!boxHit(node, o, inv, tnear, tfar)) continue;
+      if (node.count > 0)
+      {
+        for (int j = 0; j < node.count; ++j)
+        {
+          const int ti = order[node.left + j];
+          float t, uu, vv;
+          if (intersectTri(tris[ti], o, d, tnear, tfar, t, uu, vv) && f(ti, t, uu, vv)) return true;
+        }
+      }
+      else
+      {
+        if (sp + 2 > 128) throw std::runtime_error("oracle BVH stack overflow");
+        stack[sp++] = node.left;
+        stack[sp++] = node.left + 1;
+      }
+    }
+    return false;
+  }
+
 private:
   struct C3 { float c[3]; };
   struct B3 { float lo[3], hi[3]; };
@@ -437,16 +472,36 @@ protected:
     }
   }
 
+  // Shadow rays. With a filter (the transparent-shadow filter, render/transparent_filter.h:42)
+  // every candidate hit is handed to it as a one-lane ray/hit pair whose far is the hit
+  // distance, and the ray is occluded when the filter accepts a hit.
   template <int N>
-  void occludedStream(RayStream<N>& rays, int count, IntersectorFilterSimd* filter)
+  void occludedStream(RayStream<N>& rays, int count, IntersectorFilterSimd* filter, void* payload)
   {
-    if (filter)
-      throw std::logic_error("oracle intersector: intersection filters are not supported");
     for (int i = 0; i < count; ++i)
     {
       const float o[3] = {rays.org.x[i], rays.org.y[i], rays.org.z[i]};
       const float d[3] = {rays.dir.x[i], rays.dir.y[i], rays.dir.z[i]};
-      if (bvh.occluded(o, d, rays.near[i], rays.far[i]))
+      bool occ;
+      if (!filter)
+        occ = bvh.occluded(o, d, rays.near[i], rays.far[i]);
+      else
+        occ = bvh.occludedFiltered(o, d, rays.near[i], rays.far[i], [&](int ti, float t, float u, float v) {
+          RaySimd ray;
+          ray.org = Vec3vf(vfloat(o[0]), vfloat(o[1]), vfloat(o[2]));
+          ray.dir = Vec3vf(vfloat(d[0]), vfloat(d[1]), vfloat(d[2]));
+          ray.near = vfloat(rays.near[i]);
+          ray.far = vfloat(t);
+          HitSimd hit;
+          hit.primId = vint(bvh.tris[ti].primId);
+          hit.geomId = vint(bvh.tris[ti].geomId);
+          hit.instId = vint(-1);
+          hit.u = vfloat(u);
+          hit.v = vfloat(v);
+          const vbool lane0 = vint(step) == vint(0);
+          return any(lane0 & filter->filter(lane0, vint(i), ray, hit, payload));
+        });
+      if (occ)
         rays.far[i] = 0.f;
     }
   }
@@ -470,9 +525,9 @@ public:
   void occluded(RayStream<streamSize>& rays, int count, RayStats& stats,
                 RayHint hint, IntersectorFilterSimd* filter, void* payload) override
   {
-    (void)hint; (void)payload;
+    (void)hint;
     stats.rayCount += count;
-    occludedStream(rays, count, filter);
+    occludedStream(rays, count, filter, payload);
   }
 };
 

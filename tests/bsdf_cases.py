@@ -48,6 +48,33 @@ def cases():
                                                coat_weight=0.8, coat_roughness=0.1, coat_thickness=2.0,
                                                coat_color=(0.9, 0.7, 0.5), sheen_weight=0.7, sheen_tint=0.5,
                                                sheen_roughness=0.3), 0),
+        ("subsurface_half", T.material(base_color=(0.6, 0.5, 0.4), specular_weight=0.0, subsurface_weight=0.5,
+                                       subsurface_color=(0.9, 0.4, 0.3), subsurface_anisotropy=0.2), 0),
+        ("subsurface_full_plastic", T.material(base_color=(0.6, 0.5, 0.4), specular_roughness=0.3,
+                                               subsurface_weight=1.0, subsurface_color=(0.3, 0.8, 0.5),
+                                               subsurface_anisotropy=-0.3), 0),
+        ("subsurface_btdf_only", T.material(base_color=(0.5, 0.5, 0.5), specular_weight=0.0, subsurface_weight=0.7,
+                                            subsurface_color=(0.8, 0.7, 0.2), subsurface_anisotropy=1.0), 0),
+        ("subsurface_rough", T.material(base_color=(0.4, 0.6, 0.7), diffuse_roughness=0.5, specular_roughness=0.2,
+                                        subsurface_weight=0.4, subsurface_color=(0.9, 0.9, 0.6)), 0),
+        ("thin_glass_smooth", T.material(transmission_weight=1.0, thin_walled=1, specular_roughness=0.0,
+                                         transmission_color=(0.8, 0.9, 0.7)), 0),
+        ("thin_glass_rough", T.material(transmission_weight=1.0, thin_walled=1, specular_roughness=0.25,
+                                        transmission_color=(0.7, 0.8, 0.9), transmission_depth=0.5), 0),
+        ("thin_glass_coat", T.material(transmission_weight=0.8, thin_walled=1, specular_roughness=0.15,
+                                       base_color=(0.6, 0.3, 0.3), coat_weight=0.5, coat_roughness=0.1), 0),
+        ("transparent_ior1", T.material(transmission_weight=1.0, specular_ior=1.0), 0),
+        ("half_transparent_ior1", T.material(transmission_weight=0.5, specular_ior=1.0, base_color=(0.2, 0.7, 0.4)), 0),
+        ("opacity_lambert", T.material(base_color=(0.7, 0.5, 0.3), specular_weight=0.0, opacity=0.4), 0),
+        ("opacity_coat_plastic", T.material(base_color=(0.3, 0.4, 0.8), specular_roughness=0.3, coat_weight=0.5,
+                                            coat_roughness=0.2, opacity=0.7), 0),
+        ("opacity_zero", T.material(base_color=(0.5, 0.5, 0.5), opacity=0.0), 0),
+        ("principled_thin_backlight", T.principled(base_color=(0.7, 0.5, 0.3), specular_ior=1.5,
+                                                   specular_roughness=0.3, thin_walled=1, backlight=0.8), 0),
+        ("principled_thin_glass", T.principled(transmission_weight=1.0, specular_ior=1.5, specular_roughness=0.15,
+                                               thin_walled=1, thickness=0.5, transmission_color=(0.9, 0.8, 0.6)), 0),
+        ("principled_opacity", T.principled(base_color=(0.2, 0.6, 0.8), specular_ior=1.5, specular_roughness=0.3,
+                                            opacity=0.6), 0),
     ]
 
 

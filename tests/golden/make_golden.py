@@ -17,6 +17,8 @@ Fixtures (small, seeded, committed):
   terrain_img.npz  small terrain renders (96^2 heightfield, 24 spheres of all four material
                    kinds, sun-sky) at 128x64: 16 spp and 256 spp, seeds 0 and 1
   lobes_img.npz    the small scene with Oren-Nayar, sheen and layered spheres, 16 spp, seeds 0, 1
+  translucent_img.npz  the small scene with thin glass, opacity, subsurface, transparent and backlit
+                   surfaces (shadow rays through transparent surfaces), 16 spp, seeds 0, 1
   siblings_img.npz primaryStream, aoStream, diffuseStream, diffuse2Stream renders of the small scene
   film.npz         sample variance, tone-mapped LDR images and frame errors of the small scene
   bsdf.npz         the reference's Standard-material BSDF (eval, sample) on 512 seeded tuples
@@ -116,6 +118,20 @@ def make_lobe_images():
     np.savez_compressed(OUT / "lobes_img.npz", **out)
 
 
+def make_translucent_images():
+    """The small scene with thin glass, opacity, subsurface, transparent and backlit surfaces at
+    16 spp, seeds 0 and 1 (shadow rays through the reference's transparent-shadow filter)."""
+    out = {}
+    for seed in (0, 1):
+        s = prt_scenes.cornell_translucent(seed=0)
+        dev = ref.RefDevice(s, seed=seed)
+        st = dev.render(16)
+        out[f"spp16_seed{seed}"] = dev.blit()
+        out[f"spp16_seed{seed}_rays"] = np.float64(st["rays"])
+        dev.close()
+    np.savez_compressed(OUT / "translucent_img.npz", **out)
+
+
 def sibling_scene(kind):
     s = prt_scenes.cornell(seed=0, width=64, height=64, spp=4)
     s.renderer_type = kind
@@ -191,13 +207,16 @@ def make_sunsky():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["sobol", "rays", "images", "sunsky", "bsdf", "terrain", "lobes", "siblings", "film"]
+    which = sys.argv[1:] or ["sobol", "rays", "images", "sunsky", "bsdf", "terrain", "lobes", "translucent", "siblings",
+                             "film"]
     if "terrain" in which:
         make_terrain_images()
     if "bsdf" in which:
         make_bsdf()
     if "lobes" in which:
         make_lobe_images()
+    if "translucent" in which:
+        make_translucent_images()
     if "siblings" in which:
         make_sibling_images()
     if "film" in which:

@@ -147,6 +147,20 @@ def test_lobes_same_seed_tracks_oracle(device, golden):
     assert abs(st["rays"] / float(z["spp16_seed0_rays"]) - 1.0) < 0.01
 
 
+def test_translucent_same_seed_tracks_oracle(device, golden):
+    """Thin smooth and rough glass, opacity, Standard subsurface (also thin-walled, Oren-Nayar),
+    transmission at the ambient IOR, with shadow rays through transparent surfaces (the reference's
+    transparent-shadow filter): the same-seed render follows the reference's far closer than
+    two seeds do, with the same ray count within 1%."""
+    z = golden("translucent_img.npz")
+    img, st = render(device, prt_scenes.cornell_translucent(seed=0), seed=0, spp=16)
+    assert np.isfinite(img).all()
+    same = rel_mse(img, z["spp16_seed0"])
+    other = rel_mse(z["spp16_seed1"], z["spp16_seed0"])
+    assert same < 0.2 * other, (same, other)
+    assert abs(st["rays"] / float(z["spp16_seed0_rays"]) - 1.0) < 0.01
+
+
 @pytest.mark.parametrize("kind", [1, 2, 3, 4], ids=["primary", "ao", "diffuse", "diffuse2"])
 def test_sibling_renderers_match_oracle(device, golden, kind):
     """primaryStream / aoStream / diffuseStream / diffuse2Stream: the same samples, hits and
