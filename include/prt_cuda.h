@@ -103,6 +103,13 @@ typedef struct prt_material
  * prt_cuda_principled_defaults() fills its defaults. */
 #define PRT_MATERIAL_STANDARD   0
 #define PRT_MATERIAL_PRINCIPLED 1
+/* A material whose surfaces end the path as if the ray had missed them (environment light,
+ * no shading), while still blocking shadow rays. The reference's stream renderer sorts hits
+ * by material id with id 0 as its miss bucket (render/renderer_stream.h:108-181); rkscene
+ * scenes keep id 0 for a dummy material, but a .mesh scene gives it to its first material
+ * (render/scene.cpp:136-172), whose surfaces therefore render as misses. The .mesh loader
+ * marks that material so. */
+#define PRT_MATERIAL_MISS       2
 
 /* An RGB FP32 image (row 0 at the top, as stored by the reference's ImageIo). */
 typedef struct prt_texture
@@ -282,28 +289,36 @@ int prt_cuda_scene_bvh(prt_context* ctx, void* nodes, int64_t node_capacity, voi
                        int64_t* node_count, int64_t* tri_count);
 
 /* ---- scene files -------------------------------------------------------------------------
- * The reference's rkscene format: a JSON document (.rkscene) with one binary buffer (.rkbin) of
- * typed arrays (rkscene/rkscene.h:264-905). A loaded scene is the flat description above:
- * every file material a Standard material (texture maps for baseColor only, read from
- * little-endian colour PFM images, UV set 0, no transform), geometries without a valid
- * material bound to the default (Principled) material appended after the file's, and each
- * object's geometries added once, or once per instance transform with positions and normals
- * transformed (instances are always flattened), in file order (render/scene.cpp:174-362). The
- * file's lights list is checked but, as in Scene::loadScene, not used: the environment comes
- * from the caller. Host-only: no GPU is needed to load or describe a file. */
-typedef struct prt_rkscene prt_rkscene;
+ * The reference's scene files, read on the host into the flat description above (Scene::Scene
+ * picks the loader by extension, render/scene.cpp:65-77):
+ *   .rkscene -- a JSON document with one binary buffer (.rkbin) of typed arrays
+ *     (rkscene/rkscene.h:264-905): every file material a Standard material, geometries
+ *     without a valid material bound to the default (Principled) material appended after the
+ *     file's, each object's geometries added once, or once per instance transform with
+ *     positions and normals transformed (instances are always flattened), in file order
+ *     (render/scene.cpp:174-362). The file's lights list is checked but, as in
+ *     Scene::loadScene, not used.
+ *   .mesh -- the TriangleMesh blob (geometry/triangle_mesh.cpp:362-378) with the material
+ *     library <name>.mtl (material/mtl_loader.cpp): materials per Scene::loadMesh
+ *     (render/scene.cpp:136-172) and MaterialFactory::make ("Standard", "Principled", or the
+ *     default "OBJ" mapping onto Principled); the triangles are split into one mesh per
+ *     material.
+ * Texture maps are supported for the base colour only, read from little-endian colour PFM
+ * images, UV set 0, no transform. The environment comes from the caller. Host-only: no GPU is
+ * needed to load or describe a file. */
+typedef struct prt_scene_file prt_scene_file;
 
 /* Loads `path`. On failure returns PRT_ERR_INVALID_ARG (malformed or unsupported content) or
  * PRT_ERR_LOGIC (a file that cannot be opened or read) and writes the reason to msg
  * (msg_capacity bytes, may be 0). */
-int prt_rkscene_load(const char* path, prt_rkscene** out, char* msg, int32_t msg_capacity);
-/* Points desc at the loaded scene's arrays (valid until prt_rkscene_free); env is zeroed and
+int prt_scene_file_load(const char* path, prt_scene_file** out, char* msg, int32_t msg_capacity);
+/* Points desc at the loaded scene's arrays (valid until prt_scene_file_free); env is zeroed and
  * bvh_build is PRT_BVH_HOST: set them before prt_cuda_scene_upload. */
-int prt_rkscene_desc(const prt_rkscene* scene, prt_scene_desc* desc);
-int prt_rkscene_free(prt_rkscene* scene);
+int prt_scene_file_desc(const prt_scene_file* scene, prt_scene_desc* desc);
+int prt_scene_file_free(prt_scene_file* scene);
 
 /* Device::initScene(path, props) + initLights(props) (render/device_cpu.cpp:96-110) for an
- * rkscene file: loads it, applies the environment lights (env may be NULL: none) and the BVH
+ * .rkscene or .mesh file: loads it, applies the environment lights (env may be NULL: none) and the BVH
  * builder, and uploads it as prt_cuda_scene_upload does. A file that cannot be read or parsed
  * gives PRT_ERR_INVALID_ARG with the reason in prt_cuda_last_error. */
 int prt_cuda_scene_load(prt_context* ctx, const char* path, const prt_env_desc* env, int32_t bvh_build);

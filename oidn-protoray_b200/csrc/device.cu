@@ -4,7 +4,7 @@
 #include "../../include/prt_cuda.h"
 #include "runtime.h"
 #include "bvh_build.h"
-#include "rkscene_load.h"
+#include "scene_file.h"
 
 #include <algorithm>
 #include <cfloat>
@@ -24,7 +24,7 @@ struct prt_context
   Context c;
 };
 
-struct prt_rkscene
+struct prt_scene_file
 {
   RkScene scene;
 };
@@ -165,6 +165,14 @@ DevMaterial resolveMaterial(const prt_material& m, std::vector<float>& media, in
   };
   d.ambientIor = ior(m.ambient_ior > 0.f ? m.ambient_ior : 1.f);
   d.principled = m.model == PRT_MATERIAL_PRINCIPLED ? 1 : 0;
+  if (m.model == PRT_MATERIAL_MISS)
+  {
+    d.type = kMatMiss;
+    d.shadeClass = 0;
+    d.baseColorTex = -1;
+    d.opacity = 1.f;
+    return d;
+  }
   if (m.model != PRT_MATERIAL_STANDARD && m.model != PRT_MATERIAL_PRINCIPLED)
     throw std::invalid_argument("unknown material model");
   d.baseWeight = m.base_weight;
@@ -973,7 +981,7 @@ int prt_cuda_scene_load(prt_context* ctx, const char* path, const prt_env_desc* 
     RkScene scene;
     try
     {
-      loadRkScene(path, scene);
+      loadSceneFile(path, scene);
     }
     catch (const std::runtime_error& e)
     {
@@ -1182,7 +1190,7 @@ int prt_bvh8_check(const void* nodes, int64_t node_count, const void* tris, int6
   }
 }
 
-int prt_rkscene_load(const char* path, prt_rkscene** out, char* msg, int32_t msg_capacity)
+int prt_scene_file_load(const char* path, prt_scene_file** out, char* msg, int32_t msg_capacity)
 {
   auto report = [&](const char* what) {
     if (msg && msg_capacity > 0)
@@ -1197,8 +1205,8 @@ int prt_rkscene_load(const char* path, prt_rkscene** out, char* msg, int32_t msg
   *out = nullptr;
   try
   {
-    std::unique_ptr<prt_rkscene> r(new prt_rkscene);
-    loadRkScene(path, r->scene);
+    std::unique_ptr<prt_scene_file> r(new prt_scene_file);
+    loadSceneFile(path, r->scene);
     *out = r.release();
     return PRT_OK;
   }
@@ -1214,14 +1222,14 @@ int prt_rkscene_load(const char* path, prt_rkscene** out, char* msg, int32_t msg
   }
 }
 
-int prt_rkscene_desc(const prt_rkscene* scene, prt_scene_desc* desc)
+int prt_scene_file_desc(const prt_scene_file* scene, prt_scene_desc* desc)
 {
   if (!scene || !desc) return PRT_ERR_INVALID_ARG;
   scene->scene.describe(*desc);
   return PRT_OK;
 }
 
-int prt_rkscene_free(prt_rkscene* scene)
+int prt_scene_file_free(prt_scene_file* scene)
 {
   delete scene;
   return PRT_OK;

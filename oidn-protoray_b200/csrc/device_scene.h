@@ -13,6 +13,7 @@ enum : int
   kMatTransmissive = 1 << 1,
   kMatMediaInterface = 1 << 2,
   kMatTransparent = 1 << 3,
+  kMatMiss = 1 << 4,          // PRT_MATERIAL_MISS: hits end the path as misses
 };
 
 // Lobe features of a Standard material, known per material at upload. A shading kernel

@@ -527,7 +527,11 @@ __global__ void __launch_bounds__(256) kShadeEnd(Launch L, const int* __restrict
       const float lastPdf = tp.w;
       const int lastType = __float_as_int(ra.w);
       const bool aov1 = (pixelId & kPathAov1Flag) == 0u;
-      if (triId < 0)
+      // A hit on a PRT_MATERIAL_MISS material is shaded as a miss.
+      const bool miss =
+        triId < 0 ||
+        (E.sc.materials[__ldg(E.sc.meshMaterial + __ldg(&E.sc.triVerts[triId].w))].type & kMatMiss) != 0;
+      if (miss)
       {
         float lightPdf;
         const f3 Le = evalEnvLights(E.sc, dir, lightPdf);

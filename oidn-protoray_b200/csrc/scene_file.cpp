@@ -1,6 +1,6 @@
-// rkscene loader: JSON parser, typed buffer reads, material / geometry / object mapping.
-// See rkscene_load.h.
-#include "rkscene_load.h"
+// Scene-file loaders: the rkscene JSON reader, typed buffer reads and material / geometry /
+// object mapping; the TriangleMesh blob and Wavefront material-library reader. See scene_file.h.
+#include "scene_file.h"
 
 #include <cmath>
 #include <cstdio>
@@ -9,6 +9,7 @@
 #include <fstream>
 #include <iterator>
 #include <map>
+#include <sstream>
 #include <stdexcept>
 
 namespace prt {
@@ -722,6 +723,384 @@ void loadRkScene(const std::string& path, RkScene& out)
     m.indices = out.indices[i].empty() ? nullptr : out.indices[i].data();
   }
   for (size_t i = 0; i < out.textures.size(); ++i) out.textures[i].rgb = out.texturePixels[i].data();
+}
+
+namespace {
+
+// ---- .mesh: TriangleMesh blob + .mtl ------------------------------------------------------------
+
+constexpr int32_t kTriangleMeshBlobId = 0x04df8666;  // geometry/triangle_mesh.h:21
+
+class BlobReader
+{
+public:
+  explicit BlobReader(const std::string& path) : f(path, std::ios::binary)
+  {
+    if (!f) throw std::runtime_error("mesh: failed to open file: " + path);
+  }
+  template <class T>
+  T get()
+  {
+    T v;
+    raw(&v, sizeof(T));
+    return v;
+  }
+  void raw(void* dst, size_t bytes)
+  {
+    if (bytes && !f.read(reinterpret_cast<char*>(dst), (std::streamsize)bytes))
+      throw std::runtime_error("mesh: unexpected end of stream");
+  }
+  std::string str()
+  {
+    const int32_t n = get<int32_t>();
+    if (n < 0 || n > (1 << 20)) throw std::invalid_argument("mesh: invalid string size in stream");
+    std::string s((size_t)n, '\0');
+    raw(&s[0], (size_t)n);
+    return s;
+  }
+
+private:
+  std::ifstream f;
+};
+
+// One material's statements from a material library: key -> value, the value kept as the
+// reference's MtlLoader keeps it (material/mtl_loader.cpp:66-90): three or two numbers as a
+// vector, anything else as the text after the key.
+struct MtlValue
+{
+  int kind = 0;  // 0 text, 2 vec2, 3 vec3
+  std::string text;
+  float v[3] = {0.f, 0.f, 0.f};
+};
+using MtlProps = std::map<std::string, MtlValue>;
+
+void parseMtl(const std::string& path, std::map<std::string, MtlProps>& lib)
+{
+  std::ifstream f(path);
+  if (!f) return;
+  std::string name, line;
+  while (std::getline(f, line))
+  {
+    std::istringstream ls(line);
+    std::string head;
+    if (!(ls >> head)) continue;
+    std::string rest;
+    std::getline(ls, rest);
+    if (head == "newmtl")
+    {
+      std::istringstream rs(rest);
+      if (!(rs >> name)) throw std::invalid_argument("mesh: invalid material in " + path);
+      continue;
+    }
+    if (head[0] == '#') continue;
+    MtlValue val;
+    const int n = std::sscanf(rest.c_str(), "%f %f %f", &val.v[0], &val.v[1], &val.v[2]);
+    if (n == 3 || n == 2)
+      val.kind = n;
+    else
+    {
+      const size_t b = rest.find_first_not_of(" \t\r");
+      if (b == std::string::npos) throw std::invalid_argument("mesh: invalid statement in " + path);
+      val.text = rest.substr(b);
+      while (!val.text.empty() && (val.text.back() == '\r' || val.text.back() == ' ')) val.text.pop_back();
+    }
+    lib[name][head] = val;
+  }
+}
+
+// Typed reads with the conversions of the reference's Props values (sys/value.h:200-276):
+// text converts as a stream read (a lone number fills all three components of a vector).
+struct MtlReader
+{
+  const MtlProps& p;
+  bool has(const char* k) const { return p.count(k) != 0; }
+  float f(const char* k, float def) const
+  {
+    auto it = p.find(k);
+    if (it == p.end()) return def;
+    if (it->second.kind != 0) throw std::invalid_argument(std::string("mesh: ") + k + " has an incompatible type");
+    std::istringstream s(it->second.text);
+    float x = 0.f;
+    s >> x;
+    return x;
+  }
+  void v3(const char* k, float* out) const
+  {
+    auto it = p.find(k);
+    if (it == p.end()) return;
+    if (it->second.kind == 3)
+      for (int c = 0; c < 3; ++c) out[c] = it->second.v[c];
+    else if (it->second.kind == 0)
+    {
+      std::istringstream s(it->second.text);
+      float x = 0.f;
+      s >> x;
+      out[0] = out[1] = out[2] = x;
+    }
+    else
+      throw std::invalid_argument(std::string("mesh: ") + k + " has an incompatible type");
+  }
+  std::string text(const char* k) const
+  {
+    auto it = p.find(k);
+    if (it == p.end()) return std::string();
+    if (it->second.kind != 0) throw std::invalid_argument(std::string("mesh: ") + k + " must be text");
+    return it->second.text;
+  }
+};
+
+// MaterialFactory::make (material/material_factory.cpp:29-96) for the types the device has.
+prt_material mtlMaterial(const MtlProps& props, Loader& L)
+{
+  MtlReader r{props};
+  std::string type = r.has("type") ? r.text("type") : std::string("OBJ");
+  MtlProps p2 = props;  // the OBJ mapping adds Principled keys
+  if (type == "OBJ")
+  {
+    auto copy = [&](const char* to, const char* from) {
+      if (props.count(from)) p2[to] = props.at(from);
+    };
+    if (!r.has("baseColor") && !r.has("baseColorMap"))
+    {
+      copy("baseColor", "Kd");
+      copy("baseColorMap", "map_Kd");
+    }
+    if (!r.has("bumpMap") && !r.has("normalMap"))
+    {
+      copy("bumpMap", "map_Bump");
+      copy("normalMap", "map_bump");
+    }
+    if (!r.has("opacityMap")) copy("opacityMap", "map_d");
+    if (!r.has("roughness") && r.has("Ns"))
+    {
+      MtlValue v;
+      std::ostringstream s;
+      s.precision(9);
+      s << std::sqrt(std::sqrt(2.f / (r.f("Ns", 0.f) + 2.f)));  // Walter et al. 2007
+      v.text = s.str();
+      p2["roughness"] = v;
+    }
+    if (!r.has("transmission") && r.has("Tf"))
+    {
+      float tf[3] = {1.f, 1.f, 1.f};
+      r.v3("Tf", tf);
+      if (std::min(tf[0], std::min(tf[1], tf[2])) < 1.f)
+      {
+        MtlValue one, col;
+        one.text = "1";
+        col.kind = 3;
+        for (int c = 0; c < 3; ++c) col.v[c] = 1.f - tf[c];  // 3ds Max convention
+        p2["transmission"] = one;
+        p2["transmissionColor"] = col;
+      }
+    }
+    if (!r.has("ior") && r.has("Ks"))
+    {
+      float ks[3] = {0.f, 0.f, 0.f};
+      r.v3("Ks", ks);
+      const float f0 = (ks[0] + ks[1] + ks[2]) * (1.f / 3.f) * 0.08f;
+      MtlValue v;
+      std::ostringstream s;
+      s.precision(9);
+      s << (1.f + std::sqrt(f0)) / (1.f - std::sqrt(f0));
+      v.text = s.str();
+      p2["ior"] = v;
+    }
+    type = "Principled";
+  }
+  MtlReader q{p2};
+  for (const char* k : {"normalMap", "bumpMap", "coatNormalMap", "coatBumpMap", "baseNormalMap", "baseBumpMap"})
+    if (q.has(k)) throw std::invalid_argument("mesh: normal and bump maps are not supported on the device");
+  if (q.has("opacityMap")) throw std::invalid_argument("mesh: opacity maps are not supported on the device");
+  for (const auto& kv : p2)
+    if (kv.first.size() > 3 && kv.first.compare(kv.first.size() - 3, 3, "Map") == 0 && kv.first != "baseColorMap")
+      throw std::invalid_argument("mesh: texture maps are supported for baseColor only on the device");
+  prt_material m;
+  auto base = [&](float* color, int* tex) {
+    if (q.has("baseColorMap"))
+    {
+      *tex = L.texture(q.text("baseColorMap"));
+      if (!q.has("baseColor")) color[0] = color[1] = color[2] = 1.f;
+    }
+  };
+  if (type == "Standard")
+  {
+    prt_cuda_material_defaults(&m);
+    m.ambient_ior = q.f("ambientIOR", 1.f);
+    m.base_weight = q.f("baseWeight", 1.f);
+    q.v3("baseColor", m.base_color);
+    base(m.base_color, &m.base_color_texture);
+    m.metalness = q.f("metalness", 0.f);
+    m.diffuse_roughness = q.f("diffuseRoughness", 0.f);
+    m.specular_weight = q.f("specularWeight", 1.f);
+    q.v3("specularColor", m.specular_color);
+    m.specular_roughness = q.f("specularRoughness", 0.3f);
+    m.specular_ior = q.f("specularIOR", 1.5f);
+    m.transmission_weight = q.f("transmissionWeight", 0.f);
+    q.v3("transmissionColor", m.transmission_color);
+    m.transmission_depth = q.f("transmissionDepth", 1.f);
+    m.subsurface_weight = q.f("subsurfaceWeight", 0.f);
+    q.v3("subsurfaceColor", m.subsurface_color);
+    m.subsurface_anisotropy = q.f("subsurfaceAnisotropy", 0.f);
+    m.coat_weight = q.f("coatWeight", 0.f);
+    q.v3("coatColor", m.coat_color);
+    m.coat_roughness = q.f("coatRoughness", 0.f);
+    m.coat_ior = q.f("coatIOR", 1.6f);
+    m.sheen_weight = q.f("sheenWeight", 0.f);
+    q.v3("sheenColor", m.sheen_color);
+    m.sheen_roughness = q.f("sheenRoughness", 0.3f);
+    m.emission_luminance = q.f("emissionLuminance", 0.f);
+    q.v3("emissionColor", m.emission_color);
+    m.thin_walled = (int)q.f("thinWalled", 0.f);
+    m.opacity = q.f("opacity", 1.f);
+    return m;
+  }
+  if (type == "Principled")
+  {
+    prt_cuda_principled_defaults(&m);
+    q.v3("baseColor", m.base_color);
+    base(m.base_color, &m.base_color_texture);
+    q.v3("edgeColor", m.specular_color);
+    m.metalness = q.f("metallic", 0.f);
+    m.base_weight = q.f("diffuse", 1.f);
+    m.specular_weight = q.f("specular", 1.f);
+    m.ambient_ior = q.f("outsideIor", 1.f);
+    m.specular_ior = q.f("ior", m.ambient_ior);
+    m.transmission_weight = q.f("transmission", 0.f);
+    q.v3("transmissionColor", m.transmission_color);
+    m.transmission_depth = q.f("transmissionDepth", 1.f);
+    m.specular_roughness = q.f("roughness", 0.f);
+    m.coat_weight = q.f("coat", 0.f);
+    m.coat_ior = q.f("coatIor", 1.5f);
+    q.v3("coatColor", m.coat_color);
+    m.coat_thickness = q.f("coatThickness", 1.f);
+    m.coat_roughness = q.f("coatRoughness", 0.f);
+    m.sheen_weight = q.f("sheen", 0.f);
+    q.v3("sheenColor", m.sheen_color);
+    m.sheen_tint = q.f("sheenTint", 0.f);
+    m.sheen_roughness = q.f("sheenRoughness", 0.2f);
+    m.thin_walled = (int)q.f("thin", 0.f);
+    m.backlight = q.f("backlight", 0.f);
+    m.thickness = q.f("thickness", 1.f);
+    m.opacity = q.f("opacity", 1.f);
+    return m;
+  }
+  throw std::invalid_argument("mesh: material type " + type + " is not supported on the device");
+}
+
+} // namespace
+
+void loadMeshScene(const std::string& path, RkScene& out)
+{
+  out = RkScene();
+  BlobReader b(path);
+  if (b.get<int32_t>() != kTriangleMeshBlobId) throw std::invalid_argument("mesh: file has wrong blob ID: " + path);
+  float bounds[6];
+  b.raw(bounds, sizeof(bounds));
+  const int32_t triCount = b.get<int32_t>(), vertexCount = b.get<int32_t>();
+  const uint8_t hasNormals = b.get<uint8_t>();
+  const int8_t numTexcoords = b.get<int8_t>();
+  if (triCount < 0 || vertexCount < 0 || numTexcoords < 0)
+    throw std::invalid_argument("mesh: invalid triangle mesh data in stream");
+  std::vector<int32_t> idx((size_t)triCount * 3);
+  b.raw(idx.data(), idx.size() * sizeof(int32_t));
+  std::vector<int32_t> matIds((size_t)triCount);  // one per triangle (TriangleMesh::alloc's default)
+  b.raw(matIds.data(), matIds.size() * sizeof(int32_t));
+  const int stride = 3 + (hasNormals ? 3 : 0) + 2 * numTexcoords;
+  std::vector<float> attribs((size_t)vertexCount * stride);
+  b.raw(attribs.data(), attribs.size() * sizeof(float));
+  const int32_t nameCount = b.get<int32_t>();
+  if (nameCount < 0 || nameCount > (1 << 20)) throw std::invalid_argument("mesh: invalid array size in stream");
+  std::vector<std::string> names;
+  for (int i = 0; i < nameCount; ++i) names.push_back(b.str());
+  for (int32_t v : idx)
+    if (v < 0 || v >= vertexCount) throw std::invalid_argument("mesh: triangle index out of range");
+
+  // Materials (Scene::loadMesh): one per material name, from <path without extension>.mtl,
+  // the default (Principled) material for names the library lacks or for a blob without names.
+  const size_t dot = path.find_last_of('.');
+  const size_t slash = path.find_last_of('/');
+  const std::string stem = (dot != std::string::npos && (slash == std::string::npos || dot > slash)) ? path.substr(0, dot) : path;
+  std::map<std::string, MtlProps> lib;
+  parseMtl(stem + ".mtl", lib);
+  Loader L{out, directoryOf(path), {}};
+  prt_material def;
+  prt_cuda_principled_defaults(&def);
+  if (names.empty())
+    out.materials.push_back(def);
+  for (const std::string& n : names)
+  {
+    auto it = lib.find(n);
+    out.materials.push_back(it != lib.end() ? mtlMaterial(it->second, L) : def);
+  }
+  const int matCount = (int)out.materials.size();
+  // Scene::Scene (render/scene.cpp:119-130) needs the emissive materials at ids 1..k.
+  int lightMaterials = 0;
+  for (int i = 1; i < matCount; ++i)
+  {
+    const prt_material& m = out.materials[i];
+    if (m.model == PRT_MATERIAL_STANDARD && m.emission_luminance > 0.f)
+    {
+      ++lightMaterials;
+      if (i > lightMaterials) throw std::invalid_argument("mesh: the material IDs must be remapped");
+    }
+  }
+  for (int32_t& m : matIds)
+    if (m < 0 || m >= matCount) throw std::invalid_argument("mesh: material id out of range");
+  // Id 0 is the stream renderer's miss bucket (PRT_MATERIAL_MISS).
+  out.materials[0].model = PRT_MATERIAL_MISS;
+
+  // Vertex arrays (positions, normals, UV set 0) shared by the per-material meshes.
+  std::vector<float> pos((size_t)vertexCount * 3), nrm, uv;
+  if (hasNormals) nrm.resize((size_t)vertexCount * 3);
+  if (numTexcoords > 0) uv.resize((size_t)vertexCount * 2);
+  for (int64_t v = 0; v < vertexCount; ++v)
+  {
+    const float* a = &attribs[(size_t)v * stride];
+    for (int k = 0; k < 3; ++k) pos[3 * v + k] = a[k];
+    if (hasNormals)
+      for (int k = 0; k < 3; ++k) nrm[3 * v + k] = a[3 + k];
+    if (numTexcoords > 0)
+      for (int k = 0; k < 2; ++k) uv[2 * v + k] = a[3 + (hasNormals ? 3 : 0) + k];
+  }
+  for (int m = 0; m < matCount; ++m)
+  {
+    std::vector<int32_t> tri;
+    for (int32_t t = 0; t < triCount; ++t)
+      if (matIds[t] == m) tri.insert(tri.end(), {idx[3 * t], idx[3 * t + 1], idx[3 * t + 2]});
+    if (tri.empty()) continue;
+    out.positions.push_back(pos);
+    out.normals.push_back(nrm);
+    out.texcoords.push_back(uv);
+    out.indices.push_back(std::move(tri));
+    prt_mesh mesh;
+    std::memset(&mesh, 0, sizeof(mesh));
+    mesh.vertex_count = vertexCount;
+    mesh.tri_count = (int32_t)(out.indices.back().size() / 3);
+    mesh.material = m;
+    out.meshes.push_back(mesh);
+    out.triangleCount += mesh.tri_count;
+  }
+  for (size_t i = 0; i < out.meshes.size(); ++i)
+  {
+    prt_mesh& m = out.meshes[i];
+    m.positions = out.positions[i].empty() ? nullptr : out.positions[i].data();
+    m.normals = out.normals[i].empty() ? nullptr : out.normals[i].data();
+    m.texcoords = out.texcoords[i].empty() ? nullptr : out.texcoords[i].data();
+    m.indices = out.indices[i].data();
+  }
+  for (size_t i = 0; i < out.textures.size(); ++i) out.textures[i].rgb = out.texturePixels[i].data();
+}
+
+void loadSceneFile(const std::string& path, RkScene& out)
+{
+  auto endsWith = [&](const char* ext) {
+    const size_t n = std::strlen(ext);
+    return path.size() >= n && path.compare(path.size() - n, n, ext) == 0;
+  };
+  if (endsWith(".rkscene")) return loadRkScene(path, out);
+  if (endsWith(".mesh")) return loadMeshScene(path, out);
+  throw std::invalid_argument("unknown scene format: " + path);
 }
 
 } // namespace prt

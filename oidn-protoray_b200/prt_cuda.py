@@ -92,9 +92,9 @@ def load_library():
                                    P(C.c_float), P(C.c_int64), P(C.c_int64)]
     lib.prt_bvh8_build_host.argtypes = [P(C.c_float), C.c_int64, vp, C.c_int64, vp, C.c_int64, P(C.c_int64),
                                         P(C.c_int32)]
-    lib.prt_rkscene_load.argtypes = [C.c_char_p, P(vp), C.c_char_p, C.c_int32]
-    lib.prt_rkscene_desc.argtypes = [vp, P(T.SceneDesc)]
-    lib.prt_rkscene_free.argtypes = [vp]
+    lib.prt_scene_file_load.argtypes = [C.c_char_p, P(vp), C.c_char_p, C.c_int32]
+    lib.prt_scene_file_desc.argtypes = [vp, P(T.SceneDesc)]
+    lib.prt_scene_file_free.argtypes = [vp]
     lib.prt_cuda_scene_load.argtypes = [vp, C.c_char_p, P(T.EnvDesc), C.c_int32]
     _lib = lib
     return lib
@@ -120,28 +120,28 @@ BVH8_NODE_BYTES = 80
 BVH8_TRI_BYTES = 48
 
 
-class RkScene:
-    """An rkscene file loaded on the host (prt_rkscene_load): the flat scene description the
-    device uploads, readable as numpy arrays. Raises ValueError for malformed or unsupported
-    content and OSError for files that cannot be read."""
+class SceneFile:
+    """A scene file (.rkscene or .mesh) loaded on the host (prt_scene_file_load): the flat scene
+    description the device uploads, readable as numpy arrays. Raises ValueError for malformed or
+    unsupported content and OSError for files that cannot be read."""
 
     def __init__(self, path):
         self.lib = load_library()
         self.h = None
         h = C.c_void_p()
         msg = C.create_string_buffer(512)
-        rc = self.lib.prt_rkscene_load(str(path).encode(), C.byref(h), msg, 512)
+        rc = self.lib.prt_scene_file_load(str(path).encode(), C.byref(h), msg, 512)
         if rc == T.PRT_ERR_INVALID_ARG:
             raise ValueError(msg.value.decode())
         if rc != T.PRT_OK:
             raise OSError(msg.value.decode())
         self.h = h
         self.d = T.SceneDesc()
-        self.lib.prt_rkscene_desc(self.h, C.byref(self.d))
+        self.lib.prt_scene_file_desc(self.h, C.byref(self.d))
 
     def close(self):
         if getattr(self, "h", None):
-            self.lib.prt_rkscene_free(self.h)
+            self.lib.prt_scene_file_free(self.h)
             self.h = None
 
     def __del__(self):
@@ -268,7 +268,7 @@ class DeviceCuda:
         self.scene = scene
 
     def load_scene(self, path, env=None, bvh_build=T.PRT_BVH_HOST):
-        """Device::initScene(path) + initLights: uploads an rkscene file (prt_cuda_scene_load);
+        """Device::initScene(path) + initLights: uploads a .rkscene or .mesh file (prt_cuda_scene_load);
         `env` is a prt_types.EnvDesc or None (no environment light)."""
         self._check(self.lib.prt_cuda_scene_load(self.h, str(path).encode(), C.byref(env) if env is not None else None,
                                                  int(bvh_build)))

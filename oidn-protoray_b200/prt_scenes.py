@@ -645,3 +645,72 @@ def write_rkscene(scene, path, objects=None):
     bin_path.write_bytes(bytes(blob))
     path.write_text(json.dumps(doc, indent=2))
     return path
+
+
+_MESH_BLOB_ID = 0x04df8666  # TriangleMesh::blobId (geometry/triangle_mesh.h:21)
+
+
+def write_mesh(scene, path):
+    """Writes `scene`'s meshes as one TriangleMesh blob (.mesh: blob id, bounds, counts, indices,
+    per-triangle material ids, interleaved position / normal / UV attributes, material names;
+    geometry/triangle_mesh.cpp:362-378) with its material library (.mtl of Standard materials,
+    "type Standard") and PFM textures beside it. Meshes are concatenated; normals and UVs are
+    written when every mesh has them. Materials are reordered so that the emissive ones take ids
+    1..k, the order Scene::Scene requires of a mesh file (render/scene.cpp:119-130)."""
+    import struct
+
+    path = pathlib.Path(path)
+    n = len(scene.materials)
+    emissive = [i for i in range(n) if scene.materials[i].emission_luminance > 0.0]
+    others = [i for i in range(n) if i not in emissive]
+    order = others[:1] + emissive + others[1:]
+    new_id = {old: k for k, old in enumerate(order)}
+    materials = [scene.materials[i] for i in order]
+    pos, nrm, uv, idx, mid = [], [], [], [], []
+    base = 0
+    has_n = all(m["normals"] is not None for m in scene.meshes)
+    has_t = all(m["texcoords"] is not None for m in scene.meshes)
+    for m in scene.meshes:
+        pos.append(m["positions"])
+        if has_n:
+            nrm.append(m["normals"])
+        if has_t:
+            uv.append(m["texcoords"])
+        idx.append(m["indices"] + base)
+        mid.append(np.full(m["indices"].shape[0], new_id[m["material"]], np.int32))
+        base += m["positions"].shape[0]
+    P = np.concatenate(pos).astype(np.float32)
+    cols = [P] + ([np.concatenate(nrm).astype(np.float32)] if has_n else []) + \
+           ([np.concatenate(uv).astype(np.float32)] if has_t else [])
+    attribs = np.concatenate(cols, 1)
+    I = np.concatenate(idx).astype(np.int32)
+    M = np.concatenate(mid).astype(np.int32)
+    names = [f"mat{i}" for i in range(len(materials))]
+    with open(path, "wb") as f:
+        f.write(struct.pack("<i", _MESH_BLOB_ID))
+        f.write(np.concatenate([P.min(0), P.max(0)]).astype("<f4").tobytes())
+        f.write(struct.pack("<iiBb", I.shape[0], P.shape[0], 1 if has_n else 0, 1 if has_t else 0))
+        f.write(I.astype("<i4").tobytes())
+        f.write(M.astype("<i4").tobytes())
+        f.write(attribs.astype("<f4").tobytes())
+        f.write(struct.pack("<i", len(names)))
+        for n in names:
+            f.write(struct.pack("<i", len(n)) + n.encode())
+    lines = []
+    for i, m in enumerate(materials):
+        if m.model != T.PRT_MATERIAL_STANDARD:
+            raise ValueError("the material library is written with Standard materials")
+        lines.append(f"newmtl {names[i]}")
+        lines.append("type Standard")
+        for key, field in _RK_SCALARS:
+            lines.append(f"{key} {float(getattr(m, field))!r}")
+        lines.append("baseColor " + " ".join(repr(float(x)) for x in m.base_color))
+        for key, field in _RK_COLORS:
+            lines.append(f"{key} " + " ".join(repr(float(x)) for x in getattr(m, field)))
+        if m.base_color_texture >= 0:
+            lines.append(f"baseColorMap {path.stem}_tex{m.base_color_texture}.pfm")
+        lines.append(f"thinWalled {int(m.thin_walled)}")
+    path.with_suffix(".mtl").write_text("\n".join(lines) + "\n")
+    for k, t in enumerate(scene.textures):
+        write_pfm(path.parent / f"{path.stem}_tex{k}.pfm", t)
+    return path

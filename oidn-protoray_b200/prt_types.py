@@ -131,6 +131,7 @@ def material(**kw):
 
 PRT_MATERIAL_STANDARD = 0
 PRT_MATERIAL_PRINCIPLED = 1
+PRT_MATERIAL_MISS = 2
 
 
 def principled(**kw):

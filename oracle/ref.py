@@ -134,7 +134,9 @@ def write_rkscene(scene, directory):
 class RefDevice:
     """The reference's DeviceCpu running pathStream/sobolBurley on a Scene."""
 
-    def __init__(self, scene, seed=0, aov_mask=0, sunsky=None):
+    def __init__(self, scene, seed=0, aov_mask=0, sunsky=None, scene_path=None):
+        """`scene_path` (a .rkscene or .mesh file) makes the reference load that file itself;
+        the camera, frame, renderer and lights still come from `scene`."""
         self.scene = scene
         self.desc = scene.desc(oracle=True)
         self.rdesc = scene.renderer_desc()
@@ -145,9 +147,11 @@ class RefDevice:
             self._ss = ss_arr
             ss = T.fptr(ss_arr)
         h = C.c_void_p()
-        _check(_lib().ref_create(C.byref(self.desc), C.byref(scene.camera), C.byref(self.rdesc),
-                                 scene.width, scene.height, aov_mask, seed, self.tmp.name.encode(), ss,
-                                 C.byref(h)))
+        lib = _lib()
+        lib.ref_create_file.argtypes = [C.c_char_p] + list(lib.ref_create.argtypes)
+        _check(lib.ref_create_file(None if scene_path is None else str(scene_path).encode(), C.byref(self.desc),
+                                   C.byref(scene.camera), C.byref(self.rdesc), scene.width, scene.height, aov_mask,
+                                   seed, self.tmp.name.encode(), ss, C.byref(h)))
         self.h = h
 
     def close(self):

@@ -208,16 +208,30 @@ int ref_hardware_threads() { return tbb::this_task_arena::max_concurrency(); }
 // Creates a DeviceCpu with the scene, camera, frame and pathStream renderer loaded.
 // sunsky: NULL, or 5 floats (direction xyz, turbidity, ground albedo) for the reference's
 // sun-sky light (render/scene.cpp:412-431) in addition to the env lights of the scene.
+int ref_create_file(const char* scene_path, const prt_scene_desc* scene, const prt_camera_desc* cam,
+                    const prt_renderer_desc* rd, int width, int height, int aov_mask, uint32_t seed,
+                    const char* workdir, const float* sunsky, void** out);
+
 int ref_create(const prt_scene_desc* scene, const prt_camera_desc* cam, const prt_renderer_desc* rd,
                int width, int height, int aov_mask, uint32_t seed, const char* workdir,
                const float* sunsky, void** out)
+{
+  return ref_create_file(nullptr, scene, cam, rd, width, height, aov_mask, seed, workdir, sunsky, out);
+}
+
+// The reference's DeviceCpu on a given scene file (scene_path: .rkscene or .mesh, loaded by the
+// reference's own Scene::Scene), or, with scene_path null, on `scene` written as an rkscene; the
+// lights always come from `scene`'s environment description.
+int ref_create_file(const char* scene_path, const prt_scene_desc* scene, const prt_camera_desc* cam,
+                    const prt_renderer_desc* rd, int width, int height, int aov_mask, uint32_t seed,
+                    const char* workdir, const float* sunsky, void** out)
 {
   try
   {
     auto h = std::make_unique<RefHandle>();
     h->dir = workdir;
     std::filesystem::create_directories(h->dir);
-    const std::string path = writeScene(scene, h->dir);
+    const std::string path = scene_path ? std::string(scene_path) : writeScene(scene, h->dir);
     h->scenePath = path;
     h->sceneProps = lightProps(scene, h->dir, sunsky);
     h->device.initScene(path, h->sceneProps);

@@ -17,6 +17,8 @@ Fixtures (small, seeded, committed):
   terrain_img.npz  small terrain renders (96^2 heightfield, 24 spheres of all four material
                    kinds, sun-sky) at 128x64: 16 spp and 256 spp, seeds 0 and 1
   lobes_img.npz    the small scene with Oren-Nayar, sheen and layered spheres, 16 spp, seeds 0, 1
+  mesh_img.npz     the textured room written as a .mesh file and loaded by the reference's
+                   Scene::loadMesh (material 0 renders as a miss there), 16 spp, seeds 0, 1
   translucent_img.npz  the small scene with thin glass, opacity, subsurface, transparent and backlit
                    surfaces (shadow rays through transparent surfaces), 16 spp, seeds 0, 1
   siblings_img.npz primaryStream, aoStream, diffuseStream, diffuse2Stream renders of the small scene
@@ -132,6 +134,28 @@ def make_translucent_images():
     np.savez_compressed(OUT / "translucent_img.npz", **out)
 
 
+def mesh_scene():
+    return prt_scenes.cornell_inverse(seed=0, width=128, height=128, spp=16, tex_size=64)[0]
+
+
+def make_mesh_images():
+    """The textured room written as a .mesh file (prt_scenes.write_mesh) and loaded by the
+    reference's own Scene::loadMesh, 16 spp, seeds 0 and 1."""
+    import tempfile
+
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        s = mesh_scene()
+        path = prt_scenes.write_mesh(s, pathlib.Path(d) / "room.mesh")
+        for seed in (0, 1):
+            dev = ref.RefDevice(s, seed=seed, scene_path=path)
+            st = dev.render(16)
+            out[f"spp16_seed{seed}"] = dev.blit()
+            out[f"spp16_seed{seed}_rays"] = np.float64(st["rays"])
+            dev.close()
+    np.savez_compressed(OUT / "mesh_img.npz", **out)
+
+
 def sibling_scene(kind):
     s = prt_scenes.cornell(seed=0, width=64, height=64, spp=4)
     s.renderer_type = kind
@@ -208,7 +232,7 @@ def make_sunsky():
 
 if __name__ == "__main__":
     which = sys.argv[1:] or ["sobol", "rays", "images", "sunsky", "bsdf", "terrain", "lobes", "translucent", "siblings",
-                             "film"]
+                             "film", "mesh"]
     if "terrain" in which:
         make_terrain_images()
     if "bsdf" in which:
@@ -217,6 +241,8 @@ if __name__ == "__main__":
         make_lobe_images()
     if "translucent" in which:
         make_translucent_images()
+    if "mesh" in which:
+        make_mesh_images()
     if "siblings" in which:
         make_sibling_images()
     if "film" in which:

@@ -1,4 +1,4 @@
-"""rkscene ingestion on the host (prt_rkscene_load): the loader against files written by the
+"""rkscene ingestion on the host (prt_scene_file_load): the loader against files written by the
 reference's own rkscene::save (through the oracle), instances, default materials, and the
 errors rkscene::load reports.
 
@@ -35,7 +35,7 @@ SCENES = {
 @pytest.mark.parametrize("name", list(SCENES))
 def test_reference_written_file_loads_exactly(name, tmp_path):
     s = SCENES[name]()
-    r = prt_cuda.RkScene(reference_written(s, tmp_path))
+    r = prt_cuda.SceneFile(reference_written(s, tmp_path))
     meshes = r.meshes()
     assert len(meshes) == len(s.meshes)
     for a, b in zip(meshes, s.meshes):
@@ -63,7 +63,7 @@ def test_reference_written_file_loads_exactly(name, tmp_path):
 
 def test_own_writer_round_trip(tmp_path):
     s = prt_scenes.cornell_inverse(seed=2, width=16, height=16, tex_size=16)[0]
-    r = prt_cuda.RkScene(prt_scenes.write_rkscene(s, tmp_path / "room.rkscene"))
+    r = prt_cuda.SceneFile(prt_scenes.write_rkscene(s, tmp_path / "room.rkscene"))
     for a, b in zip(r.meshes(), s.meshes):
         assert np.array_equal(a["positions"], b["positions"]) and np.array_equal(a["indices"], b["indices"])
     assert all(bytes(a) == bytes(b) for a, b in zip(r.materials(), s.materials))
@@ -89,7 +89,7 @@ def test_instances_are_flattened(tmp_path):
         lin = rng.normal(size=(3, 3)).astype(np.float32) + 2 * np.eye(3, dtype=np.float32)
         xfs.append(np.concatenate([lin, rng.normal(size=(3, 1)).astype(np.float32)], 1))
     path = prt_scenes.write_rkscene(s, tmp_path / "inst.rkscene", objects=[([0, 1], xfs)])
-    meshes = prt_cuda.RkScene(path).meshes()
+    meshes = prt_cuda.SceneFile(path).meshes()
     assert len(meshes) == 6  # instance-major: (inst 0: geom 0, geom 1), (inst 1: ...), ...
     for k, mesh in enumerate(meshes):
         xf, src = xfs[k // 2], s.meshes[k % 2]
@@ -107,7 +107,7 @@ def test_missing_and_unknown_materials_get_the_default(tmp_path):
     s = small_scene()
     s.meshes[0]["material"] = -1
     s.meshes[1]["material"] = 7
-    r = prt_cuda.RkScene(prt_scenes.write_rkscene(s, tmp_path / "d.rkscene"))
+    r = prt_cuda.SceneFile(prt_scenes.write_rkscene(s, tmp_path / "d.rkscene"))
     mats = r.materials()
     assert len(mats) == 2 and mats[1].model == T.PRT_MATERIAL_PRINCIPLED
     assert [m["material"] for m in r.meshes()] == [1, 1]
@@ -139,14 +139,14 @@ def edit(path, fn):
 def test_errors(tmp_path, change, kind, text):
     path = edit(prt_scenes.write_rkscene(small_scene(), tmp_path / "e.rkscene"), change)
     with pytest.raises(kind, match=text):
-        prt_cuda.RkScene(path)
+        prt_cuda.SceneFile(path)
 
 
 def test_index_out_of_range(tmp_path):
     s = small_scene()
     s.meshes[1]["indices"] = s.meshes[1]["indices"] + 10
     with pytest.raises(ValueError, match="index out of range"):
-        prt_cuda.RkScene(prt_scenes.write_rkscene(s, tmp_path / "i.rkscene"))
+        prt_cuda.SceneFile(prt_scenes.write_rkscene(s, tmp_path / "i.rkscene"))
 
 
 @pytest.mark.parametrize("text", ["", "{", "[1,]", '{"a" 1}', '{"a": tru}', '{"a": "\\x"}', '{"a": 01}',
@@ -155,7 +155,7 @@ def test_malformed_json(tmp_path, text):
     p = tmp_path / "bad.rkscene"
     p.write_text(text)
     with pytest.raises(ValueError, match="invalid JSON|document"):
-        prt_cuda.RkScene(p)
+        prt_cuda.SceneFile(p)
 
 
 def test_json_details(tmp_path):
@@ -166,7 +166,7 @@ def test_json_details(tmp_path):
     doc["lights"] = None
     doc["extra"] = {"nested": [1, 2.5e-3, -0.0, True, False, None]}
     path.write_text(json.dumps(doc, ensure_ascii=True))
-    assert len(prt_cuda.RkScene(path).meshes()) == 2
+    assert len(prt_cuda.SceneFile(path).meshes()) == 2
 
 
 def test_gzip_buffers_are_reported(tmp_path):
@@ -174,4 +174,85 @@ def test_gzip_buffers_are_reported(tmp_path):
     binp = path.with_suffix(".rkbin")
     binp.rename(binp.with_name(binp.name + ".gz"))
     with pytest.raises(OSError, match="gzip"):
-        prt_cuda.RkScene(path)
+        prt_cuda.SceneFile(path)
+
+
+# -- .mesh + .mtl ------------------------------------------------------------------------------
+
+def test_mesh_file_loads_exactly(tmp_path):
+    s = prt_scenes.cornell_inverse(seed=0, width=16, height=16, tex_size=16)[0]
+    f = prt_cuda.SceneFile(prt_scenes.write_mesh(s, tmp_path / "room.mesh"))
+    mats = f.materials()
+    # write_mesh puts the first non-emissive material first, then the emissive ones.
+    n = len(s.materials)
+    emissive = [i for i in range(n) if s.materials[i].emission_luminance > 0.0]
+    others = [i for i in range(n) if i not in emissive]
+    order = others[:1] + emissive + others[1:]
+    assert len(mats) == n
+    assert mats[0].model == T.PRT_MATERIAL_MISS  # id 0: the stream renderer's miss bucket
+    for k in range(1, n):
+        assert bytes(mats[k]) == bytes(s.materials[order[k]]), k
+    # One mesh per material, the source triangles in order, shared vertex arrays.
+    P = np.concatenate([m["positions"] for m in s.meshes])
+    base = np.cumsum([0] + [m["positions"].shape[0] for m in s.meshes])
+    meshes = f.meshes()
+    for mesh in meshes:
+        assert np.array_equal(mesh["positions"], P)
+        src = [(k, m) for k, m in enumerate(s.meshes) if order[mesh["material"]] == m["material"]]
+        want = np.concatenate([m["indices"] + base[k] for k, m in src])
+        assert np.array_equal(mesh["indices"], want)
+    assert sum(m["indices"].shape[0] for m in meshes) == s.tri_count
+    for a, b in zip(f.textures(), s.textures):
+        assert np.array_equal(a, b)
+
+
+def test_mesh_obj_materials_map_to_principled(tmp_path):
+    s = small_scene()
+    s.meshes[1]["material"] = s.add_material(T.material(base_color=(0.9, 0.9, 0.9)))
+    path = prt_scenes.write_mesh(s, tmp_path / "obj.mesh")
+    mtl = path.with_suffix(".mtl")
+    mtl.write_text("newmtl mat0\nKd 0.2 0.3 0.4\n"
+                   "newmtl mat1\nKd 0.5 0.6 0.7\nNs 62\nKs 1 1 1\nTf 0.25 0.5 1\n")
+    mats = prt_cuda.SceneFile(path).materials()
+    m = mats[1]
+    assert m.model == T.PRT_MATERIAL_PRINCIPLED
+    assert np.allclose(list(m.base_color), [0.5, 0.6, 0.7])
+    rough = np.sqrt(np.sqrt(np.float32(2.0) / (np.float32(62.0) + np.float32(2.0))))
+    assert np.isclose(m.specular_roughness, rough, rtol=1e-6)
+    f0 = np.float32(1.0) * np.float32(0.08)
+    assert np.isclose(m.specular_ior, (1 + np.sqrt(f0)) / (1 - np.sqrt(f0)), rtol=1e-6)
+    assert m.transmission_weight == 1.0 and np.allclose(list(m.transmission_color), [0.75, 0.5, 0.0])
+
+
+def test_mesh_errors(tmp_path):
+    s = small_scene()
+    path = prt_scenes.write_mesh(s, tmp_path / "e.mesh")
+    data = path.read_bytes()
+    bad = tmp_path / "bad.mesh"
+    bad.write_bytes(b"\x00\x00\x00\x00" + data[4:])
+    with pytest.raises(ValueError, match="blob ID"):
+        prt_cuda.SceneFile(bad)
+    bad.write_bytes(data[:40])
+    with pytest.raises(OSError, match="end of stream"):
+        prt_cuda.SceneFile(bad)
+    path.with_suffix(".mtl").write_text("newmtl mat0\ntype CarPaint\n")
+    with pytest.raises(ValueError, match="not supported"):
+        prt_cuda.SceneFile(path)
+    with pytest.raises(ValueError, match="unknown scene format"):
+        prt_cuda.SceneFile(tmp_path / "x.obj")
+
+
+def test_mesh_emissive_materials_must_come_first(tmp_path):
+    """Scene::Scene needs the emissive materials at ids 1..k (render/scene.cpp:119-130)."""
+    s = small_scene()
+    s.add_material(T.material(base_color=(0.1, 0.2, 0.3)))
+    s.add_material(T.material(emission_luminance=5.0))
+    s.meshes[1]["material"] = 2
+    path = prt_scenes.write_mesh(s, tmp_path / "l.mesh")  # the writer puts the emissive one at id 1
+    assert len(prt_cuda.SceneFile(path).meshes()) == 2
+    # Swap the library's definitions of ids 1 and 2: the emissive material now sits at id 2.
+    text = path.with_suffix(".mtl").read_text()
+    text = text.replace("newmtl mat1", "newmtl X").replace("newmtl mat2", "newmtl mat1").replace("newmtl X", "newmtl mat2")
+    path.with_suffix(".mtl").write_text(text)
+    with pytest.raises(ValueError, match="remapped"):
+        prt_cuda.SceneFile(path)
