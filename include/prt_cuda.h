@@ -190,12 +190,21 @@ typedef struct prt_renderer_desc
  * DIFFUSE  "diffuseStream": white diffuse paths lit by a white sky, throughput x 0.8 per bounce
  *          (render/diffuse_renderer_stream.h);
  * DIFFUSE2 "diffuse2Stream": the same with a cosine-sampled sky ray per bounce, half-weighted
- *          (render/diffuse2_renderer_stream.h). */
+ *          (render/diffuse2_renderer_stream.h).
+ * The *_FAST types are the "...StreamFast" variants: the same renderers on the simple shading
+ * context (the unflipped geometric normal, SimpleShadingContextSimd, core/shading_context.h:
+ * 227-243, geometry/triangle_mesh.cpp:278-298) writing each sample over the pixel instead of
+ * accumulating (AccumBuffer::set, image/accum_buffer.h:547-570): the frame holds the last
+ * sample. */
 #define PRT_RENDERER_PATH     0
 #define PRT_RENDERER_PRIMARY  1
 #define PRT_RENDERER_AO       2
 #define PRT_RENDERER_DIFFUSE  3
 #define PRT_RENDERER_DIFFUSE2 4
+#define PRT_RENDERER_PRIMARY_FAST  5
+#define PRT_RENDERER_AO_FAST       6
+#define PRT_RENDERER_DIFFUSE_FAST  7
+#define PRT_RENDERER_DIFFUSE2_FAST 8
 
 /* AOV selection bits for prt_cuda_frame (render/device_cpu.cpp:178-232). */
 #define PRT_AOV_ALBEDO1  (1 << 0)   /* "aovAlbedo1": first-hit albedo */

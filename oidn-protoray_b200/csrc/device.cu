@@ -838,7 +838,7 @@ int prt_cuda_renderer(prt_context* ctx, const prt_renderer_desc* r)
 {
   return guarded(ctx, [&](Context& c) {
     if (!r || r->max_depth < 0 || r->max_depth > 1000) throw std::invalid_argument("invalid renderer settings");
-    if (r->type < PRT_RENDERER_PATH || r->type > PRT_RENDERER_DIFFUSE2) throw std::invalid_argument("invalid renderer type");
+    if (r->type < PRT_RENDERER_PATH || r->type > PRT_RENDERER_DIFFUSE2_FAST) throw std::invalid_argument("invalid renderer type");
     if (r->samples < 0 || r->samples > 4096) throw std::invalid_argument("invalid renderer samples");
     c.renderer.type = r->type;
     c.renderer.aoSamples = r->samples ? r->samples : 16;

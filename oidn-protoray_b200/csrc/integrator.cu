@@ -757,7 +757,9 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
 //          the camera.
 // Bounce k draws its directions from dimensions 4 + 2k (4 + 4k and 4 + 4k + 2 for type 4, AO ray
 // k from 4 + 2k). Writes ps.out, which kAccumulate adds in sample order.
-template <int Type>
+// Fast: the "...StreamFast" variant on the simple shading context -- the geometric normal as
+// computed, not flipped toward the ray, and the frame made from it.
+template <int Type, bool Fast>
 __global__ void __launch_bounds__(256) kSimpleRender(Launch L)
 {
   const int64_t P = (int64_t)L.pixelCount * L.samples;
@@ -792,6 +794,13 @@ __global__ void __launch_bounds__(256) kSimpleRender(Launch L)
       }
       ShadeCtx ctx;
       postIntersect(L.sc, org, dir, h.t, h.triId, h.u, h.v, ctx);
+      if (Fast)
+      {
+        // SimpleShadingContextSimd: N = Ng = normalize(cross(p1 - p0, p2 - p0)), unflipped.
+        const f3 Ng = ctx.backfacing ? -ctx.Ng : ctx.Ng;
+        ctx.f.N = Ng;
+        makeFrame(Ng, ctx.f.U, ctx.f.V);
+      }
       if (Type == 1)
       {
         color = (ctx.f.N + mk(1.f)) * 0.5f;
@@ -855,8 +864,10 @@ __global__ void __launch_bounds__(256) kSimpleRender(Launch L)
 // Also keeps, per pixel, the checkpoint copy of the sums taken before every power-of-two-th
 // sample (AccumBuffer::begin, image/accum_buffer.h:252-260; `count` = samples since the clear)
 // and, when enabled, the sums of squared samples (addSerial, :439-486).
+// overwrite: each sample replaces the pixel (AccumBuffer::set, image/accum_buffer.h:547-570), for
+// the renderers that do not accumulate.
 __global__ void kAccumulate(Launch L, float4* __restrict__ accum, float4* __restrict__ accA, float4* __restrict__ accN,
-                            float4* __restrict__ accC, float4* __restrict__ acc2, long long countBase)
+                            float4* __restrict__ accC, float4* __restrict__ acc2, long long countBase, int overwrite)
 {
   const int n = L.pixelCount;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
@@ -873,6 +884,12 @@ __global__ void kAccumulate(Launch L, float4* __restrict__ accum, float4* __rest
       if (accC && (count & (count - 1)) == 0) accC[q] = acc;
       const int64_t p = (int64_t)s * L.pixelCount + idx;
       const float4 o = L.ps.out[p];
+      if (overwrite)
+      {
+        acc = make_float4(o.x, o.y, o.z, 1.f);
+        if (acc2) sq = make_float4(o.x * o.x, o.y * o.y, o.z * o.z, 0.f);
+        continue;
+      }
       acc.x += o.x;
       acc.y += o.y;
       acc.z += o.z;
@@ -1357,10 +1374,18 @@ cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
     {
       const int P = pixelCount * S;
       begin(0);
-      if (type == PRT_RENDERER_PRIMARY) kSimpleRender<1><<<gridFor(ctx, P), 256, 0, ctx.stream>>>(L);
-      else if (type == PRT_RENDERER_AO) kSimpleRender<2><<<gridFor(ctx, P), 256, 0, ctx.stream>>>(L);
-      else if (type == PRT_RENDERER_DIFFUSE) kSimpleRender<3><<<gridFor(ctx, P), 256, 0, ctx.stream>>>(L);
-      else kSimpleRender<4><<<gridFor(ctx, P), 256, 0, ctx.stream>>>(L);
+      const int g = gridFor(ctx, P);
+      switch (type)
+      {
+      case PRT_RENDERER_PRIMARY: kSimpleRender<1, false><<<g, 256, 0, ctx.stream>>>(L); break;
+      case PRT_RENDERER_AO: kSimpleRender<2, false><<<g, 256, 0, ctx.stream>>>(L); break;
+      case PRT_RENDERER_DIFFUSE: kSimpleRender<3, false><<<g, 256, 0, ctx.stream>>>(L); break;
+      case PRT_RENDERER_DIFFUSE2: kSimpleRender<4, false><<<g, 256, 0, ctx.stream>>>(L); break;
+      case PRT_RENDERER_PRIMARY_FAST: kSimpleRender<1, true><<<g, 256, 0, ctx.stream>>>(L); break;
+      case PRT_RENDERER_AO_FAST: kSimpleRender<2, true><<<g, 256, 0, ctx.stream>>>(L); break;
+      case PRT_RENDERER_DIFFUSE_FAST: kSimpleRender<3, true><<<g, 256, 0, ctx.stream>>>(L); break;
+      default: kSimpleRender<4, true><<<g, 256, 0, ctx.stream>>>(L); break;
+      }
       end();
       rc.launches++;
       e = cudaGetLastError();
@@ -1369,7 +1394,7 @@ cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
     kAccumulate<<<gridFor(ctx, pixelCount), 256, 0, ctx.stream>>>(
       L, reinterpret_cast<float4*>(ctx.accum), reinterpret_cast<float4*>(ctx.accumA),
       reinterpret_cast<float4*>(ctx.accumN), reinterpret_cast<float4*>(ctx.accumC),
-      reinterpret_cast<float4*>(ctx.accum2), (long long)ctx.accumCount);
+      reinterpret_cast<float4*>(ctx.accum2), (long long)ctx.accumCount, type >= PRT_RENDERER_PRIMARY_FAST ? 1 : 0);
     ctx.accumCount += S;
     rc.launches++;
     e = cudaGetLastError();

@@ -224,6 +224,10 @@ PRT_RENDERER_PRIMARY = 1
 PRT_RENDERER_AO = 2
 PRT_RENDERER_DIFFUSE = 3
 PRT_RENDERER_DIFFUSE2 = 4
+PRT_RENDERER_PRIMARY_FAST = 5
+PRT_RENDERER_AO_FAST = 6
+PRT_RENDERER_DIFFUSE_FAST = 7
+PRT_RENDERER_DIFFUSE2_FAST = 8
 
 
 class RenderStats(C.Structure):

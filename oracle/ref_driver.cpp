@@ -244,8 +244,10 @@ int ref_create_file(const char* scene_path, const prt_scene_desc* scene, const p
     h->size = Vec2i(width, height);
     h->device.initFrame(h->size, frameProps);
     Props rprops;
-    static const char* kTypes[] = {"pathStream", "primaryStream", "aoStream", "diffuseStream", "diffuse2Stream"};
-    rprops.set("type", kTypes[(rd->type >= 0 && rd->type <= 4) ? rd->type : 0]);
+    static const char* kTypes[] = {"pathStream",        "primaryStream",     "aoStream",
+                                   "diffuseStream",     "diffuse2Stream",    "primaryStreamFast",
+                                   "aoStreamFast",      "diffuseStreamFast", "diffuse2StreamFast"};
+    rprops.set("type", kTypes[(rd->type >= 0 && rd->type <= 8) ? rd->type : 0]);
     rprops.set("samples", rd->samples > 0 ? rd->samples : 16);
     rprops.set("sampler", "sobolBurley");
     rprops.set("maxDepth", rd->max_depth);

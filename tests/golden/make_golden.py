@@ -21,7 +21,8 @@ Fixtures (small, seeded, committed):
                    Scene::loadMesh (material 0 renders as a miss there), 16 spp, seeds 0, 1
   translucent_img.npz  the small scene with thin glass, opacity, subsurface, transparent and backlit
                    surfaces (shadow rays through transparent surfaces), 16 spp, seeds 0, 1
-  siblings_img.npz primaryStream, aoStream, diffuseStream, diffuse2Stream renders of the small scene
+  siblings_img.npz primaryStream, aoStream, diffuseStream, diffuse2Stream and their ...Fast variants
+                   rendered on the small scene
   film.npz         sample variance, tone-mapped LDR images and frame errors of the small scene
   bsdf.npz         the reference's Standard-material BSDF (eval, sample) on 512 seeded tuples
                    for each case of tests/bsdf_cases.py
@@ -164,10 +165,10 @@ def sibling_scene(kind):
 
 
 def make_sibling_images():
-    """primaryStream, aoStream (8 rays), diffuseStream, diffuse2Stream on the small scene,
-    64x64, 4 spp, seed 0."""
+    """primaryStream, aoStream (8 rays), diffuseStream, diffuse2Stream and their ...Fast
+    variants on the small scene, 64x64, 4 spp, seed 0."""
     out = {}
-    for kind in (1, 2, 3, 4):
+    for kind in (1, 2, 3, 4, 5, 6, 7, 8):
         dev = ref.RefDevice(sibling_scene(kind), seed=0)
         st = dev.render(4)
         out[f"type{kind}"] = dev.blit()

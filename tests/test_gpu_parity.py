@@ -161,10 +161,12 @@ def test_translucent_same_seed_tracks_oracle(device, golden):
     assert abs(st["rays"] / float(z["spp16_seed0_rays"]) - 1.0) < 0.01
 
 
-@pytest.mark.parametrize("kind", [1, 2, 3, 4], ids=["primary", "ao", "diffuse", "diffuse2"])
+@pytest.mark.parametrize("kind", [1, 2, 3, 4, 5, 6, 7, 8], ids=["primary", "ao", "diffuse", "diffuse2", "primary_fast",
+                                                          "ao_fast", "diffuse_fast", "diffuse2_fast"])
 def test_sibling_renderers_match_oracle(device, golden, kind):
-    """primaryStream / aoStream / diffuseStream / diffuse2Stream: the same samples, hits and
-    directions as the reference, so the images agree to rounding (rare near-tie hits aside)."""
+    """primaryStream / aoStream / diffuseStream / diffuse2Stream and their ...Fast variants
+    (unflipped geometric normal, last sample only): the same samples, hits and directions as the
+    reference, so the images agree to rounding (rare near-tie hits aside)."""
     z = golden("siblings_img.npz")
     s = prt_scenes.cornell(seed=0, width=64, height=64, spp=4)
     s.renderer_type = kind
