@@ -380,6 +380,8 @@ typedef struct prt_tuning
   int32_t wave_paths;
   int32_t top_stage;   /* 1: traversal reads the top 3 BVH levels from shared memory; 2: from
                           global memory (the default); 0 keeps the current value */
+  int32_t ray_bins;    /* 1: each bounce's extended rays are traced grouped by direction octant;
+                          2: in the order shading produced them (the default); 0 keeps */
 } prt_tuning;
 
 int prt_cuda_set_tuning(prt_context* ctx, const prt_tuning* tuning);

@@ -634,6 +634,7 @@ void ensurePathState(Context& c, int spp)
   f(s.queue[0]); f(s.queue[1]); f(s.classQueues);
   c.waveSamples = want;
   const int64_t cap = (int64_t)want * px;
+  if (cap > (int64_t)kQueuePathMask) throw std::invalid_argument("path capacity above 2^29 - 1");
   s.capacity = cap;
   auto a4 = [&](size_t n) { return (float4*)devAlloc(c, n * sizeof(float4), nullptr); };
   s.rayO = a4(cap); s.rayD = a4(cap); s.hit = a4(cap); s.thr = a4(cap); s.rad = a4(cap);
@@ -651,10 +652,11 @@ void ensurePathState(Context& c, int spp)
 
 void ensureCounters(Context& c)
 {
-  const size_t need = sizeof(int) * 16 * (size_t)(c.renderer.maxDepth + 2);
+  const size_t blocks = 16 * (size_t)(c.renderer.maxDepth + 2);
   cudaStreamSynchronize(c.stream);
   if (c.ps.counters) cudaFree(c.ps.counters);
-  c.ps.counters = (int*)devAlloc(c, need, nullptr);
+  c.ps.counters = (int*)devAlloc(c, sizeof(int) * (blocks + 16), nullptr);
+  c.ps.octBins = c.ps.counters + blocks;
 }
 
 // Borrowed buffer: device memory is used in place, host memory is staged through a
@@ -1322,9 +1324,10 @@ int prt_cuda_set_tuning(prt_context* ctx, const prt_tuning* t)
   return guarded(ctx, [&](Context& c) {
     if (!t) throw std::invalid_argument("null tuning");
     if (t->trace_blocks < 0 || t->trace_blocks > 32 || t->shade_blocks < 0 || t->shade_blocks > 32 || t->wave_paths < 0 ||
-        t->top_stage < 0 || t->top_stage > 2)
+        t->top_stage < 0 || t->top_stage > 2 || t->ray_bins < 0 || t->ray_bins > 2)
       throw std::invalid_argument("tuning out of range");
     if (t->top_stage) c.topStage = t->top_stage == 1 ? 1 : 0;
+    if (t->ray_bins) c.rayBins = t->ray_bins == 1 ? 1 : 0;
     if (t->trace_blocks) c.traceBlocks = t->trace_blocks;
     if (t->shade_blocks) c.shadeBlocks = t->shade_blocks;
     if (t->wave_paths) c.wavePaths = t->wave_paths;
@@ -1339,6 +1342,7 @@ int prt_cuda_get_tuning(prt_context* ctx, prt_tuning* t)
     t->shade_blocks = c.shadeBlocks;
     t->wave_paths = (int32_t)std::min<int64_t>(c.wavePaths, 0x7fffffff);
     t->top_stage = c.topStage ? 1 : 2;
+    t->ray_bins = c.rayBins ? 1 : 2;
   });
 }
 
@@ -1349,11 +1353,12 @@ int prt_cuda_autotune(prt_context* ctx, int32_t spp, prt_tuning* chosen, double*
     if (!c.hasRenderer || !c.hasCamera || !c.accum) throw ApiError{PRT_ERR_STATE, "renderer, camera and frame are required"};
     if (spp <= 0) throw std::invalid_argument("spp must be > 0");
     cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
-    auto timeOne = [&](int tb, int sb, int64_t wave, int top) {
+    auto timeOne = [&](int tb, int sb, int64_t wave, int top, int bins) {
       c.traceBlocks = tb;
       c.shadeBlocks = sb;
       c.wavePaths = wave;
       c.topStage = top;
+      c.rayBins = bins;
       ensurePathState(c, spp);
       RenderCounters rc;
       cuCheck(cudaEventRecord(c.ev0, c.stream), "event");
@@ -1366,33 +1371,39 @@ int prt_cuda_autotune(prt_context* ctx, int32_t spp, prt_tuning* chosen, double*
     };
     const int profile = c.profileFlags;
     c.profileFlags = 0;
-    int bT = c.traceBlocks, bS = c.shadeBlocks, bTop = c.topStage;
+    int bT = c.traceBlocks, bS = c.shadeBlocks, bTop = c.topStage, bBins = c.rayBins;
     int64_t bW = c.wavePaths;
-    timeOne(bT, bS, bW, bTop);  // warm-up
+    timeOne(bT, bS, bW, bTop, bBins);  // warm-up
     double best = -1.0;
     // One axis at a time: wave size (paths in flight), traversal and shading grids, staging
-    // of the top BVH levels in shared memory.
+    // of the top BVH levels in shared memory, octant binning of extended rays.
     for (int64_t w : {8ll << 20, 16ll << 20, 32ll << 20})
     {
-      const double v = timeOne(bT, bS, w, bTop);
+      const double v = timeOne(bT, bS, w, bTop, bBins);
       if (v > best) { best = v; bW = w; }
     }
     for (int tb : {4, 6, 8, 12})
     {
-      const double v = timeOne(tb, bS, bW, bTop);
+      const double v = timeOne(tb, bS, bW, bTop, bBins);
       if (v > best) { best = v; bT = tb; }
     }
     for (int sb : {2, 4, 8})
     {
-      const double v = timeOne(bT, sb, bW, bTop);
+      const double v = timeOne(bT, sb, bW, bTop, bBins);
       if (v > best) { best = v; bS = sb; }
     }
     for (int top : {0, 1})
     {
-      const double v = timeOne(bT, bS, bW, top);
+      const double v = timeOne(bT, bS, bW, top, bBins);
       if (v > best) { best = v; bTop = top; }
     }
+    for (int bins : {0, 1})
+    {
+      const double v = timeOne(bT, bS, bW, bTop, bins);
+      if (v > best) { best = v; bBins = bins; }
+    }
     c.topStage = bTop;
+    c.rayBins = bBins;
     c.traceBlocks = bT;
     c.shadeBlocks = bS;
     c.wavePaths = bW;
@@ -1404,6 +1415,7 @@ int prt_cuda_autotune(prt_context* ctx, int32_t spp, prt_tuning* chosen, double*
     if (chosen)
     {
       chosen->trace_blocks = bT;
+      chosen->ray_bins = bBins ? 1 : 2;
       chosen->shade_blocks = bS;
       chosen->wave_paths = (int32_t)bW;
       chosen->top_stage = bTop ? 1 : 2;
@@ -1639,7 +1651,7 @@ int prt_cuda_batch_create(prt_context* ctx, const prt_batch_item* items, int32_t
         B.items.push_back(bi);
       }
       // Shared path pool: as many slots as the frame form's wave, at most the whole batch.
-      const int64_t C = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(c.wavePaths, B.workTotal), 1ll << 30));
+      const int64_t C = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(c.wavePaths, B.workTotal), (int64_t)kQueuePathMask));
       PathState& s = B.ps;
       s.capacity = C;
       auto a4 = [&](int64_t n) { return (float4*)devAlloc(c, (size_t)n * sizeof(float4), &B.bufs); };

@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(256) kTrace(Launch L, const int* __restrict__ 
     int cls = -1, p = 0;
     if (i < n)
     {
-      p = queue ? __ldg(queue + i) : i;
+      p = queue ? (int)((uint32_t)__ldg(queue + i) & kQueuePathMask) : i;
       const float4 a = L.ps.rayO[p], b = L.ps.rayD[p];
       uint32_t item = 0u;
       int pathDepth = depth;
@@ -371,6 +371,93 @@ __global__ void __launch_bounds__(256) kTrace(Launch L, const int* __restrict__ 
     }
   }
   if (Count) addCounts(L.ps.travCounts, tc);
+}
+
+// ---- ray binning: the next bounce's queue grouped by direction octant -------------------------
+//
+// kShadeSurface tags each extended path's queue entry with the octant of its new direction
+// (kQueueOctShift). Two passes over the entries (a counting sort on 3 bits) rewrite the queue so
+// that each octant's rays are contiguous, in their previous order within an octant. A warp of
+// kTrace then takes rays that visit the children of every node in the same order, and rays
+// from nearby origins walk the same subtrees at the same time. bins[0..7] count the entries of
+// each octant, bins[8..15] are the octants' fill cursors; both start at zero.
+
+// Counts the entries of each octant (one add per octant and block).
+__global__ void __launch_bounds__(256) kRayBinCount(const int* __restrict__ queue, const int* __restrict__ count,
+                                                    int* __restrict__ bins)
+{
+  __shared__ int sCount[8];
+  if (threadIdx.x < 8) sCount[threadIdx.x] = 0;
+  __syncthreads();
+  const int n = *count;
+  const int lane = laneId();
+  int mine = 0;  // lane o < 8 sums octant o
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < n; base += warps * 32)
+  {
+    const int i = base + lane;
+    const uint32_t oct = i < n ? (uint32_t)__ldg(queue + i) >> kQueueOctShift : 8u;
+#pragma unroll
+    for (int o = 0; o < 8; ++o)
+    {
+      const int c = __popc(__ballot_sync(0xffffffffu, oct == (uint32_t)o));
+      if (lane == o) mine += c;
+    }
+  }
+  if (lane < 8 && mine) atomicAdd(&sCount[lane], mine);
+  __syncthreads();
+  if (threadIdx.x < 8 && sCount[threadIdx.x]) atomicAdd(bins + threadIdx.x, sCount[threadIdx.x]);
+}
+
+// Writes each entry's path slot into its octant's range of `out`. Tiles of 256 entries: one
+// cursor add per octant and tile, ranks within the tile by warp ballots. Needs 256 threads.
+__global__ void __launch_bounds__(256) kRayBinScatter(const int* __restrict__ queue, const int* __restrict__ count,
+                                                      int* __restrict__ bins, int* __restrict__ out)
+{
+  __shared__ int sBase[8];     // first slot of each octant's range
+  __shared__ int sWarp[8][8];  // [warp][octant]: the warp's count, then its first slot in the range
+  const int n = *count;
+  const int lane = laneId(), warp = threadIdx.x >> 5;
+  if (threadIdx.x < 8)
+  {
+    int b = 0;
+    for (int o = 0; o < (int)threadIdx.x; ++o) b += bins[o];
+    sBase[threadIdx.x] = b;
+  }
+  for (int64_t tile = blockIdx.x; tile * 256 < n; tile += gridDim.x)
+  {
+    const int i = (int)(tile * 256) + (int)threadIdx.x;
+    const bool active = i < n;
+    const uint32_t v = active ? (uint32_t)__ldg(queue + i) : 0u;
+    const uint32_t oct = active ? v >> kQueueOctShift : 8u;
+    unsigned same = 0u;
+    int warpCount = 0;
+#pragma unroll
+    for (int o = 0; o < 8; ++o)
+    {
+      const unsigned b = __ballot_sync(0xffffffffu, oct == (uint32_t)o);
+      if (oct == (uint32_t)o) same = b;
+      if (lane == o) warpCount = __popc(b);
+    }
+    if (lane < 8) sWarp[warp][lane] = warpCount;
+    __syncthreads();
+    if (threadIdx.x < 8)
+    {
+      const int o = threadIdx.x;
+      int total = 0;
+      for (int w = 0; w < 8; ++w) total += sWarp[w][o];
+      int run = total ? atomicAdd(bins + 8 + o, total) : 0;
+      for (int w = 0; w < 8; ++w)
+      {
+        const int c = sWarp[w][o];
+        sWarp[w][o] = run;
+        run += c;
+      }
+    }
+    __syncthreads();
+    if (active) out[sBase[oct] + sWarp[warp][oct] + __popc(same & ((1u << lane) - 1u))] = (int)(v & kQueuePathMask);
+    __syncthreads();
+  }
 }
 
 // Ends path p with radiance `rad`. Frame form: ps.out, summed later by kAccumulate. Batch
@@ -587,6 +674,7 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
     bool extend = false;
     bool shadow = false;
     bool freed = false;
+    uint32_t extTag = 0u;  // direction octant of the extended ray, in the queue entry's top bits
     float4 shO = make_float4(0.f, 0.f, 0.f, 0.f), shD = shO, shL = shO;
     if (active)
     {
@@ -711,6 +799,7 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
       {
         L.ps.rayO[p] = make_float4(ctx.p.x, ctx.p.y, ctx.p.z, ctx.eps);
         L.ps.rayD[p] = make_float4(wi.x, wi.y, wi.z, kPosMax);
+        extTag = ((wi.x < 0.f ? 1u : 0u) | (wi.y < 0.f ? 2u : 0u) | (wi.z < 0.f ? 4u : 0u)) << kQueueOctShift;
         const bool update = (bsdfType & kBsdfContinuation) == 0;
         L.ps.thr[p] = make_float4(T.x, T.y, T.z, update ? bsdfPdf : lastPdf);
         ra.w = __int_as_float(update ? bsdfType : lastType);
@@ -730,7 +819,7 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
       if (shadow) shL.w = __uint_as_float((uint32_t)p | (extend ? 0u : kShadowFinish));
     }
     const int e = warpAppend(extCount, extend);
-    if (extend) queueOut[e] = p;
+    if (extend) queueOut[e] = (int)((uint32_t)p | extTag);
     const int sidx = warpAppend(shadowCount, shadow);
     if (shadow)
     {
@@ -1245,12 +1334,14 @@ static cudaError_t bounceLoop(Context& ctx, const Launch& L, int P, bool replay,
   if (e != cudaSuccess) return e;
   kRaygen<<<gridFor(ctx, P), 256, 0, ctx.stream>>>(L);
   rc.launches++;
+  const bool bins = ctx.rayBins && ctx.ps.octBins;
+  int inBuf = 1;  // queue buffer that holds this bounce's paths (camera rays need none)
   for (int depth = 0; depth <= maxDepth; ++depth)
   {
     int* cnt = counts + kCntStride * depth;
     int* next = counts + kCntStride * (depth + 1);
-    const int* q = depth == 0 ? nullptr : ctx.ps.queue[depth & 1];
-    int* qOut = ctx.ps.queue[(depth + 1) & 1];
+    const int* q = depth == 0 ? nullptr : ctx.ps.queue[inBuf];
+    int* qOut = ctx.ps.queue[inBuf ^ 1];
     begin(0);
     if (counting)
       kTrace<true, false><<<persistent, 256, 0, ctx.stream>>>(L, q, cnt, cnt + kCntWorkTrace, depth,
@@ -1299,6 +1390,17 @@ static cudaError_t bounceLoop(Context& ctx, const Launch& L, int P, bool replay,
       end();
       rc.launches++;
     }
+    if (bins)
+    {
+      // Group the extended paths by direction octant into the buffer this bounce has read.
+      e = cudaMemsetAsync(ctx.ps.octBins, 0, 16 * sizeof(int), ctx.stream);
+      if (e != cudaSuccess) return e;
+      kRayBinCount<<<shadeGrid, 256, 0, ctx.stream>>>(qOut, next, ctx.ps.octBins);
+      kRayBinScatter<<<shadeGrid, 256, 0, ctx.stream>>>(qOut, next, ctx.ps.octBins, ctx.ps.queue[inBuf]);
+      rc.launches += 2;
+    }
+    else
+      inBuf ^= 1;
     rc.traceLaunches++;
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;

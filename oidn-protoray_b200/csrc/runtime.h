@@ -20,6 +20,11 @@ struct DevBuf
   size_t bytes = 0;
 };
 
+// Queue entries of extended paths: the path slot in bits 0-28 and the octant of the new ray's
+// direction (bit k set when component k is negative) in bits 29-31. Readers mask the slot.
+constexpr uint32_t kQueueOctShift = 29;
+constexpr uint32_t kQueuePathMask = (1u << kQueueOctShift) - 1u;
+
 // Path state of one wave, structure of arrays indexed by path slot.
 struct PathState
 {
@@ -39,6 +44,7 @@ struct PathState
   int* queue[2] = {nullptr, nullptr};
   int* classQueues = nullptr;  // kShadeClasses queues of `capacity` entries each
   int* counters = nullptr;  // per bounce: input and shadow counts, then the work counters
+  int* octBins = nullptr;   // ray binning: 8 octant counts, then 8 octant cursors (frame form)
   unsigned long long* travCounts = nullptr;  // closest nodes, closest tris, shadow nodes, shadow tris
   uint32_t* err = nullptr;
 };
@@ -142,6 +148,7 @@ struct Context
   int shadeBlocks = 8;
   int64_t wavePaths = 32ll << 20;
   int topStage = 0;               // stage the top BVH levels in shared memory (frame form)
+  int rayBins = 0;                // group each bounce's extended rays by direction octant (frame form)
 };
 
 // Per-call statistics gathered by renderSamples.

@@ -270,6 +270,7 @@ class Tuning(C.Structure):
         ("shade_blocks", C.c_int32),
         ("wave_paths", C.c_int32),
         ("top_stage", C.c_int32),
+        ("ray_bins", C.c_int32),
     ]
 
 

@@ -1,7 +1,8 @@
 """Launch tuning (prt_cuda_set_tuning / prt_cuda_autotune) changes speed, never the image.
 
 Every tuning axis -- path-pool size (samples per wave), traversal and shading blocks per SM,
-staging of the top BVH levels in shared memory -- leaves each path's samples and shading
+staging of the top BVH levels in shared memory, grouping each bounce's extended rays by
+direction octant (which reorders the traversal queue) -- leaves each path's samples and shading
 unchanged and the accumulation adds each pixel's samples in sample order, so images are
 bit-identical across tunings.
 """
@@ -36,6 +37,8 @@ def render(dev, spp):
     dict(top_stage=2, trace_blocks=4, shade_blocks=2),
     dict(wave_paths=256 * 128 * 3),          # 3 samples per wave: waves of 3, 3, 2 samples
     dict(trace_blocks=12, shade_blocks=16, top_stage=1),
+    dict(ray_bins=2),                        # queue in shading order instead of octant groups
+    dict(ray_bins=1, top_stage=1, wave_paths=256 * 128 * 3),
 ])
 def test_tuning_keeps_the_image(dev, tuning):
     default = dev.get_tuning()
@@ -56,6 +59,7 @@ def test_autotune_returns_a_valid_tuning(dev):
         chosen, mrays = dev.autotune(2)
         assert mrays > 0
         assert chosen["top_stage"] in (1, 2) and 1 <= chosen["trace_blocks"] <= 32
+        assert chosen["ray_bins"] in (1, 2)
         assert dev.get_tuning() == chosen
         img, _ = render(dev, 4)
         assert np.array_equal(img, ref)
@@ -68,3 +72,5 @@ def test_tuning_rejects_out_of_range(dev):
         dev.set_tuning(trace_blocks=64)
     with pytest.raises(ValueError):
         dev.set_tuning(top_stage=3)
+    with pytest.raises(ValueError):
+        dev.set_tuning(ray_bins=3)
