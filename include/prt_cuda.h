@@ -372,7 +372,8 @@ int prt_cuda_render_static(prt_context* ctx, uint32_t first_sample, int32_t spp,
 /* Launch tuning of the wavefront kernels; 0 in a field keeps the current value.
  * trace_blocks / shade_blocks: persistent blocks of 256 threads per SM for the traversal and
  *   shading kernels;
- * wave_paths: upper bound on paths in flight per wave (path state is ~170 bytes per path). */
+ * wave_paths: upper bound on paths in flight per wave (path state is ~170-240 bytes per path);
+ *   134,217,728 by default (a 1920x1080 x 64-spp frame in one wave). */
 typedef struct prt_tuning
 {
   int32_t trace_blocks;

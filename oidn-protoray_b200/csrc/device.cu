@@ -610,8 +610,9 @@ void allocFrame(Context& c, int width, int height, int aovMask)
 }
 
 // Per-bounce counter blocks of 16 ints (see renderSamples), maxDepth + 2 of them.
-// Path state for waves of `samples` whole-frame samples (at least one), capped at ~16M paths
-// (about 3.5 GB). Allocated on the first render and grown when a call needs more.
+// Path state for waves of `samples` whole-frame samples (at least one), capped at wavePaths
+// paths (128M by default: one 64-spp 1080p frame, about 31 GB). Allocated on the first render
+// and grown when a call needs more.
 void ensurePathState(Context& c, int spp)
 {
   const int64_t px = (int64_t)c.width * c.height;
@@ -1377,7 +1378,7 @@ int prt_cuda_autotune(prt_context* ctx, int32_t spp, prt_tuning* chosen, double*
     double best = -1.0;
     // One axis at a time: wave size (paths in flight), traversal and shading grids, staging
     // of the top BVH levels in shared memory, octant binning of extended rays.
-    for (int64_t w : {8ll << 20, 16ll << 20, 32ll << 20})
+    for (int64_t w : {8ll << 20, 16ll << 20, 32ll << 20, 64ll << 20, 128ll << 20})
     {
       const double v = timeOne(bT, bS, w, bTop, bBins);
       if (v > best) { best = v; bW = w; }

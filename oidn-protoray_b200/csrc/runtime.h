@@ -146,7 +146,7 @@ struct Context
   int profileFlags = 0;
   int traceBlocks = 8;            // launch tuning (prt_tuning)
   int shadeBlocks = 8;
-  int64_t wavePaths = 32ll << 20;
+  int64_t wavePaths = 128ll << 20;
   int topStage = 0;               // stage the top BVH levels in shared memory (frame form)
   int rayBins = 0;                // group each bounce's extended rays by direction octant (frame form)
 };
