@@ -132,8 +132,16 @@ typedef struct prt_env_desc
   int32_t image_width;
   int32_t image_height;
   int32_t image_lut_size;       /* "imageLightLutSize"; 0 = the reference default */
-  int32_t reserved;
+  int32_t flags;                /* PRT_ENV_*; 0 = the order distant, ambient, image */
 } prt_env_desc;
+
+/* Scene::initLights (render/scene.cpp:372-440) adds its environment lights in the order
+ * distantLight, ambientLight, imageLight, then a sun-sky light's sun (a distant light) and sky (an
+ * image light); light selection is by power over that list, so the order decides which light a
+ * given sample picks. A sun-sky light crosses this boundary as its two products in the distant and
+ * image fields; when an ambient light is also present, the reference's order puts the ambient light
+ * first, which this flag selects: ambient, distant, image. */
+#define PRT_ENV_AMBIENT_FIRST 1
 
 typedef struct prt_scene_desc
 {
@@ -287,9 +295,17 @@ typedef struct prt_scene_stats
   int32_t depth;        /* wide levels */
   int32_t top_count;    /* nodes of the first three levels, stored first */
   int32_t iterations;   /* device build: clustering iterations; host build: 0 */
+  float   bounds_lo[3]; /* scene bounds over all triangle vertices (Scene::getBounds) */
+  float   bounds_hi[3];
 } prt_scene_stats;
 
 int prt_cuda_scene_stats(prt_context* ctx, prt_scene_stats* out);
+
+/* Device::initLights (render/device_cpu.cpp:101-104 -> Scene::initLights, render/scene.cpp:365-450):
+ * replaces the environment lights of the uploaded scene and rebuilds the light-selection table
+ * (area lights first, then the environment lights); geometry, BVH, materials and area lights stay.
+ * Also reached through the `env` of prt_cuda_scene_upload / prt_cuda_scene_load. */
+int prt_cuda_scene_lights(prt_context* ctx, const prt_env_desc* env);
 
 /* Copies the uploaded scene's BVH8 to host memory: min(node_capacity, node_count) 80-byte
  * nodes and min(tri_capacity, tri_count) 48-byte triangle records (bvh8.h layout; either
@@ -358,7 +374,9 @@ int prt_cuda_render(prt_context* ctx, int32_t spp, prt_render_stats* stats);
  * Renders `spp` samples per pixel numbered from `first_sample` (the same samples prt_cuda_render
  * draws at that sample index) with the current scene, camera, renderer and seed, and writes
  * their average to `hdr_out`: width*height RGB floats, row-major, in device or managed memory the
- * caller owns. The frame and sample index of prt_cuda_render are left untouched.
+ * caller owns on the context's device (memory of another GPU is rejected). The frame size and AOV
+ * mask come from prt_cuda_frame; the frame's own sums and the sample index of prt_cuda_render
+ * are left untouched. The call is synchronous: it returns after the image is written.
  * No device memory is allocated or freed: path state, queues, counters and sums live in one
  * scratch area compiled into the library (about 18 MB, present on every GPU that loads it until
  * the process exits), sized for frames of at most 65,536 pixels (e.g. 256x256) and

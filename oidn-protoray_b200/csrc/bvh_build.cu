@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <cmath>
 #include <chrono>
 #include <cstring>
 #include <stdexcept>
@@ -1007,8 +1008,13 @@ void buildBvh8Device(const float4* pos, const int4* triVerts, int64_t triCount, 
   Scanner<u64> scan64;
   scan64.init(s, n);
   int count = n, nodeBase = n, force = 0, iters = 0;
+  // Each iteration merges at least a 1/64 share of the clusters, or else forces the next one to
+  // pair Morton neighbours (which merges about half); so log(n)/log(64/63) iterations bound a
+  // converging run. NaN boxes could stall it, hence the cap.
+  const int maxIters = 64 + 64 * (int)std::ceil(std::log2((double)std::max<int64_t>(n, 2)));
   while (count > kTailMax)
   {
+    if (iters >= maxIters) throw std::runtime_error("BVH8 device build: clustering did not converge");
     kNearest<<<blocksFor(count, kNearestThreads), kNearestThreads, 0, st>>>(cLoA, cHiA, count, nn, force);
     kMergeFlags<<<blocksFor(count, 256), 256, 0, st>>>(nn, count, flags);
     scan64.run(flags, flags, count, st);
@@ -1016,6 +1022,7 @@ void buildBvh8Device(const float4* pos, const int4* triVerts, int64_t triCount, 
                                                     nodeBase);
     const u64 tot = readScalar(scan64.total, st);
     const int merges = (int)(tot >> 32);
+    if (merges == 0 && force) throw std::runtime_error("BVH8 device build: clustering did not converge");
     force = (int64_t)merges * 64 < count;
     nodeBase += merges;
     count = (int)(uint32_t)tot;

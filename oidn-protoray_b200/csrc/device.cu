@@ -48,6 +48,7 @@ template <class F>
 int guarded(prt_context* ctx, F&& f)
 {
   if (!ctx) return PRT_ERR_INVALID_ARG;
+  ctx->c.stageNext = 0;  // staging slots are per call (a call that threw may not have released its own)
   try
   {
     f(ctx->c);
@@ -90,9 +91,9 @@ void* devAlloc(Context& c, size_t bytes, std::vector<DevBuf>* owner)
 }
 
 template <class T>
-T* upload(Context& c, const std::vector<T>& v)
+T* upload(Context& c, const std::vector<T>& v, std::vector<DevBuf>* owner = nullptr)
 {
-  T* p = (T*)devAlloc(c, v.size() * sizeof(T), &c.sceneBufs);
+  T* p = (T*)devAlloc(c, v.size() * sizeof(T), owner ? owner : &c.sceneBufs);
   if (!v.empty()) cuCheck(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c.stream), "upload");
   return p;
 }
@@ -102,6 +103,8 @@ void freeScene(Context& c)
   cudaStreamSynchronize(c.stream);
   for (auto& b : c.sceneBufs) cudaFree(b.ptr);
   c.sceneBufs.clear();
+  for (auto& b : c.envBufs) cudaFree(b.ptr);
+  c.envBufs.clear();
   c.hasScene = false;
 }
 
@@ -296,6 +299,110 @@ DevMaterial resolveMaterial(const prt_material& m, std::vector<float>& media, in
   return d;
 }
 
+// Environment lights in Scene::initLights order (render/scene.cpp:372-440) -- distant,
+// ambient, image, or ambient first with PRT_ENV_AMBIENT_FIRST -- and the light-selection CDF
+// over the area lights (their powers in c.areaLightPowerHost) followed by them. The buffers go
+// to c.envBufs, which a later call (prt_cuda_scene_lights) frees and replaces.
+void buildEnvLights(Context& c, DevScene& sc, const prt_env_desc& e)
+{
+  if (e.flags & ~PRT_ENV_AMBIENT_FIRST) throw std::invalid_argument("unknown environment flags");
+  cudaStreamSynchronize(c.stream);
+  for (auto& buf : c.envBufs) cudaFree(buf.ptr);
+  c.envBufs.clear();
+  sc.image = DevImageLight{};
+  std::vector<float> lightPower = c.areaLightPowerHost;
+  const float sceneRadius = c.sceneRadius;
+  const float pi = 3.14159265358979323846f;
+  auto pos3 = [](const float* v) { return v[0] > 0.f || v[1] > 0.f || v[2] > 0.f; };
+  int ne = 0;
+  auto addAmbient = [&]() {
+    if (!pos3(e.ambient_color)) return;
+    DevEnvLight& L = sc.env[ne++];
+    L.kind = kEnvAmbient;
+    for (int k = 0; k < 3; ++k) L.color[k] = e.ambient_color[k];
+    lightPower.push_back(4.f * pi * pi * sceneRadius * sceneRadius * luminanceHost(L.color));
+  };
+  if (e.flags & PRT_ENV_AMBIENT_FIRST) addAmbient();
+  if (pos3(e.distant_color))
+  {
+    DevEnvLight& L = sc.env[ne++];
+    L.kind = kEnvDistant;
+    for (int k = 0; k < 3; ++k) L.color[k] = e.distant_color[k];
+    float d[3] = {e.distant_dir[0], e.distant_dir[1], e.distant_dir[2]};
+    const float il = 1.f / std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    for (int k = 0; k < 3; ++k) L.dir[k] = d[k] * il;
+    makeFrameHost(L.dir, L.frameU, L.frameV);
+    L.halfAngle = e.distant_angle * 0.5f;
+    L.cosAngle = std::cos(L.halfAngle);
+    const float sh = std::sin(0.5f * L.halfAngle);
+    L.conePdf = 1.f / (4.f * pi * sh * sh);
+    lightPower.push_back(4.f * pi * pi * sh * sh * sceneRadius * sceneRadius * luminanceHost(L.color));
+  }
+  if (!(e.flags & PRT_ENV_AMBIENT_FIRST)) addAmbient();
+  if (e.image_rgb)
+  {
+    if (e.image_width <= 0 || e.image_height <= 0) throw std::invalid_argument("invalid image light");
+    DevEnvLight& L = sc.env[ne++];
+    L.kind = kEnvImage;
+    const int W = e.image_width, H = e.image_height;
+    // Texture-row order (bottom row first), as ImageTextureBuffer stores it.
+    std::vector<float> tex((size_t)W * H * 3);
+    for (int y = 0; y < H; ++y)
+      std::memcpy(&tex[(size_t)y * W * 3], e.image_rgb + (size_t)(H - 1 - y) * W * 3, sizeof(float) * 3 * W);
+    // ImageLight LUT (light/image_light.h:19-62).
+    int lw = W, lh = H, bucket = 1;
+    if (e.image_lut_size > 0)
+      while (std::max(lw, lh) > e.image_lut_size && lw % 2 == 0 && lh % 2 == 0)
+      {
+        lw /= 2;
+        lh /= 2;
+        bucket *= 2;
+      }
+    std::vector<float> weights((size_t)lw * lh);
+    for (int y = 0; y < lh; ++y)
+      for (int x = 0; x < lw; ++x)
+      {
+        float sum = 0.f;
+        for (int y2 = 0; y2 < bucket; ++y2)
+          for (int x2 = 0; x2 < bucket; ++x2)
+            sum += luminanceHost(&tex[3 * ((size_t)(y * bucket + y2) * W + (x * bucket + x2))]);
+        weights[(size_t)y * lw + x] = sum * std::sin((y + 0.5f) / lh * pi);
+      }
+    // Distribution2D::init (sampling/distribution2d.cpp:13-30).
+    std::vector<float> xCdfs((size_t)lh * (lw + 1)), fy(lh), yCdf(lh + 1);
+    for (int y = 0; y < lh; ++y)
+    {
+      fy[y] = 0.f;
+      for (int x = 0; x < lw; ++x) fy[y] += weights[(size_t)y * lw + x];
+      cdfInit(&xCdfs[(size_t)y * (lw + 1)], &weights[(size_t)y * lw], lw);
+    }
+    cdfInit(yCdf.data(), fy.data(), lh);
+    sc.image.rgb = upload(c, tex, &c.envBufs);
+    sc.image.width = W;
+    sc.image.height = H;
+    sc.image.lutW = lw;
+    sc.image.lutH = lh;
+    sc.image.yCdf = upload(c, yCdf, &c.envBufs);
+    sc.image.xCdfs = upload(c, xCdfs, &c.envBufs);
+    float sumL = 0.f;
+    for (int i = 0; i < W * H; ++i) sumL += luminanceHost(&tex[3 * (size_t)i]);
+    lightPower.push_back(4.f * pi * pi * sceneRadius * sceneRadius * (sumL / float(W * H)));
+  }
+  if (sc.areaLightCount == 0 && ne == 0)
+  {
+    // Default ambient light (render/scene.cpp:435-440).
+    DevEnvLight& L = sc.env[ne++];
+    L.kind = kEnvAmbient;
+    L.color[0] = L.color[1] = L.color[2] = 1.f;
+    lightPower.push_back(4.f * pi * pi * sceneRadius * sceneRadius * luminanceHost(L.color));
+  }
+  sc.envCount = ne;
+  sc.lightCount = sc.areaLightCount + ne;
+  std::vector<float> lightCdf(sc.lightCount + 1);
+  cdfInit(lightCdf.data(), lightPower.data(), sc.lightCount);
+  sc.lightCdf = upload(c, lightCdf, &c.envBufs);
+}
+
 void uploadScene(Context& c, const prt_scene_desc* s)
 {
   if (!s || s->mesh_count < 0 || s->material_count <= 0 || !s->materials)
@@ -484,95 +591,14 @@ void uploadScene(Context& c, const prt_scene_desc* s)
   sc.areaCdfOffset = upload(c, areaCdfOff);
   sc.areaCdf = upload(c, areaCdf);
   sc.etris = upload(c, etris);
-  // Environment lights in Scene::initLights order (render/scene.cpp:372-440).
-  const prt_env_desc& e = s->env;
-  const float pi = 3.14159265358979323846f;
-  auto pos3 = [](const float* v) { return v[0] > 0.f || v[1] > 0.f || v[2] > 0.f; };
-  int ne = 0;
-  if (pos3(e.distant_color))
+  c.areaLightPowerHost = lightPower;
+  c.sceneRadius = sceneRadius;
+  for (int k = 0; k < 3; ++k)
   {
-    DevEnvLight& L = sc.env[ne++];
-    L.kind = kEnvDistant;
-    for (int k = 0; k < 3; ++k) L.color[k] = e.distant_color[k];
-    float d[3] = {e.distant_dir[0], e.distant_dir[1], e.distant_dir[2]};
-    const float il = 1.f / std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-    for (int k = 0; k < 3; ++k) L.dir[k] = d[k] * il;
-    makeFrameHost(L.dir, L.frameU, L.frameV);
-    L.halfAngle = e.distant_angle * 0.5f;
-    L.cosAngle = std::cos(L.halfAngle);
-    const float sh = std::sin(0.5f * L.halfAngle);
-    L.conePdf = 1.f / (4.f * pi * sh * sh);
-    lightPower.push_back(4.f * pi * pi * sh * sh * sceneRadius * sceneRadius * luminanceHost(L.color));
+    c.boundsLo[k] = lo[k];
+    c.boundsHi[k] = hi[k];
   }
-  if (pos3(e.ambient_color))
-  {
-    DevEnvLight& L = sc.env[ne++];
-    L.kind = kEnvAmbient;
-    for (int k = 0; k < 3; ++k) L.color[k] = e.ambient_color[k];
-    lightPower.push_back(4.f * pi * pi * sceneRadius * sceneRadius * luminanceHost(L.color));
-  }
-  if (e.image_rgb)
-  {
-    if (e.image_width <= 0 || e.image_height <= 0) throw std::invalid_argument("invalid image light");
-    DevEnvLight& L = sc.env[ne++];
-    L.kind = kEnvImage;
-    const int W = e.image_width, H = e.image_height;
-    // Texture-row order (bottom row first), as ImageTextureBuffer stores it.
-    std::vector<float> tex((size_t)W * H * 3);
-    for (int y = 0; y < H; ++y)
-      std::memcpy(&tex[(size_t)y * W * 3], e.image_rgb + (size_t)(H - 1 - y) * W * 3, sizeof(float) * 3 * W);
-    // ImageLight LUT (light/image_light.h:19-62).
-    int lw = W, lh = H, bucket = 1;
-    if (e.image_lut_size > 0)
-      while (std::max(lw, lh) > e.image_lut_size && lw % 2 == 0 && lh % 2 == 0)
-      {
-        lw /= 2;
-        lh /= 2;
-        bucket *= 2;
-      }
-    std::vector<float> weights((size_t)lw * lh);
-    for (int y = 0; y < lh; ++y)
-      for (int x = 0; x < lw; ++x)
-      {
-        float sum = 0.f;
-        for (int y2 = 0; y2 < bucket; ++y2)
-          for (int x2 = 0; x2 < bucket; ++x2)
-            sum += luminanceHost(&tex[3 * ((size_t)(y * bucket + y2) * W + (x * bucket + x2))]);
-        weights[(size_t)y * lw + x] = sum * std::sin((y + 0.5f) / lh * pi);
-      }
-    // Distribution2D::init (sampling/distribution2d.cpp:13-30).
-    std::vector<float> xCdfs((size_t)lh * (lw + 1)), fy(lh), yCdf(lh + 1);
-    for (int y = 0; y < lh; ++y)
-    {
-      fy[y] = 0.f;
-      for (int x = 0; x < lw; ++x) fy[y] += weights[(size_t)y * lw + x];
-      cdfInit(&xCdfs[(size_t)y * (lw + 1)], &weights[(size_t)y * lw], lw);
-    }
-    cdfInit(yCdf.data(), fy.data(), lh);
-    sc.image.rgb = upload(c, tex);
-    sc.image.width = W;
-    sc.image.height = H;
-    sc.image.lutW = lw;
-    sc.image.lutH = lh;
-    sc.image.yCdf = upload(c, yCdf);
-    sc.image.xCdfs = upload(c, xCdfs);
-    float sumL = 0.f;
-    for (int i = 0; i < W * H; ++i) sumL += luminanceHost(&tex[3 * (size_t)i]);
-    lightPower.push_back(4.f * pi * pi * sceneRadius * sceneRadius * (sumL / float(W * H)));
-  }
-  if (sc.areaLightCount == 0 && ne == 0)
-  {
-    // Default ambient light (render/scene.cpp:435-440).
-    DevEnvLight& L = sc.env[ne++];
-    L.kind = kEnvAmbient;
-    L.color[0] = L.color[1] = L.color[2] = 1.f;
-    lightPower.push_back(4.f * pi * pi * sceneRadius * sceneRadius * luminanceHost(L.color));
-  }
-  sc.envCount = ne;
-  sc.lightCount = sc.areaLightCount + ne;
-  std::vector<float> lightCdf(sc.lightCount + 1);
-  cdfInit(lightCdf.data(), lightPower.data(), sc.lightCount);
-  sc.lightCdf = upload(c, lightCdf);
+  buildEnvLights(c, sc, s->env);
   std::vector<float> mediaColor;
   for (size_t i = 0; i < media.size() / 4; ++i) mediaColor.insert(mediaColor.end(), {media[4 * i], media[4 * i + 1], media[4 * i + 2]});
   sc.mediaColor = upload(c, mediaColor);
@@ -660,8 +686,11 @@ void ensureCounters(Context& c)
   c.ps.octBins = c.ps.counters + blocks;
 }
 
-// Borrowed buffer: device memory is used in place, host memory is staged through a
-// temporary device allocation.
+// Borrowed buffer: device memory is used in place; host memory (pinned or pageable) is staged
+// through one of the context's staging slots. A call's k-th Staged takes slot k, which keeps its
+// allocation for later calls, so repeated calls (a blit per frame) allocate nothing. Growing a
+// slot frees its old buffer only after the stream has drained. Slots are taken and released in
+// LIFO order (Staged objects are locals of one entry point).
 struct Staged
 {
   void* dev = nullptr;
@@ -683,8 +712,21 @@ struct Staged
     }
     cudaGetLastError();
     host = const_cast<void*>(p);
+    const size_t slot = (size_t)ctx.stageNext;
+    if (ctx.stage.size() <= slot) ctx.stage.resize(slot + 1);
+    DevBuf& b = ctx.stage[slot];
+    const size_t need = std::max<size_t>(n, 256);
+    if (b.bytes < need)
+    {
+      cuCheck(cudaStreamSynchronize(ctx.stream), "staging sync");
+      if (b.ptr) cudaFree(b.ptr);
+      b = DevBuf{};
+      cuCheck(cudaMalloc(&b.ptr, need), "cudaMalloc (staging)");
+      b.bytes = need;
+    }
+    ++ctx.stageNext;
     owned = true;
-    cuCheck(cudaMalloc(&dev, std::max<size_t>(n, 16)), "cudaMalloc");
+    dev = b.ptr;
     if (copyIn && n) cuCheck(cudaMemcpyAsync(dev, p, n, cudaMemcpyHostToDevice, ctx.stream), "copy in");
   }
   void copyOut()
@@ -693,13 +735,24 @@ struct Staged
   }
   ~Staged()
   {
-    if (owned && dev)
+    if (owned)
     {
+      // The call returns only after its copies of the caller's host memory are done (a pinned
+      // buffer is read or written asynchronously otherwise).
       cudaStreamSynchronize(c->stream);
-      cudaFree(dev);
+      --c->stageNext;
     }
   }
 };
+
+void freeStaging(Context& c)
+{
+  cudaStreamSynchronize(c.stream);
+  for (auto& buf : c.stage)
+    if (buf.ptr) cudaFree(buf.ptr);
+  c.stage.clear();
+  c.stageNext = 0;
+}
 
 void checkDeviceErrors(Context& c)
 {
@@ -774,6 +827,7 @@ int prt_cuda_destroy(prt_context* ctx)
   cudaSetDevice(c.device);
   freeScene(c);
   freeFrame(c);
+  freeStaging(c);
   if (c.ps.counters) cudaFree(c.ps.counters);
   if (c.ps.err) cudaFree(c.ps.err);
   if (c.ps.travCounts) cudaFree(c.ps.travCounts);
@@ -1011,6 +1065,24 @@ int prt_cuda_scene_stats(prt_context* ctx, prt_scene_stats* out)
     out->depth = c.bvhDepth;
     out->top_count = c.bvhTop;
     out->iterations = c.bvhIterations;
+    for (int k = 0; k < 3; ++k)
+    {
+      out->bounds_lo[k] = c.boundsLo[k];
+      out->bounds_hi[k] = c.boundsHi[k];
+    }
+  });
+}
+
+int prt_cuda_scene_lights(prt_context* ctx, const prt_env_desc* env)
+{
+  return guarded(ctx, [&](Context& c) {
+    if (!env) throw std::invalid_argument("null environment description");
+    requireScene(c);
+    cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+    DevScene sc = c.scene;
+    buildEnvLights(c, sc, *env);
+    cuCheck(cudaStreamSynchronize(c.stream), "scene lights");
+    c.scene = sc;
   });
 }
 
@@ -1450,7 +1522,9 @@ constexpr size_t kStaticPathPlanes = 12;  // rayO rayD hit thr rad info shO shD 
 constexpr size_t kStaticOffQueues = kStaticPathPlanes * kStaticPlane;
 constexpr size_t kStaticOffAccum = kStaticOffQueues + (2 + kShadeClasses) * kStaticQueue;
 constexpr size_t kStaticOffCounters = kStaticOffAccum + 3 * kStaticPlane;
-constexpr size_t kStaticOffTrav = kStaticOffCounters + staticRound(sizeof(int) * 16 * (kStaticMaxDepth + 2));
+// Per-bounce counter blocks (16 ints each) followed by the 16 ints of the octant bins, the layout
+// ensureCounters gives the allocating path.
+constexpr size_t kStaticOffTrav = kStaticOffCounters + staticRound(sizeof(int) * (16 * (kStaticMaxDepth + 2) + 16));
 constexpr size_t kStaticOffErr = kStaticOffTrav + staticRound(4 * sizeof(unsigned long long));
 constexpr size_t kStaticBytes = kStaticOffErr + kStaticAlign;
 
@@ -1516,7 +1590,10 @@ int prt_cuda_render_static(prt_context* ctx, uint32_t first_sample, int32_t spp,
 {
   return guarded(ctx, [&](Context& c) {
     requireScene(c);
-    if (!c.hasRenderer || !c.hasCamera || !c.accum) throw ApiError{PRT_ERR_STATE, "renderer, camera and frame are required"};
+    // Only the frame's size and AOV mask are used: the sums live in the scratch area, so the
+    // frame planes prt_cuda_frame allocated are neither needed nor touched.
+    if (!c.hasRenderer || !c.hasCamera || c.width <= 0 || c.height <= 0)
+      throw ApiError{PRT_ERR_STATE, "renderer, camera and frame size are required"};
     if (spp <= 0) throw std::invalid_argument("spp must be > 0");
     if (!hdr_out) throw std::invalid_argument("null output");
     const int64_t px = (int64_t)c.width * c.height;
@@ -1532,13 +1609,18 @@ int prt_cuda_render_static(prt_context* ctx, uint32_t first_sample, int32_t spp,
       cudaGetLastError();
       throw std::invalid_argument("hdr_out must be device or managed memory");
     }
+    // Device memory of another GPU would be written across the interconnect (or fault without
+    // peer access): only this context's device is accepted.
+    if (attr.type == cudaMemoryTypeDevice && attr.device != c.device)
+      throw std::invalid_argument("hdr_out is on device " + std::to_string(attr.device) +
+                                  ", the context renders on device " + std::to_string(c.device));
     cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
     unsigned char* base = staticScratchOf(c.device);
 
     StaticSwap keep(c);
-  c.accumC = nullptr;   // the static render keeps no checkpoint or variance of its own
-  c.accum2 = nullptr;
-  c.accumCount = 0;
+    c.accumC = nullptr;  // the static render keeps no checkpoint or variance of its own
+    c.accum2 = nullptr;
+    c.accumCount = 0;
     PathState s;
     s.capacity = kStaticPaths;
     float4* planes[kStaticPathPlanes];
@@ -1551,6 +1633,7 @@ int prt_cuda_render_static(prt_context* ctx, uint32_t first_sample, int32_t spp,
     s.queue[1] = reinterpret_cast<int*>(base + kStaticOffQueues + kStaticQueue);
     s.classQueues = reinterpret_cast<int*>(base + kStaticOffQueues + 2 * kStaticQueue);
     s.counters = reinterpret_cast<int*>(base + kStaticOffCounters);
+    s.octBins = s.counters + 16 * (c.renderer.maxDepth + 2);
     s.travCounts = reinterpret_cast<unsigned long long*>(base + kStaticOffTrav);
     s.err = reinterpret_cast<uint32_t*>(base + kStaticOffErr);
     c.ps = s;

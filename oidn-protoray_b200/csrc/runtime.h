@@ -113,6 +113,10 @@ struct Context
   std::string lastError;
   int smCount = 0;
   std::vector<DevBuf> sceneBufs;  // freed on re-upload
+  std::vector<DevBuf> envBufs;    // environment lights and the light CDF, replaced by prt_cuda_scene_lights
+  std::vector<float> areaLightPowerHost;  // area-light powers, the head of the light CDF
+  float sceneRadius = 0.f;        // half the diagonal of the scene bounds (render/scene.cpp:367)
+  float boundsLo[3] = {0.f, 0.f, 0.f}, boundsHi[3] = {0.f, 0.f, 0.f};
   DevScene scene{};
   bool hasScene = false;
   Bvh8 bvh;                       // host copy of a host-built tree
@@ -149,6 +153,10 @@ struct Context
   int64_t wavePaths = 128ll << 20;
   int topStage = 0;               // stage the top BVH levels in shared memory (frame form)
   int rayBins = 0;                // group each bounce's extended rays by direction octant (frame form)
+  // Device buffers that stage host memory passed to an entry point (one per buffer argument of
+  // a call, reused by later calls and grown when a call needs more; freed with the context).
+  std::vector<DevBuf> stage;
+  int stageNext = 0;              // slots in use by the current call
 };
 
 // Per-call statistics gathered by renderSamples.

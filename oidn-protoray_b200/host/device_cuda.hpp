@@ -6,8 +6,8 @@
 // size not divisible by the 32x8 tile, render/path_renderer_stream.h:109-112), and
 // std::runtime_error for CUDA, memory, state and device-abort failures.
 //
-// Header-only; link with libprt_cuda.so. INTEGRATION.md shows the adapter that derives the
-// reference's prt::Device from this class so that `-dev cuda` selects it.
+// Header-only; link with libprt_cuda.so. A reference-side adapter derives the reference's
+// prt::Device and forwards each virtual to the same entry points, so that `-dev cuda` selects it.
 #pragma once
 
 #include <cstdint>

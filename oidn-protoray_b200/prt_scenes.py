@@ -11,6 +11,12 @@ deterministically from a seed, with the shapes and value distributions of each w
   2.6M triangles, four material kinds and a sun-sky light, 1920x1080, 64 spp, depth 8,
   Russian roulette from depth 3.
 
+A sun-sky light is described by the reference's parameters (Scene.sunsky: direction,
+turbidity, ground albedo). The device takes its two products, the sun as a distant light and the
+sky as an image light (what the reference's SunSkyLight computes from the parameters); the
+caller supplies them with Scene.set_sunsky_products, or once per parameter set with
+register_sunsky_products, after which every generated scene with those parameters gets them.
+
 A Scene keeps every numpy array alive for as long as its ctypes descriptor is in use.
 """
 import ctypes as C
@@ -32,6 +38,7 @@ class Scene:
         self.env = T.EnvDesc()
         self.env_image = None
         self.sunsky = None    # (dir xyz, turbidity, albedo) for the reference's SunSkyLight
+        self.sunsky_applied = False
         self.camera = None
         self.width = 0
         self.height = 0
@@ -65,6 +72,17 @@ class Scene:
         self.env.image_height = self.env_image.shape[0]
         self.env.image_lut_size = lut_size
 
+    def set_sunsky_products(self, sun_color, sun_angle, sky):
+        """The sun-sky light's products as environment lights: the sun (radiance, angular
+        diameter) as the distant light toward sunsky[0:3], the sky (equirectangular RGB, top row
+        first) as the image light with the reference's 128-entry LUT."""
+        d = self.sunsky[0:3]
+        self.env.distant_color[:] = tuple(float(c) for c in sun_color)
+        self.env.distant_dir[:] = tuple(float(c) for c in d)
+        self.env.distant_angle = float(sun_angle)
+        self.set_env_image(sky, lut_size=128)
+        self.sunsky_applied = True
+
     @property
     def tri_count(self):
         return sum(m["indices"].shape[0] for m in self.meshes)
@@ -97,9 +115,13 @@ class Scene:
         d.bvh_build = getattr(self, "bvh_build", T.PRT_BVH_HOST)
         d.env = self.env
         d.env.image_rgb = T.fptr(self.env_image)
-        if oracle and self.sunsky is not None:
-            d.env.distant_color[:] = (0.0, 0.0, 0.0)
-            d.env.image_rgb = None
+        if self.sunsky is not None:
+            if oracle:
+                d.env.distant_color[:] = (0.0, 0.0, 0.0)
+                d.env.image_rgb = None
+            elif not self.sunsky_applied:
+                raise ValueError("the scene has a sun-sky light but no sun-sky products: call set_sunsky_products "
+                                 "or register_sunsky_products for its parameters")
         self._keep = [meshes, mats, texs]
         return d
 
@@ -381,7 +403,6 @@ def lit_plane(albedo=(0.5, 0.5, 0.5), width=128, height=128, spp=64, sun_elevati
 
 # ---- large plain-render scene: fBm terrain + icospheres under a sun-sky ----------------------
 
-SUNSKY_FIXTURE = pathlib.Path(__file__).resolve().parent.parent / "tests" / "golden" / "sunsky_t3_e30.npz"
 SUN_ELEVATION_DEG = 30.0
 SUN_AZIMUTH_DEG = 45.0
 SUN_TURBIDITY = 3.0
@@ -416,17 +437,32 @@ def value_noise_fbm(x, z, rng_seed, octaves=8, lacunarity=2.0, gain=0.5, base_fr
     return total
 
 
-def load_sunsky():
-    """Sun (radiance, angular diameter) and sky image of the reference's sun-sky model for the
-    terrain's sun, produced by the oracle (tests/golden/make_golden.py)."""
-    z = np.load(SUNSKY_FIXTURE)
-    return z["sun_color"], float(z["sun_angle"]), z["sky"]
+_SUNSKY_PRODUCTS = {}
+
+
+def _sunsky_key(params):
+    return tuple(np.asarray(params, np.float32).tolist())
+
+
+def register_sunsky_products(params, sun_color, sun_angle, sky):
+    """Products of the reference's SunSkyLight for `params` = (direction xyz, turbidity, ground
+    albedo): every scene generated afterwards with those parameters gets them."""
+    _SUNSKY_PRODUCTS[_sunsky_key(params)] = (np.asarray(sun_color, np.float32), float(sun_angle),
+                                             np.ascontiguousarray(sky, np.float32))
+
+
+def sunsky_params(elevation_deg=SUN_ELEVATION_DEG, azimuth_deg=SUN_AZIMUTH_DEG, turbidity=SUN_TURBIDITY,
+                  albedo=SUN_GROUND_ALBEDO):
+    d = sun_direction(elevation_deg, azimuth_deg)
+    return np.array([d[0], d[1], d[2], turbidity, albedo], np.float32)
 
 
 def terrain(seed=0, grid=1024, n_spheres=400, sphere_subdiv=3, width=1920, height=1080, spp=64, max_depth=8,
-            rr_depth=3, extent=50.0, relief=10.0, with_sky=True):
+            rr_depth=3, extent=50.0, relief=10.0, sun_elevation_deg=SUN_ELEVATION_DEG, turbidity=SUN_TURBIDITY):
     """The large plain-render scene: grid^2 fBm heightfield (2 (grid-1)^2 triangles) plus
-    n_spheres icospheres; spheres get one of four materials uniformly at random."""
+    n_spheres icospheres; spheres get one of four materials uniformly at random. Lit by a sun-sky
+    light (sun at sun_elevation_deg, azimuth 45 degrees, ground albedo 0.2) whose products are
+    applied when they were registered for those parameters."""
     rng = np.random.default_rng(seed)
     s = Scene()
     # Heightfield over [-extent, extent]^2 in xz, UVs = grid coordinates in [0, 1].
@@ -480,14 +516,10 @@ def terrain(seed=0, grid=1024, n_spheres=400, sphere_subdiv=3, width=1920, heigh
         s.add_mesh(sv * r + np.array([cx, hy + r * 0.9, cz]), sf, mid, normals=sv)
     # Sun-sky light: the reference computes it from (direction, turbidity, albedo); the device
     # takes its two products, the sun as a distant light and the sky as an image light.
-    d = sun_direction()
-    s.sunsky = np.array([d[0], d[1], d[2], SUN_TURBIDITY, SUN_GROUND_ALBEDO], np.float32)
-    if with_sky:
-        sun_color, sun_angle, sky = load_sunsky()
-        s.env.distant_color[:] = tuple(float(c) for c in sun_color)
-        s.env.distant_dir[:] = tuple(float(c) for c in d)
-        s.env.distant_angle = sun_angle
-        s.set_env_image(sky, lut_size=128)
+    s.sunsky = sunsky_params(sun_elevation_deg, SUN_AZIMUTH_DEG, turbidity, SUN_GROUND_ALBEDO)
+    products = _SUNSKY_PRODUCTS.get(_sunsky_key(s.sunsky))
+    if products is not None:
+        s.set_sunsky_products(*products)
     s.camera = look_at((0.0, 0.56 * extent, 1.24 * extent), (0.0, 0.0, -0.1 * extent), fov_deg=45.0)
     s.width, s.height, s.spp, s.max_depth, s.rr_depth = width, height, spp, max_depth, rr_depth
     return s

@@ -19,6 +19,7 @@ PRT_ERR_STATE = -6
 PRT_AOV_ALBEDO1 = 1 << 0
 PRT_AOV_NORMAL1 = 1 << 1
 PRT_AOV_HDR_VAR = 1 << 2
+PRT_ENV_AMBIENT_FIRST = 1
 
 PRT_BLIT_HDR = 0
 PRT_BLIT_ALBEDO1 = 1
@@ -164,7 +165,7 @@ class EnvDesc(C.Structure):
         ("image_width", C.c_int32),
         ("image_height", C.c_int32),
         ("image_lut_size", C.c_int32),
-        ("reserved", C.c_int32),
+        ("flags", C.c_int32),
     ]
 
 
@@ -194,6 +195,8 @@ class SceneStats(C.Structure):
         ("depth", C.c_int32),
         ("top_count", C.c_int32),
         ("iterations", C.c_int32),
+        ("bounds_lo", F3),
+        ("bounds_hi", F3),
     ]
 
 

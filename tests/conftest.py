@@ -19,6 +19,17 @@ for p in (PKG, ROOT / "oracle", ROOT):
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+    register_sunsky_fixtures()
+
+
+def register_sunsky_fixtures():
+    """The reference's sun-sky products for the sun-sky parameters the tests use (fixtures made
+    by golden/make_golden.py from the reference's SunSkyLight), handed to the scene generators."""
+    import prt_scenes
+
+    for path in sorted(GOLDEN.glob("sunsky_*.npz")):
+        z = np.load(path)
+        prt_scenes.register_sunsky_products(z["params"], z["sun_color"], float(z["sun_angle"]), z["sky"])
 
 
 @pytest.fixture(scope="session")

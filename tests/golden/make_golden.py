@@ -26,8 +26,12 @@ Fixtures (small, seeded, committed):
   film.npz         sample variance, tone-mapped LDR images and frame errors of the small scene
   bsdf.npz         the reference's Standard-material BSDF (eval, sample) on 512 seeded tuples
                    for each case of tests/bsdf_cases.py
-  sunsky_t3_e30.npz the reference's sun-sky products (sun radiance and angle, 512x256 sky) for
-                   the terrain scene's sun (elevation 30 deg, turbidity 3, ground albedo 0.2)
+  aov_img.npz      first-hit albedo1 and normal1 AOVs with the HDR image: the small scene and the
+                   small terrain, 16 spp, seeds 0 and 1
+  sunsky_t3_e30.npz, sunsky_t5_e60.npz  the reference's sun-sky products (sun radiance and angle,
+                   512x256 sky) for the terrain scene's sun (elevation 30 deg, turbidity 3, ground
+                   albedo 0.2) and for a second sun (elevation 60 deg, turbidity 5)
+  terrain_e60_img.npz the small terrain under the second sun, 16 spp, seeds 0 and 1
 """
 import pathlib
 import sys
@@ -208,8 +212,7 @@ def make_bsdf():
 
 
 def small_terrain(spp):
-    return prt_scenes.terrain(seed=1, grid=96, n_spheres=24, width=128, height=64, spp=spp, extent=12.0, relief=3.0,
-                              with_sky=False)
+    return prt_scenes.terrain(seed=1, grid=96, n_spheres=24, width=128, height=64, spp=spp, extent=12.0, relief=3.0)
 
 
 def make_terrain_images():
@@ -224,16 +227,58 @@ def make_terrain_images():
     np.savez_compressed(OUT / "terrain_img.npz", **out)
 
 
+def make_aovs():
+    """First-hit AOVs (albedo1, normal1) as DeviceCpu::blitFrame writes them, with the HDR image,
+    for the small scene (128x128) and the small terrain (128x64, sun-sky), 16 spp, seeds 0 and 1."""
+    out = {}
+    mask = T.PRT_AOV_ALBEDO1 | T.PRT_AOV_NORMAL1
+    for name, scene in (("cornell", small_scene(128, 128, 16)), ("terrain", small_terrain(16))):
+        for seed in (0, 1):
+            dev = ref.RefDevice(scene, seed=seed, aov_mask=mask)
+            st = dev.render(16)
+            out[f"{name}_seed{seed}_hdr"] = dev.blit(T.PRT_BLIT_HDR)
+            out[f"{name}_seed{seed}_albedo1"] = dev.blit(T.PRT_BLIT_ALBEDO1)
+            out[f"{name}_seed{seed}_normal1"] = dev.blit(T.PRT_BLIT_NORMAL1)
+            out[f"{name}_seed{seed}_rays"] = np.float64(st["rays"])
+            dev.close()
+    np.savez_compressed(OUT / "aov_img.npz", **out)
+
+
+# (sun elevation in degrees, turbidity) of the sun-sky fixtures: the terrain workload's, and a
+# second sun for the boundary tests.
+SUNSKY_SETS = [(30.0, 3.0), (60.0, 5.0)]
+
+
 def make_sunsky():
-    d = prt_scenes.sun_direction()
-    sun, angle, sky = ref.sunsky(d, prt_scenes.SUN_TURBIDITY, prt_scenes.SUN_GROUND_ALBEDO)
-    np.savez_compressed(prt_scenes.SUNSKY_FIXTURE, sun_color=sun, sun_angle=np.float32(angle), sky=sky,
-                        direction=d)
+    for elevation, turbidity in SUNSKY_SETS:
+        params = prt_scenes.sunsky_params(elevation, turbidity=turbidity)
+        sun, angle, sky = ref.sunsky(params[0:3], float(params[3]), float(params[4]))
+        np.savez_compressed(OUT / f"sunsky_t{turbidity:g}_e{elevation:g}.npz", params=params, sun_color=sun,
+                            sun_angle=np.float32(angle), sky=sky, direction=params[0:3])
+
+
+def make_terrain_e60_images():
+    """The small terrain under the second sun (elevation 60 degrees, turbidity 5), 16 spp, seeds 0
+    and 1: the reference builds its SunSkyLight from the parameters itself."""
+    out = {}
+    for seed in (0, 1):
+        s = prt_scenes.terrain(seed=1, grid=96, n_spheres=24, width=128, height=64, spp=16, extent=12.0, relief=3.0,
+                               sun_elevation_deg=60.0, turbidity=5.0)
+        dev = ref.RefDevice(s, seed=seed)
+        st = dev.render(16)
+        out[f"spp16_seed{seed}"] = dev.blit()
+        out[f"spp16_seed{seed}_rays"] = np.float64(st["rays"])
+        dev.close()
+    np.savez_compressed(OUT / "terrain_e60_img.npz", **out)
 
 
 if __name__ == "__main__":
     which = sys.argv[1:] or ["sobol", "rays", "images", "sunsky", "bsdf", "terrain", "lobes", "translucent", "siblings",
-                             "film", "mesh"]
+                             "film", "mesh", "aovs", "terrain_e60"]
+    if "terrain_e60" in which:
+        make_terrain_e60_images()
+    if "aovs" in which:
+        make_aovs()
     if "terrain" in which:
         make_terrain_images()
     if "bsdf" in which:

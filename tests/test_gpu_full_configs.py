@@ -1,0 +1,83 @@
+"""Parity at the full sizes of the two plain-render workloads.
+
+* Closest hits and occlusion on the full terrain scene (2.6M triangles), on the oracle's own
+  rays, bit for bit: primary rays, bounce rays from the primary hits, random rays, shadow rays,
+  and rays through shared vertices and edges of the terrain grid, where several triangles are hit
+  at the same point and the tie rule decides (the fixture counts those rays). Both BVH builders.
+* The converged-image gate: the small scene at its full size (256x256, depth 5) at 4096 spp,
+  the GPU's relMSE against the reference's seed-0 image within 1.5x the reference's own
+  seed-0/seed-1 relMSE; the same seed far closer than that.
+
+relMSE is the mean over pixels and channels of (x - ref)^2 / (ref^2 + 1e-2).
+"""
+import numpy as np
+import pytest
+
+import prt_scenes
+import prt_types as T
+from conftest import rel_mse
+
+pytestmark = pytest.mark.gpu
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+@pytest.fixture(scope="module", params=[T.PRT_BVH_HOST, T.PRT_BVH_DEVICE], ids=["host_bvh", "device_bvh"])
+def terrain_device(request, device):
+    s = prt_scenes.terrain(seed=0, spp=1)
+    s.bvh_build = request.param
+    device.setup(s, seed=0)
+    return device
+
+
+def check_hits(device, z, key):
+    g, p, t, u, v = device.trace(z[f"{key}_rays"])
+    assert np.array_equal(g, z[f"{key}_geom"]), f"{key}: {(g != z[f'{key}_geom']).sum()} geometry IDs differ"
+    assert np.array_equal(p, z[f"{key}_prim"]), f"{key}: {(p != z[f'{key}_prim']).sum()} primitive IDs differ"
+    hit = g >= 0
+    assert np.array_equal(bits(t[hit]), bits(z[f"{key}_t"][hit])), key
+    assert np.array_equal(bits(u[hit]), bits(z[f"{key}_u"][hit])), key
+    assert np.array_equal(bits(v[hit]), bits(z[f"{key}_v"][hit])), key
+    return int(hit.sum())
+
+
+def test_terrain_hits_bit_exact_on_oracle_rays(terrain_device, golden):
+    z = golden("terrain_rays.npz")
+    hits = {key: check_hits(terrain_device, z, key) for key in ("primary", "bounce", "random")}
+    assert min(hits.values()) > 1000, hits
+    occ = terrain_device.occluded(z["shadow_rays"])
+    assert np.array_equal(occ, z["shadow_occ"]), f"{(occ != z['shadow_occ']).sum()} occlusion results differ"
+
+
+def test_terrain_tie_hits_bit_exact(terrain_device, golden):
+    """Rays through grid vertices (six triangles meet) and cell diagonals (two): the closest hit
+    among triangles hit at the same point follows the reference's tie rule on every ray."""
+    z = golden("terrain_ties.npz")
+    for key in ("vertex", "diagonal", "oblique"):
+        check_hits(terrain_device, z, key)
+        g, p = z[f"{key}_geom"], z[f"{key}_prim"]
+        ties = int(np.sum((g == 0) & np.any(p[:, None] == z[f"{key}_incident"], 1)))
+        assert ties == int(z[f"{key}_ties"]) and ties > 2000, (key, ties)
+
+
+def render(device, scene, seed, spp):
+    device.setup(scene, seed=seed)
+    device.clear_frame()
+    st = device.render(spp)
+    return device.blit_frame(), st
+
+
+def test_cornell_full_size_converged_gate(device, golden):
+    """256x256, depth 5, 4096 spp: the workload's own frame at the north star's sample count."""
+    z = golden("cornell_full.npz")
+    spp = int(z["spp"])
+    seeds = rel_mse(z["seed1"], z["seed0"])
+    scene = prt_scenes.cornell(seed=0, width=256, height=256, spp=spp)
+    same, st = render(device, scene, seed=0, spp=spp)
+    assert np.isfinite(same).all()
+    assert rel_mse(same, z["seed0"]) < 0.2 * seeds, (rel_mse(same, z["seed0"]), seeds)
+    assert abs(st["rays"] / float(z["seed0_rays"]) - 1.0) < 0.002
+    other, _ = render(device, scene, seed=2, spp=spp)
+    assert rel_mse(other, z["seed0"]) <= 1.5 * seeds, (rel_mse(other, z["seed0"]), seeds)

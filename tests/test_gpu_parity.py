@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 import prt_scenes
+import prt_types as T
 from conftest import rel_mse
 
 pytestmark = pytest.mark.gpu
@@ -177,3 +178,45 @@ def test_sibling_renderers_match_oracle(device, golden, kind):
     assert diff.mean() < 2e-3, diff.mean()
     assert np.mean(diff > 1e-3) < 0.01, np.mean(diff > 1e-3)
     assert abs(st["rays"] / float(z[f"type{kind}_rays"]) - 1.0) < 1e-3
+
+
+def aov_scenes():
+    return {"cornell": small_scene(128, 128, 16), "terrain": small_terrain(16)}
+
+
+@pytest.mark.parametrize("name", ["cornell", "terrain"])
+def test_first_hit_aovs_match_oracle(device, golden, name):
+    """albedo1 and normal1 as DeviceCpu::blitFrame writes them (render/device_cpu.cpp:189-205,
+    render/path_renderer_stream.h:346-414,483-581,732-874): same seed, so the same pixel
+    samples and first hits; the AOVs agree to rounding except at the rare pixel whose first hit
+    is a near tie. The HDR image of the same render tracks the reference's as in the image tests."""
+    z = golden("aov_img.npz")
+    scene = aov_scenes()[name]
+    device.setup(scene, seed=0, aov_mask=T.PRT_AOV_ALBEDO1 | T.PRT_AOV_NORMAL1)
+    device.clear_frame()
+    st = device.render(16)
+    for aov, blit in (("albedo1", T.PRT_BLIT_ALBEDO1), ("normal1", T.PRT_BLIT_NORMAL1)):
+        img = device.blit_frame(blit)
+        ref = z[f"{name}_seed0_{aov}"]
+        assert np.isfinite(img).all()
+        diff = np.abs(img.astype(np.float64) - ref)
+        assert diff.mean() < 1e-4, (aov, diff.mean())
+        assert np.mean(diff > 1e-3) < 0.002, (aov, np.mean(diff > 1e-3))
+        # The other seed's AOVs differ far more (different pixel samples), so the bar is sharp.
+        assert np.abs(z[f"{name}_seed1_{aov}"].astype(np.float64) - ref).mean() > 20 * diff.mean()
+    hdr = device.blit_frame()
+    assert rel_mse(hdr, z[f"{name}_seed0_hdr"]) < 0.5 * rel_mse(z[f"{name}_seed1_hdr"], z[f"{name}_seed0_hdr"])
+    assert abs(st["rays"] / float(z[f"{name}_seed0_rays"]) - 1.0) < 0.02
+
+
+def test_terrain_second_sun_same_seed_tracks_oracle(device, golden):
+    """A second sun (elevation 60 degrees, turbidity 5): the reference builds its SunSkyLight from
+    the parameters; the device takes the products of that light (registered from the fixture)."""
+    z = golden("terrain_e60_img.npz")
+    s = prt_scenes.terrain(seed=1, grid=96, n_spheres=24, width=128, height=64, spp=16, extent=12.0, relief=3.0,
+                           sun_elevation_deg=60.0, turbidity=5.0)
+    img, st = render(device, s, seed=0, spp=16)
+    same = rel_mse(img, z["spp16_seed0"])
+    other = rel_mse(z["spp16_seed1"], z["spp16_seed0"])
+    assert same < 0.5 * other, (same, other)
+    assert abs(st["rays"] / float(z["spp16_seed0_rays"]) - 1.0) < 0.02

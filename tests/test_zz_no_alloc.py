@@ -85,6 +85,65 @@ def test_static_render_matches_allocating_render_on_two_calls(ctx):
     assert np.array_equal(dev.blit_frame(), second)
 
 
+def test_static_render_allocates_nothing_on_a_fresh_context():
+    """A context that has never rendered through the allocating path: after one warm-up call
+    (which loads the library's kernels and looks up the scratch area's address), further calls
+    leave the device's free memory exactly as it was, and give the allocating path's images."""
+    torch = pytest.importorskip("torch")
+    dev = prt_cuda.DeviceCuda(0)
+    try:
+        scene = prt_scenes.cornell(seed=0)
+        scene.width, scene.height, scene.spp = W, H, SPP
+        dev.setup(scene, seed=5)
+        fn = bind(dev.lib)
+        outs = [torch.full((H, W, 3), float("nan"), dtype=torch.float32, device="cuda") for _ in range(3)]
+        torch.cuda.synchronize()
+
+        def call(k, first):
+            rc = fn(dev.h, first, SPP, C.c_void_p(outs[k].data_ptr()))
+            assert rc == T.PRT_OK, dev.lib.prt_cuda_last_error(dev.h)
+
+        call(0, 0)  # warm-up
+        free_before, _ = torch.cuda.mem_get_info()
+        call(1, 0)
+        call(2, SPP)
+        torch.cuda.synchronize()
+        free_after, _ = torch.cuda.mem_get_info()
+        assert free_after == free_before, (free_before, free_after)
+
+        warm, a, b = (o.cpu().numpy() for o in outs)
+        assert np.isfinite(a).all() and a.mean() > 0
+        assert rel_diff(warm, a) <= 1e-6
+        # The allocating path on the same context afterwards: samples 0..7, then 8..15.
+        dev.clear_frame()
+        dev.render(SPP)
+        assert rel_diff(a, dev.blit_frame()) <= 1e-6
+        dev.clear_frame()
+        dev.render(SPP)
+        assert rel_diff(b, dev.blit_frame()) <= 1e-6
+    finally:
+        dev.close()
+
+
+def test_static_render_rejects_another_devices_memory():
+    """The output must live on the context's own device."""
+    torch = pytest.importorskip("torch")
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs a second GPU to hold the output")
+    dev = prt_cuda.DeviceCuda(0)
+    try:
+        scene = prt_scenes.cornell(seed=0)
+        scene.width, scene.height, scene.spp = W, H, SPP
+        dev.setup(scene, seed=0)
+        fn = bind(dev.lib)
+        other = torch.zeros((H, W, 3), dtype=torch.float32, device="cuda:1")
+        rc = fn(dev.h, 0, 1, C.c_void_p(other.data_ptr()))
+        assert rc == T.PRT_ERR_INVALID_ARG
+        assert b"device 1" in dev.lib.prt_cuda_last_error(dev.h)
+    finally:
+        dev.close()
+
+
 def test_static_render_rejects_frames_beyond_the_scratch_limit(ctx):
     dev, fn, torch = ctx
     big = prt_scenes.cornell(seed=0)
