@@ -279,9 +279,11 @@ public:
     camera = std::make_shared<PinholeCamera>(props);
     const Basis3f b = props.get<Basis3f>("basis");
     const Vec3f p = props.get<Vec3f>("position");
-    const prt_camera_desc c{{p.x, p.y, p.z},       {b.U.x, b.U.y, b.U.z}, {b.V.x, b.V.y, b.V.z},
-                            {b.N.x, b.N.y, b.N.z}, props.get<float>("fov"), props.get<float>("nearClip")};
-    check(prt_cuda_camera(ctx, &c));
+    cameraDesc = prt_camera_desc{{p.x, p.y, p.z},       {b.U.x, b.U.y, b.U.z}, {b.V.x, b.V.y, b.V.z},
+                                 {b.N.x, b.N.y, b.N.z}, props.get<float>("fov"), props.get<float>("nearClip")};
+    // The reference's camera carries its own raster size, so initCamera may come before
+    // initFrame; the device's camera takes the frame's aspect, so it is set once a frame exists.
+    if (size.x > 0) check(prt_cuda_camera(ctx, &cameraDesc));
   }
 
   void initCamera(const Props& props, const Props&, const Props&) override { initCamera(props); }
@@ -310,6 +312,7 @@ public:
     check(prt_cuda_frame(ctx, s.x, s.y, aov));
     size = s;
     aovMask = aov;
+    if (camera) check(prt_cuda_camera(ctx, &cameraDesc));
   }
 
   void initFilter(const Props& props) override
@@ -399,6 +402,7 @@ private:
   Vec2i size = Vec2i(0);
   int aovMask = 0;
   std::shared_ptr<PinholeCamera> camera;
+  prt_camera_desc cameraDesc{};
 };
 
 } // namespace prt

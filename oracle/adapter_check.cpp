@@ -125,6 +125,11 @@ int adapter_render(const char* scene_path, const char* light_props, const float*
   return guard([&] {
     DeviceCuda device(0);
     device.initScene(scene_path, parseProps(light_props));
+    // The reference application's order: frame, then camera (main/render/render_window.cpp:317,745).
+    Props frame;
+    if (aov_mask & PRT_AOV_ALBEDO1) frame.set("aovAlbedo1");
+    if (aov_mask & PRT_AOV_NORMAL1) frame.set("aovNormal1");
+    device.initFrame(Vec2i(width, height), frame);
     Props cam;
     cam.set("type", "pinhole");
     cam.set("position", Vec3f(camera[0], camera[1], camera[2]));
@@ -135,10 +140,6 @@ int adapter_render(const char* scene_path, const char* light_props, const float*
     cam.set("width", width);
     cam.set("height", height);
     device.initCamera(cam);
-    Props frame;
-    if (aov_mask & PRT_AOV_ALBEDO1) frame.set("aovAlbedo1");
-    if (aov_mask & PRT_AOV_NORMAL1) frame.set("aovNormal1");
-    device.initFrame(Vec2i(width, height), frame);
     Props filter;
     filter.set("filter", "box");
     device.initFilter(filter);

@@ -36,7 +36,7 @@ import ref  # noqa: E402
 
 OUT = pathlib.Path(__file__).resolve().parent
 SPP_CORNELL = 4096
-SPP_TERRAIN = 4096
+SPP_TERRAIN = 1024
 CHUNK = 256
 
 
