@@ -536,6 +536,18 @@ int prt_cuda_query_primary(prt_context* ctx, uint32_t sample_index, float* rays_
 int prt_cuda_bsdf_query(prt_context* ctx, const prt_material* material, int32_t medium_id, int64_t n,
                         const float* tuples, float* out);
 
+/* Microfacet-distribution sampling on the device for n tuples of (alpha, s.x, s.y, wo.x, wo.y,
+ * wo.z) (6 floats each, canonical frame N = z); out gets (m.x, m.y, m.z, pdf) per tuple.
+ *   PRT_MICROFACET_BECKMANN:     BeckmannDistribution::sample (bsdf/beckmann_distribution.h:21-42),
+ *                                the distribution of the reference's CarPaint flakes
+ *                                (material/flakes.h:59); wo is unused.
+ *   PRT_MICROFACET_GGX_VISIBLE:  GGXDistribution::sampleVisible (bsdf/ggx_distribution.h:52-82),
+ *                                isotropic alpha, visible normals of wo.
+ * Used for sampler parity. */
+#define PRT_MICROFACET_BECKMANN    1
+#define PRT_MICROFACET_GGX_VISIBLE 2
+int prt_cuda_microfacet_query(prt_context* ctx, int32_t distribution, int64_t n, const float* in, float* out);
+
 /* Copies the BSDF energy-compensation tables the context computed at creation (the
  * reference's precomputeAlbedoTables, bsdf/albedo_tables.cpp:173-188) to out, concatenated in
  * the order GGX dir (32x32), GGX avg (32), dielectric eta dir (16^3), eta avg (16^2), dielectric

@@ -195,6 +195,27 @@ struct GGX
   }
 };
 
+// ---- Beckmann distribution (bsdf/beckmann_distribution.h:14-43) -------------------------------
+// Samples a microfacet normal m with density D(m) cos(theta_m) (Walter et al. 2007, eqs. 28-29):
+// tan^2(theta) = -alpha^2 log(1 - s.x), phi = 2 pi s.y, pdf = (1 - s.x) / (pi alpha^2 cos^3(theta)).
+// The reference uses it for the flakes of its CarPaint material.
+struct Beckmann
+{
+  float alpha;
+
+  PRT_D f3 sample(float& pdf, float sx, float sy) const
+  {
+    const float a2 = alpha * alpha;
+    const float tanTheta2 = -a2 * logf(1.f - sx);
+    const float cosTheta = 1.f / sqrtf(1.f + tanTheta2);
+    const float sinTheta = sqrtf(fmaxf(1.f - cosTheta * cosTheta, 0.f));
+    float sinPhi, cosPhi;
+    sincospif(2.f * sy, &sinPhi, &cosPhi);
+    pdf = (1.f - sx) / (kPi * a2 * (cosTheta * cosTheta * cosTheta));
+    return mk(cosPhi * sinTheta, sinPhi * sinTheta, cosTheta);
+  }
+};
+
 // ---- Fresnel (bsdf/optics.h) -------------------------------------------------------------------
 PRT_D float fresnelDielectric(float cosI, float cosT, float eta)
 {

@@ -1374,6 +1374,22 @@ int prt_cuda_bsdf_query(prt_context* ctx, const prt_material* material, int32_t 
   });
 }
 
+int prt_cuda_microfacet_query(prt_context* ctx, int32_t distribution, int64_t n, const float* in, float* out)
+{
+  return guarded(ctx, [&](Context& c) {
+    if (distribution != PRT_MICROFACET_BECKMANN && distribution != PRT_MICROFACET_GGX_VISIBLE)
+      throw std::invalid_argument("unknown microfacet distribution");
+    if (n < 0 || (n > 0 && (!in || !out))) throw std::invalid_argument("invalid microfacet query");
+    if (n == 0) return;
+    cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+    Staged i(c, in, (size_t)n * 6 * sizeof(float), true);
+    Staged o(c, out, (size_t)n * 4 * sizeof(float), false);
+    cuCheck(launchMicrofacetQuery(c, distribution, n, (const float*)i.dev, (float*)o.dev), "microfacet query");
+    o.copyOut();
+    cuCheck(cudaStreamSynchronize(c.stream), "microfacet sync");
+  });
+}
+
 int prt_cuda_albedo_tables(prt_context* ctx, float* out, int64_t capacity, int64_t* count)
 {
   return guarded(ctx, [&](Context& c) {

@@ -123,6 +123,27 @@ __global__ void kPrimary(DevScene sc, DevCamera cam, int width, int height, uint
   }
 }
 
+// Microfacet-distribution sampling queries (see prt_cuda_microfacet_query): per tuple (alpha,
+// s.x, s.y, wo.x, wo.y, wo.z) -> (m.x, m.y, m.z, pdf).
+__global__ void kMicrofacetQuery(int distribution, int64_t n, const float* __restrict__ in, float* __restrict__ out)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+  {
+    const float* t = in + 6 * i;
+    float pdf = 0.f;
+    f3 m;
+    if (distribution == PRT_MICROFACET_BECKMANN)
+      m = Beckmann{t[0]}.sample(pdf, t[1], t[2]);
+    else
+      m = GGX{t[0], t[0]}.sampleVisible(mk(t[3], t[4], t[5]), pdf, t[1], t[2]);
+    float* o = out + 4 * i;
+    o[0] = m.x;
+    o[1] = m.y;
+    o[2] = m.z;
+    o[3] = pdf;
+  }
+}
+
 // BSDF parity queries in a canonical shading context (see prt_cuda_bsdf_query).
 __global__ void kBsdfQuery(DevTables tab, DevMaterial m, int mediumId, int64_t n, const float* __restrict__ tuples,
                            float* __restrict__ out)
@@ -1186,6 +1207,12 @@ cudaError_t launchPrimary(Context& ctx, uint32_t sampleIndex, float* raysOut, in
   kPrimary<<<gridFor(ctx, n, 128), 128, 0, ctx.stream>>>(ctx.scene, ctx.camera, ctx.width, ctx.height,
                                                           ctx.renderer.seed, sampleIndex,
                                                           reinterpret_cast<float4*>(raysOut), triOut, t, ctx.ps.err);
+  return cudaGetLastError();
+}
+
+cudaError_t launchMicrofacetQuery(Context& ctx, int distribution, int64_t n, const float* in, float* out)
+{
+  kMicrofacetQuery<<<gridFor(ctx, n, 128), 128, 0, ctx.stream>>>(distribution, n, in, out);
   return cudaGetLastError();
 }
 

@@ -199,6 +199,7 @@ cudaError_t launchAdjoint(Context& ctx, uint32_t firstSample, int spp, const flo
 cudaError_t launchTextureUpdate(Context& ctx, const DevTexture& t, const float* rgb);
 cudaError_t launchClear(Context& ctx);
 cudaError_t launchBsdfQuery(Context& ctx, const DevMaterial& m, int mediumId, int64_t n, const float* tuples, float* out);
+cudaError_t launchMicrofacetQuery(Context& ctx, int distribution, int64_t n, const float* in, float* out);
 // Builds the BSDF energy-compensation tables on the current device (albedo.cu).
 cudaError_t buildAlbedoTables(DevTables& t, float** storage);
 

@@ -61,7 +61,8 @@ PRT_D bool intersectTriFx(const float4* __restrict__ tris, uint32_t idx, f3 o, f
 struct RayPre
 {
   f3 o, invd;
-  uint32_t oct;   // bit k set when direction component k is negative
+  uint32_t oct;             // bit k set when direction component k is negative
+  uint32_t permLo, permHi;  // byte_perm selectors: byte s of an 8-byte child row -> position s ^ oct
 };
 
 PRT_D RayPre rayPre(f3 o, f3 d)
@@ -74,6 +75,16 @@ PRT_D RayPre rayPre(f3 o, f3 d)
   const float dz = fabsf(d.z) < tiny ? copysignf(tiny, d.z) : d.z;
   r.invd = mk(__frcp_rn(dx), __frcp_rn(dy), __frcp_rn(dz));
   r.oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+  // Output byte j of a permuted row is source byte j ^ oct (bytes 0-3 from the row's low word,
+  // 4-7 from its high word): nibble j of the selectors.
+  r.permLo = 0u;
+  r.permHi = 0u;
+#pragma unroll
+  for (uint32_t j = 0; j < 4; ++j)
+  {
+    r.permLo |= (j ^ r.oct) << (4 * j);
+    r.permHi |= ((j + 4) ^ r.oct) << (4 * j);
+  }
   return r;
 }
 
@@ -82,12 +93,34 @@ PRT_D uint32_t byteOf(uint2 w, int i)
   return (i < 4 ? (w.x >> (8 * i)) : (w.y >> (8 * (i - 4)))) & 0xffu;
 }
 
-// Intersects the 8 children of one node; returns the node group of hit inner children
-// (bits 24-31: hit flags at position slot ^ oct; bits 0-7: imask) and the triangle bits.
+// An 8-byte child row (one byte per slot) reordered so that position j holds slot j ^ oct.
+PRT_D uint2 permuteRow(uint2 w, const RayPre& r)
+{
+  return make_uint2(__byte_perm(w.x, w.y, r.permLo), __byte_perm(w.x, w.y, r.permHi));
+}
+
+// Bit s of an 8-bit mask moved to bit s ^ oct.
+PRT_D uint32_t permuteBits(uint32_t x, uint32_t oct)
+{
+  if (oct & 1u) x = ((x & 0x55u) << 1) | ((x >> 1) & 0x55u);
+  if (oct & 2u) x = ((x & 0x33u) << 2) | ((x >> 2) & 0x33u);
+  if (oct & 4u) x = ((x & 0x0fu) << 4) | ((x >> 4) & 0x0fu);
+  return x;
+}
+
 // Shared-memory copy of the breadth-first top levels of the BVH (bvh8.h), filled by a
 // traversal kernel that stages them; with Top = true node i < topCount is read from here.
 static __shared__ uint4 gTopNodes[5 * kBvh8TopNodes];
 
+// Intersects the 8 children of one node; returns the node group of hit inner children
+// (bits 24-31: hit flags at position slot ^ oct; bits 0-7: imask) and the triangle bits.
+//
+// The child rows are permuted into the ray's octant order once per node, so that child j of the
+// loop is slot j ^ oct and its hit flag lands at bit j, the position the node group uses. The
+// slab slack (2e-6 relative, which keeps the rounded interval from culling a box the exact
+// interval reaches) is applied by scaling the near planes by 1 / 1.000002 instead of scaling
+// every far plane up. Empty slots (meta 0, not inner) may pass the slab test; as leaves without
+// triangles they add nothing.
 template <bool Top>
 PRT_D void intersectNode(const uint4* __restrict__ nodes, uint32_t nodeIdx, const RayPre& r, float tnear,
                          float tfar, uint2& ngroup, uint2& tgroup, int topCount = 0)
@@ -113,40 +146,48 @@ PRT_D void intersectNode(const uint4* __restrict__ nodes, uint32_t nodeIdx, cons
   const uint32_t ex = w0.w & 0xffu, ey = (w0.w >> 8) & 0xffu, ez = (w0.w >> 16) & 0xffu;
   const uint32_t imask = (w0.w >> 24) & 0xffu;
   const uint32_t childBase = w1.x, triBase = w1.y;
-  const uint2 meta = make_uint2(w1.z, w1.w);
-  uint2 qlox = make_uint2(w2.x, w2.y), qloy = make_uint2(w2.z, w2.w);
-  uint2 qloz = make_uint2(w3.x, w3.y), qhix = make_uint2(w3.z, w3.w);
-  uint2 qhiy = make_uint2(w4.x, w4.y), qhiz = make_uint2(w4.z, w4.w);
   // Near plane = lo for positive directions, hi for negative ones.
-  if (r.oct & 1u) { const uint2 t = qlox; qlox = qhix; qhix = t; }
-  if (r.oct & 2u) { const uint2 t = qloy; qloy = qhiy; qhiy = t; }
-  if (r.oct & 4u) { const uint2 t = qloz; qloz = qhiz; qhiz = t; }
+  const uint2 lox = make_uint2(w2.x, w2.y), loy = make_uint2(w2.z, w2.w);
+  const uint2 loz = make_uint2(w3.x, w3.y), hix = make_uint2(w3.z, w3.w);
+  const uint2 hiy = make_uint2(w4.x, w4.y), hiz = make_uint2(w4.z, w4.w);
+  const uint2 nx = permuteRow((r.oct & 1u) ? hix : lox, r), fx = permuteRow((r.oct & 1u) ? lox : hix, r);
+  const uint2 ny = permuteRow((r.oct & 2u) ? hiy : loy, r), fy = permuteRow((r.oct & 2u) ? loy : hiy, r);
+  const uint2 nz = permuteRow((r.oct & 4u) ? hiz : loz, r), fz = permuteRow((r.oct & 4u) ? loz : hiz, r);
+  const float kNear = 1.f / 1.000002f;
   const float ax = __fmul_rn(px - r.o.x, r.invd.x);
   const float ay = __fmul_rn(py - r.o.y, r.invd.y);
   const float az = __fmul_rn(pz - r.o.z, r.invd.z);
   const float bx = expToScale(ex) * r.invd.x;
   const float by = expToScale(ey) * r.invd.y;
   const float bz = expToScale(ez) * r.invd.z;
-  const float tmaxLimit = tfar * 1.000002f;
-  uint32_t inner = 0u, tri = 0u;
+  const float axn = ax * kNear, ayn = ay * kNear, azn = az * kNear;
+  const float bxn = bx * kNear, byn = by * kNear, bzn = bz * kNear;
+  const float tnearK = tnear * kNear;
+  uint32_t hits = 0u;
 #pragma unroll
-  for (int s = 0; s < 8; ++s)
+  for (int j = 0; j < 8; ++j)
   {
-    const uint32_t m = byteOf(meta, s);
-    const bool isInner = (imask >> s) & 1u;
-    const float x0 = fmaf((float)byteOf(qlox, s), bx, ax), x1 = fmaf((float)byteOf(qhix, s), bx, ax);
-    const float y0 = fmaf((float)byteOf(qloy, s), by, ay), y1 = fmaf((float)byteOf(qhiy, s), by, ay);
-    const float z0 = fmaf((float)byteOf(qloz, s), bz, az), z1 = fmaf((float)byteOf(qhiz, s), bz, az);
-    const float tmin = fmaxf(fmaxf(x0, y0), fmaxf(z0, tnear));
-    const float tmax = fminf(fminf(x1, y1), z1);
-    const bool hit = (isInner || m != 0u) && tmin <= fminf(tmax * 1.000002f, tmaxLimit);
-    if (hit)
-    {
-      if (isInner) inner |= 1u << (s ^ r.oct);
-      else tri |= ((1u << (m >> 5)) - 1u) << (m & 31u);
-    }
+    const float x0 = fmaf((float)byteOf(nx, j), bxn, axn), x1 = fmaf((float)byteOf(fx, j), bx, ax);
+    const float y0 = fmaf((float)byteOf(ny, j), byn, ayn), y1 = fmaf((float)byteOf(fy, j), by, ay);
+    const float z0 = fmaf((float)byteOf(nz, j), bzn, azn), z1 = fmaf((float)byteOf(fz, j), bz, az);
+    const float tmin = fmaxf(fmaxf(x0, y0), fmaxf(z0, tnearK));
+    const float tmax = fminf(fminf(x1, y1), fminf(z1, tfar));
+    hits |= (tmin <= tmax ? 1u : 0u) << j;
   }
-  ngroup = make_uint2(childBase, (inner << 24) | imask);
+  const uint32_t imaskP = permuteBits(imask, r.oct);
+  uint32_t leaves = hits & ~imaskP, tri = 0u;
+  if (leaves)
+  {
+    const uint2 meta = permuteRow(make_uint2(w1.z, w1.w), r);
+    do
+    {
+      const int j = __ffs(leaves) - 1;
+      leaves &= leaves - 1u;
+      const uint32_t m = (j < 4 ? (meta.x >> (8 * j)) : (meta.y >> (8 * (j - 4)))) & 0xffu;
+      tri |= ((1u << (m >> 5)) - 1u) << (m & 31u);
+    } while (leaves);
+  }
+  ngroup = make_uint2(childBase, ((hits & imaskP) << 24) | imask);
   tgroup = make_uint2(triBase, tri);
 }
 

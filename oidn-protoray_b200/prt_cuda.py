@@ -96,6 +96,8 @@ def load_library():
     lib.prt_scene_file_desc.argtypes = [vp, P(T.SceneDesc)]
     lib.prt_scene_file_free.argtypes = [vp]
     lib.prt_cuda_scene_load.argtypes = [vp, C.c_char_p, P(T.EnvDesc), C.c_int32]
+    lib.prt_cuda_scene_lights.argtypes = [vp, P(T.EnvDesc)]
+    lib.prt_cuda_microfacet_query.argtypes = [vp, C.c_int32, C.c_int64, P(C.c_float), P(C.c_float)]
     _lib = lib
     return lib
 
@@ -429,6 +431,17 @@ class DeviceCuda:
         out = np.zeros((t.shape[0], 13), np.float32)
         self._check(self.lib.prt_cuda_bsdf_query(self.h, C.byref(material), medium_id, t.shape[0], T.fptr(t),
                                                  T.fptr(out)))
+        return out
+
+    def init_lights(self, env):
+        """Device::initLights: replaces the uploaded scene's environment lights (an EnvDesc)."""
+        self._check(self.lib.prt_cuda_scene_lights(self.h, C.byref(env)))
+
+    def microfacet_query(self, distribution, tuples):
+        """(n, 4) float32: sampled microfacet normal and pdf for (alpha, s.x, s.y, wo) tuples."""
+        t = np.ascontiguousarray(tuples, np.float32).reshape(-1, 6)
+        out = np.zeros((t.shape[0], 4), np.float32)
+        self._check(self.lib.prt_cuda_microfacet_query(self.h, distribution, t.shape[0], T.fptr(t), T.fptr(out)))
         return out
 
     def albedo_tables(self):

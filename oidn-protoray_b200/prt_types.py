@@ -20,6 +20,8 @@ PRT_AOV_ALBEDO1 = 1 << 0
 PRT_AOV_NORMAL1 = 1 << 1
 PRT_AOV_HDR_VAR = 1 << 2
 PRT_ENV_AMBIENT_FIRST = 1
+PRT_MICROFACET_BECKMANN = 1
+PRT_MICROFACET_GGX_VISIBLE = 2
 
 PRT_BLIT_HDR = 0
 PRT_BLIT_ALBEDO1 = 1

@@ -93,6 +93,29 @@ def bsdf_query(material, tuples, medium_id=0):
     return out
 
 
+def bsdf_query_scalar(material, tuples, medium_id=0):
+    """The same query through the reference's scalar BSDF path (Bsdf rather than BsdfSimd)."""
+    lib = _lib()
+    t = np.ascontiguousarray(tuples, np.float32).reshape(-1, 9)
+    out = np.zeros((t.shape[0], 13), np.float32)
+    lib.ref_bsdf_query_scalar.argtypes = [C.POINTER(T.Material), C.c_int, C.c_int64, C.POINTER(C.c_float),
+                                          C.POINTER(C.c_float)]
+    if lib.ref_bsdf_query_scalar(C.byref(material), medium_id, t.shape[0], T.fptr(t), T.fptr(out)) != 0:
+        raise RuntimeError("oracle scalar BSDF query failed")
+    return out
+
+
+def microfacet_query(distribution, tuples, simd=True):
+    """The reference's BeckmannDistribution::sample / GGXDistribution::sampleVisible on
+    (alpha, s.x, s.y, wo) tuples: (n, 4) float32 (m, pdf); SIMD or scalar instantiation."""
+    lib = _lib()
+    t = np.ascontiguousarray(tuples, np.float32).reshape(-1, 6)
+    out = np.zeros((t.shape[0], 4), np.float32)
+    lib.ref_microfacet_query.argtypes = [C.c_int, C.c_int, C.c_int64, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    _check(lib.ref_microfacet_query(distribution, 1 if simd else 0, t.shape[0], T.fptr(t), T.fptr(out)))
+    return out
+
+
 def albedo_tables():
     lib = _lib()
     lib.ref_albedo_tables.restype = C.c_int64

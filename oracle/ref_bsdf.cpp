@@ -22,6 +22,8 @@
 #include "material/material.h"
 #include "core/shading_context.h"
 #include "bsdf/bsdf.h"
+#include "bsdf/beckmann_distribution.h"
+#include "bsdf/ggx_distribution.h"
 
 #include "../include/prt_cuda.h"
 
@@ -157,6 +159,102 @@ int ref_bsdf_query(const prt_material* mat, int mediumId, int64_t n, const float
   {
     return -1;
   }
+}
+
+// The same query through the reference's scalar BSDF path (Material::getBsdf(ShadingContext&)
+// -> Bsdf::eval/sample, material/material.h:54-64, bsdf/bsdf.h:66-89), whose arithmetic is the
+// scalar library's rather than the SIMD path's approximate reciprocals and polynomials.
+int ref_bsdf_query_scalar(const prt_material* mat, int mediumId, int64_t n, const float* tuples, float* out)
+{
+  try
+  {
+    precomputeAlbedoTables();
+    MaterialFactory factory("", Props());
+    std::shared_ptr<Material> material =
+      factory.make(mat->model == PRT_MATERIAL_PRINCIPLED ? principledProps(*mat) : standardProps(*mat));
+    auto ctx = std::make_unique<ShadingContext>();
+    for (int64_t i = 0; i < n; ++i)
+    {
+      const float* t = tuples + 9 * i;
+      const Vec3f wo(t[0], t[1], t[2]), wi(t[3], t[4], t[5]), s(t[6], t[7], t[8]);
+      ctx->p = Vec3f(zero);
+      ctx->f.U = Vec3f(1.f, 0.f, 0.f);
+      ctx->f.V = Vec3f(0.f, 1.f, 0.f);
+      ctx->f.N = Vec3f(0.f, 0.f, 1.f);
+      ctx->Ng = Vec3f(0.f, 0.f, 1.f);
+      for (int u = 0; u < maxNumUVs; ++u) ctx->uv[u] = Vec2f(0.5f);
+      ctx->backfacing = false;
+      ctx->eps = 1e-6f;
+      const Bsdf* bsdf = material->getBsdf(*ctx, wo, mediumId);
+      float evalPdf = 0.f;
+      const Vec3f evalValue = bsdf->eval(*ctx, wo, wi, evalPdf);
+      Vec3f sWi = zero;
+      float sPdf = 0.f;
+      int sType = 0;
+      const Vec3f sWeight = bsdf->sample(*ctx, wo, sWi, sPdf, sType, BsdfSample(s));
+      const int flags = bsdf->getFlags();
+      float* o = out + 13 * i;
+      o[0] = evalValue.x; o[1] = evalValue.y; o[2] = evalValue.z; o[3] = evalPdf;
+      o[4] = sWeight.x; o[5] = sWeight.y; o[6] = sWeight.z;
+      o[7] = sWi.x; o[8] = sWi.y; o[9] = sWi.z;
+      o[10] = sPdf;
+      std::memcpy(&o[11], &sType, 4);
+      std::memcpy(&o[12], &flags, 4);
+    }
+    return 0;
+  }
+  catch (const std::exception&)
+  {
+    return -1;
+  }
+}
+
+// Microfacet sampling with the reference's distributions, in the layout of
+// prt_cuda_microfacet_query: per tuple (alpha, s.x, s.y, wo.x, wo.y, wo.z) -> (m.x, m.y, m.z,
+// pdf). simd != 0 runs the vfloat instantiation (8 tuples per call), else the float one.
+int ref_microfacet_query(int distribution, int simd, int64_t n, const float* in, float* out)
+{
+  if (distribution != PRT_MICROFACET_BECKMANN && distribution != PRT_MICROFACET_GGX_VISIBLE) return -1;
+  if (!simd)
+  {
+    for (int64_t i = 0; i < n; ++i)
+    {
+      const float* t = in + 6 * i;
+      float pdf = 0.f;
+      Vec3f m;
+      if (distribution == PRT_MICROFACET_BECKMANN)
+        m = BeckmannDistribution<float>(t[0]).sample(pdf, Vec2f(t[1], t[2]));
+      else
+        m = GGXDistribution<float>(Vec2f(t[0])).sampleVisible(Vec3f(t[3], t[4], t[5]), pdf, Vec2f(t[1], t[2]));
+      float* o = out + 4 * i;
+      o[0] = m.x; o[1] = m.y; o[2] = m.z; o[3] = pdf;
+    }
+    return 0;
+  }
+  for (int64_t base = 0; base < n; base += simdSize)
+  {
+    const int lanes = (int)std::min<int64_t>(simdSize, n - base);
+    vfloat alpha, sx, sy;
+    Vec3vf wo;
+    for (int k = 0; k < simdSize; ++k)
+    {
+      const float* t = in + 6 * (base + std::min(k, lanes - 1));
+      alpha[k] = t[0]; sx[k] = t[1]; sy[k] = t[2];
+      wo.x[k] = t[3]; wo.y[k] = t[4]; wo.z[k] = t[5];
+    }
+    vfloat pdf = zero;
+    Vec3vf m;
+    if (distribution == PRT_MICROFACET_BECKMANN)
+      m = BeckmannDistribution<vfloat>(alpha).sample(pdf, Vec2vf(sx, sy));
+    else
+      m = GGXDistribution<vfloat>(Vec2vf(alpha)).sampleVisible(wo, pdf, Vec2vf(sx, sy));
+    for (int k = 0; k < lanes; ++k)
+    {
+      float* o = out + 4 * (base + k);
+      o[0] = m.x[k]; o[1] = m.y[k]; o[2] = m.z[k]; o[3] = pdf[k];
+    }
+  }
+  return 0;
 }
 
 // The reference's energy-compensation tables in the order of prt_cuda_albedo_tables.
