@@ -49,6 +49,10 @@ def parse_args():
                     help="Adam steps of the batched inverse-rendering measurement")
     ap.add_argument("--headline-only", action="store_true",
                     help="skip the small-scene, batched and adjoint measurements")
+    ap.add_argument("--traffic-csv", default=None,
+                    help="ncu --csv --print-units base log (dram__bytes_read.sum, dram__bytes_write.sum) of the "
+                         "kTrace launches of a 1-spp frame of this workload, to measure roofline.traffic instead "
+                         "of using the recorded figure")
     return ap.parse_args()
 
 
@@ -299,14 +303,21 @@ def run_ours(args):
 
     # Roofline of the dominant kernel, the closest-hit BVH8 traversal (kTrace, ~60% of the
     # frame): algorithmic bytes per ray B = ray in + hit out + 80 B per node visit + 48 B per
-    # triangle test, over its CUDA-event time. Measured DRAM traffic: NCU_TRACE_DRAM_BYTES of
-    # one 1-spp frame's kTrace launches, per closest ray of that frame, times the closest rays
-    # of an average launch here.
-    b_closest = 32 + 16 + 80 * n_closest + 48 * t_closest
-    b_shadow = 32 + 4 + 80 * n_shadow + 48 * t_shadow
+    # triangle test, with the node visits and triangle tests per ray frozen on the reference
+    # tree (TERRAIN_PER_RAY), over the kernel's CUDA-event time. The counts of the tree in use
+    # are reported beside them. Measured DRAM traffic: the ncu DRAM bytes of one 1-spp frame's
+    # kTrace launches (--traffic-csv, or the recorded NCU_TRACE_DRAM_BYTES), per closest ray of
+    # that frame, times the closest rays of an average launch here.
+    fz = TERRAIN_PER_RAY
+    b_closest = 32 + 16 + 80 * fz["closest_nodes"] + 48 * fz["closest_tris"]
+    b_shadow = 32 + 4 + 80 * fz["shadow_nodes"] + 48 * fz["shadow_tris"]
     achieved = closest * b_closest / (trace_ms * 1e-3) / 1e9
     per_launch_rays = closest / max(trace_launches, 1)
-    traffic = NCU_TRACE_DRAM_BYTES / max(c["closest_rays"], 1) * per_launch_rays
+    traffic_bytes, traffic_note = NCU_TRACE_DRAM_BYTES, "recorded ncu capture (NCU_TRACE_DRAM_BYTES)"
+    if args.traffic_csv:
+        traffic_bytes = ncu_dram_bytes(args.traffic_csv, "kTrace")
+        traffic_note = f"ncu capture of this build ({args.traffic_csv})"
+    traffic = traffic_bytes / max(c["closest_rays"], 1) * per_launch_rays
     peak, peak_kind = measured_peaks()
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -328,9 +339,11 @@ def run_ours(args):
                      "launch_ms": trace_ms / max(trace_launches, 1),
                      "launches_per_step": trace_launches / args.steps,
                      "bytes_per_ray": {"closest": b_closest, "shadow": b_shadow},
-                     "per_ray": {"closest_nodes": n_closest, "closest_tris": t_closest, "shadow_nodes": n_shadow,
-                                 "shadow_tris": t_shadow},
-                     "traffic_note": "ncu DRAM bytes of a 1-spp frame's kTrace launches, scaled per closest ray"},
+                     "per_ray_reference_tree": fz,
+                     "per_ray_tree_in_use": {"closest_nodes": n_closest, "closest_tris": t_closest,
+                                             "shadow_nodes": n_shadow, "shadow_tris": t_shadow},
+                     "traffic_note": "DRAM bytes of a 1-spp frame's kTrace launches, scaled per closest ray: "
+                                     + traffic_note},
         "kernel_ms_per_step": {"trace": trace_ms / args.steps, "shadow": shadow_ms / args.steps,
                                "shade": shade_ms / args.steps},
         "rays_per_step": {"closest": closest / args.steps, "shadow": shadow / args.steps},
@@ -357,6 +370,30 @@ def run_ours(args):
 # DRAM bytes (read + write) of the 9 kTrace launches of one 1920x1080 x 1-spp terrain frame,
 # from ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum.
 NCU_TRACE_DRAM_BYTES = 738_353_920
+
+# Node visits and triangle tests per ray on the reference tree of the terrain workload: the host
+# binned-SAH BVH8 with the SAH-optimal 8-wide collapse (284,895 nodes, at most 3 triangles per
+# leaf), counted by the counting traversal over every closest and shadow ray of one
+# 1920x1080 x 1-spp frame. Frozen, so that a worse tree cannot raise the roofline's bytes.
+TERRAIN_PER_RAY = {"closest_nodes": 13.004, "closest_tris": 4.300, "shadow_nodes": 12.963, "shadow_tris": 5.543}
+
+
+def ncu_dram_bytes(path, kernel):
+    """Sum of dram__bytes_read.sum + dram__bytes_write.sum over the launches of `kernel` in an
+    ncu --csv log (units printed as base units, bytes)."""
+    import csv
+
+    with open(path) as f:
+        rows = list(csv.reader(line for line in f if line.startswith('"')))
+    head = rows[0]
+    k_name, k_metric, k_value, k_unit = (head.index(c) for c in ("Kernel Name", "Metric Name", "Metric Value",
+                                                                 "Metric Unit"))
+    scale = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}
+    total = 0.0
+    for r in rows[1:]:
+        if kernel in r[k_name] and r[k_metric] in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+            total += float(r[k_value].replace(",", "")) * scale.get(r[k_unit], 1.0)
+    return total
 
 def bvh_build_bench(dev, scene, builds=3, spp=8):
     """BVH8 build of the terrain workload on the host (binned SAH) and on the device (PLOC), the
