@@ -187,7 +187,14 @@ typedef struct prt_renderer_desc
   float   max_radiance;   /* "maxRadiance", reference default FLT_MAX (no clamping) */
   int32_t type;           /* renderer "type": PRT_RENDERER_* (0 = pathStream) */
   int32_t samples;        /* aoStream "samples" (AO rays per pixel sample; 0 = the default 16) */
+  int32_t flags;          /* PRT_RENDERER_IRRADIANCE; 0 = the standard path tracer */
 } prt_renderer_desc;
+
+/* pathStream's "irradiance" option (render/path_renderer_stream.h:130-139, 304, 598): the first
+ * surface a camera path hits is shaded with a white diffuse material (Principled, base colour 1)
+ * and a camera ray that misses sees no environment, so the image is the irradiance arriving at
+ * the first hits. Frame form only. */
+#define PRT_RENDERER_IRRADIANCE 1
 
 /* Renderer types (render/renderer_factory_stream.cpp:54-67): the path tracer and its sibling
  * stream renderers, which reuse its camera rays and traversal:
@@ -219,6 +226,9 @@ typedef struct prt_renderer_desc
 #define PRT_AOV_NORMAL1  (1 << 1)   /* "aovNormal1": first-hit normal */
 
 #define PRT_AOV_HDR_VAR  (1 << 2)   /* "aovHdrVar": per-pixel sample variance of the colour */
+#define PRT_AOV_SH       (1 << 3)   /* "aovSh": first-order spherical harmonics of the radiance that
+                                       reaches the first hit (render/path_renderer_stream.h:46-52,
+                                       257-263, 329-344, 705-709, 914-930, 980-1059); frame form only */
 
 /* AOV identifiers for prt_cuda_blit. */
 #define PRT_BLIT_HDR      0
@@ -229,6 +239,15 @@ typedef struct prt_renderer_desc
                                  per pixel (blue in bits 0-7, green 8-15, red 16-23; gamma 2.2,
                                  image/pixel.h:36-40); dst is then width * height uint32 */
 #define PRT_BLIT_LDR_RGB  5   /* FrameAovs::ldr: tone-mapped colour clamped to [0, 1], RGB floats */
+/* FrameAovs::sh[0..3] (needs PRT_AOV_SH), as DeviceCpu::blitFrame writes them
+ * (render/device_cpu.cpp:359-364): SH0 is the mean of the band-0 coefficient (the radiance
+ * scaled to irradiance, per colour channel); SH1..SH3 are the means of its products with the
+ * arrival direction's x, y and z, each divided by max(SH0, 1e-4) (AccumBuffer3f::blitRel,
+ * image/accum_buffer.h:735-750). RGB floats. */
+#define PRT_BLIT_SH0      6
+#define PRT_BLIT_SH1      7
+#define PRT_BLIT_SH2      8
+#define PRT_BLIT_SH3      9
 
 /* Tone mappers for PRT_BLIT_LDR and the frame error (render/device_cpu.cpp:286-303). */
 #define PRT_TONE_NONE     0

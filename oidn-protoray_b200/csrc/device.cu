@@ -120,10 +120,12 @@ void freeFrame(Context& c)
   f(c.accumN);
   f(c.accumC);
   f(c.accum2);
+  f(c.accumSH);
   f(c.errPartials);
   PathState& s = c.ps;
   f(s.rayO); f(s.rayD); f(s.hit); f(s.thr); f(s.rad); f(s.info);
   f(s.shO); f(s.shD); f(s.shL); f(s.out); f(s.aovA); f(s.aovN);
+  f(s.sphL); f(s.sphWi); f(s.sphDirL); f(s.sphDirWi); f(s.sphOut); f(s.sphDirScale);
   f(s.queue[0]); f(s.queue[1]); f(s.classQueues);
   s.capacity = 0;
 }
@@ -616,16 +618,19 @@ void allocFrame(Context& c, int width, int height, int aovMask)
   if (width % 32 != 0 || height % 8 != 0)
     throw std::logic_error("image size is not divisible by the tile size");
   if (width > 4096 || height > 4096) throw std::logic_error("image size is too large");
-  if (aovMask & ~(PRT_AOV_ALBEDO1 | PRT_AOV_NORMAL1 | PRT_AOV_HDR_VAR)) throw std::invalid_argument("unknown AOV bits");
+  if (aovMask & ~(PRT_AOV_ALBEDO1 | PRT_AOV_NORMAL1 | PRT_AOV_HDR_VAR | PRT_AOV_SH))
+    throw std::invalid_argument("unknown AOV bits");
   freeFrame(c);
   c.width = width;
   c.height = height;
   c.aovMask = aovMask & (PRT_AOV_ALBEDO1 | PRT_AOV_NORMAL1);  // per-path first-hit AOVs
+  c.aovSh = (aovMask & PRT_AOV_SH) != 0;
   const size_t px = (size_t)width * height;
   c.accum = (float*)devAlloc(c, px * sizeof(float4), nullptr);
   c.accumC = (float*)devAlloc(c, px * sizeof(float4), nullptr);
   c.errPartials = (double*)devAlloc(c, sizeof(double) * (size_t)c.smCount * 16, nullptr);
   if (aovMask & PRT_AOV_HDR_VAR) c.accum2 = (float*)devAlloc(c, px * sizeof(float4), nullptr);
+  if (c.aovSh) c.accumSH = (float*)devAlloc(c, 4 * px * sizeof(float4), nullptr);
   if (c.aovMask)
   {
     c.accumA = (float*)devAlloc(c, px * sizeof(float4), nullptr);
@@ -658,6 +663,7 @@ void ensurePathState(Context& c, int spp)
   };
   f(s.rayO); f(s.rayD); f(s.hit); f(s.thr); f(s.rad); f(s.info);
   f(s.shO); f(s.shD); f(s.shL); f(s.out); f(s.aovA); f(s.aovN);
+  f(s.sphL); f(s.sphWi); f(s.sphDirL); f(s.sphDirWi); f(s.sphOut); f(s.sphDirScale);
   f(s.queue[0]); f(s.queue[1]); f(s.classQueues);
   c.waveSamples = want;
   const int64_t cap = (int64_t)want * px;
@@ -671,6 +677,12 @@ void ensurePathState(Context& c, int spp)
   {
     s.aovA = a4(cap);
     s.aovN = a4(cap);
+  }
+  if (c.aovSh)
+  {
+    s.sphL = a4(cap); s.sphWi = a4(cap); s.sphDirL = a4(cap); s.sphDirWi = a4(cap);
+    s.sphOut = a4(3 * cap);
+    s.sphDirScale = (float*)devAlloc(c, cap * sizeof(float), nullptr);
   }
   s.queue[0] = (int*)devAlloc(c, cap * sizeof(int), nullptr);
   s.queue[1] = (int*)devAlloc(c, cap * sizeof(int), nullptr);
@@ -832,6 +844,7 @@ int prt_cuda_destroy(prt_context* ctx)
   if (c.ps.err) cudaFree(c.ps.err);
   if (c.ps.travCounts) cudaFree(c.ps.travCounts);
   if (c.tableStorage) cudaFree(c.tableStorage);
+  if (c.whiteMaterialDev) cudaFree(c.whiteMaterialDev);
   if (c.ev0) cudaEventDestroy(c.ev0);
   if (c.ev1) cudaEventDestroy(c.ev1);
   if (c.stream) cudaStreamDestroy(c.stream);
@@ -897,6 +910,22 @@ int prt_cuda_renderer(prt_context* ctx, const prt_renderer_desc* r)
     if (!r || r->max_depth < 0 || r->max_depth > 1000) throw std::invalid_argument("invalid renderer settings");
     if (r->type < PRT_RENDERER_PATH || r->type > PRT_RENDERER_DIFFUSE2_FAST) throw std::invalid_argument("invalid renderer type");
     if (r->samples < 0 || r->samples > 4096) throw std::invalid_argument("invalid renderer samples");
+    if (r->flags & ~PRT_RENDERER_IRRADIANCE) throw std::invalid_argument("unknown renderer flags");
+    if (r->flags && r->type != PRT_RENDERER_PATH) throw std::invalid_argument("irradiance mode is a pathStream option");
+    if (r->flags & PRT_RENDERER_IRRADIANCE)
+    {
+      // render/path_renderer_stream.h:131-139: a Principled material with base colour 1.
+      prt_material white;
+      prt_cuda_principled_defaults(&white);
+      white.base_color[0] = white.base_color[1] = white.base_color[2] = 1.f;
+      std::vector<float> media = {1.f, 1.f, 1.f, 1.f};
+      c.whiteMaterial = resolveMaterial(white, media, 0);
+      c.whiteClass = c.whiteMaterial.shadeClass;
+      if (!c.whiteMaterialDev) c.whiteMaterialDev = (DevMaterial*)devAlloc(c, sizeof(DevMaterial), nullptr);
+      cuCheck(cudaMemcpy(c.whiteMaterialDev, &c.whiteMaterial, sizeof(DevMaterial), cudaMemcpyHostToDevice),
+              "white material");
+    }
+    c.renderer.flags = r->flags;
     c.renderer.type = r->type;
     c.renderer.aoSamples = r->samples ? r->samples : 16;
     c.renderer.maxDepth = r->max_depth;
@@ -949,6 +978,7 @@ int prt_cuda_render(prt_context* ctx, int32_t spp, prt_render_stats* stats)
     requireScene(c);
     if (!c.hasRenderer || !c.hasCamera || !c.accum) throw ApiError{PRT_ERR_STATE, "renderer, camera and frame are required"};
     if (spp < 0) throw std::invalid_argument("spp must be >= 0");
+    if (c.aovSh && c.renderer.type != PRT_RENDERER_PATH) throw std::invalid_argument("the SH AOV is a pathStream AOV");
     cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
     ensurePathState(c, spp);
     cuCheck(cudaEventRecord(c.ev0, c.stream), "event");
@@ -993,8 +1023,8 @@ int prt_cuda_blit(prt_context* ctx, int32_t aov, float* dst)
 {
   return guarded(ctx, [&](Context& c) {
     if (!c.accum || !dst) throw std::invalid_argument("no frame or null destination");
-    if (aov < 0 || aov > PRT_BLIT_LDR_RGB || ((aov == PRT_BLIT_ALBEDO1 || aov == PRT_BLIT_NORMAL1) && !c.accumA) ||
-        (aov == PRT_BLIT_HDR_VAR && !c.accum2))
+    if (aov < 0 || aov > PRT_BLIT_SH3 || ((aov == PRT_BLIT_ALBEDO1 || aov == PRT_BLIT_NORMAL1) && !c.accumA) ||
+        (aov == PRT_BLIT_HDR_VAR && !c.accum2) || (aov >= PRT_BLIT_SH0 && !c.accumSH))
       throw std::invalid_argument("AOV not enabled");
     const size_t px = (size_t)c.width * c.height;
     Staged out(c, dst, aov == PRT_BLIT_LDR ? px * sizeof(uint32_t) : px * 3 * sizeof(float), false);
@@ -1715,6 +1745,7 @@ int prt_cuda_batch_create(prt_context* ctx, const prt_batch_item* items, int32_t
         if (it.width > 4096 || it.height > 4096) throw std::logic_error("image size is too large");
         if (it.renderer.max_depth < 0 || it.renderer.max_depth > 1000) throw std::invalid_argument("invalid renderer settings");
         if (it.renderer.type != PRT_RENDERER_PATH) throw std::invalid_argument("batches render with the path tracer");
+        if (it.renderer.flags) throw std::invalid_argument("batches render with the standard path tracer");
         if (it.aov_mask & ~(PRT_AOV_ALBEDO1 | PRT_AOV_NORMAL1)) throw std::invalid_argument("unknown AOV bits");
         // Scene upload through the frame form's path, into buffers the batch owns.
         Context tmp;
@@ -1924,6 +1955,8 @@ int prt_cuda_adjoint(prt_context* ctx, uint32_t first_sample, int32_t spp, const
     if (!c.hasRenderer || !c.hasCamera || !c.accum) throw ApiError{PRT_ERR_STATE, "renderer, camera and frame are required"};
     if (spp <= 0 || !d_loss_d_image) throw std::invalid_argument("invalid adjoint request");
     if (c.renderer.type != PRT_RENDERER_PATH) throw std::invalid_argument("the adjoint differentiates the path tracer");
+    if (c.renderer.flags || c.aovSh)
+      throw std::invalid_argument("the adjoint differentiates the standard path tracer without the SH AOV");
     requireAdjointMaterials(c.materialsHost);
     if (c.texturesHost.size() > 32) throw std::invalid_argument("the adjoint supports at most 32 textures");
     int64_t texFloats = 0;

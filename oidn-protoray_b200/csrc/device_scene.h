@@ -203,6 +203,7 @@ struct DevRenderer
   uint32_t seed;
   int type;        // PRT_RENDERER_*
   int aoSamples;
+  int flags;       // PRT_RENDERER_IRRADIANCE
 };
 
 // What the adjoint's replay needs per frame besides the frame itself (csrc/adjoint.cuh).

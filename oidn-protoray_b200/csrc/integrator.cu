@@ -45,6 +45,10 @@ struct Launch
   // Some scene of the launch has transparent materials: shadow rays take the transparency
   // filter (host-side choice of the kShadow instantiation).
   int anyTransparent;
+  // Irradiance mode (DevRenderer::flags, frame form): the first hit's material (device memory)
+  // and its class.
+  const DevMaterial* white;
+  int whiteClass;
 };
 
 template <int... Fs>
@@ -247,6 +251,14 @@ PRT_D void initPath(const PathState& ps, int64_t p, const DevCamera& cam, const 
     ps.aovA[p] = make_float4(0.f, 0.f, 0.f, 0.f);
     ps.aovN[p] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
+  if (ps.sphL)
+  {
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    ps.sphL[p] = z;
+    ps.sphWi[p] = z;
+    ps.sphDirL[p] = z;
+    ps.sphDirWi[p] = z;
+  }
 }
 
 // Path initialisation of a frame-form wave.
@@ -384,6 +396,8 @@ __global__ void __launch_bounds__(256) kTrace(Launch L, const int* __restrict__ 
       L.ps.hit[p] = make_float4(h.t, h.u, h.v, __int_as_float(h.triId));
       cls = 0;
       if (h.triId >= 0 && pathDepth < E.rd.maxDepth) cls = __ldg(E.sc.meshClass + __ldg(E.sc.triVerts + h.triId).w);
+      // Irradiance mode: every surface a camera ray hits is shaded with the white material.
+      if (!Batch && cls > 0 && pathDepth == 0 && (L.rd.flags & PRT_RENDERER_IRRADIANCE)) cls = L.whiteClass;
     }
     for (int c = 0; c < kShadeClasses; ++c)
     {
@@ -484,13 +498,38 @@ __global__ void __launch_bounds__(256) kRayBinScatter(const int* __restrict__ qu
 // Ends path p with radiance `rad`. Frame form: ps.out, summed later by kAccumulate. Batch
 // form: added to the item's accumulation planes at once (with the first-hit AOVs); the
 // caller returns the slot to the free list.
+// Radiance-to-irradiance scale pi / cos of a first-hit direction (render/path_renderer_stream.h:
+// 708, 919). The reference divides by max(cos, 0) with its approximate reciprocal, which gives NaN
+// for a direction at or below the BSDF's normal, and clampL turns the product into zero: such a
+// direction adds nothing, which a zero scale reproduces.
+PRT_D float shIrradianceScale(float cosTheta) { return cosTheta > 0.f ? kPi / cosTheta : 0.f; }
+
+// The path's SH sample at its end (render/path_renderer_stream.h:329-344, 1032-1041): the
+// radiance gathered after the first hit (plus `extra`, what this bounce adds to it) scaled to
+// irradiance along the first bounce's direction, plus the first hit's direct light along its
+// direction, each as first-order SH (value, value x dir.x, value x dir.y, value x dir.z,
+// math/sh.h:115-135).
+PRT_D void finishSh(const Launch& L, int p, f3 extra)
+{
+  const float4 a = L.ps.sphL[p], w = L.ps.sphWi[p], dl = L.ps.sphDirL[p], dw = L.ps.sphDirWi[p];
+  const f3 v = clampL((mk(a.x, a.y, a.z) + extra) * a.w, L.rd.maxRadiance);
+  const f3 d = clampL(mk(dl.x, dl.y, dl.z), L.rd.maxRadiance);
+  const f3 c1 = v * w.x + d * dw.x, c2 = v * w.y + d * dw.y, c3 = v * w.z + d * dw.z;
+  const f3 c0 = v + d;
+  float4* o = L.ps.sphOut + 3 * (int64_t)p;
+  o[0] = make_float4(c0.x, c0.y, c0.z, c1.x);
+  o[1] = make_float4(c1.y, c1.z, c2.x, c2.y);
+  o[2] = make_float4(c2.z, c3.x, c3.y, c3.z);
+}
+
 template <bool Batch>
-PRT_D void finishPath(const Launch& L, int p, f3 rad, const uint4& info)
+PRT_D void finishPath(const Launch& L, int p, f3 rad, const uint4& info, f3 shExtra = mk(0.f))
 {
   if (!Batch)
   {
     const f3 c = clampL(rad, L.rd.maxRadiance);
     L.ps.out[p] = make_float4(c.x, c.y, c.z, 1.f);
+    if (L.ps.sphOut) finishSh(L, p, shExtra);
     return;
   }
   const BatchItem& it = L.items[info.w];
@@ -550,7 +589,7 @@ struct ShadowFilter
 // scenes with transparent materials filter the hits (ShadowFilter).
 template <bool Count, bool Batch, bool Top = false, bool Transp = false>
 __global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__ count, int* __restrict__ work,
-                                               int parity)
+                                               int parity, int depth)
 {
   const int n = *count;
   const int top = stageTopNodes<Top && !Batch>(L);
@@ -595,6 +634,26 @@ __global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__
         r.y += c.y * T.y;
         r.z += c.z * T.z;
         L.ps.rad[p] = r;
+        // SH AOV (render/path_renderer_stream.h:1004-1017): the first hit's direct light, scaled
+        // to irradiance, with its direction; later bounces add to the gathered radiance.
+        if (!Batch && L.ps.sphOut)
+        {
+          const f3 dl = mk(c.x * T.x, c.y * T.y, c.z * T.z);
+          if (depth == 0)
+          {
+            const float sc = L.ps.sphDirScale[i];
+            L.ps.sphDirL[p] = make_float4(dl.x * sc, dl.y * sc, dl.z * sc, 0.f);
+            L.ps.sphDirWi[p] = make_float4(b.x, b.y, b.z, 0.f);
+          }
+          else
+          {
+            float4 q = L.ps.sphL[p];
+            q.x += dl.x;
+            q.y += dl.y;
+            q.z += dl.z;
+            L.ps.sphL[p] = q;
+          }
+        }
       }
       if (tag & kShadowFinish)
       {
@@ -635,16 +694,23 @@ __global__ void __launch_bounds__(256) kShadeEnd(Launch L, const int* __restrict
       const float lastPdf = tp.w;
       const int lastType = __float_as_int(ra.w);
       const bool aov1 = (pixelId & kPathAov1Flag) == 0u;
+      f3 lightL = mk(0.f);
       // A hit on a PRT_MATERIAL_MISS material is shaded as a miss.
       const bool miss =
         triId < 0 ||
         (E.sc.materials[__ldg(E.sc.meshMaterial + __ldg(&E.sc.triVerts[triId].w))].type & kMatMiss) != 0;
       if (miss)
       {
-        float lightPdf;
-        const f3 Le = evalEnvLights(E.sc, dir, lightPdf);
-        const float w = (lastType & kBsdfSmooth) == 0 ? 1.f : misWeight(lastPdf, lightPdf);
-        Lr += T * w * Le;
+        // Irradiance mode: a camera ray that misses sees no environment
+        // (render/path_renderer_stream.h:304).
+        if (Batch || depth > 0 || !(L.rd.flags & PRT_RENDERER_IRRADIANCE))
+        {
+          float lightPdf;
+          const f3 Le = evalEnvLights(E.sc, dir, lightPdf);
+          const float w = (lastType & kBsdfSmooth) == 0 ? 1.f : misWeight(lastPdf, lightPdf);
+          lightL = T * w * Le;
+          Lr += lightL;
+        }
         if (aov1 && E.aovMask)
         {
           L.ps.aovA[p] = make_float4(0.f, 0.f, 0.f, 1.f);
@@ -662,7 +728,8 @@ __global__ void __launch_bounds__(256) kShadeEnd(Launch L, const int* __restrict
           const int prim = triId - __ldg(E.sc.meshTriOffset + mesh);
           const f3 Le = evalAreaLight(E.sc, mesh, prim, dir, hh.x, lightPdf);
           const float w = (lastType & kBsdfSmooth) == 0 ? 1.f : misWeight(lastPdf, lightPdf);
-          Lr += T * w * Le;
+          lightL = T * w * Le;
+          Lr += lightL;
           if (aov1 && E.aovMask)
           {
             const f3 N = normalize(-dir);
@@ -672,7 +739,7 @@ __global__ void __launch_bounds__(256) kShadeEnd(Launch L, const int* __restrict
         }
         // else: a surface at maxDepth ends the path with its current radiance.
       }
-      finishPath<Batch>(L, p, Lr, info);
+      finishPath<Batch>(L, p, Lr, info, lightL);
     }
     freeSlots<Batch>(L, parity ^ 1, active, p);
   }
@@ -697,6 +764,7 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
     bool freed = false;
     uint32_t extTag = 0u;  // direction octant of the extended ray, in the queue entry's top bits
     float4 shO = make_float4(0.f, 0.f, 0.f, 0.f), shD = shO, shL = shO;
+    float shScale = 0.f;   // SH AOV: irradiance scale of a first-hit shadow ray
     if (active)
     {
       const float4 ro = L.ps.rayO[p], rd = L.ps.rayD[p], hh = L.ps.hit[p];
@@ -716,7 +784,10 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
       const bool aov1 = (pixelId & kPathAov1Flag) == 0u;
       ShadeCtx ctx;
       postIntersect(E.sc, org, dir, hh.x, triId, hh.y, hh.z, ctx);
-      const DevMaterial& mat = E.sc.materials[ctx.material];
+      // Irradiance mode: the first hit is shaded with the white material
+      // (render/path_renderer_stream.h:598).
+      const bool whiteHit = !Batch && depth == 0 && (L.rd.flags & PRT_RENDERER_IRRADIANCE);
+      const DevMaterial& mat = whiteHit ? *L.white : E.sc.materials[ctx.material];
       const f3 wo = -dir;
       uint32_t mediumId = info.z & kMediumMask;
       // Material::getBsdf orientation: media interfaces take it from the medium the path
@@ -771,6 +842,9 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
               shO = make_float4(ctx.p.x, ctx.p.y, ctx.p.z, ctx.eps);
               shD = make_float4(wi.x, wi.y, wi.z, dist - ctx.eps);
               shL = make_float4(dirL.x, dirL.y, dirL.z, 0.f);
+              // SH AOV: the first hit's direct light counts as irradiance, pi / cos of the
+              // light direction times its radiance (render/path_renderer_stream.h:705-709).
+              if (!Batch && L.ps.sphOut && depth == 0) shScale = shIrradianceScale(dot(wi, bsdf.normal()));
             }
           }
         }
@@ -829,6 +903,13 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
           mediumId = (int)mediumId == mat.mediumInt ? (uint32_t)mat.mediumExt : (uint32_t)mat.mediumInt;
         info.z = Batch ? (mediumId | ((uint32_t)(depth + 1) << kDepthShift)) : mediumId;
         L.ps.rad[p] = ra;
+        // SH AOV: the first bounce's direction and its irradiance scale
+        // (render/path_renderer_stream.h:914-930).
+        if (!Batch && L.ps.sphOut && depth == 0)
+        {
+          L.ps.sphL[p] = make_float4(0.f, 0.f, 0.f, shIrradianceScale(dot(wi, bsdf.normal())));
+          L.ps.sphWi[p] = make_float4(wi.x, wi.y, wi.z, 0.f);
+        }
       }
       info.x = pixelId;
       L.ps.info[p] = info;
@@ -847,6 +928,7 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
       L.ps.shO[sidx] = shO;
       L.ps.shD[sidx] = shD;
       L.ps.shL[sidx] = shL;
+      if (!Batch && L.ps.sphDirScale) L.ps.sphDirScale[sidx] = shScale;
     }
     freeSlots<Batch>(L, parity ^ 1, freed, p);
   }
@@ -977,7 +1059,8 @@ __global__ void __launch_bounds__(256) kSimpleRender(Launch L)
 // overwrite: each sample replaces the pixel (AccumBuffer::set, image/accum_buffer.h:547-570), for
 // the renderers that do not accumulate.
 __global__ void kAccumulate(Launch L, float4* __restrict__ accum, float4* __restrict__ accA, float4* __restrict__ accN,
-                            float4* __restrict__ accC, float4* __restrict__ acc2, long long countBase, int overwrite)
+                            float4* __restrict__ accC, float4* __restrict__ acc2, long long countBase, int overwrite,
+                            float4* __restrict__ accSH)
 {
   const int n = L.pixelCount;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
@@ -1030,6 +1113,26 @@ __global__ void kAccumulate(Launch L, float4* __restrict__ accum, float4* __rest
     {
       accA[q] = a;
       accN[q] = nn;
+    }
+    // SH AOV: the four coefficient planes (an AccumBuffer3f each, weight 1 per sample).
+    if (accSH && L.ps.sphOut)
+    {
+      float4 h[4];
+      for (int k = 0; k < 4; ++k) h[k] = accSH[(int64_t)k * n + q];
+      for (int s = 0; s < L.samples; ++s)
+      {
+        const float4* o = L.ps.sphOut + 3 * ((int64_t)s * L.pixelCount + idx);
+        const float4 u = o[0], v = o[1], w = o[2];
+        const float c[12] = {u.x, u.y, u.z, u.w, v.x, v.y, v.z, v.w, w.x, w.y, w.z, w.w};
+        for (int k = 0; k < 4; ++k)
+        {
+          h[k].x += c[3 * k];
+          h[k].y += c[3 * k + 1];
+          h[k].z += c[3 * k + 2];
+          h[k].w += 1.f;
+        }
+      }
+      for (int k = 0; k < 4; ++k) accSH[(int64_t)k * n + q] = h[k];
     }
   }
 }
@@ -1222,9 +1325,39 @@ cudaError_t launchBsdfQuery(Context& ctx, const DevMaterial& m, int mediumId, in
   return cudaGetLastError();
 }
 
+// SH AOV blits (DeviceCpu::blitFrame, render/device_cpu.cpp:359-364): band 0 as the mean;
+// bands 1-3 as their mean over max(band-0 mean, 1e-4) per channel (AccumBuffer3f::blitRel,
+// image/accum_buffer.h:735-750).
+__global__ void kBlitSh(const float4* __restrict__ acc0, const float4* __restrict__ acck, int n, int rel,
+                        float* __restrict__ dst)
+{
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+  {
+    const float4 a = acc0[q];
+    const float ia = rcpSafe(a.w);
+    f3 v = mk(a.x * ia, a.y * ia, a.z * ia);
+    if (rel)
+    {
+      const float4 b = acck[q];
+      const float ib = rcpSafe(b.w);
+      v = mk(b.x * ib / fmaxf(v.x, 1e-4f), b.y * ib / fmaxf(v.y, 1e-4f), b.z * ib / fmaxf(v.z, 1e-4f));
+    }
+    dst[3 * q] = v.x;
+    dst[3 * q + 1] = v.y;
+    dst[3 * q + 2] = v.z;
+  }
+}
+
 cudaError_t launchBlit(Context& ctx, int aov, float* dst)
 {
   const int n = ctx.width * ctx.height;
+  if (aov >= PRT_BLIT_SH0 && aov <= PRT_BLIT_SH3)
+  {
+    const float4* sh = reinterpret_cast<const float4*>(ctx.accumSH);
+    const int k = aov - PRT_BLIT_SH0;
+    kBlitSh<<<gridFor(ctx, n), 256, 0, ctx.stream>>>(sh, sh + (int64_t)k * n, n, k > 0 ? 1 : 0, dst);
+    return cudaGetLastError();
+  }
   const float* src = aov == 0 ? ctx.accum : (aov == 1 ? ctx.accumA : ctx.accumN);
   kBlit<<<gridFor(ctx, n), 256, 0, ctx.stream>>>(reinterpret_cast<const float4*>(src), n, dst);
   return cudaGetLastError();
@@ -1238,6 +1371,7 @@ cudaError_t launchClear(Context& ctx)
   if (e == cudaSuccess && ctx.accumN) e = cudaMemsetAsync(ctx.accumN, 0, bytes, ctx.stream);
   if (e == cudaSuccess && ctx.accumC) e = cudaMemsetAsync(ctx.accumC, 0, bytes, ctx.stream);
   if (e == cudaSuccess && ctx.accum2) e = cudaMemsetAsync(ctx.accum2, 0, bytes, ctx.stream);
+  if (e == cudaSuccess && ctx.accumSH) e = cudaMemsetAsync(ctx.accumSH, 0, 4 * bytes, ctx.stream);
   ctx.accumCount = 0;
   return e;
 }
@@ -1404,16 +1538,16 @@ static cudaError_t bounceLoop(Context& ctx, const Launch& L, int P, bool replay,
       if (L.anyTransparent)
       {
         if (counting)
-          kShadow<true, false, false, true><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0);
+          kShadow<true, false, false, true><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
         else
-          kShadow<false, false, false, true><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0);
+          kShadow<false, false, false, true><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
       }
       else if (counting)
-        kShadow<true, false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0);
+        kShadow<true, false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
       else if (ctx.topStage)
-        kShadow<false, false, true><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0);
+        kShadow<false, false, true><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
       else
-        kShadow<false, false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0);
+        kShadow<false, false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
       end();
       rc.launches++;
     }
@@ -1461,6 +1595,8 @@ static Launch frameLaunch(const Context& ctx, uint32_t firstSample, int samples)
   L.samples = samples;
   L.aovMask = ctx.aovMask;
   L.anyTransparent = ctx.scene.hasTransparent;
+  L.white = ctx.whiteMaterialDev;
+  L.whiteClass = ctx.whiteClass;
   return L;
 }
 
@@ -1523,7 +1659,8 @@ cudaError_t renderSamples(Context& ctx, int spp, RenderCounters& rc)
     kAccumulate<<<gridFor(ctx, pixelCount), 256, 0, ctx.stream>>>(
       L, reinterpret_cast<float4*>(ctx.accum), reinterpret_cast<float4*>(ctx.accumA),
       reinterpret_cast<float4*>(ctx.accumN), reinterpret_cast<float4*>(ctx.accumC),
-      reinterpret_cast<float4*>(ctx.accum2), (long long)ctx.accumCount, type >= PRT_RENDERER_PRIMARY_FAST ? 1 : 0);
+      reinterpret_cast<float4*>(ctx.accum2), (long long)ctx.accumCount, type >= PRT_RENDERER_PRIMARY_FAST ? 1 : 0,
+      ctx.aovSh ? reinterpret_cast<float4*>(ctx.accumSH) : nullptr);
     ctx.accumCount += S;
     rc.launches++;
     e = cudaGetLastError();
@@ -1650,9 +1787,9 @@ int batchIteration(const Context& ctx, const Launch& L, int a, int persistent, i
   kShadeEnd<true><<<shadeGrid, 256, 0, st>>>(L, L.ps.classQueues, ca + 1, 0, a);
   ShadeClassList::run<true>(1, L, st, shadeGrid, L.ps.classQueues, ca, 0, L.ps.queue[b], cb, ca + kBatchCntShadow, a);
   if (L.anyTransparent)
-    kShadow<false, true, false, true><<<persistent, 256, 0, st>>>(L, ca + kBatchCntShadow, ca + kBatchCntShadow + 2, a);
+    kShadow<false, true, false, true><<<persistent, 256, 0, st>>>(L, ca + kBatchCntShadow, ca + kBatchCntShadow + 2, a, 0);
   else
-    kShadow<false, true><<<persistent, 256, 0, st>>>(L, ca + kBatchCntShadow, ca + kBatchCntShadow + 2, a);
+    kShadow<false, true><<<persistent, 256, 0, st>>>(L, ca + kBatchCntShadow, ca + kBatchCntShadow + 2, a, 0);
   return 5 + (kShadeClasses - 1);
 }
 

@@ -41,6 +41,17 @@ struct PathState
   float4* out = nullptr;    // final radiance per path (w = 1 when written)
   float4* aovA = nullptr;   // first-hit albedo per path (w = 1 when written)
   float4* aovN = nullptr;   // first-hit normal per path
+  // SH AOV (PRT_AOV_SH), render/path_renderer_stream.h:46-52: the radiance gathered after the
+  // first hit (xyz) with the irradiance scale pi / cos of the first bounce (w); the first
+  // bounce's direction; the first hit's unoccluded direct light scaled to irradiance and its
+  // direction; the path's SH sample (3 float4 per path: the 4 coefficients x RGB); the
+  // irradiance scale of each first-hit shadow ray (per shadow-ray slot).
+  float4* sphL = nullptr;
+  float4* sphWi = nullptr;
+  float4* sphDirL = nullptr;
+  float4* sphDirWi = nullptr;
+  float4* sphOut = nullptr;
+  float* sphDirScale = nullptr;
   int* queue[2] = {nullptr, nullptr};
   int* classQueues = nullptr;  // kShadeClasses queues of `capacity` entries each
   int* counters = nullptr;  // per bounce: input and shadow counts, then the work counters
@@ -127,16 +138,18 @@ struct Context
   std::vector<int> meshTriOffsetHost;
   std::vector<DevMaterial> materialsHost;  // host copies of the uploaded material records
   std::vector<DevTexture> texturesHost;    // device pointers and sizes of the scene's textures
-  DevRenderer renderer{100, 8, 1e-4f, 3.402823466e38f, 0u, 0, 16};
+  DevRenderer renderer{100, 8, 1e-4f, 3.402823466e38f, 0u, 0, 16, 0};
   bool hasRenderer = false;
   DevCamera camera{};
   bool hasCamera = false;
   int width = 0, height = 0, aovMask = 0;
+  bool aovSh = false;             // PRT_AOV_SH: the SH planes of the frame and the path state
   float* accum = nullptr;         // sum rgb + weight per pixel (float4)
   float* accumA = nullptr;        // first-hit albedo sums
   float* accumN = nullptr;        // first-hit normal sums
   float* accumC = nullptr;        // checkpoint: the sums at the last power-of-two sample count
   float* accum2 = nullptr;        // squared samples (PRT_AOV_HDR_VAR)
+  float* accumSH = nullptr;       // SH coefficient sums, 4 planes of float4 (PRT_AOV_SH)
   double* errPartials = nullptr;  // per-block partial sums of the frame error
   int64_t accumCount = 0;         // samples accumulated since the last clear
   int toneType = 0;               // PRT_TONE_*
@@ -153,6 +166,9 @@ struct Context
   int64_t wavePaths = 128ll << 20;
   int topStage = 0;               // stage the top BVH levels in shared memory (frame form)
   int rayBins = 0;                // group each bounce's extended rays by direction octant (frame form)
+  DevMaterial whiteMaterial{};    // irradiance mode: the first hit's material (white Principled)
+  DevMaterial* whiteMaterialDev = nullptr;  // its device copy
+  int whiteClass = 0;             // its shading class
   // Device buffers that stage host memory passed to an entry point (one per buffer argument of
   // a call, reused by later calls and grown when a call needs more; freed with the context).
   std::vector<DevBuf> stage;

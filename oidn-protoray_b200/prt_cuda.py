@@ -292,8 +292,8 @@ class DeviceCuda:
         return nodes, tris
 
     def init_renderer(self, max_depth=100, rr_depth=8, min_weight=1e-4, max_radiance=3.4028234663852886e38,
-                      type=T.PRT_RENDERER_PATH, samples=16):
-        r = T.RendererDesc(max_depth, rr_depth, min_weight, max_radiance, type, samples)
+                      type=T.PRT_RENDERER_PATH, samples=16, flags=0):
+        r = T.RendererDesc(max_depth, rr_depth, min_weight, max_radiance, type, samples, flags)
         self._check(self.lib.prt_cuda_renderer(self.h, C.byref(r)))
 
     def init_sampler(self, seed):
@@ -400,7 +400,8 @@ class DeviceCuda:
         self.init_scene(scene)
         self.init_frame(scene.width, scene.height, aov_mask)
         self.init_camera(scene.camera)
-        self.init_renderer(scene.max_depth, scene.rr_depth, type=scene.renderer_type, samples=scene.ao_samples)
+        self.init_renderer(scene.max_depth, scene.rr_depth, type=scene.renderer_type, samples=scene.ao_samples,
+                           flags=scene.renderer_flags)
         self.init_sampler(seed)
 
     # -- queries --------------------------------------------------------------------------------

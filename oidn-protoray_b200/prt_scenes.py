@@ -47,6 +47,7 @@ class Scene:
         self.rr_depth = 8
         self.renderer_type = T.PRT_RENDERER_PATH
         self.ao_samples = 16
+        self.renderer_flags = 0   # PRT_RENDERER_IRRADIANCE
         self._keep = []
 
     # -- construction ---------------------------------------------------------------------
@@ -132,6 +133,7 @@ class Scene:
         r.min_weight = min_weight
         r.type = self.renderer_type
         r.samples = self.ao_samples
+        r.flags = self.renderer_flags
         r.max_radiance = max_radiance
         return r
 

@@ -19,6 +19,8 @@ PRT_ERR_STATE = -6
 PRT_AOV_ALBEDO1 = 1 << 0
 PRT_AOV_NORMAL1 = 1 << 1
 PRT_AOV_HDR_VAR = 1 << 2
+PRT_AOV_SH = 1 << 3
+PRT_RENDERER_IRRADIANCE = 1
 PRT_ENV_AMBIENT_FIRST = 1
 PRT_MICROFACET_BECKMANN = 1
 PRT_MICROFACET_GGX_VISIBLE = 2
@@ -29,6 +31,10 @@ PRT_BLIT_NORMAL1 = 2
 PRT_BLIT_HDR_VAR = 3
 PRT_BLIT_LDR = 4
 PRT_BLIT_LDR_RGB = 5
+PRT_BLIT_SH0 = 6
+PRT_BLIT_SH1 = 7
+PRT_BLIT_SH2 = 8
+PRT_BLIT_SH3 = 9
 PRT_TONE_NONE = 0
 PRT_TONE_LINEAR = 1
 PRT_TONE_REINHARD = 2
@@ -221,6 +227,7 @@ class RendererDesc(C.Structure):
         ("max_radiance", C.c_float),
         ("type", C.c_int32),
         ("samples", C.c_int32),
+        ("flags", C.c_int32),
     ]
 
 

@@ -241,6 +241,7 @@ int ref_create_file(const char* scene_path, const prt_scene_desc* scene, const p
     if (aov_mask & PRT_AOV_ALBEDO1) frameProps.set("aovAlbedo1");
     if (aov_mask & PRT_AOV_NORMAL1) frameProps.set("aovNormal1");
     if (aov_mask & PRT_AOV_HDR_VAR) frameProps.set("aovHdrVar");
+    if (aov_mask & PRT_AOV_SH) frameProps.set("aovSh");
     h->size = Vec2i(width, height);
     h->device.initFrame(h->size, frameProps);
     Props rprops;
@@ -255,6 +256,7 @@ int ref_create_file(const char* scene_path, const prt_scene_desc* scene, const p
     rprops.set("minWeight", rd->min_weight);
     rprops.set("maxRadiance", rd->max_radiance);
     rprops.set("imageSize", Vec2i(width, height));
+    if (rd->flags & PRT_RENDERER_IRRADIANCE) rprops.set("irradiance");
     Props stats;
     h->device.initRenderer(rprops, stats);
     h->device.initSampler(seed);
@@ -364,6 +366,19 @@ int ref_blit(void* handle, int aov, float* dst)
       aovs.hdrVar = (Vec3f*)dst;
     }
     else if (aov == PRT_BLIT_LDR_RGB) aovs.ldr = (Vec3f*)dst;
+    else if (aov >= PRT_BLIT_SH0 && aov <= PRT_BLIT_SH3)
+    {
+      // sh[1..3] are written relative to sh[0], so all four are blitted together.
+      std::vector<Vec3f> sh[4];
+      for (int k = 0; k < 4; ++k)
+      {
+        sh[k].resize((size_t)h->size.x * h->size.y);
+        aovs.sh[k] = sh[k].data();
+      }
+      h->device.blitFrame(aovs);
+      std::memcpy(dst, sh[aov - PRT_BLIT_SH0].data(), sizeof(Vec3f) * sh[0].size());
+      return 0;
+    }
     else return fail("invalid aov");
     h->device.blitFrame(aovs);
     return 0;

@@ -26,6 +26,8 @@ Fixtures (small, seeded, committed):
   film.npz         sample variance, tone-mapped LDR images and frame errors of the small scene
   bsdf.npz         the reference's Standard-material BSDF (eval, sample) on 512 seeded tuples
                    for each case of tests/bsdf_cases.py
+  sh_img.npz       the SH AOV (four coefficient images) and the irradiance mode's image of the
+                   small scene and the small terrain, 16 spp, seeds 0 and 1
   aov_img.npz      first-hit albedo1 and normal1 AOVs with the HDR image: the small scene and the
                    small terrain, 16 spp, seeds 0 and 1
   sunsky_t3_e30.npz, sunsky_t5_e60.npz  the reference's sun-sky products (sun radiance and angle,
@@ -249,6 +251,30 @@ def make_aovs():
 SUNSKY_SETS = [(30.0, 3.0), (60.0, 5.0)]
 
 
+def make_sh_images():
+    """The SH AOV (aovSh: four coefficient images) with the HDR image, and the irradiance mode's
+    HDR image, of the small scene (128x128) and the small terrain (128x64, sun-sky), 16 spp,
+    seeds 0 and 1."""
+    out = {}
+    for name, make in (("cornell", lambda: small_scene(128, 128, 16)), ("terrain", lambda: small_terrain(16))):
+        for seed in (0, 1):
+            dev = ref.RefDevice(make(), seed=seed, aov_mask=T.PRT_AOV_SH)
+            st = dev.render(16)
+            out[f"{name}_seed{seed}_hdr"] = dev.blit(T.PRT_BLIT_HDR)
+            for k in range(4):
+                out[f"{name}_seed{seed}_sh{k}"] = dev.blit(T.PRT_BLIT_SH0 + k)
+            out[f"{name}_seed{seed}_rays"] = np.float64(st["rays"])
+            dev.close()
+            s = make()
+            s.renderer_flags = T.PRT_RENDERER_IRRADIANCE
+            dev = ref.RefDevice(s, seed=seed)
+            st = dev.render(16)
+            out[f"{name}_seed{seed}_irradiance"] = dev.blit(T.PRT_BLIT_HDR)
+            out[f"{name}_seed{seed}_irradiance_rays"] = np.float64(st["rays"])
+            dev.close()
+    np.savez_compressed(OUT / "sh_img.npz", **out)
+
+
 def make_sunsky():
     for elevation, turbidity in SUNSKY_SETS:
         params = prt_scenes.sunsky_params(elevation, turbidity=turbidity)
@@ -274,7 +300,9 @@ def make_terrain_e60_images():
 
 if __name__ == "__main__":
     which = sys.argv[1:] or ["sobol", "rays", "images", "sunsky", "bsdf", "terrain", "lobes", "translucent", "siblings",
-                             "film", "mesh", "aovs", "terrain_e60"]
+                             "film", "mesh", "aovs", "terrain_e60", "sh"]
+    if "sh" in which:
+        make_sh_images()
     if "terrain_e60" in which:
         make_terrain_e60_images()
     if "aovs" in which:

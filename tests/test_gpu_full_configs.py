@@ -81,3 +81,22 @@ def test_cornell_full_size_converged_gate(device, golden):
     assert abs(st["rays"] / float(z["seed0_rays"]) - 1.0) < 0.002
     other, _ = render(device, scene, seed=2, spp=spp)
     assert rel_mse(other, z["seed0"]) <= 1.5 * seeds, (rel_mse(other, z["seed0"]), seeds)
+
+
+def test_terrain_full_size_converged_gate(device, golden):
+    """The terrain workload's own frame (1920x1080, depth 8, RR from depth 3, sun-sky) at the
+    fixture's sample count (tests/golden/make_converged.py): the GPU's same-seed image follows the
+    reference's far closer than two seeds do, and another seed's image is within 1.5x the
+    reference's own seed-0/seed-1 relMSE of the reference's seed-0 image. Glass caustics make the
+    single-seed images firefly-prone, in the reference as well."""
+    z = golden("terrain_full.npz")
+    spp = int(z["spp"])
+    ref0 = z["seed0"].astype(np.float32)
+    seeds = float(z["seed_to_seed"])
+    scene = prt_scenes.terrain(seed=0, spp=spp)
+    same, st = render(device, scene, seed=0, spp=spp)
+    assert np.isfinite(same).all()
+    assert rel_mse(same, ref0) < 0.25 * seeds, (rel_mse(same, ref0), seeds)
+    assert abs(st["rays"] / float(z["seed0_rays"]) - 1.0) < 0.01
+    other, _ = render(device, scene, seed=2, spp=spp)
+    assert rel_mse(other, ref0) <= 1.5 * seeds, (rel_mse(other, ref0), seeds)

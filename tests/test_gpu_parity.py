@@ -220,3 +220,42 @@ def test_terrain_second_sun_same_seed_tracks_oracle(device, golden):
     other = rel_mse(z["spp16_seed1"], z["spp16_seed0"])
     assert same < 0.5 * other, (same, other)
     assert abs(st["rays"] / float(z["spp16_seed0_rays"]) - 1.0) < 0.02
+
+
+@pytest.mark.parametrize("name", ["cornell", "terrain"])
+def test_sh_aov_and_irradiance_mode_track_oracle(device, golden, name):
+    """The SH AOV (aovSh, render/path_renderer_stream.h:46-52, 329-344, 705-709, 914-930,
+    980-1059) and the irradiance mode (the first hit shaded with a white Principled material, no
+    environment seen by camera rays, :130-139, 304, 598), same seed: band 0 and the image follow the
+    reference's far closer than two seeds do (relMSE < 0.5 x seed-to-seed); bands 1-3 (direction
+    moments relative to band 0) have a mean absolute difference under half the seed-to-seed one."""
+    z = golden("sh_img.npz")
+    scene = aov_scenes()[name]
+    device.setup(scene, seed=0, aov_mask=T.PRT_AOV_SH)
+    device.clear_frame()
+    st = device.render(16)
+    assert abs(st["rays"] / float(z[f"{name}_seed0_rays"]) - 1.0) < 0.02
+    hdr = device.blit_frame()
+    assert rel_mse(hdr, z[f"{name}_seed0_hdr"]) < 0.5 * rel_mse(z[f"{name}_seed1_hdr"], z[f"{name}_seed0_hdr"])
+    sh0 = device.blit_frame(T.PRT_BLIT_SH0)
+    ref0, other0 = z[f"{name}_seed0_sh0"], z[f"{name}_seed1_sh0"]
+    assert np.isfinite(sh0).all() and sh0.mean() > 0
+    assert rel_mse(sh0, ref0) < 0.5 * rel_mse(other0, ref0), (rel_mse(sh0, ref0), rel_mse(other0, ref0))
+    for k in (1, 2, 3):
+        shk = device.blit_frame(T.PRT_BLIT_SH0 + k).astype(np.float64)
+        ref_k, other_k = z[f"{name}_seed0_sh{k}"], z[f"{name}_seed1_sh{k}"]
+        same = np.abs(shk - ref_k).mean()
+        seeds = np.abs(other_k.astype(np.float64) - ref_k).mean()
+        assert same < 0.5 * seeds, (k, same, seeds)
+    # Irradiance mode.
+    device.setup(scene, seed=0)
+    device.init_renderer(scene.max_depth, scene.rr_depth, flags=T.PRT_RENDERER_IRRADIANCE)
+    device.init_sampler(0)
+    device.clear_frame()
+    st = device.render(16)
+    img = device.blit_frame()
+    ref_i, other_i = z[f"{name}_seed0_irradiance"], z[f"{name}_seed1_irradiance"]
+    assert rel_mse(img, ref_i) < 0.5 * rel_mse(other_i, ref_i), (rel_mse(img, ref_i), rel_mse(other_i, ref_i))
+    assert abs(st["rays"] / float(z[f"{name}_seed0_irradiance_rays"]) - 1.0) < 0.02
+    # The irradiance image differs from the plain render (white first hits, no direct sky).
+    assert rel_mse(img, z[f"{name}_seed0_hdr"]) > 2.0 * rel_mse(other_i, ref_i)
