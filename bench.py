@@ -45,8 +45,8 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--spp", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--inverse-steps", type=int, default=5,
-                    help="Adam steps of the batched inverse-rendering measurement")
+    ap.add_argument("--inverse-steps", type=int, default=100,
+                    help="Adam steps of the batched inverse-rendering measurement (the workload's 100)")
     ap.add_argument("--headline-only", action="store_true",
                     help="skip the small-scene, batched and adjoint measurements")
     ap.add_argument("--traffic-csv", default=None,
@@ -508,7 +508,7 @@ def adjoint_bench(dev, repeats=3):
             "gradients_per_s": 1e3 / a_ms, "parameters": n_params}
 
 
-def inverse_batched_bench(dev, count=16, steps=5, lr=1e-2):
+def inverse_batched_bench(dev, count=16, steps=100, lr=1e-2):
     """Batched differentiable workload: 16 terrain inverse-rendering problems (100k-1M
     triangles, 512x512, 16 spp, depth 6), each optimising a 512^2 RGB albedo texture on its
     terrain and the roughness of every sphere against a target render (L2 loss). One step =

@@ -575,6 +575,11 @@ int prt_cuda_microfacet_query(prt_context* ctx, int32_t distribution, int64_t n,
  * `capacity` floats and returns the total count through *count. */
 int prt_cuda_albedo_tables(prt_context* ctx, float* out, int64_t capacity, int64_t* count);
 
+/* Diagnostic: replaces the context's energy-compensation tables with `tables` (count floats, in
+ * the layout of prt_cuda_albedo_tables), e.g. the reference's own, for parity studies that
+ * separate the BSDF arithmetic from the tables' values. */
+int prt_cuda_set_albedo_tables(prt_context* ctx, const float* tables, int64_t count);
+
 /* Host-only (no GPU needed): builds the BVH8 over tri_count triangles given as 9 floats each
  * (v0, v1, v2) and walks it with the counting traversal, the scalar twin of the closest-hit
  * kernel. For each of the n rays (8 floats) writes the global triangle index (-1 on a miss)

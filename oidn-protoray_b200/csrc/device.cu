@@ -400,6 +400,9 @@ void buildEnvLights(Context& c, DevScene& sc, const prt_env_desc& e)
   }
   sc.envCount = ne;
   sc.lightCount = sc.areaLightCount + ne;
+  sc.distantLight = -1;
+  for (int k = 0; k < ne; ++k)
+    if (sc.env[k].kind == kEnvDistant) sc.distantLight = sc.areaLightCount + k;
   std::vector<float> lightCdf(sc.lightCount + 1);
   cdfInit(lightCdf.data(), lightPower.data(), sc.lightCount);
   sc.lightCdf = upload(c, lightCdf, &c.envBufs);
@@ -1435,6 +1438,19 @@ int prt_cuda_albedo_tables(prt_context* ctx, float* out, int64_t capacity, int64
     if (capacity > head)
       cuCheck(cudaMemcpy(out + head, c.tables.sheenDir, sizeof(float) * std::min<int64_t>(capacity - head, 16 * 16),
                          cudaMemcpyDeviceToHost), "table copy");
+  });
+}
+
+int prt_cuda_set_albedo_tables(prt_context* ctx, const float* tables, int64_t count)
+{
+  return guarded(ctx, [&](Context& c) {
+    const int64_t head = 32 * 32 + 32 + 3 * (16 * 16 * 16 + 16 * 16);
+    if (!tables || count != head + 16 * 16) throw std::invalid_argument("expected the tables of prt_cuda_albedo_tables");
+    cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
+    cuCheck(cudaStreamSynchronize(c.stream), "sync");
+    cuCheck(cudaMemcpy(c.tableStorage, tables, sizeof(float) * head, cudaMemcpyHostToDevice), "table copy");
+    cuCheck(cudaMemcpy(const_cast<float*>(c.tables.sheenDir), tables + head, sizeof(float) * 16 * 16,
+                       cudaMemcpyHostToDevice), "table copy");
   });
 }
 

@@ -157,6 +157,7 @@ struct DevScene
   const float* areaCdf;
   const float* etris;            // 16 floats per emissive triangle: v0 v1 v2 normal color pad
   int envCount;
+  int distantLight;              // light index of the distant environment light, -1 if none
   DevEnvLight env[4];
   DevImageLight image;
   // Media (material/medium.h): transmittance colour and IOR per medium id.

@@ -198,6 +198,16 @@ __global__ void kBsdfQuery(DevTables tab, DevMaterial m, int mediumId, int64_t n
 //    slot to the free list, and kBatchRegen refills free slots with new camera paths.
 
 // Per-path view of the scene, renderer and frame a path belongs to.
+// Per-bounce counter block (ints): [0] paths entering the bounce, [1..kShadeClasses] paths per
+// shading class, [kCntShadow] shadow rays, [kCntWorkTrace], [kCntWorkShadow] work counters, [kCntShadowSun] shadow
+// rays toward the distant light (frame form).
+constexpr int kCntShadow = 1 + kShadeClasses;
+constexpr int kCntWorkTrace = kCntShadow + 1;
+constexpr int kCntWorkShadow = kCntShadow + 2;
+constexpr int kCntShadowSun = kCntShadow + 3;
+constexpr int kCntStride = 16;
+static_assert(kCntShadowSun < kCntStride, "counter block");
+
 template <bool Batch>
 struct PathEnv;
 
@@ -591,7 +601,10 @@ template <bool Count, bool Batch, bool Top = false, bool Transp = false>
 __global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__ count, int* __restrict__ work,
                                                int parity, int depth)
 {
-  const int n = *count;
+  // Frame form: the front region holds count[0] rays, the back region (from the last slot down)
+  // the distant light's count[kCntShadowSun - kCntShadow]; work item j maps to front j or back.
+  const int nFront = *count;
+  const int n = Batch ? nFront : nFront + count[kCntShadowSun - kCntShadow];
   const int top = stageTopNodes<Top && !Batch>(L);
   TraceCount tc;
   for (;;)
@@ -600,10 +613,11 @@ __global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__
     if (laneId() == 0) base = atomicAdd(work, 32);
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= n) break;
-    const int i = base + laneId();
+    const int j = base + laneId();
+    const int i = j < nFront ? j : (int)(L.ps.capacity - 1 - (j - nFront));
     bool freed = false;
     int p = 0;
-    if (i < n)
+    if (j < n)
     {
       const float4 a = L.ps.shO[i], b = L.ps.shD[i], c = L.ps.shL[i];
       const uint32_t tag = __float_as_uint(c.w);
@@ -765,6 +779,7 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
     uint32_t extTag = 0u;  // direction octant of the extended ray, in the queue entry's top bits
     float4 shO = make_float4(0.f, 0.f, 0.f, 0.f), shD = shO, shL = shO;
     float shScale = 0.f;   // SH AOV: irradiance scale of a first-hit shadow ray
+    bool toSun = false;    // the shadow ray goes to the distant light
     if (active)
     {
       const float4 ro = L.ps.rayO[p], rd = L.ps.rayD[p], hh = L.ps.hit[p];
@@ -813,7 +828,9 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
         sobolGet3D(st, sampleDim + kDimLight, lx, ly, lz);
         f3 wi;
         float lightPdf, dist;
-        const f3 Lw = sampleLight(E.sc, ctx.p, lx, ly, lz, wi, lightPdf, dist);
+        int light;
+        const f3 Lw = sampleLight(E.sc, ctx.p, lx, ly, lz, wi, lightPdf, dist, light);
+        toSun = light == E.sc.distantLight;
         if (reduceMax(Lw) > 0.f && lightPdf > 0.f)
         {
           float bsdfPdf;
@@ -922,7 +939,14 @@ __global__ void __launch_bounds__(256) kShadeSurface(Launch L, const int* __rest
     }
     const int e = warpAppend(extCount, extend);
     if (extend) queueOut[e] = (int)((uint32_t)p | extTag);
-    const int sidx = warpAppend(shadowCount, shadow);
+    // Frame form: shadow rays toward the distant light fill the shadow arrays from the back
+    // (counter kCntShadowSun), the others from the front, so that a warp of the shadow kernel
+    // takes rays of one kind: the distant light's rays are parallel and their traversal coherent.
+    // The two regions never meet: together they hold at most one ray per path of this bounce.
+    const bool sunQueue = !Batch && !Adj && toSun;
+    const int front = warpAppend(shadowCount, shadow && !sunQueue);
+    const int back = Batch ? 0 : warpAppend(shadowCount + (kCntShadowSun - kCntShadow), shadow && sunQueue);
+    const int sidx = sunQueue ? (int)(L.ps.capacity - 1 - back) : front;
     if (shadow)
     {
       L.ps.shO[sidx] = shO;
@@ -1438,14 +1462,6 @@ struct TimedLaunch
   int kind;  // 0 trace, 1 shadow, 2 shade
 };
 
-// Per-bounce counter block (ints): [0] paths entering the bounce, [1..kShadeClasses] paths per
-// shading class, [kCntShadow] shadow rays, [kCntWorkTrace], [kCntWorkShadow] work counters.
-constexpr int kCntShadow = 1 + kShadeClasses;
-constexpr int kCntWorkTrace = kCntShadow + 1;
-constexpr int kCntWorkShadow = kCntShadow + 2;
-constexpr int kCntStride = 16;
-static_assert(kCntWorkShadow < kCntStride, "counter block");
-
 // Launches one surface-shading kernel per feature class (the class list is kShadeClassFeatures).
 template <int... Fs>
 struct ShadeLaunch;
@@ -1568,12 +1584,15 @@ static cudaError_t bounceLoop(Context& ctx, const Launch& L, int P, bool replay,
     // Paths in, shadow rays and paths out of this bounce; stop once no path is left.
     int in = 0, shadow = 0, out = 0;
     e = cudaMemcpyAsync(&in, cnt, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream);
+    int shadowSun = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&shadow, cnt + kCntShadow, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(&shadowSun, cnt + kCntShadowSun, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&out, next, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx.stream);
     if (e != cudaSuccess) return e;
     rc.closestRays += in;
-    rc.shadowRays += shadow;
+    rc.shadowRays += shadow + shadowSun;
     if (out == 0) break;
   }
   return cudaSuccess;

@@ -382,12 +382,15 @@ PRT_D f3 sampleOneLight(const DevScene& sc, int l, f3 p, float sx, float sy, flo
 }
 
 // Scene::sampleLight (render/scene.h:215-250).
-PRT_D f3 sampleLight(const DevScene& sc, f3 p, float sx, float sy, float sz, f3& wi, float& pdf, float& dist)
+PRT_D f3 sampleLight(const DevScene& sc, f3 p, float sx, float sy, float sz, f3& wi, float& pdf, float& dist,
+                     int& light)
 {
+  light = 0;
   if (sc.lightCount == 1) return sampleOneLight(sc, 0, p, sx, sy, sz, wi, pdf, dist);
   float pickProb;
   float s = sz;
   const int l = cdfSampleReuse(sc.lightCdf, sc.lightCount, pickProb, s);
+  light = l;
   const f3 w = sampleOneLight(sc, l, p, sx, sy, s, wi, pdf, dist);
   pdf *= pickProb;
   return w * (1.f / pickProb);

@@ -10,10 +10,11 @@
 // block each, inserted at the start of the classes' public section).
 //
 // Behaviour that differs from DeviceCpu, each reported with the reference's exception types:
-// * renderer types: pathStream, primaryStream, aoStream, diffuseStream, diffuse2Stream and
-//   their ...Fast variants (render/renderer_factory_stream.cpp:54-71); the sampler is
-//   sobolBurley; other types and samplers are std::invalid_argument;
-// * frame AOVs: hdr, hdrVar, ldr, albedo1, normal1; requesting another AOV in initFrame is
+// * renderer types: pathStream (with its irradiance option), primaryStream, aoStream,
+//   diffuseStream, diffuse2Stream and their ...Fast variants (render/renderer_factory_stream.cpp:
+//   54-71); the sampler is sobolBurley; other types and samplers, and the static option, are
+//   std::invalid_argument;
+// * frame AOVs: hdr, hdrVar, ldr, albedo1, normal1, sh; requesting another AOV in initFrame is
 //   std::invalid_argument; pixel filters other than box are std::invalid_argument;
 // * lights: at most one distant light and one image light reach the device, so a
 //   distantLight together with a sunSkyLight (two distant lights), or an imageLight together
@@ -210,10 +211,12 @@ public:
     if (t < 0) throw std::invalid_argument("renderer type not supported by the CUDA device: " + type);
     const std::string sampler = props.get("sampler", "sobolBurley");
     if (sampler != "sobolBurley") throw std::invalid_argument("sampler not supported by the CUDA device: " + sampler);
-    if (props.exists("irradiance") || props.exists("static"))
-      throw std::invalid_argument("the CUDA device renders the standard (non-static, radiance) path tracer");
-    const prt_renderer_desc r{props.get("maxDepth", 100), props.get("rrDepth", 8), props.get("minWeight", 1e-4f),
-                              props.get("maxRadiance", float(posMax)), t, props.get("samples", 16)};
+    if (props.exists("static")) throw std::invalid_argument("the CUDA device advances the sample index every render");
+    const int flags = props.exists("irradiance") ? PRT_RENDERER_IRRADIANCE : 0;
+    const prt_renderer_desc r{props.get("maxDepth", 100),          props.get("rrDepth", 8),
+                              props.get("minWeight", 1e-4f),       props.get("maxRadiance", float(posMax)),
+                              t,                                   props.get("samples", 16),
+                              flags};
     check(prt_cuda_renderer(ctx, &r));
     samplerType = sampler;
     stats.set("device", getInfo());
@@ -302,13 +305,13 @@ public:
   {
     static const char* kUnsupported[] = {"aovHdrUnclamp", "aovAlbedo", "aovDiffuseAlbedo", "aovDiffuseAlbedo1",
                                          "aovSpecularAlbedo", "aovSpecularAlbedo1", "aovNormal", "aovDepth",
-                                         "aovHWDepth", "aovRoughness", "aovRoughness1", "aovAlpha", "aovSh",
+                                         "aovHWDepth", "aovRoughness", "aovRoughness1", "aovAlpha",
                                          "aovMotionBack", "aovMotionFore"};
     for (const char* k : kUnsupported)
       if (props.exists(k)) throw std::invalid_argument(std::string("AOV not supported by the CUDA device: ") + k);
     const int aov = (props.exists("aovAlbedo1") ? PRT_AOV_ALBEDO1 : 0) |
                     (props.exists("aovNormal1") ? PRT_AOV_NORMAL1 : 0) |
-                    (props.exists("aovHdrVar") ? PRT_AOV_HDR_VAR : 0);
+                    (props.exists("aovHdrVar") ? PRT_AOV_HDR_VAR : 0) | (props.exists("aovSh") ? PRT_AOV_SH : 0);
     check(prt_cuda_frame(ctx, s.x, s.y, aov));
     size = s;
     aovMask = aov;
@@ -356,6 +359,12 @@ public:
     if (dest.ldr) check(prt_cuda_blit(ctx, PRT_BLIT_LDR_RGB, &dest.ldr->x));
     if (dest.albedo1) check(prt_cuda_blit(ctx, PRT_BLIT_ALBEDO1, &dest.albedo1->x));
     if (dest.normal1) check(prt_cuda_blit(ctx, PRT_BLIT_NORMAL1, &dest.normal1->x));
+    for (int k = 0; k < 4; ++k)
+      if (dest.sh[k])
+      {
+        if (!(aovMask & PRT_AOV_SH)) throw std::invalid_argument("sh needs aovSh in initFrame");
+        check(prt_cuda_blit(ctx, PRT_BLIT_SH0 + k, &dest.sh[k]->x));
+      }
   }
 
   void blitFrameLdr(Surface&, const float*, float, float) override

@@ -98,6 +98,7 @@ def load_library():
     lib.prt_cuda_scene_load.argtypes = [vp, C.c_char_p, P(T.EnvDesc), C.c_int32]
     lib.prt_cuda_scene_lights.argtypes = [vp, P(T.EnvDesc)]
     lib.prt_cuda_microfacet_query.argtypes = [vp, C.c_int32, C.c_int64, P(C.c_float), P(C.c_float)]
+    lib.prt_cuda_set_albedo_tables.argtypes = [vp, P(C.c_float), C.c_int64]
     _lib = lib
     return lib
 
@@ -444,6 +445,11 @@ class DeviceCuda:
         out = np.zeros((t.shape[0], 4), np.float32)
         self._check(self.lib.prt_cuda_microfacet_query(self.h, distribution, t.shape[0], T.fptr(t), T.fptr(out)))
         return out
+
+    def set_albedo_tables(self, tables):
+        """Replaces the context's energy-compensation tables (layout of albedo_tables())."""
+        t = np.ascontiguousarray(tables, np.float32)
+        self._check(self.lib.prt_cuda_set_albedo_tables(self.h, T.fptr(t), t.size))
 
     def albedo_tables(self):
         n = C.c_int64(0)
