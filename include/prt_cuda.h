@@ -420,6 +420,9 @@ typedef struct prt_tuning
                           global memory (the default); 0 keeps the current value */
   int32_t ray_bins;    /* 1: each bounce's extended rays are traced grouped by direction octant;
                           2: in the order shading produced them (the default); 0 keeps */
+  int32_t trace_stack; /* node-group stack entries of the traversal kernels: 24 (the default)
+                          takes the 24-entry instantiation for trees of at most 24 wide levels
+                          and the 48-entry one otherwise; 48 always the 48-entry one; 0 keeps */
 } prt_tuning;
 
 int prt_cuda_set_tuning(prt_context* ctx, const prt_tuning* tuning);
@@ -575,9 +578,12 @@ int prt_cuda_microfacet_query(prt_context* ctx, int32_t distribution, int64_t n,
  * `capacity` floats and returns the total count through *count. */
 int prt_cuda_albedo_tables(prt_context* ctx, float* out, int64_t capacity, int64_t* count);
 
-/* Diagnostic: replaces the context's energy-compensation tables with `tables` (count floats, in
- * the layout of prt_cuda_albedo_tables), e.g. the reference's own, for parity studies that
- * separate the BSDF arithmetic from the tables' values. */
+/* Replaces the context's energy-compensation tables with `tables` (count floats, in the layout of
+ * prt_cuda_albedo_tables): the reference application's own, which prt::DeviceCuda uploads at
+ * construction (the tables the context builds agree with them to ~2e-6, and the compensation
+ * terms of rough dielectrics amplify a table's last digits by 1 / (1 - E_avg)), or any other set
+ * for parity studies that separate the BSDF arithmetic from the tables' values. Synchronous;
+ * takes effect from the next render or query. */
 int prt_cuda_set_albedo_tables(prt_context* ctx, const float* tables, int64_t count);
 
 /* Host-only (no GPU needed): builds the BVH8 over tri_count triangles given as 9 floats each

@@ -7,6 +7,7 @@
 // trapezoid rule over 1025 points (integrateAvg, bsdf/albedo_tables.cpp:20-31).
 #include "bsdf.cuh"
 #include "runtime.h"
+#include "host_rcp.h"
 
 namespace prt {
 
@@ -182,12 +183,16 @@ cudaError_t buildAlbedoTables(DevTables& t, float** storage)
   float* sheenDir = take(t2);
   kGgxTable<<<(g2 + 127) / 128, 128>>>(ggxDir);
   kAvg<<<1, kGgxTableSize>>>(ggxDir, ggxAvg, kGgxTableSize, kGgxTableSize);
+  // The eta <= 1 axes run over [rcp(maxIor), rcp(minIor)] with the reference CPU build's rcp
+  // (bsdf/albedo_tables.cpp:96-97,111-112), which puts the last slice at 0.99999994 on x86-64.
   const float minIor = 1.f, maxIor = 3.f;
-  kDielTable<<<(t3 + 127) / 128, 128>>>(dielEtaDir, 1.f / maxIor, 1.f / minIor, 0);
+  t.etaLo = hostRcp(maxIor);
+  t.etaHi = hostRcp(minIor);
+  kDielTable<<<(t3 + 127) / 128, 128>>>(dielEtaDir, t.etaLo, t.etaHi, 0);
   kAvg<<<(t2 + 127) / 128, 128>>>(dielEtaDir, dielEtaAvg, t2, kTableSize);
   kDielTable<<<(t3 + 127) / 128, 128>>>(dielRcpDir, minIor, maxIor, 0);
   kAvg<<<(t2 + 127) / 128, 128>>>(dielRcpDir, dielRcpAvg, t2, kTableSize);
-  kDielTable<<<(t3 + 127) / 128, 128>>>(reflDir, 1.f / maxIor, 1.f / minIor, 1);
+  kDielTable<<<(t3 + 127) / 128, 128>>>(reflDir, t.etaLo, t.etaHi, 1);
   kAvg<<<(t2 + 127) / 128, 128>>>(reflDir, reflAvg, t2, kTableSize);
   kSheenTable<<<(t2 + 127) / 128, 128>>>(sheenDir);
   e = cudaGetLastError();

@@ -101,8 +101,7 @@ PRT_D float dielAlbedo(const DevTables& t, float cosThetaO, float eta, float rou
   const float k = (float)(kTableSize - 1);
   if (eta <= 1.f)
   {
-    const float minEta = 1.f / 3.f, maxEta = 1.f;
-    const float e = (eta - minEta) / (maxEta - minEta);
+    const float e = (eta - t.etaLo) / (t.etaHi - t.etaLo);
     return interp3D(t.dielEtaDir, kTableSize, cosThetaO * k, e * k, roughness * k);
   }
   const float e = (eta - 1.f) / (3.f - 1.f);
@@ -114,7 +113,7 @@ PRT_D float dielAlbedoAvg(const DevTables& t, float eta, float roughness)
   const float k = (float)(kTableSize - 1);
   if (eta <= 1.f)
   {
-    const float e = (eta - 1.f / 3.f) / (1.f - 1.f / 3.f);
+    const float e = (eta - t.etaLo) / (t.etaHi - t.etaLo);
     return interp2D(t.dielEtaAvg, kTableSize, e * k, roughness * k);
   }
   const float e = (eta - 1.f) / (3.f - 1.f);
@@ -125,7 +124,7 @@ PRT_D float dielAlbedoAvg(const DevTables& t, float eta, float roughness)
 PRT_D float reflAlbedo(const DevTables& t, float cosThetaO, float eta, float roughness)
 {
   const float k = (float)(kTableSize - 1);
-  const float e = (eta - 1.f / 3.f) / (1.f - 1.f / 3.f);
+  const float e = (eta - t.etaLo) / (t.etaHi - t.etaLo);
   return interp3D(t.reflDir, kTableSize, cosThetaO * k, e * k, roughness * k);
 }
 
@@ -139,7 +138,7 @@ PRT_D float sheenAlbedo(const DevTables& t, float cosThetaO, float roughness)
 PRT_D float reflAlbedoAvg(const DevTables& t, float eta, float roughness)
 {
   const float k = (float)(kTableSize - 1);
-  const float e = (eta - 1.f / 3.f) / (1.f - 1.f / 3.f);
+  const float e = (eta - t.etaLo) / (t.etaHi - t.etaLo);
   return interp2D(t.reflAvg, kTableSize, e * k, roughness * k);
 }
 
@@ -245,13 +244,8 @@ PRT_D float fresnelDielectricEx(float cosI, float& cosT, float eta)
   return fresnelDielectric(cosI, cosT, eta);
 }
 
-PRT_D float fresnelDielectricAvg(float eta)
-{
-  const float r = 1.f / eta;
-  if (r >= 1.f) return (r - 1.f) / (4.08567f + 1.00071f * r);
-  const float r2 = r * r, r3 = r2 * r;
-  return 0.997118f + 0.1014f * r - 0.965241f * r2 - 0.130607f * r3;
-}
+// fresnelDielectricAvg (bsdf/optics.h:137-149) depends on eta alone; it is evaluated on the host
+// per material and side (DevEta::favg, favgRcp).
 
 PRT_D float refractCos(float cosI, float eta)
 {
@@ -483,24 +477,26 @@ struct ConductorLobe
 // eta = etaExt / etaInt as seen from the side wo is on.
 struct DielectricLobe
 {
-  float eta;
+  float eta, rcpEta, rcpEta2;
   GGX mf;
   float roughness;
   float EavgEta, EavgRcpEta, fmsRatio;
   bool rough;
 
-  PRT_D void init(const DevTables& t, float e, float rgh, bool isRough)
+  PRT_D void init(const DevTables& t, const DevEta& e, float rgh, bool isRough)
   {
-    eta = e;
+    eta = e.eta;
+    rcpEta = e.rcpEta;
+    rcpEta2 = e.rcpEta2;
     rough = isRough;
     roughness = rgh;
     mf.ax = mf.ay = roughnessToAlpha(rgh);
     if (rough)
     {
       EavgEta = dielAlbedoAvg(t, eta, rgh);
-      EavgRcpEta = dielAlbedoAvg(t, 1.f / eta, rgh);
-      const float FavgEta = fresnelDielectricAvg(eta);
-      const float FavgRcpEta = fresnelDielectricAvg(1.f / eta);
+      EavgRcpEta = dielAlbedoAvg(t, rcpEta, rgh);
+      const float FavgEta = e.favg;
+      const float FavgRcpEta = e.favgRcp;
       const float a = (1.f - FavgEta) * (1.f / (1.f - EavgRcpEta));
       const float b = (1.f - FavgRcpEta) * (1.f / (1.f - EavgEta));
       const float x = b * (1.f / (a + b));
@@ -537,7 +533,7 @@ struct DielectricLobe
     }
     else
     {
-      pdf = (1.f - F) * (1.f / sqr(eta)) * fabsf(cosThetaIH) * (1.f / sqr(cosThetaOH + (1.f / eta) * cosThetaIH));
+      pdf = (1.f - F) * rcpEta2 * fabsf(cosThetaIH) * (1.f / sqr(cosThetaOH + rcpEta * cosThetaIH));
       value = pdf * fabsf(cosThetaOH) * (1.f / cosThetaO);
     }
     const f3 wo0 = toLocal(fr, wo), wi0 = toLocal(fr, wi), wh0 = toLocal(fr, wh);
@@ -558,7 +554,7 @@ struct DielectricLobe
       return fmsRatio * (1.f - Eo) * (1.f - Ei) * (1.f / (kPi * (1.f - EavgEta))) * cosThetaI;
     }
     const float c = fabsf(cosThetaI);
-    const float Ei = dielAlbedo(t, c, 1.f / eta, roughness);
+    const float Ei = dielAlbedo(t, c, rcpEta, roughness);
     fmsPdf = (1.f - fmsRatio) * (c * kInvPi);
     return (1.f - fmsRatio) * (1.f - Eo) * (1.f - Ei) * (1.f / (kPi * (1.f - EavgRcpEta))) * c;
   }
@@ -662,9 +658,9 @@ struct CoatLayer
   float scale;
   bool rough;
 
-  PRT_D void init(const DevTables& t, float e, f3 col, float thick, float rgh, bool isRough, float s)
+  PRT_D void init(const DevTables& t, const DevEta& e, f3 col, float thick, float rgh, bool isRough, float s)
   {
-    eta = e <= 1.f ? e : 1.f / e;
+    eta = e.eta <= 1.f ? e.eta : e.rcpEta;
     color = col;
     thickness = thick;
     rough = isRough;
@@ -673,7 +669,7 @@ struct CoatLayer
     scale = s;
     // The reference evaluates the averages with the constructor argument (before the
     // eta <= 1 fold) and the scale.
-    avg = (rough ? reflAlbedoAvg(t, e, rgh) : fresnelDielectricAvg(e)) * s;
+    avg = (rough ? reflAlbedoAvg(t, e.eta, rgh) : e.favg) * s;
   }
 
   PRT_D int flags(int baseFlags) const { return baseFlags | (rough ? kGlossyReflection : kSpecularReflection); }
@@ -1045,9 +1041,9 @@ struct ThinDielectricLobe
   float Eavg, fmsScale;
   bool rough;
 
-  PRT_D void init(const DevTables& t, float e, f3 col, float thick, float rgh, bool isRough)
+  PRT_D void init(const DevTables& t, const DevEta& e, f3 col, float thick, float rgh, bool isRough)
   {
-    eta = e;
+    eta = e.eta;
     color = col;
     thickness = thick;
     rough = isRough;
@@ -1056,7 +1052,7 @@ struct ThinDielectricLobe
     if (rough)
     {
       Eavg = ggxAlbedoAvg(t, rgh);
-      const float Favg = fresnelDielectricAvg(eta);
+      const float Favg = e.favg;
       fmsScale = Favg * (1.f - Eavg) * (1.f / (1.f - Favg * Eavg));
     }
   }
@@ -1678,8 +1674,7 @@ PRT_D void resolveStandard(const DevScene& sc, const DevTables& t, const DevMate
   if ((F & (kFeatOpaque | kFeatDielectric | kFeatThin | kFeatTransparent)) && dielectric > kMatEps)
   {
     const float transmission = clamp01(m.transmissionWeight);
-    float eta = fromOutside ? m.ambientIor * (1.f / m.specularIor) : m.specularIor * (1.f / m.ambientIor);
-    eta = fminf(fmaxf(eta, 1.f / 3.f), 3.f);
+    const DevEta& eta = m.spec[fromOutside ? 0 : 1];
     const float opaque = dielectric * (1.f - transmission);
     if ((F & kFeatOpaque) && opaque > kMatEps)
     {
@@ -1765,8 +1760,7 @@ PRT_D void resolveStandard(const DevScene& sc, const DevTables& t, const DevMate
   const float coat = clamp01(m.coatWeight);
   if ((F & kFeatCoat) && coat > kMatEps && fabsf(m.coatIor - m.ambientIor) > kMatEps)
   {
-    float coatEta = fromOutside ? m.ambientIor * (1.f / m.coatIor) : m.coatIor * (1.f / m.ambientIor);
-    coatEta = fminf(fmaxf(coatEta, 1.f / 3.f), 3.f);
+    const DevEta& coatEta = m.coat[fromOutside ? 0 : 1];
     const f3 coatColor = clamp01(mk(m.coatColor[0], m.coatColor[1], m.coatColor[2]));
     b.coat.init(t, coatEta, coatColor, m.coatThickness, clamp01(m.coatRoughness), m.hasCoatRoughness != 0, coat);
     b.hasCoat = true;
@@ -1817,10 +1811,8 @@ PRT_D f3 standardTransparency(const DevScene& sc, const DevTables& t, const DevM
       {
         if (m.thinWalled)
         {
-          float eta = m.ambientIor * (1.f / m.specularIor);
-          eta = fminf(fmaxf(eta, 1.f / 3.f), 3.f);
           ThinDielectricLobe thin;
-          thin.init(t, eta, mk(m.transmissionColor[0], m.transmissionColor[1], m.transmissionColor[2]),
+          thin.init(t, m.spec[0], mk(m.transmissionColor[0], m.transmissionColor[1], m.transmissionColor[2]),
                     m.thinThickness, clamp01(m.specularRoughness), m.hasSpecularRoughness != 0);
           T = thin.transparency(t, fr, wo) * translucent;
         }
@@ -1833,8 +1825,7 @@ PRT_D f3 standardTransparency(const DevScene& sc, const DevTables& t, const DevM
   if (coat > kMatEps && fabsf(m.coatIor - m.ambientIor) > kMatEps)
   {
     const bool fromOutside = m.thinWalled ? true : !ctx.backfacing;
-    float coatEta = fromOutside ? m.ambientIor * (1.f / m.coatIor) : m.coatIor * (1.f / m.ambientIor);
-    coatEta = fminf(fmaxf(coatEta, 1.f / 3.f), 3.f);
+    const DevEta& coatEta = m.coat[fromOutside ? 0 : 1];
     CoatLayer c;
     c.init(t, coatEta, clamp01(mk(m.coatColor[0], m.coatColor[1], m.coatColor[2])), m.coatThickness,
            clamp01(m.coatRoughness), m.hasCoatRoughness != 0, coat);

@@ -4,6 +4,7 @@
 #include "../../include/prt_cuda.h"
 #include "runtime.h"
 #include "bvh_build.h"
+#include "host_rcp.h"
 #include "scene_file.h"
 
 #include <algorithm>
@@ -166,7 +167,20 @@ DevMaterial resolveMaterial(const prt_material& m, std::vector<float>& media, in
   std::memset(&d, 0, sizeof(d));
   auto ior = [](float x) {
     x = std::max(x, 0.f);
-    return x < 1.f ? 1.f / x : x;
+    return x < 1.f ? (x > 0.f ? hostRcp(x) : INFINITY) : x;
+  };
+  // Both sides of an interface between media of these indices (DevEta).
+  auto sides = [](DevEta* out, float outsideIor, float insideIor) {
+    const float etas[2] = {outsideIor * hostRcp(insideIor), insideIor * hostRcp(outsideIor)};
+    for (int s = 0; s < 2; ++s)
+    {
+      const float e = std::min(std::max(etas[s], 1.f / 3.f), 3.f);
+      out[s].eta = e;
+      out[s].rcpEta = hostRcp(e);
+      out[s].rcpEta2 = hostRcp(e * e);
+      out[s].favg = hostFresnelDielectricAvg(e);
+      out[s].favgRcp = hostFresnelDielectricAvg(out[s].rcpEta);
+    }
   };
   d.ambientIor = ior(m.ambient_ior > 0.f ? m.ambient_ior : 1.f);
   d.principled = m.model == PRT_MATERIAL_PRINCIPLED ? 1 : 0;
@@ -203,6 +217,8 @@ DevMaterial resolveMaterial(const prt_material& m, std::vector<float>& media, in
   d.coatRoughness = m.coat_roughness;
   d.hasCoatRoughness = m.coat_roughness != 0.f;
   d.coatIor = ior(m.coat_ior);
+  sides(d.spec, d.ambientIor, d.specularIor);
+  sides(d.coat, d.ambientIor, d.coatIor);
   d.sheenWeight = m.sheen_weight;
   for (int k = 0; k < 3; ++k) d.sheenColor[k] = m.sheen_color[k];
   d.sheenRoughness = m.sheen_roughness;
@@ -1459,8 +1475,10 @@ int prt_cuda_set_tuning(prt_context* ctx, const prt_tuning* t)
   return guarded(ctx, [&](Context& c) {
     if (!t) throw std::invalid_argument("null tuning");
     if (t->trace_blocks < 0 || t->trace_blocks > 32 || t->shade_blocks < 0 || t->shade_blocks > 32 || t->wave_paths < 0 ||
-        t->top_stage < 0 || t->top_stage > 2 || t->ray_bins < 0 || t->ray_bins > 2)
+        t->top_stage < 0 || t->top_stage > 2 || t->ray_bins < 0 || t->ray_bins > 2 ||
+        (t->trace_stack != 0 && t->trace_stack != 24 && t->trace_stack != 48))
       throw std::invalid_argument("tuning out of range");
+    if (t->trace_stack) c.traceStack = t->trace_stack;
     if (t->top_stage) c.topStage = t->top_stage == 1 ? 1 : 0;
     if (t->ray_bins) c.rayBins = t->ray_bins == 1 ? 1 : 0;
     if (t->trace_blocks) c.traceBlocks = t->trace_blocks;
@@ -1478,6 +1496,7 @@ int prt_cuda_get_tuning(prt_context* ctx, prt_tuning* t)
     t->wave_paths = (int32_t)std::min<int64_t>(c.wavePaths, 0x7fffffff);
     t->top_stage = c.topStage ? 1 : 2;
     t->ray_bins = c.rayBins ? 1 : 2;
+    t->trace_stack = c.traceStack;
   });
 }
 
@@ -1488,7 +1507,8 @@ int prt_cuda_autotune(prt_context* ctx, int32_t spp, prt_tuning* chosen, double*
     if (!c.hasRenderer || !c.hasCamera || !c.accum) throw ApiError{PRT_ERR_STATE, "renderer, camera and frame are required"};
     if (spp <= 0) throw std::invalid_argument("spp must be > 0");
     cuCheck(cudaSetDevice(c.device), "cudaSetDevice");
-    auto timeOne = [&](int tb, int sb, int64_t wave, int top, int bins) {
+    auto timeOne = [&](int tb, int sb, int64_t wave, int top, int bins, int stack) {
+      c.traceStack = stack;
       c.traceBlocks = tb;
       c.shadeBlocks = sb;
       c.wavePaths = wave;
@@ -1506,37 +1526,44 @@ int prt_cuda_autotune(prt_context* ctx, int32_t spp, prt_tuning* chosen, double*
     };
     const int profile = c.profileFlags;
     c.profileFlags = 0;
-    int bT = c.traceBlocks, bS = c.shadeBlocks, bTop = c.topStage, bBins = c.rayBins;
+    int bT = c.traceBlocks, bS = c.shadeBlocks, bTop = c.topStage, bBins = c.rayBins, bStack = c.traceStack;
     int64_t bW = c.wavePaths;
-    timeOne(bT, bS, bW, bTop, bBins);  // warm-up
+    timeOne(bT, bS, bW, bTop, bBins, bStack);  // warm-up
     double best = -1.0;
     // One axis at a time: wave size (paths in flight), traversal and shading grids, staging
-    // of the top BVH levels in shared memory, octant binning of extended rays.
+    // of the top BVH levels in shared memory, octant binning of extended rays, stack depth.
     for (int64_t w : {8ll << 20, 16ll << 20, 32ll << 20, 64ll << 20, 128ll << 20})
     {
-      const double v = timeOne(bT, bS, w, bTop, bBins);
+      const double v = timeOne(bT, bS, w, bTop, bBins, bStack);
       if (v > best) { best = v; bW = w; }
     }
     for (int tb : {4, 6, 8, 12})
     {
-      const double v = timeOne(tb, bS, bW, bTop, bBins);
+      const double v = timeOne(tb, bS, bW, bTop, bBins, bStack);
       if (v > best) { best = v; bT = tb; }
     }
     for (int sb : {2, 4, 8})
     {
-      const double v = timeOne(bT, sb, bW, bTop, bBins);
+      const double v = timeOne(bT, sb, bW, bTop, bBins, bStack);
       if (v > best) { best = v; bS = sb; }
     }
     for (int top : {0, 1})
     {
-      const double v = timeOne(bT, bS, bW, top, bBins);
+      const double v = timeOne(bT, bS, bW, top, bBins, bStack);
       if (v > best) { best = v; bTop = top; }
     }
     for (int bins : {0, 1})
     {
-      const double v = timeOne(bT, bS, bW, bTop, bins);
+      const double v = timeOne(bT, bS, bW, bTop, bins, bStack);
       if (v > best) { best = v; bBins = bins; }
     }
+    if (c.bvhDepth <= 24)
+      for (int stack : {24, 48})
+      {
+        const double v = timeOne(bT, bS, bW, bTop, bBins, stack);
+        if (v > best) { best = v; bStack = stack; }
+      }
+    c.traceStack = bStack;
     c.topStage = bTop;
     c.rayBins = bBins;
     c.traceBlocks = bT;
@@ -1554,6 +1581,7 @@ int prt_cuda_autotune(prt_context* ctx, int32_t spp, prt_tuning* chosen, double*
       chosen->shade_blocks = bS;
       chosen->wave_paths = (int32_t)bW;
       chosen->top_stage = bTop ? 1 : 2;
+      chosen->trace_stack = bStack;
     }
     if (mrays) *mrays = best;
   });
@@ -1769,6 +1797,7 @@ int prt_cuda_batch_create(prt_context* ctx, const prt_batch_item* items, int32_t
         tmp.stream = c.stream;
         tmp.smCount = c.smCount;
         uploadScene(tmp, it.scene);
+        B.bvhDepth = std::max(B.bvhDepth, tmp.bvhDepth);
         B.bufs.insert(B.bufs.end(), tmp.sceneBufs.begin(), tmp.sceneBufs.end());
         tmp.sceneBufs.clear();
         B.itemMaterials.push_back(tmp.materialsHost);

@@ -48,11 +48,27 @@ constexpr int kShadeClassFeatures[kShadeClasses] = {
   kFeatAll,
 };
 
+// One side of a dielectric interface (index 0: hit from outside, 1: from inside), resolved on
+// the host with hostRcp: eta = clamp(outsideIor * rcp(insideIor), 1/3, 3) as
+// StandardMaterial::getBsdfLobes forms it (material/standard.cpp:217-218, 357), and the values
+// the lobes derive from eta with rcp (bsdf/rough_dielectric.h:39-46,105,155;
+// bsdf/rough_coating.h:41; bsdf/coating.h:33-36; bsdf/thin_rough_dielectric.h:43).
+struct DevEta
+{
+  float eta;
+  float rcpEta;    // rcp(eta)
+  float rcpEta2;   // rcp(eta^2)
+  float favg;      // fresnelDielectricAvg(eta)
+  float favgRcp;   // fresnelDielectricAvg(rcp(eta))
+};
+
 // A Standard material with its parameters read and clamped as StandardMaterial::getBsdfLobes
 // reads them (material/standard.cpp:410-620). "has*" flags mirror the MaterialParam truth
 // tests that pick rough versus smooth lobes (material/material_param.h:49,181).
 struct DevMaterial
 {
+  DevEta spec[2];        // specular interface (ambientIor | specularIor)
+  DevEta coat[2];        // coat interface (ambientIor | coatIor)
   int type;
   int features;          // kFeat* lobes the material can produce
   int shadeClass;        // index into kShadeClassFeatures (0 for emissive materials)
@@ -185,6 +201,10 @@ struct DevTables
   const float* reflEcAvg;     // 16^2
   const float* condEcDir;     // 16^4      (cosThetaO, r, g, roughness) (specular-albedo AOV only)
   const float* sheenDir;      // 16^2
+  // Bounds of the eta in [1/3, 1] axis: rcp(3) and rcp(1) as the reference's CPU build rounds
+  // them (bsdf/albedo_tables.h:66-67; hostRcp), so that lookups land on the reference's
+  // coordinates. The [1, 3] axis has exact bounds.
+  float etaLo, etaHi;
 };
 
 struct DevCamera

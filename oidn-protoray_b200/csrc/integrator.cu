@@ -372,7 +372,7 @@ PRT_D void addCounts(unsigned long long* dst, const TraceCount& c)
 // the hit and bin the path by the shading it needs (the GPU form of the reference's material
 // sort, render/renderer_stream.h:108-181): class 0 ends the path (miss, area light, maxDepth),
 // classes 1.. are the material feature classes.
-template <bool Count, bool Batch, bool Top = false>
+template <bool Count, bool Batch, bool Top = false, int Stack = kTraceStack>
 __global__ void __launch_bounds__(256) kTrace(Launch L, const int* __restrict__ queue, const int* __restrict__ count,
                                               int* __restrict__ work, int depth, int* __restrict__ classQueues,
                                               int* __restrict__ classCounts)
@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(256) kTrace(Launch L, const int* __restrict__ 
         pathDepth = (int)(info.z >> kDepthShift);
       }
       const PathEnv<Batch> E(L, item);
-      const TraceHit h = traverse<false, Count, Top && !Batch>(E.sc.nodes, E.sc.tris, mk(a.x, a.y, a.z),
+      const TraceHit h = traverse<false, Count, Top && !Batch, Stack>(E.sc.nodes, E.sc.tris, mk(a.x, a.y, a.z),
                                                                mk(b.x, b.y, b.z), a.w, b.w, L.ps.err, &tc, top);
       L.ps.hit[p] = make_float4(h.t, h.u, h.v, __int_as_float(h.triId));
       cls = 0;
@@ -597,7 +597,7 @@ struct ShadowFilter
 // Any-hit test of the queued shadow rays; adds the unoccluded NEE contribution and
 // finishes paths that ended at this bounce (render/path_renderer_stream.h:953-1010). Transp:
 // scenes with transparent materials filter the hits (ShadowFilter).
-template <bool Count, bool Batch, bool Top = false, bool Transp = false>
+template <bool Count, bool Batch, bool Top = false, bool Transp = false, int Stack = kTraceStack>
 __global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__ count, int* __restrict__ work,
                                                int parity, int depth)
 {
@@ -634,11 +634,11 @@ __global__ void __launch_bounds__(256) kShadow(Launch L, const int* __restrict__
         {
           const ShadowFilter flt{&E.sc, &L.tab, o, d, &T};
           unoccluded =
-            traverse<true, Count, Top && !Batch>(E.sc.nodes, E.sc.tris, o, d, a.w, b.w, L.ps.err, &tc, top, flt)
+            traverse<true, Count, Top && !Batch, Stack>(E.sc.nodes, E.sc.tris, o, d, a.w, b.w, L.ps.err, &tc, top, flt)
               .triId < 0;
         }
         else
-          unoccluded = traverse<true, Count, Top && !Batch>(E.sc.nodes, E.sc.tris, o, d, a.w, b.w, L.ps.err, &tc, top)
+          unoccluded = traverse<true, Count, Top && !Batch, Stack>(E.sc.nodes, E.sc.tris, o, d, a.w, b.w, L.ps.err, &tc, top)
                          .triId < 0;
       }
       float4 r = L.ps.rad[p];
@@ -1512,6 +1512,9 @@ static cudaError_t bounceLoop(Context& ctx, const Launch& L, int P, bool replay,
   kRaygen<<<gridFor(ctx, P), 256, 0, ctx.stream>>>(L);
   rc.launches++;
   const bool bins = ctx.rayBins && ctx.ps.octBins;
+  // The 24-entry traversal stack where the tree fits in it (the tree's wide depth bounds the
+  // stack: one node group per level).
+  const bool shallow = ctx.traceStack <= kTraceStackShallow && ctx.bvhDepth <= kTraceStackShallow;
   int inBuf = 1;  // queue buffer that holds this bounce's paths (camera rays need none)
   for (int depth = 0; depth <= maxDepth; ++depth)
   {
@@ -1526,6 +1529,9 @@ static cudaError_t bounceLoop(Context& ctx, const Launch& L, int P, bool replay,
     else if (ctx.topStage)
       kTrace<false, false, true><<<persistent, 256, 0, ctx.stream>>>(L, q, cnt, cnt + kCntWorkTrace, depth,
                                                                      ctx.ps.classQueues, cnt + 1);
+    else if (shallow)
+      kTrace<false, false, false, kTraceStackShallow><<<persistent, 256, 0, ctx.stream>>>(
+        L, q, cnt, cnt + kCntWorkTrace, depth, ctx.ps.classQueues, cnt + 1);
     else
       kTrace<false, false><<<persistent, 256, 0, ctx.stream>>>(L, q, cnt, cnt + kCntWorkTrace, depth,
                                                                ctx.ps.classQueues, cnt + 1);
@@ -1555,6 +1561,9 @@ static cudaError_t bounceLoop(Context& ctx, const Launch& L, int P, bool replay,
       {
         if (counting)
           kShadow<true, false, false, true><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
+        else if (shallow)
+          kShadow<false, false, false, true, kTraceStackShallow><<<persistent, 256, 0, ctx.stream>>>(
+            L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
         else
           kShadow<false, false, false, true><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
       }
@@ -1562,6 +1571,9 @@ static cudaError_t bounceLoop(Context& ctx, const Launch& L, int P, bool replay,
         kShadow<true, false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
       else if (ctx.topStage)
         kShadow<false, false, true><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
+      else if (shallow)
+        kShadow<false, false, false, false, kTraceStackShallow><<<persistent, 256, 0, ctx.stream>>>(
+          L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
       else
         kShadow<false, false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
       end();
@@ -1779,7 +1791,8 @@ int* batchCounts(BatchCtl* ctl, int parity)
 // One bounce iteration of the batch: control step, regeneration, closest hit, shading by
 // class, shadow rays. Every count is read on the device, so the sequence can be captured once
 // and replayed.
-int batchIteration(const Context& ctx, const Launch& L, int a, int persistent, int shadeGrid, int regenGrid, bool replay)
+int batchIteration(const Context& ctx, const Launch& L, int a, int persistent, int shadeGrid, int regenGrid, bool replay,
+                   bool shallow)
 {
   const int b = a ^ 1;
   int* ca = batchCounts(L.ctl, a);
@@ -1790,8 +1803,12 @@ int batchIteration(const Context& ctx, const Launch& L, int a, int persistent, i
     kBatchRegen<true><<<regenGrid, 256, 0, st>>>(L, a, L.ps.queue[a]);
   else
     kBatchRegen<false><<<regenGrid, 256, 0, st>>>(L, a, L.ps.queue[a]);
-  kTrace<false, true><<<persistent, 256, 0, st>>>(L, L.ps.queue[a], ca, ca + kBatchCntShadow + 1, 0,
-                                                  L.ps.classQueues, ca + 1);
+  if (shallow)
+    kTrace<false, true, false, kTraceStackShallow><<<persistent, 256, 0, st>>>(
+      L, L.ps.queue[a], ca, ca + kBatchCntShadow + 1, 0, L.ps.classQueues, ca + 1);
+  else
+    kTrace<false, true><<<persistent, 256, 0, st>>>(L, L.ps.queue[a], ca, ca + kBatchCntShadow + 1, 0,
+                                                    L.ps.classQueues, ca + 1);
   if (replay)
   {
     // Adjoint replay: class-0 paths only return their slots; classes 1 and 2 (the adjoint's
@@ -1805,8 +1822,14 @@ int batchIteration(const Context& ctx, const Launch& L, int a, int persistent, i
   }
   kShadeEnd<true><<<shadeGrid, 256, 0, st>>>(L, L.ps.classQueues, ca + 1, 0, a);
   ShadeClassList::run<true>(1, L, st, shadeGrid, L.ps.classQueues, ca, 0, L.ps.queue[b], cb, ca + kBatchCntShadow, a);
-  if (L.anyTransparent)
+  if (L.anyTransparent && shallow)
+    kShadow<false, true, false, true, kTraceStackShallow><<<persistent, 256, 0, st>>>(
+      L, ca + kBatchCntShadow, ca + kBatchCntShadow + 2, a, 0);
+  else if (L.anyTransparent)
     kShadow<false, true, false, true><<<persistent, 256, 0, st>>>(L, ca + kBatchCntShadow, ca + kBatchCntShadow + 2, a, 0);
+  else if (shallow)
+    kShadow<false, true, false, false, kTraceStackShallow><<<persistent, 256, 0, st>>>(
+      L, ca + kBatchCntShadow, ca + kBatchCntShadow + 2, a, 0);
   else
     kShadow<false, true><<<persistent, 256, 0, st>>>(L, ca + kBatchCntShadow, ca + kBatchCntShadow + 2, a, 0);
   return 5 + (kShadeClasses - 1);
@@ -1861,8 +1884,9 @@ static cudaError_t runBatch(Context& ctx, BatchState& B, RenderCounters& rc, boo
     e = cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
     int kernels = 0;
+    const bool shallow = ctx.traceStack <= kTraceStackShallow && B.bvhDepth <= kTraceStackShallow;
     for (int k = 0; k < kGraphIterations; ++k)
-      kernels += batchIteration(ctx, L, k & 1, persistent, shadeGrid, regenGrid, replay);
+      kernels += batchIteration(ctx, L, k & 1, persistent, shadeGrid, regenGrid, replay, shallow);
     cudaError_t launchErr = cudaGetLastError();
     e = cudaStreamEndCapture(ctx.stream, &graph);
     if (e == cudaSuccess) e = launchErr;

@@ -103,6 +103,7 @@ struct BatchState
   BatchItem* dItems = nullptr;
   long long workTotal = 0;
   int maxDepth = 0;
+  int bvhDepth = 0;                // deepest BVH8 of the items (wide levels)
   bool anyAov = false;
   PathState ps;                    // path pool; ps.err is the context's error flag
   BatchCtl* ctl = nullptr;
@@ -166,6 +167,7 @@ struct Context
   int64_t wavePaths = 128ll << 20;
   int topStage = 0;               // stage the top BVH levels in shared memory (frame form)
   int rayBins = 0;                // group each bounce's extended rays by direction octant (frame form)
+  int traceStack = 24;            // 24: the traversal kernels' 24-entry stack where the tree fits; 48: always 48
   DevMaterial whiteMaterial{};    // irradiance mode: the first hit's material (white Principled)
   DevMaterial* whiteMaterialDev = nullptr;  // its device copy
   int whiteClass = 0;             // its shading class

@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "render/device.h"
+#include "bsdf/albedo_tables.h"
 #include "camera/pinhole_camera.h"
 #include "image/image_texture.h"
 #include "light/distant_light.h"
@@ -156,9 +157,26 @@ inline void cudaEnvLightsFromProps(const Props& props, CudaEnvLights& out)
 class DeviceCuda : public Device
 {
 public:
-  explicit DeviceCuda(int deviceOrdinal = 0)
+  // hostTables: run on the energy-compensation tables that the reference computes on the host,
+  // as DeviceCpu's constructor does (render/device_cpu.cpp:20-23), so that the compensation
+  // terms -- which amplify a table's last digits by 1 / (1 - E_avg) -- match the CPU device's.
+  // false keeps the tables the device builds on the GPU at creation (within ~2e-6 of these)
+  // and skips the ~3 s of host integration.
+  explicit DeviceCuda(int deviceOrdinal = 0, bool hostTables = true)
   {
     if (prt_cuda_create(deviceOrdinal, &ctx) != PRT_OK) throw std::runtime_error("no usable CUDA device");
+    if (hostTables)
+    {
+      try
+      {
+        uploadHostTables();
+      }
+      catch (...)
+      {
+        prt_cuda_destroy(ctx);
+        throw;
+      }
+    }
   }
 
   ~DeviceCuda() override
@@ -405,6 +423,24 @@ private:
   {
     if (!camera) throw std::logic_error("no camera");
     return *camera;
+  }
+
+  // The reference's tables (bsdf/albedo_tables.cpp:173-188) in prt_cuda_albedo_tables' layout.
+  void uploadHostTables()
+  {
+    precomputeAlbedoTables();
+    std::vector<float> t;
+    auto put = [&](const float* src, int n) { t.insert(t.end(), src, src + n); };
+    put(MicrofacetAlbedoTable::dir, 32 * 32);
+    put(MicrofacetAlbedoTable::avg, 32);
+    put(MicrofacetDielectricAlbedoTable::etaDir, 16 * 16 * 16);
+    put(MicrofacetDielectricAlbedoTable::etaAvg, 16 * 16);
+    put(MicrofacetDielectricAlbedoTable::rcpEtaDir, 16 * 16 * 16);
+    put(MicrofacetDielectricAlbedoTable::rcpEtaAvg, 16 * 16);
+    put(MicrofacetDielectricReflectionAlbedoTable::etaDir, 16 * 16 * 16);
+    put(MicrofacetDielectricReflectionAlbedoTable::etaAvg, 16 * 16);
+    put(MicrofacetSheenAlbedoTable::dir, 16 * 16);
+    check(prt_cuda_set_albedo_tables(ctx, t.data(), (int64_t)t.size()));
   }
 
   prt_context* ctx = nullptr;

@@ -315,8 +315,8 @@ class DeviceCuda:
         self._check(self.lib.prt_cuda_render(self.h, spp, C.byref(st)))
         return {name: getattr(st, name) for name, _ in T.RenderStats._fields_}
 
-    def set_tuning(self, trace_blocks=0, shade_blocks=0, wave_paths=0, top_stage=0, ray_bins=0):
-        t = T.Tuning(trace_blocks, shade_blocks, wave_paths, top_stage, ray_bins)
+    def set_tuning(self, trace_blocks=0, shade_blocks=0, wave_paths=0, top_stage=0, ray_bins=0, trace_stack=0):
+        t = T.Tuning(trace_blocks, shade_blocks, wave_paths, top_stage, ray_bins, trace_stack)
         self._check(self.lib.prt_cuda_set_tuning(self.h, C.byref(t)))
 
     def get_tuning(self):

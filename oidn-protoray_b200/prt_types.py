@@ -283,6 +283,7 @@ class Tuning(C.Structure):
         ("wave_paths", C.c_int32),
         ("top_stage", C.c_int32),
         ("ray_bins", C.c_int32),
+        ("trace_stack", C.c_int32),
     ]
 
 

@@ -93,14 +93,20 @@ def bsdf_query(material, tuples, medium_id=0):
     return out
 
 
-def bsdf_query_scalar(material, tuples, medium_id=0):
-    """The same query through the reference's scalar BSDF path (Bsdf rather than BsdfSimd)."""
+def bsdf_query_scalar(material, tuples, medium_id=0, frame=None):
+    """The same query through the reference's scalar BSDF path (Bsdf rather than BsdfSimd).
+    `frame`: the shading frame U, V, N and the geometric normal Ng (12 floats); default the
+    canonical frame (x, y, z, z)."""
     lib = _lib()
     t = np.ascontiguousarray(tuples, np.float32).reshape(-1, 9)
     out = np.zeros((t.shape[0], 13), np.float32)
-    lib.ref_bsdf_query_scalar.argtypes = [C.POINTER(T.Material), C.c_int, C.c_int64, C.POINTER(C.c_float),
-                                          C.POINTER(C.c_float)]
-    if lib.ref_bsdf_query_scalar(C.byref(material), medium_id, t.shape[0], T.fptr(t), T.fptr(out)) != 0:
+    if frame is None:
+        frame = [1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 1]
+    f = np.ascontiguousarray(frame, np.float32).reshape(12)
+    lib.ref_bsdf_query_scalar_frame.argtypes = [C.POINTER(T.Material), C.c_int, C.POINTER(C.c_float), C.c_int64,
+                                                C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    if lib.ref_bsdf_query_scalar_frame(C.byref(material), medium_id, T.fptr(f), t.shape[0], T.fptr(t),
+                                       T.fptr(out)) != 0:
         raise RuntimeError("oracle scalar BSDF query failed")
     return out
 

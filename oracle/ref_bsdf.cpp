@@ -163,8 +163,12 @@ int ref_bsdf_query(const prt_material* mat, int mediumId, int64_t n, const float
 
 // The same query through the reference's scalar BSDF path (Material::getBsdf(ShadingContext&)
 // -> Bsdf::eval/sample, material/material.h:54-64, bsdf/bsdf.h:66-89), whose arithmetic is the
-// scalar library's rather than the SIMD path's approximate reciprocals and polynomials.
-int ref_bsdf_query_scalar(const prt_material* mat, int mediumId, int64_t n, const float* tuples, float* out)
+// scalar library's rather than the SIMD path's approximate reciprocals and polynomials, in the
+// shading frame `frame` (U, V, N and the geometric normal Ng: 12 floats). A rotated frame with
+// correspondingly rotated directions poses the same problem in other coordinates: the exact
+// answer is unchanged, the reference's rounding is not.
+int ref_bsdf_query_scalar_frame(const prt_material* mat, int mediumId, const float* frame, int64_t n,
+                                const float* tuples, float* out)
 {
   try
   {
@@ -178,10 +182,10 @@ int ref_bsdf_query_scalar(const prt_material* mat, int mediumId, int64_t n, cons
       const float* t = tuples + 9 * i;
       const Vec3f wo(t[0], t[1], t[2]), wi(t[3], t[4], t[5]), s(t[6], t[7], t[8]);
       ctx->p = Vec3f(zero);
-      ctx->f.U = Vec3f(1.f, 0.f, 0.f);
-      ctx->f.V = Vec3f(0.f, 1.f, 0.f);
-      ctx->f.N = Vec3f(0.f, 0.f, 1.f);
-      ctx->Ng = Vec3f(0.f, 0.f, 1.f);
+      ctx->f.U = Vec3f(frame[0], frame[1], frame[2]);
+      ctx->f.V = Vec3f(frame[3], frame[4], frame[5]);
+      ctx->f.N = Vec3f(frame[6], frame[7], frame[8]);
+      ctx->Ng = Vec3f(frame[9], frame[10], frame[11]);
       for (int u = 0; u < maxNumUVs; ++u) ctx->uv[u] = Vec2f(0.5f);
       ctx->backfacing = false;
       ctx->eps = 1e-6f;
@@ -207,6 +211,12 @@ int ref_bsdf_query_scalar(const prt_material* mat, int mediumId, int64_t n, cons
   {
     return -1;
   }
+}
+
+int ref_bsdf_query_scalar(const prt_material* mat, int mediumId, int64_t n, const float* tuples, float* out)
+{
+  static const float canonical[12] = {1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 1.f};
+  return ref_bsdf_query_scalar_frame(mat, mediumId, canonical, n, tuples, out);
 }
 
 // Microfacet sampling with the reference's distributions, in the layout of

@@ -65,13 +65,13 @@ TABLES = [("ggx_dir", (32, 32), None), ("ggx_avg", (32,), None),
 def test_albedo_tables_match_the_reference(device):
     """Energy-compensation tables against the reference's precomputeAlbedoTables, entry by entry:
     GGX (directional and average), dielectric with eta in [1/3, 1] and in [1, 3], dielectric
-    reflection, sheen, all within 2e-5 -- except the eta = 1 slices (index 15 of the [1/3, 1]
-    tables, index 0 of the [1, 3] tables). There the integrand degenerates (the refracted half
-    vector is undefined when the two sides' indices match), and the reference's eta is its
-    approximate reciprocal rcp(1) = 0.99999994 on AVX2 rather than 1, so those entries depend on
-    the CPU; they are checked to be finite albedos in [0, 1]. The reflection-EC and
-    artistic-conductor-EC tables serve only the reference's specular-albedo AOV and are not part
-    of this path."""
+    reflection, sheen, all within 2e-5. The eta = 1 slices (index 15 of the [1/3, 1] tables,
+    index 0 of the [1, 3] tables) sit at the reference's eta, which its CPU build rounds through
+    its approximate reciprocal (rcp(1) = 0.99999994 on x86-64; the device takes the same bounds
+    from the host). There the transmitted half vector degenerates, so the directional dielectric
+    slices agree to 2e-3 only; their averages and the reflection slices to 2e-5. The reflection-EC
+    and artistic-conductor-EC tables serve only the reference's specular-albedo AOV and are not
+    part of this path."""
     import ref
 
     got = device.albedo_tables()
@@ -86,8 +86,9 @@ def test_albedo_tables_match_the_reference(device):
         keep = np.ones(shape, bool)
         if eta1 is not None:
             keep[:, eta1] = False
-            g1 = a[:, eta1]
-            assert np.isfinite(g1).all() and (g1 >= 0).all() and (g1 <= 1.0 + 1e-3).all(), name
+            d1 = np.abs(a[:, eta1] - b[:, eta1])
+            assert np.isfinite(a[:, eta1]).all(), name
+            assert d1.max() < (2e-3 if name.startswith("diel") and name.endswith("dir") else 2e-5), (name, d1.max())
         d = np.abs(a - b)[keep]
         assert d.max() < 2e-5, (name, d.max())
     assert o == len(want)
@@ -126,6 +127,40 @@ def ulp_sensitivity(query, tuples, cols, norm_blocks=(), decision=None):
             if decision is not None:
                 flips |= decision(o) != decision(base32)
     return base32, base, sens, flips
+
+
+def random_rotation(rng):
+    q, r = np.linalg.qr(rng.normal(size=(3, 3)))
+    q *= np.sign(np.diag(r))
+    if np.linalg.det(q) < 0:
+        q[:, 0] *= -1
+    return q
+
+
+def rotation_sensitivity(query_frame, tuples, base32, rotations=4, decision=None, seed=11):
+    """Per output, the largest change of the reference's scalar result when the whole query --
+    wo, wi and the shading frame with its geometric normal -- is posed in rotated coordinates
+    (sampled directions rotated back). The exact answer does not change; the reference's rounding
+    does, so this measures how much its own rounding moves each output. Input moves cannot show
+    that where an internal step cancels: e.g. the shading-normal adaptation for wo just below the
+    horizon (core/shading_context.h:57-70) forms the bent normal from wo + wi1, whose x, y parts
+    cancel to ~wo.z^2 / 2, so an ulp of its reciprocal square root moves cos(theta_o) by ~1%."""
+    base = base32.astype(np.float64)
+    sens = np.zeros_like(base)
+    flips = np.zeros(len(tuples), bool)
+    rng = np.random.default_rng(seed)
+    for _ in range(rotations):
+        R = random_rotation(rng)
+        t = tuples.astype(np.float64)
+        t[:, 0:3] = t[:, 0:3] @ R.T
+        t[:, 3:6] = t[:, 3:6] @ R.T
+        o32 = query_frame(t.astype(np.float32), np.concatenate([R[:, 0], R[:, 1], R[:, 2], R[:, 2]]))
+        o = o32.astype(np.float64)
+        o[:, 7:10] = o[:, 7:10] @ R
+        sens = np.maximum(sens, np.abs(o - base))
+        if decision is not None:
+            flips |= decision(o32) != decision(base32)
+    return sens, flips
 
 
 @pytest.mark.parametrize("dist", ["beckmann", "ggx_visible"])
@@ -169,14 +204,25 @@ def test_microfacet_sampling_matches_the_reference(device, dist):
 def test_bsdf_misses_are_ill_conditioned_tuples(device, name, material, medium):
     """The BSDF arithmetic, separated from the energy-compensation tables: with the reference's own
     tables loaded into the device, every miss beyond 1e-5 sits where the output is ill-conditioned
-    -- a 2-ulp move of one input (wo, wi or the sample) moves the reference's own scalar result by
-    at least a quarter of the miss. The per-tuple tolerance is 1e-5 relative (1e-6 absolute) plus 4x
-    that sensitivity; the reference's SIMD path meets it against the reference's scalar path on all
-    but ~1e-4 of the tuples (sampling decisions of delta lobes exactly at a threshold), and so must
-    the device, on 32k seeded tuples per case; the success of sampling and the BSDF flags agree
-    outright. (With the device's own tables, which agree with the reference's to 2.2e-6, the
-    (1 - E) factors of the energy compensation amplify that to ~1e-4 relative on a rough
-    dielectric's multiple-scattering samples; the million-tuple test above bounds that case.)"""
+    in the reference's own arithmetic -- a 2-ulp move of one input (wo, wi or the sample), or the
+    same query posed in rotated coordinates (rotation_sensitivity), moves the reference's scalar
+    result by at least a quarter of the miss. The per-tuple tolerance is 1e-5 relative (1e-6
+    absolute) plus 4x that sensitivity; sampling decisions that such a move flips are exempt. The
+    reference's SIMD path meets it against the scalar path on every tuple, and the device may miss
+    it on at most max(2x the SIMD path's misses, 2e-4) of 32k seeded tuples per case; the success
+    of sampling and the BSDF flags agree outright. (The residue the floor admits: decisions taken
+    on an internally rounded value with no input dependence, e.g. the visible-normal sampler's
+    basis switch at V.z < 0.9999 (bsdf/ggx_distribution.h:57) for a stretched V.z half an ulp
+    below it.)
+
+    This holds because eta and the values derived from it (rcp(eta), rcp(eta^2), the Fresnel
+    averages, the bounds of the eta <= 1 table axis) carry the reference's own rounding: the
+    reference forms them with its approximate reciprocal, and an ulp of eta moves a rough
+    dielectric's multiple-scattering share by up to 1 / (1 - E_avg) ulps -- 1.4e-5 relative for
+    glass at roughness 0.2, 3e-3 at 0.05. (With the device's own tables, which agree with the
+    reference's to 2.2e-6, the same factor amplifies the table difference to ~1e-4 relative; the
+    million-tuple test above bounds that case, and the reference-side adapter uploads the
+    reference's tables.)"""
     import ref
 
     tup = bsdf_cases.tuples(1 << 15, 3)
@@ -188,6 +234,10 @@ def test_bsdf_misses_are_ill_conditioned_tuples(device, name, material, medium):
 
     base32, base, sens, flips = ulp_sensitivity(lambda t: ref.bsdf_query_scalar(material, t, medium), tup, range(9),
                                                 [(0, 3), (3, 6)], decision)
+    rsens, rflips = rotation_sensitivity(lambda t, f: ref.bsdf_query_scalar(material, t, medium, frame=f), tup,
+                                         base32, decision=decision)
+    sens = np.maximum(sens, rsens)
+    flips |= rflips
     own = device.albedo_tables()
     device.set_albedo_tables(ref.albedo_tables())
     try:
