@@ -21,7 +21,8 @@ namespace prt {
 constexpr int kTraceStack = kBvh8TraceStack;  // node-group stack entries per ray
 // The shallow stack of the traversal kernels' second instantiation, taken for trees of at most
 // this many wide levels (the host-built tree of the 2.6M-triangle terrain has 10): half the
-// local-memory frame, and 2% less kTrace time on the terrain frame.
+// local-memory frame. On the terrain frame both instantiations run equally fast (the stack's
+// upper entries are never touched there); the choice is a tuning axis for other scenes.
 constexpr int kTraceStackShallow = 24;
 constexpr int kTraceMaxIter = 1 << 20;    // loop cap: a corrupt tree ends the ray, not the kernel
 constexpr uint32_t kErrStackOverflow = 1u;
