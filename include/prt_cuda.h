@@ -420,9 +420,10 @@ typedef struct prt_tuning
                           global memory (the default); 0 keeps the current value */
   int32_t ray_bins;    /* 1: each bounce's extended rays are traced grouped by direction octant;
                           2: in the order shading produced them (the default); 0 keeps */
-  int32_t trace_stack; /* node-group stack entries of the traversal kernels: 24 (the default)
-                          takes the 24-entry instantiation for trees of at most 24 wide levels
-                          and the 48-entry one otherwise; 48 always the 48-entry one; 0 keeps */
+  int32_t trace_stack; /* node-group stack of the traversal kernels: 12 (the default) a 12-entry
+                          stack in shared memory for trees of at most 12 wide levels, else as
+                          24; 24 the 24-entry local-memory stack for trees of at most 24 levels,
+                          else as 48; 48 always the 48-entry one; 0 keeps */
 } prt_tuning;
 
 int prt_cuda_set_tuning(prt_context* ctx, const prt_tuning* tuning);

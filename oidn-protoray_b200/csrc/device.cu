@@ -1476,7 +1476,7 @@ int prt_cuda_set_tuning(prt_context* ctx, const prt_tuning* t)
     if (!t) throw std::invalid_argument("null tuning");
     if (t->trace_blocks < 0 || t->trace_blocks > 32 || t->shade_blocks < 0 || t->shade_blocks > 32 || t->wave_paths < 0 ||
         t->top_stage < 0 || t->top_stage > 2 || t->ray_bins < 0 || t->ray_bins > 2 ||
-        (t->trace_stack != 0 && t->trace_stack != 24 && t->trace_stack != 48))
+        (t->trace_stack != 0 && t->trace_stack != 12 && t->trace_stack != 24 && t->trace_stack != 48))
       throw std::invalid_argument("tuning out of range");
     if (t->trace_stack) c.traceStack = t->trace_stack;
     if (t->top_stage) c.topStage = t->top_stage == 1 ? 1 : 0;
@@ -1557,8 +1557,8 @@ int prt_cuda_autotune(prt_context* ctx, int32_t spp, prt_tuning* chosen, double*
       const double v = timeOne(bT, bS, bW, bTop, bins, bStack);
       if (v > best) { best = v; bBins = bins; }
     }
-    if (c.bvhDepth <= 24)
-      for (int stack : {24, 48})
+    for (int stack : {12, 24, 48})
+      if (c.bvhDepth <= stack && stack != bStack)
       {
         const double v = timeOne(bT, bS, bW, bTop, bBins, stack);
         if (v > best) { best = v; bStack = stack; }

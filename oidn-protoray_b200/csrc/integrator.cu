@@ -1514,7 +1514,8 @@ static cudaError_t bounceLoop(Context& ctx, const Launch& L, int P, bool replay,
   const bool bins = ctx.rayBins && ctx.ps.octBins;
   // The 24-entry traversal stack where the tree fits in it (the tree's wide depth bounds the
   // stack: one node group per level).
-  const bool shallow = ctx.traceStack <= kTraceStackShallow && ctx.bvhDepth <= kTraceStackShallow;
+  const bool shared = ctx.traceStack <= kTraceStackShared && ctx.bvhDepth <= kTraceStackShared;
+  const bool shallow = !shared && ctx.traceStack <= kTraceStackShallow && ctx.bvhDepth <= kTraceStackShallow;
   int inBuf = 1;  // queue buffer that holds this bounce's paths (camera rays need none)
   for (int depth = 0; depth <= maxDepth; ++depth)
   {
@@ -1529,6 +1530,9 @@ static cudaError_t bounceLoop(Context& ctx, const Launch& L, int P, bool replay,
     else if (ctx.topStage)
       kTrace<false, false, true><<<persistent, 256, 0, ctx.stream>>>(L, q, cnt, cnt + kCntWorkTrace, depth,
                                                                      ctx.ps.classQueues, cnt + 1);
+    else if (shared)
+      kTrace<false, false, false, kTraceStackShared><<<persistent, 256, 0, ctx.stream>>>(
+        L, q, cnt, cnt + kCntWorkTrace, depth, ctx.ps.classQueues, cnt + 1);
     else if (shallow)
       kTrace<false, false, false, kTraceStackShallow><<<persistent, 256, 0, ctx.stream>>>(
         L, q, cnt, cnt + kCntWorkTrace, depth, ctx.ps.classQueues, cnt + 1);
@@ -1561,6 +1565,9 @@ static cudaError_t bounceLoop(Context& ctx, const Launch& L, int P, bool replay,
       {
         if (counting)
           kShadow<true, false, false, true><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
+        else if (shared)
+          kShadow<false, false, false, true, kTraceStackShared><<<persistent, 256, 0, ctx.stream>>>(
+            L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
         else if (shallow)
           kShadow<false, false, false, true, kTraceStackShallow><<<persistent, 256, 0, ctx.stream>>>(
             L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
@@ -1571,6 +1578,9 @@ static cudaError_t bounceLoop(Context& ctx, const Launch& L, int P, bool replay,
         kShadow<true, false><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
       else if (ctx.topStage)
         kShadow<false, false, true><<<persistent, 256, 0, ctx.stream>>>(L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
+      else if (shared)
+        kShadow<false, false, false, false, kTraceStackShared><<<persistent, 256, 0, ctx.stream>>>(
+          L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
       else if (shallow)
         kShadow<false, false, false, false, kTraceStackShallow><<<persistent, 256, 0, ctx.stream>>>(
           L, cnt + kCntShadow, cnt + kCntWorkShadow, 0, depth);
@@ -1792,7 +1802,7 @@ int* batchCounts(BatchCtl* ctl, int parity)
 // class, shadow rays. Every count is read on the device, so the sequence can be captured once
 // and replayed.
 int batchIteration(const Context& ctx, const Launch& L, int a, int persistent, int shadeGrid, int regenGrid, bool replay,
-                   bool shallow)
+                   bool shared, bool shallow)
 {
   const int b = a ^ 1;
   int* ca = batchCounts(L.ctl, a);
@@ -1803,7 +1813,10 @@ int batchIteration(const Context& ctx, const Launch& L, int a, int persistent, i
     kBatchRegen<true><<<regenGrid, 256, 0, st>>>(L, a, L.ps.queue[a]);
   else
     kBatchRegen<false><<<regenGrid, 256, 0, st>>>(L, a, L.ps.queue[a]);
-  if (shallow)
+  if (shared)
+    kTrace<false, true, false, kTraceStackShared><<<persistent, 256, 0, st>>>(
+      L, L.ps.queue[a], ca, ca + kBatchCntShadow + 1, 0, L.ps.classQueues, ca + 1);
+  else if (shallow)
     kTrace<false, true, false, kTraceStackShallow><<<persistent, 256, 0, st>>>(
       L, L.ps.queue[a], ca, ca + kBatchCntShadow + 1, 0, L.ps.classQueues, ca + 1);
   else
@@ -1822,11 +1835,17 @@ int batchIteration(const Context& ctx, const Launch& L, int a, int persistent, i
   }
   kShadeEnd<true><<<shadeGrid, 256, 0, st>>>(L, L.ps.classQueues, ca + 1, 0, a);
   ShadeClassList::run<true>(1, L, st, shadeGrid, L.ps.classQueues, ca, 0, L.ps.queue[b], cb, ca + kBatchCntShadow, a);
-  if (L.anyTransparent && shallow)
+  if (L.anyTransparent && shared)
+    kShadow<false, true, false, true, kTraceStackShared><<<persistent, 256, 0, st>>>(
+      L, ca + kBatchCntShadow, ca + kBatchCntShadow + 2, a, 0);
+  else if (L.anyTransparent && shallow)
     kShadow<false, true, false, true, kTraceStackShallow><<<persistent, 256, 0, st>>>(
       L, ca + kBatchCntShadow, ca + kBatchCntShadow + 2, a, 0);
   else if (L.anyTransparent)
     kShadow<false, true, false, true><<<persistent, 256, 0, st>>>(L, ca + kBatchCntShadow, ca + kBatchCntShadow + 2, a, 0);
+  else if (shared)
+    kShadow<false, true, false, false, kTraceStackShared><<<persistent, 256, 0, st>>>(
+      L, ca + kBatchCntShadow, ca + kBatchCntShadow + 2, a, 0);
   else if (shallow)
     kShadow<false, true, false, false, kTraceStackShallow><<<persistent, 256, 0, st>>>(
       L, ca + kBatchCntShadow, ca + kBatchCntShadow + 2, a, 0);
@@ -1884,9 +1903,10 @@ static cudaError_t runBatch(Context& ctx, BatchState& B, RenderCounters& rc, boo
     e = cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
     int kernels = 0;
-    const bool shallow = ctx.traceStack <= kTraceStackShallow && B.bvhDepth <= kTraceStackShallow;
+    const bool shared = ctx.traceStack <= kTraceStackShared && B.bvhDepth <= kTraceStackShared;
+    const bool shallow = !shared && ctx.traceStack <= kTraceStackShallow && B.bvhDepth <= kTraceStackShallow;
     for (int k = 0; k < kGraphIterations; ++k)
-      kernels += batchIteration(ctx, L, k & 1, persistent, shadeGrid, regenGrid, replay, shallow);
+      kernels += batchIteration(ctx, L, k & 1, persistent, shadeGrid, regenGrid, replay, shared, shallow);
     cudaError_t launchErr = cudaGetLastError();
     e = cudaStreamEndCapture(ctx.stream, &graph);
     if (e == cudaSuccess) e = launchErr;

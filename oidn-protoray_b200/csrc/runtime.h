@@ -167,7 +167,7 @@ struct Context
   int64_t wavePaths = 128ll << 20;
   int topStage = 0;               // stage the top BVH levels in shared memory (frame form)
   int rayBins = 0;                // group each bounce's extended rays by direction octant (frame form)
-  int traceStack = 24;            // 24: the traversal kernels' 24-entry stack where the tree fits; 48: always 48
+  int traceStack = 12;            // smallest traversal stack to try: 12 (shared memory), 24 or 48 (local)
   DevMaterial whiteMaterial{};    // irradiance mode: the first hit's material (white Principled)
   DevMaterial* whiteMaterialDev = nullptr;  // its device copy
   int whiteClass = 0;             // its shading class

@@ -39,8 +39,9 @@ def render(dev, spp):
     dict(trace_blocks=12, shade_blocks=16, top_stage=1),
     dict(ray_bins=2),                        # queue in shading order instead of octant groups
     dict(ray_bins=1, top_stage=1, wave_paths=256 * 128 * 3),
-    dict(trace_stack=48),                    # the 48-entry traversal stack instead of 24
+    dict(trace_stack=48),                    # the 48-entry local-memory stack instead of shared memory
     dict(trace_stack=48, top_stage=1),
+    dict(trace_stack=24),                    # the 24-entry local-memory stack
 ])
 def test_tuning_keeps_the_image(dev, tuning):
     default = dev.get_tuning()
@@ -61,7 +62,7 @@ def test_autotune_returns_a_valid_tuning(dev):
         chosen, mrays = dev.autotune(2)
         assert mrays > 0
         assert chosen["top_stage"] in (1, 2) and 1 <= chosen["trace_blocks"] <= 32
-        assert chosen["ray_bins"] in (1, 2) and chosen["trace_stack"] in (24, 48)
+        assert chosen["ray_bins"] in (1, 2) and chosen["trace_stack"] in (12, 24, 48)
         assert dev.get_tuning() == chosen
         img, _ = render(dev, 4)
         assert np.array_equal(img, ref)
@@ -80,8 +81,8 @@ def test_tuning_rejects_out_of_range(dev):
         dev.set_tuning(trace_stack=32)
 
 
-def test_default_stack_is_the_shallow_one(dev):
-    """The terrain's tree is far shallower than 24 wide levels, so the default tuning runs the
-    24-entry instantiation of the traversal kernels."""
-    assert dev.get_tuning()["trace_stack"] == 24
-    assert dev.scene_stats()["depth"] <= 24
+def test_default_stack_is_the_shared_one(dev):
+    """The terrain's tree has at most 12 wide levels, so the default tuning runs the traversal
+    kernels with their 12-entry stack in shared memory."""
+    assert dev.get_tuning()["trace_stack"] == 12
+    assert dev.scene_stats()["depth"] <= 12
