@@ -369,7 +369,7 @@ def run_ours(args):
 
 # DRAM bytes (read + write) of the 9 kTrace launches of one 1920x1080 x 1-spp terrain frame,
 # from ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum.
-NCU_TRACE_DRAM_BYTES = 740_325_120
+NCU_TRACE_DRAM_BYTES = 699_916_032
 
 # Node visits and triangle tests per ray on the reference tree of the terrain workload: the host
 # binned-SAH BVH8 with the SAH-optimal 8-wide collapse (284,895 nodes, at most 3 triangles per
