@@ -1,9 +1,10 @@
 // Test infrastructure: drives the reference-side adapter prt::DeviceCuda
 // (oidn-protoray_b200/host/reference/device_cuda.h) compiled against the reference's own headers,
 // with the light accessors inserted as the integration inserts them (oracle/Makefile, target
-// adapter). Two entry points for the tests:
+// adapter). Three entry points for the tests:
 //   adapter_env    -- the environment lights the adapter forwards for a set of light Props
 //                     (Scene::initLights's keys), read back from the reference's light objects;
+//   adapter_tables -- the energy-compensation tables a DeviceCuda's context holds;
 //   adapter_render -- a whole render through prt::Device's interface: initScene(path, props),
 //                     initCamera, initFrame, initRenderer, initSampler, spp x render, blitFrame.
 // Props are passed as text, one per line: "<key> f <x>" (float), "i <n>" (int),
@@ -112,6 +113,18 @@ int adapter_env(const char* props_spec, float* env_f, int32_t* env_i, float* ima
     env_i[2] = e.image_lut_size;
     env_i[3] = e.flags;
     if (image && e.image_rgb) std::memcpy(image, e.image_rgb, sizeof(float) * 3 * e.image_width * e.image_height);
+  });
+}
+
+// The energy-compensation tables of a DeviceCuda's context (prt_cuda_albedo_tables layout), as
+// constructed with hostTables = host_tables. Writes at most `capacity` floats; *count gets the
+// total.
+int adapter_tables(int host_tables, float* out, int64_t capacity, int64_t* count)
+{
+  return guard([&] {
+    DeviceCuda device(0, host_tables != 0);
+    if (prt_cuda_albedo_tables(device.handle(), out, capacity, count) != PRT_OK)
+      throw std::runtime_error(prt_cuda_last_error(device.handle()));
   });
 }
 

@@ -73,3 +73,25 @@ def test_first_hit_aovs_through_the_reference_device_interface(golden, tmp_path)
     for got, key in ((alb, "albedo1"), (nrm, "normal1")):
         diff = np.abs(got.astype(np.float64) - z[f"terrain_seed0_{key}"])
         assert diff.mean() < 1e-4 and np.mean(diff > 1e-3) < 0.002, (key, diff.mean())
+
+
+def test_adapter_runs_on_the_reference_tables():
+    """prt::DeviceCuda uploads the energy-compensation tables the reference computes on the host
+    (precomputeAlbedoTables, as DeviceCpu's constructor does): its context holds them bit for
+    bit. With hostTables = false it keeps the tables the context built on the GPU, which differ
+    from them in the last digits."""
+    L = lib()
+    P = C.POINTER(C.c_float)
+    L.adapter_tables.argtypes = [C.c_int, P, C.c_int64, C.POINTER(C.c_int64)]
+    want = ref.albedo_tables()
+    got = {}
+    for host in (1, 0):
+        out = np.zeros(want.size, np.float32)
+        n = C.c_int64(0)
+        rc = L.adapter_tables(host, T.fptr(out), out.size, C.byref(n))
+        assert rc == 0, L.adapter_last_error().decode()
+        assert n.value == want.size
+        got[host] = out
+    assert np.array_equal(got[1].view(np.uint32), want.view(np.uint32))
+    assert not np.array_equal(got[0], want)
+    assert np.abs(got[0] - want).max() < 2e-3
