@@ -20,14 +20,14 @@ pytestmark = pytest.mark.gpu
 CASES = bsdf_cases.cases()
 
 
-def check(gpu, ref):
+def check(gpu, ref, eval_tight=0.999, eval_loose=0.9999, sample_tight=0.98, sample_loose=0.999):
     tight = bsdf_cases.compare(gpu, ref, rel=1e-5)
     loose = bsdf_cases.compare(gpu, ref, rel=1e-3)
     assert tight["flags"].all()
-    assert tight["eval"].mean() >= 0.999, 1 - tight["eval"].mean()
-    assert loose["eval"].mean() >= 0.9999, 1 - loose["eval"].mean()
-    assert tight["sample"].mean() >= 0.98, 1 - tight["sample"].mean()
-    assert loose["sample"].mean() >= 0.999, 1 - loose["sample"].mean()
+    assert tight["eval"].mean() >= eval_tight, 1 - tight["eval"].mean()
+    assert loose["eval"].mean() >= eval_loose, 1 - loose["eval"].mean()
+    assert tight["sample"].mean() >= sample_tight, 1 - tight["sample"].mean()
+    assert loose["sample"].mean() >= sample_loose, 1 - loose["sample"].mean()
 
 
 @pytest.mark.parametrize("name,material,medium", CASES, ids=[c[0] for c in CASES])
@@ -45,12 +45,25 @@ def test_bsdf_matches_fixture(device, golden, name, material, medium):
 
 @pytest.mark.parametrize("name,material,medium", CASES, ids=[c[0] for c in CASES])
 def test_bsdf_million_tuples(device, name, material, medium):
-    """1M seeded tuples per case against the live oracle (skipped where it is not built)."""
+    """1M seeded tuples per case against the live oracle (skipped where it is not built): on the
+    device's own energy-compensation tables with the bars of the module docstring, and on the
+    reference's own tables (what the reference-side adapter runs on) with tighter ones: >= 99.95%
+    of evaluations within 1e-5 and >= 99.995% within 1e-3, >= 99% of samples within 1e-5 and
+    >= 99.98% within 1e-3. Measured worst cases on the reference's tables: evaluations 2.4e-4 and
+    1.4e-5 (rough gold), samples 5.5e-3 and 6.9e-5 (rough glass from inside, rough metal)."""
     ref_mod = pytest.importorskip("ref")
     if not ref_mod.ref_available():
         pytest.skip("oracle/_ref not built")
     tup = bsdf_cases.tuples(1 << 20, 2)
-    check(device.bsdf_query(material, tup, medium), ref_mod.bsdf_query(material, tup, medium))
+    want = ref_mod.bsdf_query(material, tup, medium)
+    check(device.bsdf_query(material, tup, medium), want)
+    own = device.albedo_tables()
+    device.set_albedo_tables(ref_mod.albedo_tables())
+    try:
+        got = device.bsdf_query(material, tup, medium)
+    finally:
+        device.set_albedo_tables(own)
+    check(got, want, eval_tight=0.9995, eval_loose=0.99995, sample_tight=0.99, sample_loose=0.9998)
 
 
 # Layout of prt_cuda_albedo_tables (bsdf/albedo_tables.cpp:95-130): 3D tables are
