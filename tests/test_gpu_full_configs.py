@@ -70,7 +70,7 @@ def render(device, scene, seed, spp):
 
 
 def test_cornell_full_size_converged_gate(device, golden):
-    """256x256, depth 5, 4096 spp: the workload's own frame at the north star's sample count."""
+    """256x256, depth 5, 4096 spp: the workload's own frame at its converged sample count."""
     z = golden("cornell_full.npz")
     spp = int(z["spp"])
     seeds = rel_mse(z["seed1"], z["seed0"])
