@@ -42,6 +42,11 @@ struct Launch
   AdjointView adj;
   // Batch form: radiance of every work item (pixel-sample) when the batch is differentiable.
   float4* pathL;
+  // Batch form, forward render: each work item's clamped radiance (w = 1 once written) and its
+  // first-hit albedo and normal (w = 1 where set), summed per pixel by kBatchAccumulate.
+  float4* workOut;
+  float4* workA;
+  float4* workN;
   // Some scene of the launch has transparent materials: shadow rays take the transparency
   // filter (host-side choice of the kShadow instantiation).
   int anyTransparent;
@@ -546,15 +551,62 @@ PRT_D void finishPath(const Launch& L, int p, f3 rad, const uint4& info, f3 shEx
   const f3 c = clampL(rad, it.rd.maxRadiance);
   const uint32_t pid = info.x;
   const int px = (int)(pid & 0x0fffu), py = (int)((pid >> 16) & 0x0fffu);
-  const int q = py * it.width + px;
-  atomicAdd(it.accum + q, make_float4(c.x, c.y, c.z, 1.f));
-  if (L.pathL)
-    L.pathL[it.workBase + (long long)info.y * it.pixelCount + slotOfPixel(px, py, it.width)] = make_float4(c.x, c.y, c.z, 0.f);
-  if (it.aovMask)
+  const long long w = it.workBase + (long long)info.y * it.pixelCount + slotOfPixel(px, py, it.width);
+  if (L.workOut)
   {
-    const float4 va = L.ps.aovA[p], vn = L.ps.aovN[p];
-    if (va.w != 0.f) atomicAdd(it.accA + q, make_float4(va.x, va.y, va.z, 1.f));
-    if (vn.w != 0.f) atomicAdd(it.accN + q, make_float4(vn.x, vn.y, vn.z, 1.f));
+    L.workOut[w] = make_float4(c.x, c.y, c.z, 1.f);
+    if (it.aovMask)
+    {
+      L.workA[w] = L.ps.aovA[p];
+      L.workN[w] = L.ps.aovN[p];
+    }
+  }
+  if (L.pathL) L.pathL[w] = make_float4(c.x, c.y, c.z, 0.f);
+}
+
+// The batch's per-pixel sums of one item: its work items' radiance (and first-hit AOVs) added in
+// sample order, as kAccumulate adds a frame's, so that each frame's image does not depend on the
+// order in which its paths finished. Replaces the item's planes.
+__global__ void kBatchAccumulate(const BatchItem* __restrict__ items, int item, const float4* __restrict__ workOut,
+                                 const float4* __restrict__ workA, const float4* __restrict__ workN)
+{
+  const BatchItem& it = items[item];
+  const int spp = (int)(it.workCount / it.pixelCount);
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < it.pixelCount; q += gridDim.x * blockDim.x)
+  {
+    const int x = q % it.width, y = q / it.width;
+    const long long base = it.workBase + slotOfPixel(x, y, it.width);
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f), a = acc, nn = acc;
+    for (int s = 0; s < spp; ++s)
+    {
+      const long long w = base + (long long)s * it.pixelCount;
+      const float4 o = workOut[w];
+      if (o.w != 0.f)
+      {
+        acc.x += o.x;
+        acc.y += o.y;
+        acc.z += o.z;
+        acc.w += 1.f;
+      }
+      if (it.aovMask)
+      {
+        const float4 va = workA[w], vn = workN[w];
+        if (va.w != 0.f)
+        {
+          a.x += va.x; a.y += va.y; a.z += va.z; a.w += 1.f;
+        }
+        if (vn.w != 0.f)
+        {
+          nn.x += vn.x; nn.y += vn.y; nn.z += vn.z; nn.w += 1.f;
+        }
+      }
+    }
+    it.accum[q] = acc;
+    if (it.aovMask)
+    {
+      it.accA[q] = a;
+      it.accN[q] = nn;
+    }
   }
 }
 
@@ -1861,13 +1913,13 @@ static cudaError_t runBatch(Context& ctx, BatchState& B, RenderCounters& rc, boo
   rc = RenderCounters();
   cudaError_t e = cudaSuccess;
   const int64_t C = B.ps.capacity;
-  for (const BatchItem& it : B.items)
+  if (!replay)  // the replay only scatters gradients
   {
-    if (replay) break;  // the replay only scatters gradients
-    const size_t bytes = (size_t)it.pixelCount * sizeof(float4);
-    e = cudaMemsetAsync(it.accum, 0, bytes, ctx.stream);
-    if (e == cudaSuccess && it.accA) e = cudaMemsetAsync(it.accA, 0, bytes, ctx.stream);
-    if (e == cudaSuccess && it.accN) e = cudaMemsetAsync(it.accN, 0, bytes, ctx.stream);
+    // Work items that never finish (none should) then add nothing to their pixel.
+    const size_t bytes = (size_t)B.workTotal * sizeof(float4);
+    e = cudaMemsetAsync(B.workOut, 0, bytes, ctx.stream);
+    if (e == cudaSuccess && B.workA) e = cudaMemsetAsync(B.workA, 0, bytes, ctx.stream);
+    if (e == cudaSuccess && B.workN) e = cudaMemsetAsync(B.workN, 0, bytes, ctx.stream);
     if (e != cudaSuccess) return e;
   }
   BatchCtl h;
@@ -1895,6 +1947,12 @@ static cudaError_t runBatch(Context& ctx, BatchState& B, RenderCounters& rc, boo
     L.freeList[0] = B.freeList[0];
     L.freeList[1] = B.freeList[1];
     L.pathL = B.pathL;
+    if (!replay)
+    {
+      L.workOut = B.workOut;
+      L.workA = B.workA;
+      L.workN = B.workN;
+    }
     for (const BatchItem& it : B.items) L.anyTransparent |= it.sc.hasTransparent;
     const int persistent = ctx.smCount * ctx.traceBlocks;
     const int shadeGrid = ctx.smCount * ctx.shadeBlocks;
@@ -1942,6 +2000,15 @@ static cudaError_t runBatch(Context& ctx, BatchState& B, RenderCounters& rc, boo
   }
   cudaFreeHost(done);
   if (e != cudaSuccess) return e;
+  if (!replay)
+  {
+    for (int k = 0; k < (int)B.items.size(); ++k)
+      kBatchAccumulate<<<gridFor(ctx, B.items[k].pixelCount), 256, 0, ctx.stream>>>(B.dItems, k, B.workOut, B.workA,
+                                                                                      B.workN);
+    rc.launches += (int)B.items.size();
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   e = cudaMemcpy(&h, B.ctl, sizeof(h), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return e;
   rc.closestRays = (int64_t)h.rays[0];

@@ -110,6 +110,11 @@ struct BatchState
   int* freeList[2] = {nullptr, nullptr};
   cudaGraphExec_t exec = nullptr;  // kGraphIterations bounce iterations
   int graphKernels = 0;
+  // Forward render: per work item (pixel-sample) the clamped radiance and the first-hit albedo and
+  // normal (the latter two when an item has AOVs), summed per pixel in sample order at the end.
+  float4* workOut = nullptr;
+  float4* workA = nullptr;
+  float4* workN = nullptr;
   // Differentiable batches: radiance per work item (float4) and the replay graph.
   float4* pathL = nullptr;
   cudaGraphExec_t execReplay = nullptr;

@@ -3,9 +3,11 @@
 A batch renders many frames in one persistent wavefront with path regeneration. Every path
 of a frame is the path the frame form traces for it (same Sobol samples, same shading), so:
   * the ray counts match the per-frame renders exactly;
-  * beauty, albedo1 and normal1 images match the per-frame renders up to the order of the FP32
-    additions per pixel (the batch adds finished paths as they arrive): relative difference
-    <= 1e-4 where the pixel value exceeds 1e-3, absolute <= 1e-6 below it.
+  * finished paths store their results per pixel-sample and each pixel's samples are summed in
+    sample order, as the frame form sums them: a batch renders identically every time, its
+    albedo1 and normal1 images equal the per-frame renders bit for bit, and its beauty image
+    matches them within a relative 1e-4 where the pixel value exceeds 1e-3 (absolute 1e-6
+    below it).
 """
 import numpy as np
 import pytest
@@ -61,13 +63,14 @@ def test_batch_matches_per_frame_renders(dev):
         rays += rst["rays"]
         got = [batch.blit(k, T.PRT_BLIT_HDR), batch.blit(k, T.PRT_BLIT_ALBEDO1), batch.blit(k, T.PRT_BLIT_NORMAL1)]
         assert np.isfinite(got[0]).all() and got[0].mean() > 0
-        for g, r in zip(got, ref):
-            assert close(g, r), k
+        assert close(got[0], ref[0]), k
+        for g, r in zip(got[1:], ref[1:]):
+            assert np.array_equal(g.view(np.uint32), r.view(np.uint32)), k
     assert st["rays"] == rays
     batch.close()
 
 
-def test_batch_renders_twice_identically_up_to_addition_order(dev):
+def test_batch_renders_twice_identically(dev):
     frames = small_batch(4, seed=9)
     batch = prt_cuda.Batch(dev, frames)
     st1 = batch.render()
@@ -75,7 +78,7 @@ def test_batch_renders_twice_identically_up_to_addition_order(dev):
     st2 = batch.render()
     assert st1["rays"] == st2["rays"]
     for k in range(len(frames)):
-        assert close(batch.blit(k), first[k])
+        assert np.array_equal(batch.blit(k).view(np.uint32), first[k].view(np.uint32)), k
     batch.close()
 
 
@@ -95,6 +98,26 @@ def test_batch_small_pool_regenerates_paths(dev):
         assert close(batch.blit(k), ref[0])
     assert st["rays"] == rays
     batch.close()
+
+
+def test_batch_destroy_returns_its_memory(dev):
+    """A batch owns every buffer its items' uploads made -- scene, environment lights, path pool --
+    so creating, rendering and destroying one leaves the device's free memory where it was."""
+    import torch
+
+    frames = small_batch(16, 5)
+    b = prt_cuda.Batch(dev, frames)
+    b.render()
+    b.close()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(0)[0]
+    for _ in range(3):
+        b = prt_cuda.Batch(dev, frames)
+        b.render()
+        b.close()
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info(0)[0]
+    assert free0 - free1 < (4 << 20), free0 - free1
 
 
 def test_batch_rejects_bad_items(dev):
