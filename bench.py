@@ -49,6 +49,9 @@ def parse_args():
                     help="Adam steps of the batched inverse-rendering measurement (the workload's 100)")
     ap.add_argument("--headline-only", action="store_true",
                     help="skip the small-scene, batched and adjoint measurements")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="run only the batched measurement (64-frame batch against 64 frame-form renders) and "
+                         "print it as one JSON line, for profiling it")
     ap.add_argument("--traffic-csv", default=None,
                     help="ncu --csv --print-units base log (dram__bytes_read.sum, dram__bytes_write.sum) of the "
                          "kTrace launches of a 1-spp frame of this workload, to measure roofline.traffic instead "
@@ -614,6 +617,12 @@ C_CAMERA_BYTES = 4 * 14  # prt_camera_desc: 12 floats of basis and position + fo
 
 def main():
     args = parse_args()
+    if args.batched_only:
+        import prt_cuda
+
+        register_sunsky()
+        print(json.dumps({"batched": batched_bench(prt_cuda.DeviceCuda(0))}))
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
