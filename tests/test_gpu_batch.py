@@ -5,9 +5,10 @@ of a frame is the path the frame form traces for it (same Sobol samples, same sh
   * the ray counts match the per-frame renders exactly;
   * finished paths store their results per pixel-sample and each pixel's samples are summed in
     sample order, as the frame form sums them: a batch renders identically every time, its
-    albedo1 and normal1 images equal the per-frame renders bit for bit, and its beauty image
-    matches them within a relative 1e-4 where the pixel value exceeds 1e-3 (absolute 1e-6
-    below it).
+    albedo1 and normal1 images equal the per-frame renders bit for bit, and its beauty image is
+    within 8 ulps of theirs per channel (measured: at most 3, in ~15% of the pixels; with equal
+    ray counts and bit-identical AOVs, this is FP32 rounding inside the two instantiations of the
+    shading kernels rather than different paths).
 """
 import numpy as np
 import pytest
@@ -19,12 +20,11 @@ import prt_types as T
 pytestmark = pytest.mark.gpu
 
 
-def close(a, b):
-    a = np.asarray(a, np.float64)
-    b = np.asarray(b, np.float64)
-    big = np.abs(b) > 1e-3
-    rel = np.abs(a - b)[big] / np.abs(b)[big]
-    return (rel.max() if rel.size else 0.0) <= 1e-4 and np.abs(a - b)[~big].max(initial=0.0) <= 1e-6
+def max_ulps(a, b):
+    """Largest distance in units in the last place between two arrays of non-negative floats."""
+    ia = np.ascontiguousarray(a, np.float32).view(np.int32).astype(np.int64)
+    ib = np.ascontiguousarray(b, np.float32).view(np.int32).astype(np.int64)
+    return int(np.abs(ia - ib).max(initial=0))
 
 
 def small_batch(count, seed):
@@ -63,7 +63,7 @@ def test_batch_matches_per_frame_renders(dev):
         rays += rst["rays"]
         got = [batch.blit(k, T.PRT_BLIT_HDR), batch.blit(k, T.PRT_BLIT_ALBEDO1), batch.blit(k, T.PRT_BLIT_NORMAL1)]
         assert np.isfinite(got[0]).all() and got[0].mean() > 0
-        assert close(got[0], ref[0]), k
+        assert max_ulps(got[0], ref[0]) <= 8, (k, max_ulps(got[0], ref[0]))
         for g, r in zip(got[1:], ref[1:]):
             assert np.array_equal(g.view(np.uint32), r.view(np.uint32)), k
     assert st["rays"] == rays
@@ -95,7 +95,7 @@ def test_batch_small_pool_regenerates_paths(dev):
     for k, (scene, seed, aov) in enumerate(frames):
         ref, rst = plain_render(dev, scene, seed, aov)
         rays += rst["rays"]
-        assert close(batch.blit(k), ref[0])
+        assert max_ulps(batch.blit(k), ref[0]) <= 8, k
     assert st["rays"] == rays
     batch.close()
 
