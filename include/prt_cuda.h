@@ -442,7 +442,11 @@ int prt_cuda_autotune(prt_context* ctx, int32_t spp, prt_tuning* chosen, double*
  * frames' paths share one path pool, terminated paths are replaced by new camera paths of any
  * frame (path regeneration), and the bounce loop is a CUDA graph replayed until every frame
  * has all its samples. Each frame gets the image that prt_cuda_render would produce for it
- * (samples 0..spp-1 of its seed), up to the order of floating-point additions per pixel. */
+ * (samples 0..spp-1 of its seed): every path's result is kept per pixel-sample and each pixel's
+ * samples are added in sample order, as the frame form adds them, so repeated renders of a batch
+ * are identical, the albedo1 and normal1 AOVs equal the frame form's, and the beauty image is
+ * within a few ulps of it. Device memory: 48 bytes per pixel-sample of the batch, plus the scenes
+ * and the path pool. */
 typedef struct prt_batch prt_batch;
 
 typedef struct prt_batch_item
