@@ -11,6 +11,7 @@ import pytest
 
 import prt_cuda
 import prt_scenes
+import prt_types as T
 
 pytestmark = pytest.mark.gpu
 
@@ -86,3 +87,46 @@ def test_default_stack_is_the_shared_one(dev):
     kernels with their 12-entry stack in shared memory."""
     assert dev.get_tuning()["trace_stack"] == 12
     assert dev.scene_stats()["depth"] <= 12
+
+
+def chain_scene(n=150, ratio=1.7):
+    """Small triangles at x = ratio^k along the x axis: each binned-SAH split peels off the farthest
+    few, so the tree is a chain -- 19 wide levels for the defaults, deeper than the 12-entry
+    shared-memory stack and within the 24-entry one. The camera looks along the chain, so its rays
+    walk the whole depth."""
+    s = prt_scenes.Scene()
+    m = s.add_material(T.material(base_color=(0.7, 0.7, 0.7), specular_weight=0.0))
+    x = ratio ** np.arange(n, dtype=np.float64)
+    v = np.zeros((n, 3, 3), np.float32)
+    v[:, :, 0] = x[:, None]
+    v[:, 1, 1] = 0.5
+    v[:, 2, 2] = 0.5
+    s.add_mesh(v.reshape(-1, 3), np.arange(3 * n, dtype=np.int32).reshape(-1, 3), m)
+    s.env.distant_color[:] = (0.0, 0.0, 0.0)
+    s.env.ambient_color[:] = (1.0, 1.0, 1.0)
+    s.camera = prt_scenes.look_at((-3.0, 2.0, 3.0), (4.0, 0.2, 0.2), fov_deg=50.0)
+    s.width, s.height, s.spp, s.max_depth, s.rr_depth = 64, 64, 4, 3, 8
+    return s
+
+
+def test_deep_tree_takes_a_stack_that_fits():
+    """A tree deeper than 12 wide levels: the default (12, shared memory) falls back to the
+    24-entry stack, and every stack setting renders the same image with the same rays."""
+    d = prt_cuda.DeviceCuda(0)
+    try:
+        d.setup(chain_scene(), seed=1)
+        depth = d.scene_stats()["depth"]
+        assert 12 < depth <= 24, depth
+        out = {}
+        for stack in (12, 24, 48):
+            d.set_tuning(trace_stack=stack)
+            d.init_sampler(1)
+            d.clear_frame()
+            st = d.render(4)
+            out[stack] = (d.blit_frame(), st["rays"])
+        for stack in (12, 24):
+            assert np.array_equal(out[stack][0], out[48][0]), stack
+            assert out[stack][1] == out[48][1], stack
+        assert np.isfinite(out[48][0]).all()
+    finally:
+        d.close()
