@@ -125,3 +125,22 @@ def test_batch_rejects_bad_items(dev):
     scene.width, scene.height = 100, 64   # width not a multiple of 32
     with pytest.raises(prt_cuda.LogicError):
         prt_cuda.Batch(dev, [(scene, 0, 0)])
+
+
+def test_batch_with_a_deep_tree_matches_per_frame_renders(dev):
+    """The batch takes the stack its deepest tree fits (a 19-level chain beside a terrain: the
+    24-entry stack for both), and each frame still matches its per-frame render."""
+    from test_gpu_tuning import chain_scene
+
+    terrain = prt_scenes.terrain(seed=4, grid=64, n_spheres=8, width=64, height=64, spp=4, extent=10.0,
+                                 relief=2.0, max_depth=4)
+    frames = [(chain_scene(), 1, 0), (terrain, 2, 0)]
+    batch = prt_cuda.Batch(dev, frames)
+    st = batch.render()
+    rays = 0
+    for k, (scene, seed, aov) in enumerate(frames):
+        ref, rst = plain_render(dev, scene, seed, aov)
+        rays += rst["rays"]
+        assert max_ulps(batch.blit(k), ref[0]) <= 8, k
+    assert st["rays"] == rays
+    batch.close()
